@@ -1,0 +1,320 @@
+"""The oracle: CPU checkers for the B-spline cost function.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference arm may import this package; the
+product (plastimatch_b200) never does.
+
+Two checkers live here:
+
+* ``port``  -- oracle/liborc.so, the plain-C restatement of the reference
+  (oracle/bspline_oracle.c): float routines in the reference's operation
+  order plus double-precision versions used as the error yardstick.
+* ``ref``   -- oracle/_ref/libplmref.so, the reference's own C++ flavours
+  compiled from its sources by oracle/build_ref.sh (present when the
+  reference tree was available at build time).
+
+Inputs are plastimatch_b200.geometry.Volume / BsplineGrid objects.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liborc.so")
+REF_SO = os.path.join(HERE, "_ref", "libplmref.so")
+
+f32p = C.POINTER(C.c_float)
+f64p = C.POINTER(C.c_double)
+i64p = C.POINTER(C.c_int64)
+
+
+def _p(a, t=f32p):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class OrcVol(C.Structure):
+    _fields_ = [("dim", C.c_int64 * 3), ("origin", C.c_float * 3),
+                ("spacing", C.c_float * 3), ("dcos", C.c_float * 9),
+                ("inv_dcos", C.c_float * 9), ("step", C.c_float * 9),
+                ("proj", C.c_float * 9)]
+
+
+class OrcGrid(C.Structure):
+    _fields_ = [("img_origin", C.c_float * 3), ("img_spacing", C.c_float * 3),
+                ("img_dim", C.c_int64 * 3), ("roi_offset", C.c_int64 * 3),
+                ("roi_dim", C.c_int64 * 3), ("vox_per_rgn", C.c_int64 * 3),
+                ("grid_spac", C.c_float * 3), ("rdims", C.c_int64 * 3),
+                ("cdims", C.c_int64 * 3), ("num_knots", C.c_int64),
+                ("num_coeff", C.c_int64)]
+
+
+class OrcHist(C.Structure):
+    _fields_ = [("bins", C.c_int64), ("offset", C.c_float),
+                ("delta", C.c_float)]
+
+
+class RefGeom(C.Structure):
+    _fields_ = [("dim", C.c_int64 * 3), ("origin", C.c_float * 3),
+                ("spacing", C.c_float * 3), ("dcos", C.c_float * 9)]
+
+
+class RefGrid(C.Structure):
+    _fields_ = [("roi_offset", C.c_int64 * 3), ("roi_dim", C.c_int64 * 3),
+                ("vox_per_rgn", C.c_int64 * 3)]
+
+
+class RefResult(C.Structure):
+    _fields_ = [("score", C.c_float), ("total_score", C.c_float),
+                ("rmetric", C.c_float), ("num_vox", C.c_int64),
+                ("num_coeff", C.c_int64), ("fixed_bins", C.c_int64),
+                ("moving_bins", C.c_int64), ("f_offset", C.c_float),
+                ("f_delta", C.c_float), ("m_offset", C.c_float),
+                ("m_delta", C.c_float)]
+
+
+@dataclass
+class Result:
+    score: float
+    grad: np.ndarray
+    num_vox: int = 0
+    f_hist: np.ndarray | None = None
+    m_hist: np.ndarray | None = None
+    j_hist: np.ndarray | None = None
+
+
+_port = None
+_ref = None
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_SO):
+            raise RuntimeError("oracle/liborc.so not built (make -C oracle)")
+        _port = C.CDLL(PORT_SO)
+    return _port
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError("oracle/_ref/libplmref.so not built "
+                               "(oracle/build_ref.sh)")
+        _ref = C.CDLL(REF_SO)
+    return _ref
+
+
+# ---------------------------------------------------------------- port ---
+
+def orc_vol(v) -> OrcVol:
+    o = OrcVol()
+    d = (C.c_int64 * 3)(*v.dim)
+    org = (C.c_float * 3)(*v.origin)
+    sp = (C.c_float * 3)(*v.spacing)
+    dc = (C.c_float * 9)(*v.dcos)
+    if port().orc_vol_init(C.byref(o), d, org, sp, dc) != 0:
+        raise ValueError("singular direction cosines")
+    return o
+
+
+def orc_grid(grid, fixed) -> OrcGrid:
+    g = OrcGrid()
+    rc = port().orc_grid_init(C.byref(g), C.byref(orc_vol(fixed)),
+                              (C.c_int64 * 3)(*grid.roi_offset),
+                              (C.c_int64 * 3)(*grid.roi_dim),
+                              (C.c_int64 * 3)(*grid.vox_per_rgn))
+    if rc:
+        raise ValueError("bad grid")
+    return g
+
+
+def port_volume_grad(v) -> np.ndarray:
+    out = np.zeros(v.npix * 3, np.float32)
+    port().orc_volume_grad(C.byref(orc_vol(v)), _p(v.img), _p(out))
+    return out
+
+
+def port_basis_lut(vpr: int) -> np.ndarray:
+    out = np.zeros(4 * vpr, np.float32)
+    port().orc_basis_lut(_p(out), C.c_int64(vpr))
+    return out
+
+
+def port_mse(grid, fixed, moving, coeff, moving_grad=None, grad_mode=0,
+             precision="f32") -> Result:
+    if moving_grad is None and grad_mode == 0:
+        moving_grad = port_volume_grad(moving)
+    g = orc_grid(grid, fixed)
+    nv = C.c_int64(0)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    if precision == "f32":
+        s = C.c_float(0)
+        gr = np.zeros(grid.num_coeff, np.float32)
+        rc = port().orc_mse_f32(C.byref(g), C.byref(orc_vol(fixed)),
+                                _p(fixed.img), C.byref(orc_vol(moving)),
+                                _p(moving.img), _p(moving_grad), _p(coeff),
+                                C.c_int(grad_mode), C.byref(s), _p(gr),
+                                C.byref(nv))
+    else:
+        s = C.c_double(0)
+        gr = np.zeros(grid.num_coeff, np.float64)
+        rc = port().orc_mse_f64(C.byref(g), C.byref(orc_vol(fixed)),
+                                _p(fixed.img), C.byref(orc_vol(moving)),
+                                _p(moving.img), _p(moving_grad), _p(coeff),
+                                C.c_int(grad_mode), C.byref(s), _p(gr, f64p),
+                                C.byref(nv))
+    if rc:
+        raise RuntimeError(f"oracle mse failed rc={rc}")
+    return Result(s.value, gr, nv.value)
+
+
+def port_hist_eqsp(img: np.ndarray, bins: int) -> OrcHist:
+    h = OrcHist(bins, 0.0, 0.0)
+    a = np.ascontiguousarray(img, np.float32).ravel()
+    port().orc_hist_eqsp(C.byref(h), _p(a), C.c_int64(a.size))
+    return h
+
+
+def port_mi(grid, fixed, moving, coeff, bins=32, precision="f32") -> Result:
+    g = orc_grid(grid, fixed)
+    fh, mh = port_hist_eqsp(fixed.img, bins), port_hist_eqsp(moving.img, bins)
+    nv = C.c_int64(0)
+    f_hist = np.zeros(bins)
+    m_hist = np.zeros(bins)
+    j_hist = np.zeros(bins * bins)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    if precision == "f32":
+        s = C.c_float(0)
+        gr = np.zeros(grid.num_coeff, np.float32)
+        fn, gp = port().orc_mi_f32, _p(gr)
+    else:
+        s = C.c_double(0)
+        gr = np.zeros(grid.num_coeff, np.float64)
+        fn, gp = port().orc_mi_f64, _p(gr, f64p)
+    rc = fn(C.byref(g), C.byref(orc_vol(fixed)), _p(fixed.img),
+            C.byref(orc_vol(moving)), _p(moving.img), _p(coeff),
+            C.byref(fh), C.byref(mh), C.byref(s), gp, C.byref(nv),
+            _p(f_hist, f64p), _p(m_hist, f64p), _p(j_hist, f64p))
+    if rc:
+        raise RuntimeError(f"oracle mi failed rc={rc}")
+    return Result(s.value, gr, nv.value, f_hist, m_hist,
+                  j_hist.reshape(bins, bins))
+
+
+def penalties(curvature=0.0, diffusion=0.0, lame_1=0.0, lame_2=0.0,
+              total_displacement=0.0, third_order=0.0,
+              linear_elastic_multiplier=1.0, curvature_mixed_weight=1.0):
+    return np.array([curvature, diffusion, lame_1, lame_2, total_displacement,
+                     third_order, linear_elastic_multiplier,
+                     curvature_mixed_weight], np.float32)
+
+
+def port_reg(grid, fixed, coeff, pen, precision="f32") -> Result:
+    g = orc_grid(grid, fixed)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    if precision == "f32":
+        s = C.c_float(0)
+        gr = np.zeros(grid.num_coeff, np.float32)
+        rc = port().orc_reg_f32(C.byref(g), _p(coeff), _p(pen), C.byref(s),
+                                _p(gr))
+    else:
+        s = C.c_double(0)
+        gr = np.zeros(grid.num_coeff, np.float64)
+        rc = port().orc_reg_f64(C.byref(g), _p(coeff), _p(pen), C.byref(s),
+                                _p(gr, f64p))
+    if rc:
+        raise RuntimeError("oracle reg failed")
+    return Result(s.value, gr)
+
+
+# ----------------------------------------------------------- reference ---
+
+def _ref_geom(v) -> RefGeom:
+    return RefGeom((C.c_int64 * 3)(*v.dim), (C.c_float * 3)(*v.origin),
+                   (C.c_float * 3)(*v.spacing), (C.c_float * 9)(*v.dcos))
+
+
+def _ref_grid(grid) -> RefGrid:
+    return RefGrid((C.c_int64 * 3)(*grid.roi_offset),
+                   (C.c_int64 * 3)(*grid.roi_dim),
+                   (C.c_int64 * 3)(*grid.vox_per_rgn))
+
+
+def ref_metric(grid, fixed, moving, coeff, flavor="g", metric="mse",
+               bins=32, threads=0, moving_grad=None) -> Result:
+    """One reference flavour evaluation (bspline_score_mse / _mi)."""
+    gr = np.zeros(grid.num_coeff, np.float32)
+    res = RefResult()
+    fh = np.zeros(bins)
+    mh = np.zeros(bins)
+    jh = np.zeros(bins * bins)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = ref().ref_metric(
+        C.byref(_ref_geom(fixed)), _p(fixed.img), C.byref(_ref_geom(moving)),
+        _p(moving.img), _p(moving_grad), C.byref(_ref_grid(grid)), _p(coeff),
+        C.c_char(flavor.encode()), C.c_int(1 if metric == "mi" else 0),
+        C.c_int(bins), C.c_int(threads), _p(gr), C.byref(res),
+        _p(fh, f64p), _p(mh, f64p), _p(jh, f64p))
+    if rc:
+        raise RuntimeError("reference metric failed")
+    r = Result(res.score, gr, res.num_vox)
+    if metric == "mi":
+        r.f_hist, r.m_hist, r.j_hist = fh, mh, jh.reshape(bins, bins)
+    return r
+
+
+def ref_regularize(grid, fixed, coeff, curvature, impl="c",
+                   threads=0) -> Result:
+    gr = np.zeros(grid.num_coeff, np.float32)
+    res = RefResult()
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = ref().ref_regularize(C.byref(_ref_geom(fixed)),
+                              C.byref(_ref_grid(grid)), _p(coeff),
+                              C.c_char(impl.encode()), C.c_float(curvature),
+                              C.c_int(threads), _p(gr), C.byref(res))
+    if rc:
+        raise RuntimeError("reference regularize failed")
+    return Result(res.rmetric, gr)
+
+
+def ref_score(grid, fixed, moving, coeff, flavor="g", metric="mse", bins=32,
+              reg_impl="", curvature=0.0, threads=0) -> Result:
+    """The whole bspline_score(): metric + optional analytic regulariser."""
+    gr = np.zeros(grid.num_coeff, np.float32)
+    res = RefResult()
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = ref().ref_score(
+        C.byref(_ref_geom(fixed)), _p(fixed.img), C.byref(_ref_geom(moving)),
+        _p(moving.img), None, C.byref(_ref_grid(grid)), _p(coeff),
+        C.c_char(flavor.encode()), C.c_int(1 if metric == "mi" else 0),
+        C.c_int(bins), C.c_char(reg_impl.encode() if reg_impl else b"\0"),
+        C.c_float(curvature), C.c_int(threads), _p(gr), C.byref(res))
+    if rc:
+        raise RuntimeError("reference score failed")
+    return Result(res.total_score, gr, res.num_vox)
+
+
+def ref_volume_grad(v) -> np.ndarray:
+    out = np.zeros(v.npix * 3, np.float32)
+    ref().ref_volume_grad(C.byref(_ref_geom(v)), _p(v.img), _p(out))
+    return out
+
+
+def ref_luts(grid, fixed):
+    vpr = grid.vox_per_rgn
+    bx = np.zeros(4 * vpr[0], np.float32)
+    by = np.zeros(4 * vpr[1], np.float32)
+    bz = np.zeros(4 * vpr[2], np.float32)
+    q = np.zeros(64 * vpr[0] * vpr[1] * vpr[2], np.float32)
+    ref().ref_luts(C.byref(_ref_geom(fixed)), C.byref(_ref_grid(grid)),
+                   _p(bx), _p(by), _p(bz), _p(q))
+    return bx, by, bz, q

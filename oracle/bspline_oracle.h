@@ -1,0 +1,101 @@
+/* CPU restatement of Plastimatch's B-spline registration cost function.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+ * against (tests/, __graft_entry__.smoke(), bench.py's cpu_baseline leg);
+ * nothing in the product links or calls it.
+ *
+ * Each function restates one reference routine (file:line given at the
+ * definition) in plain C.  The "_f32" entry points reproduce the
+ * reference's float arithmetic in the reference's order (compile with
+ * -ffp-contract=off), so on the same inputs they agree with the compiled
+ * reference bit for bit up to the order of OpenMP reductions.  The "_f64"
+ * entry points evaluate the same algorithm entirely in double precision and
+ * serve as the error yardstick for the GPU forms. */
+#ifndef BSPLINE_ORACLE_H
+#define BSPLINE_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Volume geometry; step/proj are filled by orc_vol_init. */
+typedef struct {
+    int64_t dim[3];
+    float origin[3];
+    float spacing[3];
+    float dcos[9];
+    float inv_dcos[9];
+    float step[9];
+    float proj[9];
+} orc_vol;
+
+/* B-spline grid over the fixed image (Bspline_header fields). */
+typedef struct {
+    float img_origin[3];
+    float img_spacing[3];
+    int64_t img_dim[3];
+    int64_t roi_offset[3];
+    int64_t roi_dim[3];
+    int64_t vox_per_rgn[3];
+    float grid_spac[3];
+    int64_t rdims[3];
+    int64_t cdims[3];
+    int64_t num_knots;
+    int64_t num_coeff;
+} orc_grid;
+
+/* MI histogram parameters (Histogram, EQSP). */
+typedef struct {
+    int64_t bins;
+    float offset;
+    float delta;
+} orc_hist;
+
+int orc_vol_init (orc_vol* v, const int64_t dim[3], const float origin[3],
+    const float spacing[3], const float dcos[9]);
+int orc_grid_init (orc_grid* g, const orc_vol* fixed,
+    const int64_t roi_offset[3], const int64_t roi_dim[3],
+    const int64_t vox_per_rgn[3]);
+void orc_basis_lut (float* lut, int64_t vpr);
+void orc_q_lut (float* q_lut, const int64_t vpr[3]);
+
+/* volume_calc_grad: central differences, interleaved xyz. */
+void orc_volume_grad (const orc_vol* v, const float* img, float* grad);
+
+/* MSE.  grad_mode 0: reference default flavours g/h/c (dc/dv from the
+ * nearest-voxel moving gradient image); grad_mode 1: flavour o (exact
+ * derivative of the trilinear interpolant, no moving gradient image). */
+int orc_mse_f32 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+    const orc_vol* moving, const float* m_img, const float* m_grad,
+    const float* coeff, int grad_mode, float* score, float* grad,
+    int64_t* num_vox);
+int orc_mse_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+    const orc_vol* moving, const float* m_img, const float* m_grad,
+    const float* coeff, int grad_mode, double* score, double* grad,
+    int64_t* num_vox);
+
+/* Mattes MI with PVI-8 histograms (flavour g). */
+void orc_hist_eqsp (orc_hist* h, const float* img, int64_t n);
+int orc_mi_f32 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+    const orc_vol* moving, const float* m_img, const float* coeff,
+    const orc_hist* fh, const orc_hist* mh, float* score, float* grad,
+    int64_t* num_vox, double* f_hist, double* m_hist, double* j_hist);
+int orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+    const orc_vol* moving, const float* m_img, const float* coeff,
+    const orc_hist* fh, const orc_hist* mh, double* score, double* grad,
+    int64_t* num_vox, double* f_hist, double* m_hist, double* j_hist);
+
+/* Analytic regulariser (flavour c).  penalties[] = {curvature, diffusion,
+ * lame_1, lame_2, total_displacement, third_order, linear_elastic_multiplier,
+ * curvature_mixed_weight}. */
+int orc_reg_f32 (const orc_grid* g, const float* coeff,
+    const float penalties[8], float* rmetric, float* grad);
+int orc_reg_f64 (const orc_grid* g, const float* coeff,
+    const float penalties[8], double* rmetric, double* grad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

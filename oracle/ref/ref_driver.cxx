@@ -1,0 +1,324 @@
+/* C-ABI driver around Plastimatch's own B-spline cost function, compiled
+ * from the reference sources as a CPU oracle (oracle/_ref/libplmref.so).
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/ as the parity checker and by
+ * bench.py's reference / cpu_baseline arm.  The product never links it.
+ *
+ * Each entry point builds the reference's own objects (Volume,
+ * Bspline_xform, Bspline_parms, Bspline_state, Bspline_optimize,
+ * Metric_state) exactly as Bspline_optimize::optimize() does
+ * (src/register/bspline_optimize.cxx:122-153) and then calls the reference
+ * flavour function that the caller names, so the numbers are the
+ * reference's numbers. */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+#include <fcntl.h>
+#include <omp.h>
+
+#include "bspline.h"
+#include "bspline_mi.h"
+#include "bspline_mse.h"
+#include "bspline_optimize.h"
+#include "bspline_parms.h"
+#include "bspline_regularize.h"
+#include "bspline_state.h"
+#include "bspline_xform.h"
+#include "joint_histogram.h"
+#include "metric_state.h"
+#include "regularization_parms.h"
+#include "volume.h"
+#include "volume_grad.h"
+
+extern "C" {
+
+/* Geometry of one volume: dim, origin (mm), spacing (mm), direction
+ * cosines (row-major 3x3), as the reference's Volume constructor takes
+ * them (src/base/volume.h:60-67). */
+typedef struct {
+    int64_t dim[3];
+    float origin[3];
+    float spacing[3];
+    float dcos[9];
+} ref_geom;
+
+/* B-spline grid: the arguments of Bspline_xform::initialize
+ * (src/base/bspline_xform.cxx:491-507). */
+typedef struct {
+    int64_t roi_offset[3];
+    int64_t roi_dim[3];
+    int64_t vox_per_rgn[3];
+} ref_grid;
+
+typedef struct {
+    float score;            /* bst->ssd.curr_smetric (or total_score) */
+    float total_score;      /* bst->ssd.total_score after bspline_score */
+    float rmetric;          /* bst->ssd.rmetric */
+    int64_t num_vox;        /* bst->ssd.curr_num_vox */
+    int64_t num_coeff;
+    /* MI only: the joint histogram the flavour built (double) */
+    int64_t fixed_bins, moving_bins;
+    float f_offset, f_delta, m_offset, m_delta;
+} ref_result;
+
+}
+
+/* The reference logs every step to stdout (src/sys/logfile.cxx:45-62);
+ * keep the checker quiet by pointing fd 1 at /dev/null for the call. */
+class Quiet {
+public:
+    int saved;
+    Quiet () {
+        fflush (stdout);
+        saved = dup (1);
+        int fd = open ("/dev/null", O_WRONLY);
+        dup2 (fd, 1);
+        close (fd);
+    }
+    ~Quiet () {
+        fflush (stdout);
+        dup2 (saved, 1);
+        close (saved);
+    }
+};
+
+static Volume::Pointer
+make_volume (const ref_geom* g, const float* img, int planes)
+{
+    Volume::Pointer v = Volume::New (
+        g->dim, g->origin, g->spacing, g->dcos,
+        planes == 1 ? PT_FLOAT : PT_VF_FLOAT_INTERLEAVED, planes);
+    memcpy (v->img, img, sizeof(float) * planes * v->npix);
+    return v;
+}
+
+struct Ref_setup {
+    Bspline_xform bxf;
+    Bspline_parms parms;
+    Regularization_parms rparms;
+    Bspline_optimize bod;
+    Metric_state::Pointer ms;
+};
+
+static void
+setup (Ref_setup* s, const ref_geom* fg, const float* fimg,
+    const ref_geom* mg, const float* mimg, const float* mgrad,
+    const ref_grid* grid, const float* coeff, char flavor,
+    int metric_mi, int bins, char reg_impl, float reg_lambda,
+    int threads)
+{
+    if (threads > 0) omp_set_num_threads (threads);
+    float origin[3], spacing[3];
+    plm_long dim[3], roi_offset[3], roi_dim[3], vpr[3];
+    for (int d = 0; d < 3; d++) {
+        origin[d] = fg->origin[d];
+        spacing[d] = fg->spacing[d];
+        dim[d] = fg->dim[d];
+        roi_offset[d] = grid->roi_offset[d];
+        roi_dim[d] = grid->roi_dim[d];
+        vpr[d] = grid->vox_per_rgn[d];
+    }
+    float dcos[9];
+    memcpy (dcos, fg->dcos, sizeof dcos);
+    s->bxf.initialize (origin, spacing, dim, roi_offset, roi_dim, vpr, dcos);
+    if (coeff) {
+        memcpy (s->bxf.coeff, coeff, sizeof(float) * s->bxf.num_coeff);
+    }
+
+    s->parms.threading = BTHR_CPU;
+    s->parms.implementation = flavor;
+    s->parms.mi_hist_fixed_bins = bins;
+    s->parms.mi_hist_moving_bins = bins;
+    s->rparms.implementation = reg_impl;
+    s->rparms.curvature_penalty = reg_lambda;
+    s->parms.regularization_parms = &s->rparms;
+
+    s->bod.set_bspline_parms (&s->parms);
+    s->bod.set_bspline_xform (&s->bxf);
+    Bspline_state* bst = s->bod.get_bspline_state ();
+
+    if (fimg) {
+        s->ms = Metric_state::New ();
+        s->ms->fixed_ss = make_volume (fg, fimg, 1);
+        s->ms->moving_ss = make_volume (mg, mimg, 1);
+        if (mgrad) {
+            s->ms->moving_grad = make_volume (mg, mgrad, 3);
+        } else {
+            s->ms->moving_grad = volume_gradient (s->ms->moving_ss);
+        }
+        s->ms->metric_type = metric_mi
+            ? SIMILARITY_METRIC_MI_MATTES : SIMILARITY_METRIC_MSE;
+        s->ms->metric_lambda = 1.0f;
+        bst->similarity_data.push_back (s->ms);
+    }
+    bst->initialize (&s->bxf, &s->parms);
+    if (fimg) {
+        bst->initialize_mi_histograms ();
+        bst->set_metric_state (s->ms);
+    }
+}
+
+extern "C" {
+
+/* One similarity-metric evaluation with the named flavour, exactly as the
+ * metric loop of bspline_score() runs it (src/register/bspline.cxx:575-616):
+ * reset_score, set_metric_state, bspline_score_mse/_mi.  Writes
+ * curr_smetric, curr_smetric_grad and curr_num_vox.  For MI, also the
+ * histograms (f_hist[bins], m_hist[bins], j_hist[bins*bins], double). */
+int
+ref_metric (const ref_geom* fg, const float* fimg,
+    const ref_geom* mg, const float* mimg, const float* mgrad,
+    const ref_grid* grid, const float* coeff, char flavor, int metric_mi,
+    int bins, int threads, float* grad, ref_result* res,
+    double* f_hist, double* m_hist, double* j_hist)
+{
+    Quiet q;
+    Ref_setup s;
+    setup (&s, fg, fimg, mg, mimg, mgrad, grid, coeff, flavor, metric_mi,
+        bins, '\0', 0.f, threads);
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    bst->ssd.reset_score ();
+    if (metric_mi) {
+        bspline_score_mi (&s.bod);
+    } else {
+        bspline_score_mse (&s.bod);
+    }
+    res->score = bst->ssd.curr_smetric;
+    res->num_vox = bst->ssd.curr_num_vox;
+    res->num_coeff = s.bxf.num_coeff;
+    memcpy (grad, bst->ssd.curr_smetric_grad, sizeof(float) * s.bxf.num_coeff);
+    if (metric_mi) {
+        Joint_histogram* jh = bst->get_mi_hist ();
+        res->fixed_bins = jh->fixed.bins;
+        res->moving_bins = jh->moving.bins;
+        res->f_offset = jh->fixed.offset;
+        res->f_delta = jh->fixed.delta;
+        res->m_offset = jh->moving.offset;
+        res->m_delta = jh->moving.delta;
+        if (f_hist) memcpy (f_hist, jh->f_hist, sizeof(double) * jh->fixed.bins);
+        if (m_hist) memcpy (m_hist, jh->m_hist, sizeof(double) * jh->moving.bins);
+        if (j_hist) memcpy (j_hist, jh->j_hist,
+            sizeof(double) * jh->fixed.bins * jh->moving.bins);
+    }
+    return 0;
+}
+
+/* The analytic regulariser alone (flavour 'b' serial or 'c' OpenMP):
+ * Bspline_regularize::compute_score into a freshly reset Bspline_score
+ * (src/register/bspline_regularize.cxx:95-126).  Writes rmetric and the
+ * regulariser's contribution to total_grad. */
+int
+ref_regularize (const ref_geom* fg, const ref_grid* grid, const float* coeff,
+    char reg_impl, float curvature_penalty, int threads, float* grad,
+    ref_result* res)
+{
+    Quiet q;
+    Ref_setup s;
+    setup (&s, fg, 0, 0, 0, 0, grid, coeff, 'g', 0, 32, reg_impl,
+        curvature_penalty, threads);
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    bst->ssd.reset_score ();
+    bst->rst.compute_score (&bst->ssd, &s.rparms, &s.bxf);
+    res->rmetric = bst->ssd.rmetric;
+    res->num_coeff = s.bxf.num_coeff;
+    memcpy (grad, bst->ssd.total_grad, sizeof(float) * s.bxf.num_coeff);
+    return 0;
+}
+
+/* The whole cost function: bspline_score() (src/register/bspline.cxx:
+ * 558-632) with one MSE or MI metric and, when reg_impl != 0, the analytic
+ * regulariser.  Writes total_score and total_grad. */
+int
+ref_score (const ref_geom* fg, const float* fimg,
+    const ref_geom* mg, const float* mimg, const float* mgrad,
+    const ref_grid* grid, const float* coeff, char flavor, int metric_mi,
+    int bins, char reg_impl, float curvature_penalty, int threads,
+    float* grad, ref_result* res)
+{
+    Quiet q;
+    Ref_setup s;
+    setup (&s, fg, fimg, mg, mimg, mgrad, grid, coeff, flavor, metric_mi,
+        bins, reg_impl, curvature_penalty, threads);
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    bspline_score (&s.bod);
+    res->total_score = bst->ssd.total_score;
+    res->rmetric = bst->ssd.rmetric;
+    res->num_coeff = s.bxf.num_coeff;
+    res->score = bst->ssd.metric_record.empty ()
+        ? 0.f : bst->ssd.metric_record[0].score;
+    memcpy (grad, bst->ssd.total_grad, sizeof(float) * s.bxf.num_coeff);
+    return 0;
+}
+
+/* volume_gradient() (src/base/volume_grad.cxx:9-76): central-difference
+ * moving-image gradient, interleaved xyz. */
+int
+ref_volume_grad (const ref_geom* g, const float* img, float* grad_out)
+{
+    Quiet q;
+    Volume::Pointer v = make_volume (g, img, 1);
+    Volume::Pointer gr = volume_gradient (v);
+    memcpy (grad_out, gr->img, sizeof(float) * 3 * gr->npix);
+    return 0;
+}
+
+/* B-spline grid sizes the reference derives (Bspline_header::set,
+ * src/base/bspline_header.cxx:28-62). */
+int
+ref_grid_dims (const ref_geom* fg, const ref_grid* grid, int64_t rdims[3],
+    int64_t cdims[3], int64_t* num_coeff)
+{
+    Quiet q;
+    Bspline_xform bxf;
+    float origin[3], spacing[3], dcos[9];
+    plm_long dim[3], roi_offset[3], roi_dim[3], vpr[3];
+    for (int d = 0; d < 3; d++) {
+        origin[d] = fg->origin[d]; spacing[d] = fg->spacing[d];
+        dim[d] = fg->dim[d]; roi_offset[d] = grid->roi_offset[d];
+        roi_dim[d] = grid->roi_dim[d]; vpr[d] = grid->vox_per_rgn[d];
+    }
+    memcpy (dcos, fg->dcos, sizeof dcos);
+    bxf.initialize (origin, spacing, dim, roi_offset, roi_dim, vpr, dcos);
+    for (int d = 0; d < 3; d++) {
+        rdims[d] = bxf.rdims[d];
+        cdims[d] = bxf.cdims[d];
+    }
+    *num_coeff = bxf.num_coeff;
+    return 0;
+}
+
+/* The reference's basis lookup tables (Bspline_xform::allocate,
+ * src/base/bspline_xform.cxx:361-488): bx/by/bz_lut [vpr*4] and
+ * q_lut [vpr^3 * 64]. */
+int
+ref_luts (const ref_geom* fg, const ref_grid* grid, float* bx, float* by,
+    float* bz, float* q_lut)
+{
+    Quiet q;
+    Bspline_xform bxf;
+    float origin[3], spacing[3], dcos[9];
+    plm_long dim[3], roi_offset[3], roi_dim[3], vpr[3];
+    for (int d = 0; d < 3; d++) {
+        origin[d] = fg->origin[d]; spacing[d] = fg->spacing[d];
+        dim[d] = fg->dim[d]; roi_offset[d] = grid->roi_offset[d];
+        roi_dim[d] = grid->roi_dim[d]; vpr[d] = grid->vox_per_rgn[d];
+    }
+    memcpy (dcos, fg->dcos, sizeof dcos);
+    bxf.initialize (origin, spacing, dim, roi_offset, roi_dim, vpr, dcos);
+    memcpy (bx, bxf.bx_lut, sizeof(float) * 4 * vpr[0]);
+    memcpy (by, bxf.by_lut, sizeof(float) * 4 * vpr[1]);
+    memcpy (bz, bxf.bz_lut, sizeof(float) * 4 * vpr[2]);
+    memcpy (q_lut, bxf.q_lut, sizeof(float) * 64 * vpr[0] * vpr[1] * vpr[2]);
+    return 0;
+}
+
+}
+
+/* L-BFGS-B comes from ITK's netlib port (v3p_netlib_setulb_), which is not
+ * vendored with the reference; bspline_optimize.cxx still names it. */
+extern "C" void
+bspline_optimize_lbfgsb (Bspline_optimize*)
+{
+    fprintf (stderr, "oracle: reference L-BFGS-B is not available\n");
+}

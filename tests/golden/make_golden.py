@@ -1,0 +1,105 @@
+"""Generate tests/golden/*.npz from the reference's own CPU flavours.
+
+Run where the reference tree is available and oracle/_ref/libplmref.so has
+been built (oracle/build_ref.sh):
+
+    python tests/golden/make_golden.py
+
+Each fixture holds the inputs (images, geometry, grid, coefficients) and
+the outputs of the compiled reference on them, so parity is pinned even
+where the reference itself is absent (the GPU host).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+from plastimatch_b200 import synth  # noqa: E402
+from plastimatch_b200.geometry import BsplineGrid, Volume  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+ROT = (0.894427190999916, 0.447213595499958, 0.0,
+       -0.447213595499958, 0.894427190999916, 0.0, 0.0, 0.0, 1.0)
+
+
+def make_pair(dim, spacing, seed, dcos=None, remap=None, moving_shift=(0.5, -0.3, 0.2)):
+    fixed = synth.gaussian_blobs(dim, spacing=spacing, seed=seed)
+    if dcos is not None:
+        fixed = Volume(fixed.img, origin=(-3.0, 2.0, 1.0), spacing=spacing, dcos=dcos)
+    g0 = BsplineGrid.for_volume(fixed, (8, 7, 6))
+    c0 = synth.random_coeff(g0, 2.0, seed=seed + 1)
+    mov = synth.warp_trilinear(fixed, fixed, g0, c0)
+    if remap is not None:
+        mov = synth.intensity_remap(mov, remap, 5.0, seed + 2)
+    org = tuple(o + s for o, s in zip(fixed.origin, moving_shift))
+    moving = Volume(mov.img, origin=org, spacing=spacing, dcos=fixed.dcos)
+    return fixed, moving
+
+
+CASES = {
+    # name: (dim, spacing, vpr, roi_offset, roi_dim, seed, dcos, remap, coeff sigma)
+    "mse_small": ((24, 20, 18), (1.0, 1.1, 1.3), (5, 4, 6), (0, 0, 0), None, 11, None, None, 1.5),
+    "mse_roi": ((26, 22, 17), (0.9, 1.0, 1.2), (4, 5, 4), (2, 3, 1), (19, 15, 13), 21, None, None, 1.2),
+    "mse_dcos": ((22, 20, 16), (1.0, 1.0, 1.5), (5, 5, 4), (0, 0, 0), None, 31, ROT, None, 1.0),
+    "mse_vpr8": ((33, 31, 30), (1.0, 1.0, 1.0), (8, 8, 8), (0, 0, 0), None, 41, None, None, 2.0),
+    "mi_small": ((24, 22, 18), (1.0, 1.1, 1.3), (5, 6, 4), (0, 0, 0), None, 51, None, 0.7, 1.5),
+    "mi_dcos": ((22, 20, 16), (1.0, 1.0, 1.5), (5, 5, 4), (0, 0, 0), None, 61, ROT, 1.6, 1.0),
+}
+
+
+def main():
+    if not O.ref_available():
+        raise SystemExit("oracle/_ref/libplmref.so missing; run oracle/build_ref.sh")
+    for name, (dim, sp, vpr, roff, rdim, seed, dcos, remap, csig) in CASES.items():
+        fixed, moving = make_pair(dim, sp, seed, dcos, remap)
+        grid = BsplineGrid.for_volume(fixed, vpr, roi_offset=roff,
+                                      roi_dim=rdim)
+        coeff = synth.random_coeff(grid, csig, seed=seed + 3)
+        rec = dict(
+            fixed=fixed.img, moving=moving.img,
+            f_origin=np.array(fixed.origin, np.float32),
+            f_spacing=np.array(fixed.spacing, np.float32),
+            m_origin=np.array(moving.origin, np.float32),
+            m_spacing=np.array(moving.spacing, np.float32),
+            dcos=np.array(fixed.dcos, np.float32),
+            roi_offset=np.array(grid.roi_offset), roi_dim=np.array(grid.roi_dim),
+            vpr=np.array(grid.vox_per_rgn), coeff=coeff)
+        rec["moving_grad"] = O.ref_volume_grad(moving)
+        if name.startswith("mse"):
+            # flavours c and o scan the whole fixed image (p = fijk/vpr), so
+            # they are only defined when the ROI is the whole image
+            flavors = "gh" if rdim is not None else "gco"
+            for fl in flavors:
+                r = O.ref_metric(grid, fixed, moving, coeff, flavor=fl)
+                rec[f"{fl}_score"] = np.float32(r.score)
+                rec[f"{fl}_grad"] = r.grad
+                rec[f"{fl}_num_vox"] = np.int64(r.num_vox)
+            rr = O.ref_regularize(grid, fixed, coeff, 0.005, impl="c")
+            rec["reg_score"] = np.float32(rr.score)
+            rec["reg_grad"] = rr.grad
+            rt = O.ref_score(grid, fixed, moving, coeff, flavor="g",
+                             reg_impl="c", curvature=0.005)
+            rec["total_score"] = np.float32(rt.score)
+            rec["total_grad"] = rt.grad
+        else:
+            if rdim is not None:
+                raise SystemExit("MI flavour g needs the whole image as ROI")
+            r = O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                             metric="mi", bins=32)
+            rec["mi_score"] = np.float32(r.score)
+            rec["mi_grad"] = r.grad
+            rec["mi_num_vox"] = np.int64(r.num_vox)
+            rec["f_hist"], rec["m_hist"], rec["j_hist"] = r.f_hist, r.m_hist, r.j_hist
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **rec)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+"""The oracle pinned against the reference's own outputs.
+
+The golden vectors in tests/golden/ were produced by the reference's
+compiled CPU flavours (tests/golden/make_golden.py).  The C restatement
+keeps the reference's float operation order, so it must reproduce them bit
+for bit; the double-precision restatement must agree to within float
+rounding.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_names, load_golden, rel_err
+
+
+@pytest.mark.parametrize("name", golden_names("mse"))
+def test_port_mse_g_bit_exact(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.port_mse(grid, fixed, moving, coeff, moving_grad=rec["moving_grad"])
+    assert np.float32(r.score) == rec["g_score"]
+    assert r.num_vox == rec["g_num_vox"]
+    np.testing.assert_array_equal(r.grad, rec["g_grad"])
+
+
+@pytest.mark.parametrize("name", [n for n in golden_names("mse") if n != "mse_roi"])
+def test_port_mse_o_bit_exact(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.port_mse(grid, fixed, moving, coeff, grad_mode=1)
+    assert np.float32(r.score) == rec["o_score"]
+    np.testing.assert_array_equal(r.grad, rec["o_grad"])
+
+
+@pytest.mark.parametrize("name", golden_names("mse"))
+def test_port_mse_f64_close(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.port_mse(grid, fixed, moving, coeff, moving_grad=rec["moving_grad"],
+                   precision="f64")
+    assert abs(r.score - rec["g_score"]) <= 1e-5 * abs(rec["g_score"])
+    assert rel_err(r.grad, rec["g_grad"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", golden_names("mse"))
+def test_port_volume_grad_bit_exact(name):
+    _, moving, _, _, rec = load_golden(name)
+    np.testing.assert_array_equal(O.port_volume_grad(moving), rec["moving_grad"])
+
+
+@pytest.mark.parametrize("name", golden_names("mse"))
+def test_port_regularizer_bit_exact(name):
+    fixed, _, grid, coeff, rec = load_golden(name)
+    r = O.port_reg(grid, fixed, coeff, O.penalties(curvature=0.005))
+    assert np.float32(r.score) == rec["reg_score"]
+    np.testing.assert_array_equal(r.grad, rec["reg_grad"])
+    r64 = O.port_reg(grid, fixed, coeff, O.penalties(curvature=0.005),
+                     precision="f64")
+    assert abs(r64.score - rec["reg_score"]) <= 1e-6 * abs(rec["reg_score"])
+    assert rel_err(r64.grad, rec["reg_grad"]) < 1e-6
+
+
+@pytest.mark.parametrize("name", golden_names("mse"))
+def test_total_score_is_metric_plus_regularizer(name):
+    """bspline_score(): total = lambda*smetric + rmetric, grads likewise."""
+    _, _, _, _, rec = load_golden(name)
+    assert abs(float(rec["total_score"]) - (float(rec["g_score"])
+               + float(rec["reg_score"]))) <= 1e-6 * abs(float(rec["total_score"]))
+    np.testing.assert_allclose(rec["total_grad"], rec["g_grad"] + rec["reg_grad"],
+                               rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("name", golden_names("mi"))
+def test_port_mi_bit_exact(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.port_mi(grid, fixed, moving, coeff, bins=32)
+    np.testing.assert_array_equal(r.f_hist, rec["f_hist"])
+    np.testing.assert_array_equal(r.m_hist, rec["m_hist"])
+    np.testing.assert_array_equal(r.j_hist, rec["j_hist"])
+    assert np.float32(r.score) == rec["mi_score"]
+    assert r.num_vox == rec["mi_num_vox"]
+    np.testing.assert_array_equal(r.grad, rec["mi_grad"])
+
+
+@pytest.mark.parametrize("name", golden_names("mi"))
+def test_port_mi_f64_close(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.port_mi(grid, fixed, moving, coeff, bins=32, precision="f64")
+    assert abs(r.score - rec["mi_score"]) <= 1e-5 * abs(rec["mi_score"])
+    assert rel_err(r.grad, rec["mi_grad"]) < 1e-3
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference oracle not built")
+@pytest.mark.parametrize("name", golden_names("mse_small"))
+def test_reference_reproduces_golden(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                     moving_grad=rec["moving_grad"])
+    np.testing.assert_array_equal(r.grad, rec["g_grad"])
