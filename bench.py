@@ -1,0 +1,366 @@
+"""Benchmark: B-spline MSE score + gradient throughput (Gvox/s) on B200.
+
+Workload (one "step" = one complete cost-function evaluation, coefficients
+in -> score + gradient out):
+    fixed/moving 256x256x128 CT-like volumes (int16 HU converted to float,
+    0.98x0.98x2.5 mm), vox_per_rgn 5x5x5 (70,304 tiles, 263,175
+    coefficients), coefficients N(0, 3 mm), MSE with the reference's
+    nearest-voxel gradient semantics.  Synthetic, seeded (no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form tc|fp32]
+    python bench.py --impl reference      # the reference's CPU flavour g
+
+value   device-resident throughput: inputs already in HBM, coefficients and
+        outputs in device memory, CUDA events on the evaluation stream, L2
+        flushed (256 MiB write) before every timed step and excluded.
+e2e     the same evaluation through the public C ABI with host (pinned)
+        buffers: coefficient upload, kernels, gradient + score download.
+N > 1   independent replicas, one per GPU (weak scaling, no collective on
+        the data path); max device time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "B-spline score+grad Gvox/s: BF16-TC vs FP32 form, one B200, grad err<=1e-3"
+WORKLOAD = {"workload": "mse_score_grad_256x256x128_vpr5",
+            "dims": [256, 256, 128], "spacing_mm": [0.98, 0.98, 2.5],
+            "vox_per_rgn": [5, 5, 5], "coeff_sigma_mm": 3.0,
+            "content": "CT-like int16 phantom (body/lung/bone ellipsoids + N(0,20))",
+            "gradient": "nearest-voxel moving gradient (reference flavour g)"}
+ALGO_BYTES_PER_VOXEL = 20   # fixed f32 + moving f32 + moving gradient 3xf32
+
+
+def make_workload(seed=20261205):
+    from plastimatch_b200 import synth
+    from plastimatch_b200.geometry import BsplineGrid, Volume
+    fixed = synth.ct_phantom((256, 256, 128), spacing=(0.98, 0.98, 2.5),
+                             seed=seed)
+    mov = synth.ct_phantom((256, 256, 128), spacing=(0.98, 0.98, 2.5),
+                           seed=seed + 1)
+    # shift the moving phantom by a fraction of a voxel so every sample is
+    # a genuine trilinear blend
+    moving = Volume(mov.img, origin=(0.37, -0.21, 0.55), spacing=mov.spacing)
+    grid = BsplineGrid.for_volume(fixed, 5)
+    coeff = synth.random_coeff(grid, 3.0, seed + 2)
+    return fixed, moving, grid, coeff
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(form):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(form)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:6]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_time(fixed, moving, grid, coeff, evals, threads,
+                       warmup=1):
+    """Seconds per evaluation of the reference's own OpenMP flavour g
+    (oracle/_ref), or of the single-thread restatement when absent."""
+    import oracle as O
+    if O.ref_available():
+        kind = "reference"
+        fn = lambda: O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                                  threads=threads)
+    else:
+        kind, threads = "port", 1
+        mg = O.port_volume_grad(moving)
+        fn = lambda: O.port_mse(grid, fixed, moving, coeff, moving_grad=mg)
+    for _ in range(warmup):
+        fn()
+    ts = []
+    for _ in range(evals):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts)), kind, threads
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    fixed, moving, grid, coeff = make_workload()
+    import oracle as O
+    threads = host_threads()
+    if O.ref_available():
+        kind = "reference"
+        fn = lambda: O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                                  threads=threads)
+    else:
+        kind, threads = "port", 1
+        mg = O.port_volume_grad(moving)
+        fn = lambda: O.port_mse(grid, fixed, moving, coeff, moving_grad=mg)
+    for _ in range(args.warmup):
+        fn()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    sec = float(np.sum(ts)) / args.steps
+    v = grid.num_roi_voxels / sec / 1e9
+    out = {"metric": METRIC, "impl": "reference", "value": v,
+           "unit": "Gvox/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": sec * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic",
+           "config": dict(WORKLOAD, form="reference CPU flavour g (OpenMP)"),
+           "cpu_baseline": {"value": v, "unit": "Gvox/s", "cores": threads,
+                            "kind": kind,
+                            "sample": "one full 256x256x128 evaluation per step"},
+           "e2e": {"value": v, "unit": "Gvox/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--form", default="tc", choices=["tc", "fp32"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-evals", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import plastimatch_b200 as P
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    fixed, moving, grid, coeff = make_workload()
+    ctx = P.Context(fixed, moving, grid, form=args.form, device=local_rank)
+    stream = torch.cuda.Stream(device=local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_images()
+    ctx.enable_timing(True)
+
+    d_coeff = torch.from_numpy(coeff).to(f"cuda:{local_rank}")
+    d_grad = torch.zeros(grid.num_coeff, device=f"cuda:{local_rank}")
+    d_score = torch.zeros(1, device=f"cuda:{local_rank}")
+    d_nvox = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local_rank}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8,
+                        device=f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+
+    def step():
+        ctx.score_mse(d_coeff, grad_out=d_grad, score_out=d_score,
+                      nvox_out=d_nvox)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            step()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    main_ms = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.fill_(1)
+                ev[i][0].record(stream)
+                step()
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        # per-evaluation main-kernel time (library events on the same stream)
+        for _ in range(3):
+            flush.fill_(1)
+            stream.synchronize()
+            s_h, g_h, n_h = ctx.score_mse(d_coeff)
+            _, m_ms, launches = ctx.last_timing()
+            main_ms.append(m_ms)
+    if dist:
+        dist.barrier()
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    t = torch.tensor([dev_ms], device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms = float(t.item())
+
+    # end to end through the C ABI with pinned host buffers
+    h_coeff = torch.from_numpy(coeff).pin_memory()
+    h_grad = torch.zeros(grid.num_coeff).pin_memory()
+    import ctypes as C
+    lib = P.lib()
+    s_c = C.c_float()
+    n_c = C.c_int64()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rc = lib.b200bsp_score_mse(ctx._h, h_coeff.data_ptr(), C.addressof(s_c),
+                                   h_grad.data_ptr(), C.addressof(n_c))
+        b.record(stream)
+        b.synchronize()
+        if rc:
+            raise RuntimeError(P.lib().b200bsp_last_error(ctx._h))
+        if i >= args.warmup:
+            e2e.append(a.elapsed_time(b))
+    e2e_ms = float(np.mean(e2e))
+    t = torch.tensor([e2e_ms], device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+
+    nvox = grid.num_roi_voxels
+    value = world * nvox / (dev_ms * 1e-3) / 1e9
+    e2e_value = world * nvox / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    main = float(np.median(main_ms))
+    achieved = ALGO_BYTES_PER_VOXEL * nvox / (main * 1e-3) / 1e9
+    out = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            sec, kind, th = cpu_reference_time(fixed, moving, grid, coeff,
+                                               args.cpu_evals, host_threads())
+            cpu = {"value": nvox / sec / 1e9, "unit": "Gvox/s", "cores": th,
+                   "kind": kind,
+                   "sample": f"{args.cpu_evals} full evaluations of the same "
+                             "256x256x128 workload (median)"}
+        traffic = profile_traffic(args.form)
+        out = {
+            "metric": METRIC, "value": value, "unit": "Gvox/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, form=args.form,
+                           l2="inputs 167 MB > L2 and 256 MiB flush write "
+                              "before every timed step (excluded)",
+                           parallelism=f"replicas x{world}"),
+            "e2e": {"value": e2e_value, "unit": "Gvox/s",
+                    "h2d_bytes_per_step": 4 * grid.num_coeff,
+                    "d2h_bytes_per_step": 4 * grid.num_coeff + 32},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "kernel_ms": main,
+                         "algorithmic_bytes_per_launch":
+                             ALGO_BYTES_PER_VOXEL * nvox},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+            "score": s_h, "num_vox": n_h,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

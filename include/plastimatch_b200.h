@@ -1,0 +1,209 @@
+/* plastimatch_b200 -- B200-native B-spline registration cost function.
+ *
+ * C ABI of libplastimatch_b200.so.  Plain C types only: the caller passes
+ * volume geometry, image and coefficient pointers (host or device memory;
+ * the library finds out which) and gets the score and gradient back in the
+ * reference's layout and normalisation.
+ *
+ * The entry points replace the reference's CUDA plugin interface for the
+ * B-spline cost function (Plastimatch src/register/cuda/bspline_cuda.h:
+ * 124-300), which the reference loads with dlopen/dlsym
+ * (src/sys/cuda_delayload.h:23-56) and calls from its flavour dispatchers
+ * (src/register/bspline_mse.cxx:1937-1962, src/register/bspline_mi.cxx:
+ * 3103-3141).  Differences from that interface, by design:
+ *   - every call returns a status code (B200BSP_OK / B200BSP_E_*) and never
+ *     exits the process (the reference plugin calls exit()),
+ *   - device state lives in an opaque context created once per registration
+ *     stage instead of the Dev_Pointers_Bspline struct.
+ *
+ * Threading: one context per host thread (the reference is single-threaded
+ * per registration as well).  Contexts are independent; several may share
+ * a device.
+ */
+#ifndef PLASTIMATCH_B200_H
+#define PLASTIMATCH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define B200BSP_OK              0
+#define B200BSP_E_BADARG       -1   /* invalid argument or geometry */
+#define B200BSP_E_OOM          -2   /* device or pinned allocation failed */
+#define B200BSP_E_CUDA         -3   /* CUDA runtime error (see last_error) */
+#define B200BSP_E_TIMEOUT      -4   /* a bounded device-side wait gave up */
+#define B200BSP_E_STATE        -5   /* call out of order (e.g. no images) */
+#define B200BSP_E_UNSUPPORTED  -6   /* valid request this build cannot do */
+
+/* Kernel forms. */
+#define B200BSP_FORM_TC    0   /* tcgen05 tensor-core field + adjoint (default) */
+#define B200BSP_FORM_FP32  1   /* plain FP32 SIMT, one thread per voxel */
+
+/* MSE gradient semantics. */
+#define B200BSP_MSE_GRAD_NEAREST    0  /* dc/dv = diff * moving_grad[nearest voxel]
+                                          (reference flavours c/g/h/i/k/l) */
+#define B200BSP_MSE_GRAD_TRILINEAR  1  /* dc/dv = diff * d(trilinear)/dx
+                                          (reference flavours o/p/q/r) */
+
+/* Geometry of one volume, as Plastimatch's Volume holds it
+ * (src/base/volume.h:37-57): dim in voxels (x fastest), origin and spacing
+ * in mm, direction cosines row-major. */
+typedef struct {
+    int64_t dim[3];
+    float origin[3];
+    float spacing[3];
+    float dcos[9];
+} b200bsp_volume;
+
+/* The B-spline control grid over the fixed image: the ROI and knot spacing
+ * of Bspline_xform::initialize (src/base/bspline_xform.cxx:491-507).  The
+ * grid's image origin/spacing/dcos are the fixed volume's. */
+typedef struct {
+    int64_t roi_offset[3];
+    int64_t roi_dim[3];
+    int64_t vox_per_rgn[3];
+} b200bsp_grid;
+
+/* Options fixed for the life of a context. */
+typedef struct {
+    int form;           /* B200BSP_FORM_* */
+    int mse_grad;       /* B200BSP_MSE_GRAD_* */
+    int mi_bins;        /* fixed and moving histogram bins (reference default 32) */
+    int device;         /* CUDA device ordinal */
+    int reserved[4];    /* zero */
+} b200bsp_opts;
+
+/* Regularisation weights of Regularization_parms
+ * (src/register/regularization_parms.h:16-43). */
+typedef struct {
+    float curvature_penalty;
+    float diffusion_penalty;
+    float lame_coefficient_1;
+    float lame_coefficient_2;
+    float total_displacement_penalty;
+    float third_order_penalty;
+    float linear_elastic_multiplier;   /* reference default 1 */
+    float curvature_mixed_weight;      /* reference default 1 */
+} b200bsp_reg_parms;
+
+typedef struct b200bsp_ctx b200bsp_ctx;
+
+/* Fill opts with defaults: TC form, nearest-voxel MSE gradient, 32 bins,
+ * device 0. */
+void b200bsp_default_opts (b200bsp_opts* opts);
+
+/* Library version string. */
+const char* b200bsp_version (void);
+
+/* Create a context for one fixed/moving pair and B-spline grid.  Replaces
+ * bspline_cuda_state_create + CUDA_bspline_mse_init_j / CUDA_bspline_mi_init_a
+ * (src/register/bspline_state.cxx:165-212, bspline_cuda.h:124-140).
+ * Computes rdims/cdims and the basis tables as Bspline_xform::allocate does
+ * (src/base/bspline_xform.cxx:361-488).  Allocates all device memory the
+ * evaluations need; later calls allocate nothing. */
+int b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
+    const b200bsp_grid* grid, const b200bsp_opts* opts, b200bsp_ctx** out);
+
+/* Release the context (bspline_cuda_state_destroy,
+ * src/register/bspline_state.cxx:214-271).  NULL is accepted. */
+int b200bsp_destroy (b200bsp_ctx* ctx);
+
+/* rdims, cdims and num_coeff of the grid (Bspline_header fields). */
+int b200bsp_grid_info (const b200bsp_ctx* ctx, int64_t rdims[3],
+    int64_t cdims[3], int64_t* num_coeff);
+
+/* Upload the images.  fixed_img/moving_img: float32, dim[0]*dim[1]*dim[2]
+ * voxels, x fastest.  moving_grad: float32 xyz interleaved (the output of
+ * volume_gradient, src/base/volume_grad.cxx:137-145) or NULL, in which case
+ * it is computed on the device with the reference's formula.  For MI the
+ * histogram ranges are set here (EQSP, src/register/joint_histogram.cxx:
+ * 115-139).  Pointers may be host or device memory. */
+int b200bsp_set_images (b200bsp_ctx* ctx, const float* fixed_img,
+    const float* moving_img, const float* moving_grad);
+
+/* Use this CUDA stream (cudaStream_t) for all work of the context.  NULL
+ * selects the context's own stream. */
+int b200bsp_set_stream (b200bsp_ctx* ctx, void* stream);
+
+/* MSE score and gradient: the work of bspline_score_mse for one metric
+ * (src/register/bspline_mse.cxx:1865-1964) followed by
+ * bspline_score_normalize (:43-72).  Writes curr_smetric (score/N),
+ * curr_smetric_grad (2*dC/dp/N, num_coeff floats, xyz interleaved per knot)
+ * and curr_num_vox.  With no overlapping voxel, score = FLT_MAX and the
+ * gradient is zero, as in the reference.  coeff/score/grad/num_vox may be
+ * host or device pointers; with all of them in device memory the call is
+ * stream-ordered and returns without waiting. */
+int b200bsp_score_mse (b200bsp_ctx* ctx, const float* coeff, float* score,
+    float* grad, int64_t* num_vox);
+
+/* As b200bsp_score_mse with double-precision outputs (the device
+ * accumulates the score and gradient in double; this skips the final
+ * rounding to float). */
+int b200bsp_score_mse_f64 (b200bsp_ctx* ctx, const float* coeff,
+    double* score, double* grad, int64_t* num_vox);
+
+/* Mattes mutual information with PVI-8 histograms, flavour g semantics
+ * (src/register/bspline_mi.cxx:1505-1750): score = -MI, gradient dS/dp,
+ * plus the histograms of pass 1 when f_hist/m_hist/j_hist are non-NULL
+ * (host pointers; bins, bins, bins*bins doubles). */
+int b200bsp_score_mi (b200bsp_ctx* ctx, const float* coeff, float* score,
+    float* grad, int64_t* num_vox, double* f_hist, double* m_hist,
+    double* j_hist);
+
+/* Analytic regulariser (Bspline_regularize::compute_score with
+ * implementation 'b'/'c', src/register/bspline_regularize.cxx:95-126;
+ * src/register/bspline_regularize_analytic.cxx:637-1059).  Writes rmetric
+ * and ADDS the regulariser gradient into grad (as the reference adds into
+ * total_grad). */
+int b200bsp_regularize (b200bsp_ctx* ctx, const float* coeff,
+    const b200bsp_reg_parms* parms, float* rmetric, float* grad);
+
+/* The whole cost function bspline_score() (src/register/bspline.cxx:
+ * 558-632) for one similarity metric: metric_type 0 = MSE, 1 = MI;
+ * total_score = lambda * smetric (+ rmetric when reg != NULL), total_grad
+ * likewise. */
+int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
+    float lambda, const b200bsp_reg_parms* reg, float* total_score,
+    float* total_grad, float* smetric, int64_t* num_vox);
+
+/* Dense displacement field over the ROI (bspline_interpolate_vf,
+ * src/base/bspline_interpolate.cxx:112-142): vf is dim[0]*dim[1]*dim[2]*3
+ * floats of the fixed image, xyz interleaved; voxels outside the ROI are
+ * zero. */
+int b200bsp_interpolate_vf (b200bsp_ctx* ctx, const float* coeff, float* vf);
+
+/* Warp the moving image onto the fixed grid with trilinear interpolation
+ * and `default_value` outside (bspline_warp, src/base/bspline_warp.cxx:
+ * 171-227, linear interpolation, no vector-field output). */
+int b200bsp_warp (b200bsp_ctx* ctx, const float* coeff, float default_value,
+    float* warped);
+
+/* Moving-image gradient alone (volume_calc_grad,
+ * src/base/volume_grad.cxx:9-76) for an arbitrary volume. */
+int b200bsp_volume_grad (const b200bsp_volume* vol, const float* img,
+    float* grad_out, int device);
+
+/* Turn per-evaluation device timing (CUDA events on the context's stream)
+ * on or off; off by default. */
+int b200bsp_enable_timing (b200bsp_ctx* ctx, int on);
+
+/* Device time of the last evaluation in milliseconds (all its kernels and
+ * copies, from the first launch to the last), and the number of kernel
+ * launches it made.  Needs timing enabled. */
+int b200bsp_last_timing (const b200bsp_ctx* ctx, float* ms, int* launches);
+
+/* Device time of the last evaluation's main tile kernel alone (ms). */
+int b200bsp_last_main_ms (const b200bsp_ctx* ctx, float* ms);
+
+/* Text of the last error on this context (or the last create failure when
+ * ctx is NULL). */
+const char* b200bsp_last_error (const b200bsp_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

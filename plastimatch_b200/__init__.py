@@ -1,0 +1,299 @@
+"""plastimatch_b200: B200-native B-spline registration cost function.
+
+Python binding over the C ABI of libplastimatch_b200.so
+(include/plastimatch_b200.h).  The compute path is the CUDA library only:
+if the shared library is missing or fails to load, importing the binding's
+entry points raises -- there is no CPU fallback.
+
+    from plastimatch_b200 import Context
+    from plastimatch_b200.geometry import Volume, BsplineGrid
+    ctx = Context(fixed, moving, grid)          # b200bsp_create
+    ctx.set_images()                            # b200bsp_set_images
+    score, grad, nvox = ctx.score_mse(coeff)    # b200bsp_score_mse
+
+Arrays may be numpy (host) or torch CUDA tensors (device); results come
+back as numpy arrays unless `out` tensors are given.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .geometry import BsplineGrid, Volume  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplastimatch_b200.so")
+
+B200BSP_OK = 0
+FORMS = {"tc": 0, "fp32": 1}
+MSE_GRAD = {"nearest": 0, "trilinear": 1}
+ERRORS = {-1: "E_BADARG", -2: "E_OOM", -3: "E_CUDA", -4: "E_TIMEOUT",
+          -5: "E_STATE", -6: "E_UNSUPPORTED"}
+
+
+class B200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class VolumeDesc(C.Structure):
+    _fields_ = [("dim", C.c_int64 * 3), ("origin", C.c_float * 3),
+                ("spacing", C.c_float * 3), ("dcos", C.c_float * 9)]
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("roi_offset", C.c_int64 * 3), ("roi_dim", C.c_int64 * 3),
+                ("vox_per_rgn", C.c_int64 * 3)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("form", C.c_int), ("mse_grad", C.c_int), ("mi_bins", C.c_int),
+                ("device", C.c_int), ("reserved", C.c_int * 4)]
+
+
+class RegParms(C.Structure):
+    _fields_ = [("curvature_penalty", C.c_float),
+                ("diffusion_penalty", C.c_float),
+                ("lame_coefficient_1", C.c_float),
+                ("lame_coefficient_2", C.c_float),
+                ("total_displacement_penalty", C.c_float),
+                ("third_order_penalty", C.c_float),
+                ("linear_elastic_multiplier", C.c_float),
+                ("curvature_mixed_weight", C.c_float)]
+
+
+def reg_parms(curvature=0.0, diffusion=0.0, lame_1=0.0, lame_2=0.0,
+              total_displacement=0.0, third_order=0.0,
+              linear_elastic_multiplier=1.0,
+              curvature_mixed_weight=1.0) -> RegParms:
+    return RegParms(curvature, diffusion, lame_1, lame_2, total_displacement,
+                    third_order, linear_elastic_multiplier,
+                    curvature_mixed_weight)
+
+
+_lib = None
+
+# Every entry point of include/plastimatch_b200.h with its ctypes signature.
+_VP = C.c_void_p
+_SIGS = {
+    "b200bsp_default_opts": (None, [_VP]),
+    "b200bsp_version": (C.c_char_p, []),
+    "b200bsp_create": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_destroy": (C.c_int, [_VP]),
+    "b200bsp_grid_info": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "b200bsp_set_images": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "b200bsp_set_stream": (C.c_int, [_VP, _VP]),
+    "b200bsp_score_mse": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_score_mse_f64": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_score_mi": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_regularize": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_score": (C.c_int, [_VP, _VP, C.c_int, C.c_float, _VP, _VP, _VP,
+                                _VP, _VP]),
+    "b200bsp_interpolate_vf": (C.c_int, [_VP, _VP, _VP]),
+    "b200bsp_warp": (C.c_int, [_VP, _VP, C.c_float, _VP]),
+    "b200bsp_volume_grad": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "b200bsp_enable_timing": (C.c_int, [_VP, C.c_int]),
+    "b200bsp_last_timing": (C.c_int, [_VP, _VP, _VP]),
+    "b200bsp_last_main_ms": (C.c_int, [_VP, _VP]),
+    "b200bsp_last_error": (C.c_char_p, [_VP]),
+}
+
+
+def lib():
+    """Load libplastimatch_b200.so (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with "
+                "`python -m plastimatch_b200.build` (no CPU fallback exists)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _vol_desc(v: Volume) -> VolumeDesc:
+    return VolumeDesc((C.c_int64 * 3)(*v.dim), (C.c_float * 3)(*v.origin),
+                      (C.c_float * 3)(*v.spacing), (C.c_float * 9)(*v.dcos))
+
+
+def _ptr(a, dtype=np.float32):
+    """Raw pointer of a numpy array or torch tensor (None passes through)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if not (a.flags["C_CONTIGUOUS"] and a.dtype == dtype):
+        raise ValueError(f"need a C-contiguous {np.dtype(dtype)} array")
+    return a.ctypes.data
+
+
+def _check(rc, ctx_handle=None):
+    if rc != B200BSP_OK:
+        msg = lib().b200bsp_last_error(ctx_handle)
+        raise B200Error(rc, msg.decode() if msg else "")
+
+
+def volume_grad(vol: Volume, device: int = 0) -> np.ndarray:
+    """Moving-image gradient on the device (volume_calc_grad)."""
+    out = np.zeros(vol.npix * 3, np.float32)
+    d = _vol_desc(vol)
+    _check(lib().b200bsp_volume_grad(C.byref(d), _ptr(vol.img), _ptr(out),
+                                     device))
+    return out
+
+
+class Context:
+    """One registration stage's device state (b200bsp_ctx)."""
+
+    def __init__(self, fixed: Volume, moving: Volume, grid: BsplineGrid,
+                 form: str = "tc", mse_grad: str = "nearest",
+                 mi_bins: int = 32, device: int = 0):
+        L = lib()
+        self.fixed, self.moving, self.grid = fixed, moving, grid
+        self.form = form
+        self.mi_bins = mi_bins
+        o = Opts()
+        L.b200bsp_default_opts(C.byref(o))
+        o.form = FORMS[form]
+        o.mse_grad = MSE_GRAD[mse_grad]
+        o.mi_bins = mi_bins
+        o.device = device
+        self._fd, self._md = _vol_desc(fixed), _vol_desc(moving)
+        self._gd = GridDesc((C.c_int64 * 3)(*grid.roi_offset),
+                            (C.c_int64 * 3)(*grid.roi_dim),
+                            (C.c_int64 * 3)(*grid.vox_per_rgn))
+        h = C.c_void_p()
+        rc = L.b200bsp_create(C.byref(self._fd), C.byref(self._md),
+                              C.byref(self._gd), C.byref(o), C.byref(h))
+        _check(rc)
+        self._h = h
+        rd = (C.c_int64 * 3)()
+        cd = (C.c_int64 * 3)()
+        nc = C.c_int64()
+        _check(L.b200bsp_grid_info(h, rd, cd, C.byref(nc)), h)
+        self.rdims, self.cdims = tuple(rd), tuple(cd)
+        self.num_coeff = nc.value
+        assert self.rdims == grid.rdims and self.num_coeff == grid.num_coeff
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().b200bsp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_images(self, fixed_img=None, moving_img=None, moving_grad=None):
+        f = self.fixed.img if fixed_img is None else fixed_img
+        m = self.moving.img if moving_img is None else moving_img
+        _check(lib().b200bsp_set_images(self._h, _ptr(f), _ptr(m),
+                                        _ptr(moving_grad)), self._h)
+        return self
+
+    def set_stream(self, stream_handle: int | None):
+        _check(lib().b200bsp_set_stream(self._h, stream_handle), self._h)
+
+    def enable_timing(self, on=True):
+        _check(lib().b200bsp_enable_timing(self._h, int(on)), self._h)
+
+    def last_timing(self):
+        ms = C.c_float()
+        n = C.c_int()
+        main = C.c_float()
+        _check(lib().b200bsp_last_timing(self._h, C.byref(ms), C.byref(n)),
+               self._h)
+        _check(lib().b200bsp_last_main_ms(self._h, C.byref(main)), self._h)
+        return ms.value, main.value, n.value
+
+    def score_mse(self, coeff, grad_out=None, score_out=None, nvox_out=None):
+        """(score, grad, num_vox).  With torch CUDA tensors for coeff and
+        all outputs the call is stream-ordered and returns the tensors."""
+        if grad_out is not None:
+            _check(lib().b200bsp_score_mse(self._h, _ptr(coeff),
+                                           _ptr(score_out), _ptr(grad_out),
+                                           _ptr(nvox_out)), self._h)
+            return score_out, grad_out, nvox_out
+        g = np.zeros(self.num_coeff, np.float32)
+        s = C.c_float()
+        n = C.c_int64()
+        _check(lib().b200bsp_score_mse(self._h, _ptr(coeff), C.addressof(s),
+                                       _ptr(g), C.addressof(n)), self._h)
+        return s.value, g, n.value
+
+    def score_mse_f64(self, coeff):
+        g = np.zeros(self.num_coeff, np.float64)
+        s = C.c_double()
+        n = C.c_int64()
+        _check(lib().b200bsp_score_mse_f64(self._h, _ptr(coeff),
+                                           C.addressof(s), _ptr(g, np.float64),
+                                           C.addressof(n)), self._h)
+        return s.value, g, n.value
+
+    def score_mi(self, coeff, with_hist=False):
+        b = None
+        g = np.zeros(self.num_coeff, np.float32)
+        s = C.c_float()
+        n = C.c_int64()
+        fh = mh = jh = None
+        if with_hist:
+            b = self.mi_bins
+            fh, mh, jh = np.zeros(b), np.zeros(b), np.zeros(b * b)
+        _check(lib().b200bsp_score_mi(self._h, _ptr(coeff), C.addressof(s),
+                                      _ptr(g), C.addressof(n),
+                                      _ptr(fh, np.float64), _ptr(mh, np.float64),
+                                      _ptr(jh, np.float64)), self._h)
+        if with_hist:
+            return s.value, g, n.value, (fh, mh, jh.reshape(b, b))
+        return s.value, g, n.value
+
+    def regularize(self, coeff, parms: RegParms, grad=None):
+        """(rmetric, grad): grad accumulates the regulariser gradient."""
+        g = np.zeros(self.num_coeff, np.float32) if grad is None else grad
+        s = C.c_float()
+        _check(lib().b200bsp_regularize(self._h, _ptr(coeff), C.byref(parms),
+                                        C.addressof(s), _ptr(g)), self._h)
+        return s.value, g
+
+    def score(self, coeff, metric="mse", lam=1.0, reg: RegParms | None = None):
+        """bspline_score(): (total_score, total_grad, smetric, num_vox)."""
+        g = np.zeros(self.num_coeff, np.float32)
+        ts, sm = C.c_float(), C.c_float()
+        n = C.c_int64()
+        _check(lib().b200bsp_score(self._h, _ptr(coeff),
+                                   0 if metric == "mse" else 1, lam,
+                                   C.byref(reg) if reg is not None else None,
+                                   C.addressof(ts), _ptr(g), C.addressof(sm),
+                                   C.addressof(n)), self._h)
+        return ts.value, g, sm.value, n.value
+
+    def interpolate_vf(self, coeff):
+        nx, ny, nz = self.fixed.dim
+        vf = np.zeros(nx * ny * nz * 3, np.float32)
+        _check(lib().b200bsp_interpolate_vf(self._h, _ptr(coeff), _ptr(vf)),
+               self._h)
+        return vf.reshape(nz, ny, nx, 3)
+
+    def warp(self, coeff, default_value=0.0):
+        nx, ny, nz = self.fixed.dim
+        out = np.zeros(nx * ny * nz, np.float32)
+        _check(lib().b200bsp_warp(self._h, _ptr(coeff), default_value,
+                                  _ptr(out)), self._h)
+        return out.reshape(nz, ny, nx)
+

@@ -1,0 +1,171 @@
+// Device-side geometry and per-voxel steps of the B-spline cost function,
+// shared by every kernel form.
+//
+// Each helper restates one step of the reference's voxel loop
+// (Plastimatch src/register/bspline_mse.cxx:519-720, flavour g):
+//   world position      POSITION_FROM_COORDS   src/base/volume_macros.h:78-94
+//   correspondence      bspline_find_correspondence_dcos
+//                                              src/util/bspline_correspond.cxx:80-107
+//   inside test         Volume::is_inside      src/base/volume.cxx:900-906
+//   clamp + fractions   li_clamp               src/base/interpolate.cxx:17-41
+//   trilinear value     li_value               src/base/interpolate.cxx:135-158
+//   trilinear gradient  li_value_dx/dy/dz      src/base/interpolate.cxx:161-257
+// Linear voxel indices are 32-bit: volumes are limited to < 2^31 voxels
+// (checked when a context is created).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200 {
+
+// Geometry of one evaluation, passed by value to every kernel.
+struct BspGeom {
+    int fdim[3];          // fixed image dims (x fastest)
+    float img_origin[3];  // B-spline grid's image origin (Bspline_xform::img_origin)
+    float fstep[9];       // fixed step = dcos * spacing
+    int mdim[3];          // moving image dims
+    float morigin[3];
+    float mproj[9];       // moving proj = inv(dcos) / spacing
+    float minv_spacing[3];
+    int roi_off[3];
+    int roi_dim[3];
+    int vpr[3];           // voxels per region (tile edge)
+    int rdims[3];         // tiles per axis
+    int cdims[3];         // knots per axis = rdims + 3
+    int ntiles;
+    int nknots;
+};
+
+// Where one fixed voxel lands in the moving image.
+struct Sample {
+    int mvf;        // linear index of the floor corner
+    int mvr;        // linear index of the nearest ("round") voxel
+    float w1[3];    // fraction for the lower corner, per axis
+    float w2[3];    // fraction for the upper corner, per axis
+};
+
+// World position of fixed voxel (i, j, k): origin + step * ijk.
+__device__ __forceinline__ void
+fixed_position (const BspGeom& g, int i, int j, int k, float xyz[3])
+{
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        xyz[d] = g.img_origin[d] + i * g.fstep[3*d+0] + j * g.fstep[3*d+1]
+            + k * g.fstep[3*d+2];
+    }
+}
+
+// Project the displaced position into the moving image, test that it lies
+// strictly inside (-0.5, dim-0.5) on every axis and compute the clamped
+// trilinear corner and fractions.  Returns false when outside.
+__device__ __forceinline__ bool
+locate (const BspGeom& g, const float fxyz[3], const float dxyz[3], Sample& s)
+{
+    float t0 = (fxyz[0] + dxyz[0]) - g.morigin[0];
+    float t1 = (fxyz[1] + dxyz[1]) - g.morigin[1];
+    float t2 = (fxyz[2] + dxyz[2]) - g.morigin[2];
+    int f[3], r[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        float ma = t0 * g.mproj[3*d+0] + t1 * g.mproj[3*d+1]
+            + t2 * g.mproj[3*d+2];
+        if (!(ma > -0.5f && ma < (float) g.mdim[d] - 0.5f)) return false;
+        int dmax = g.mdim[d] - 1;
+        float w2;
+        if (ma < 0.f) {
+            f[d] = 0; r[d] = 0; w2 = 0.f;
+        } else if (ma >= (float) dmax) {
+            f[d] = dmax - 1; r[d] = dmax; w2 = 1.f;
+        } else {
+            float fl = floorf (ma);
+            f[d] = (int) fl;
+            w2 = ma - fl;                  // exact: ma and fl are close
+            r[d] = f[d] + (w2 >= 0.5f);    // == (long)((double)ma + 0.5)
+        }
+        s.w2[d] = w2;
+        s.w1[d] = 1.f - w2;
+    }
+    s.mvf = f[0] + g.mdim[0] * (f[1] + g.mdim[1] * f[2]);
+    s.mvr = r[0] + g.mdim[0] * (r[1] + g.mdim[1] * r[2]);
+    return true;
+}
+
+// The eight corner values of a trilinear cell, in li_value's order.
+struct Corners { float m[8]; };
+
+__device__ __forceinline__ Corners
+load_corners (const float* __restrict__ img, int mvf, int dx, int dxy)
+{
+    Corners c;
+    c.m[0] = __ldg (img + mvf);
+    c.m[1] = __ldg (img + mvf + 1);
+    c.m[2] = __ldg (img + mvf + dx);
+    c.m[3] = __ldg (img + mvf + dx + 1);
+    c.m[4] = __ldg (img + mvf + dxy);
+    c.m[5] = __ldg (img + mvf + dxy + 1);
+    c.m[6] = __ldg (img + mvf + dxy + dx);
+    c.m[7] = __ldg (img + mvf + dxy + dx + 1);
+    return c;
+}
+
+__device__ __forceinline__ float
+trilinear (const Sample& s, const Corners& c)
+{
+    const float* f1 = s.w1;
+    const float* f2 = s.w2;
+    return f1[0] * f1[1] * f1[2] * c.m[0] + f2[0] * f1[1] * f1[2] * c.m[1]
+        + f1[0] * f2[1] * f1[2] * c.m[2] + f2[0] * f2[1] * f1[2] * c.m[3]
+        + f1[0] * f1[1] * f2[2] * c.m[4] + f2[0] * f1[1] * f2[2] * c.m[5]
+        + f1[0] * f2[1] * f2[2] * c.m[6] + f2[0] * f2[1] * f2[2] * c.m[7];
+}
+
+// Derivative of the trilinear interpolant along each index axis, scaled by
+// 1/spacing (li_value_dx/dy/dz; no rotation by the direction cosines).
+__device__ __forceinline__ void
+trilinear_grad (const BspGeom& g, const Sample& s, const Corners& c,
+    float out[3])
+{
+    const float* f1 = s.w1;
+    const float* f2 = s.w2;
+    float rx = g.minv_spacing[0], ry = g.minv_spacing[1];
+    float rz = g.minv_spacing[2];
+    out[0] = rx * (f1[1] * f1[2] * (c.m[1] - c.m[0])
+        + f2[1] * f1[2] * (c.m[3] - c.m[2])
+        + f1[1] * f2[2] * (c.m[5] - c.m[4])
+        + f2[1] * f2[2] * (c.m[7] - c.m[6]));
+    out[1] = ry * (f1[0] * f1[2] * (c.m[2] - c.m[0])
+        + f2[0] * f1[2] * (c.m[3] - c.m[1])
+        + f1[0] * f2[2] * (c.m[6] - c.m[4])
+        + f2[0] * f2[2] * (c.m[7] - c.m[5]));
+    out[2] = rz * (f1[0] * f1[1] * (c.m[4] - c.m[0])
+        + f2[0] * f1[1] * (c.m[5] - c.m[1])
+        + f1[0] * f2[1] * (c.m[6] - c.m[2])
+        + f2[0] * f2[1] * (c.m[7] - c.m[3]));
+}
+
+// Deterministic block-wide sum of a double and an int (fixed tree order).
+template <int NT>
+__device__ __forceinline__ void
+block_sum (double& v, int& n, double* sh_v, int* sh_n)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_down_sync (0xffffffffu, v, o);
+        n += __shfl_down_sync (0xffffffffu, n, o);
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sh_v[w] = v; sh_n[w] = n; }
+    __syncthreads ();
+    if (w == 0) {
+        v = (l < NT / 32) ? sh_v[l] : 0.0;
+        n = (l < NT / 32) ? sh_n[l] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v += __shfl_down_sync (0xffffffffu, v, o);
+            n += __shfl_down_sync (0xffffffffu, n, o);
+        }
+    }
+}
+
+} // namespace b200

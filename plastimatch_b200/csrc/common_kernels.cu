@@ -1,0 +1,206 @@
+// Reductions shared by all forms:
+//   reduce_score  -- sum of the per-CTA score/count partials (fixed order)
+//   gather_grad   -- per-knot sum of the partial gradients written by the
+//                    tile kernels, normalised as bspline_score_normalize
+//                    (Plastimatch src/register/bspline_mse.cxx:43-72);
+//                    replaces the reference's serial condense
+//                    (bspline_condense_smetric_grad, src/register/bspline.cxx:
+//                    400-413) with one thread per knot, each summing its
+//                    contributions in a fixed order in double precision, so
+//                    the result is deterministic without atomics.
+//   volume_grad   -- volume_calc_grad (src/base/volume_grad.cxx:9-76)
+#include <cfloat>
+
+#include "kernels.cuh"
+
+namespace b200 {
+
+constexpr int RED_THREADS = 1024;
+
+__global__ void __launch_bounds__ (RED_THREADS)
+reduce_score_kernel (const double* __restrict__ sp, const int* __restrict__ cp,
+    int n, DevResult* __restrict__ res, int mode)
+{
+    __shared__ double sh_v[RED_THREADS / 32];
+    __shared__ int sh_n[RED_THREADS / 32];
+    double v = 0.0;
+    long long nn = 0;
+    for (int i = threadIdx.x; i < n; i += RED_THREADS) {
+        v += sp[i];
+        nn += cp[i];
+    }
+    int n32 = (int) nn;   // per-thread counts stay far below 2^31
+    block_sum<RED_THREADS> (v, n32, sh_v, sh_n);
+    if (threadIdx.x == 0) {
+        res->raw = v;
+        res->num_vox = n32;
+        res->error = 0;
+        if (mode == 0) {
+            if (n32 < 1) {
+                res->score = FLT_MAX;
+                res->score_f = FLT_MAX;
+            } else {
+                res->score = v / (double) n32;
+                res->score_f = (float) res->score;
+            }
+        }
+    }
+}
+
+cudaError_t
+launch_reduce_score (const double* score_part, const int* count_part, int n,
+    DevResult* res, int mode, cudaStream_t st)
+{
+    reduce_score_kernel<<<1, RED_THREADS, 0, st>>> (score_part, count_part, n,
+        res, mode);
+    return cudaGetLastError ();
+}
+
+// One thread per knot.  mode 0: MSE normalisation grad = 2*sum/N;
+// mode 1: no normalisation (MI pass-2 dc/dv already carries 1/N).
+__global__ void
+gather_grad_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
+    const DevResult* __restrict__ res, int mode, float* __restrict__ grad_out,
+    double* __restrict__ grad64_out, float* __restrict__ score_out,
+    double* __restrict__ score64_out, long long* __restrict__ nvox_out)
+{
+    int knot = blockIdx.x * blockDim.x + threadIdx.x;
+    long long N = res->num_vox;
+    if (knot == 0) {
+        if (score_out) *score_out = res->score_f;
+        if (score64_out) *score64_out = res->score;
+        if (nvox_out) *nvox_out = N;
+    }
+    if (knot >= g.nknots) return;
+    const int cx = g.cdims[0], cy = g.cdims[1];
+    const int kx = knot % cx, ky = (knot / cx) % cy, kz = knot / (cx * cy);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (lay.slots == 64) {
+        // Slot m = i + 4j + 16k of tile (kx-i, ky-j, kz-k), in slot order
+        // as the reference's condense sums them.
+        for (int k = 0; k < 4; k++) {
+            int tz = kz - k;
+            if (tz < 0 || tz >= g.rdims[2]) continue;
+            for (int j = 0; j < 4; j++) {
+                int ty = ky - j;
+                if (ty < 0 || ty >= g.rdims[1]) continue;
+                for (int i = 0; i < 4; i++) {
+                    int tx = kx - i;
+                    if (tx < 0 || tx >= g.rdims[0]) continue;
+                    int t = tx + g.rdims[0] * (ty + g.rdims[1] * tz);
+                    int m = i + 4 * j + 16 * k;
+                    const float* p = part + ((size_t) m * g.ntiles + t) * 3;
+                    s0 += p[0]; s1 += p[1]; s2 += p[2];
+                }
+            }
+        }
+    } else {
+        // Batch footprints: batch (bi, bj, bk) covers knots
+        // [bi*bx, bi*bx + bx + 3) along x, likewise y and z.
+        int bi0 = max (0, (kx - lay.bx - 2 + lay.bx - 1) / lay.bx);
+        if (kx - lay.bx - 2 < 0) bi0 = 0;
+        int bi1 = min (lay.nbx - 1, kx / lay.bx);
+        int bj0 = (ky - lay.by - 2 < 0) ? 0 : (ky - lay.by - 2 + lay.by - 1) / lay.by;
+        int bj1 = min (lay.nby - 1, ky / lay.by);
+        int bk0 = (kz - lay.bz - 2 < 0) ? 0 : (kz - lay.bz - 2 + lay.bz - 1) / lay.bz;
+        int bk1 = min (lay.nbz - 1, kz / lay.bz);
+        const int KF = lay.kx * lay.ky * lay.kz;
+        for (int bk = bk0; bk <= bk1; bk++) {
+            int lz = kz - bk * lay.bz;
+            for (int bj = bj0; bj <= bj1; bj++) {
+                int ly = ky - bj * lay.by;
+                for (int bi = bi0; bi <= bi1; bi++) {
+                    int lx = kx - bi * lay.bx;
+                    int b = bi + lay.nbx * (bj + lay.nby * bk);
+                    int kk = lx + lay.kx * (ly + lay.ky * lz);
+                    const float* p = part + ((size_t) b * KF + kk) * 3;
+                    s0 += p[0]; s1 += p[1]; s2 += p[2];
+                }
+            }
+        }
+    }
+    if (mode == 0) {
+        if (N < 1) {
+            s0 = s1 = s2 = 0.0;
+        } else {
+            double sc = 2.0 / (double) N;
+            s0 *= sc; s1 *= sc; s2 *= sc;
+        }
+    }
+    if (grad_out) {
+        grad_out[3 * knot + 0] = (float) s0;
+        grad_out[3 * knot + 1] = (float) s1;
+        grad_out[3 * knot + 2] = (float) s2;
+    }
+    if (grad64_out) {
+        grad64_out[3 * knot + 0] = s0;
+        grad64_out[3 * knot + 1] = s1;
+        grad64_out[3 * knot + 2] = s2;
+    }
+}
+
+cudaError_t
+launch_gather_grad (const BspGeom& g, const PartLayout& lay, const float* part,
+    const DevResult* res, int mode, float* grad_out, double* grad64_out,
+    float* score_out, double* score64_out, long long* nvox_out,
+    cudaStream_t st)
+{
+    int threads = 256;
+    int blocks = (g.nknots + threads - 1) / threads;
+    gather_grad_kernel<<<blocks, threads, 0, st>>> (g, lay, part, res, mode,
+        grad_out, grad64_out, score_out, score64_out, nvox_out);
+    return cudaGetLastError ();
+}
+
+// Central differences with replicated borders, divided by 2*spacing and
+// rotated by the inverse direction cosines; xyz interleaved.
+__global__ void
+volume_grad_kernel (int nx, int ny, int nz, float sx, float sy, float sz,
+    const float* __restrict__ inv_dc9, const float* __restrict__ img,
+    float* __restrict__ out)
+{
+    long long n = (long long) nx * ny * nz;
+    long long v = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    int i = (int) (v % nx), j = (int) ((v / nx) % ny), k = (int) (v / ((long long) nx * ny));
+    int ip = i > 0 ? i - 1 : 0, in = i < nx - 1 ? i + 1 : nx - 1;
+    int jp = j > 0 ? j - 1 : 0, jn = j < ny - 1 ? j + 1 : ny - 1;
+    int kp = k > 0 ? k - 1 : 0, kn = k < nz - 1 ? k + 1 : nz - 1;
+    long long row = (long long) nx * (j + (long long) ny * k);
+    float inv[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) inv[q] = inv_dc9[q];
+    // (float)(a - b) / 2.0 / spacing, evaluated in double as the reference
+    float dxv = (float) ((double) (img[row + in] - img[row + ip]) / 2.0 / (double) sx);
+    float dyv = (float) ((double) (img[nx * (jn + (long long) ny * k) + i]
+        - img[nx * (jp + (long long) ny * k) + i]) / 2.0 / (double) sy);
+    float dzv = (float) ((double) (img[nx * (j + (long long) ny * kn) + i]
+        - img[nx * (j + (long long) ny * kp) + i]) / 2.0 / (double) sz);
+    float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+    o0 = __fadd_rn (o0, __fmul_rn (dxv, inv[0]));
+    o1 = __fadd_rn (o1, __fmul_rn (dxv, inv[3]));
+    o2 = __fadd_rn (o2, __fmul_rn (dxv, inv[6]));
+    o0 = __fadd_rn (o0, __fmul_rn (dyv, inv[1]));
+    o1 = __fadd_rn (o1, __fmul_rn (dyv, inv[4]));
+    o2 = __fadd_rn (o2, __fmul_rn (dyv, inv[7]));
+    o0 = __fadd_rn (o0, __fmul_rn (dzv, inv[2]));
+    o1 = __fadd_rn (o1, __fmul_rn (dzv, inv[5]));
+    o2 = __fadd_rn (o2, __fmul_rn (dzv, inv[8]));
+    out[3 * v + 0] = o0;
+    out[3 * v + 1] = o1;
+    out[3 * v + 2] = o2;
+}
+
+cudaError_t
+launch_volume_grad (const int dim[3], const float spacing[3],
+    const float inv_dc[9], const float* img, float* grad, cudaStream_t st)
+{
+    long long n = (long long) dim[0] * dim[1] * dim[2];
+    int threads = 256;
+    long long blocks = (n + threads - 1) / threads;
+    volume_grad_kernel<<<(unsigned) blocks, threads, 0, st>>> (dim[0], dim[1],
+        dim[2], spacing[0], spacing[1], spacing[2], inv_dc, img, grad);
+    return cudaGetLastError ();
+}
+
+} // namespace b200

@@ -1,0 +1,64 @@
+// Launch wrappers shared between the runtime and the kernel files.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bsp_common.cuh"
+
+namespace b200 {
+
+// Result block written on the device by the final reduction.
+struct DevResult {
+    double score;        // normalised score (double)
+    double raw;          // raw sum (MSE: sum diff^2)
+    long long num_vox;
+    float score_f;       // the float score the reference reports
+    int error;           // non-zero when a bounded wait gave up
+};
+
+// How the per-tile-batch partial gradients are laid out (see gather).
+struct PartLayout {
+    int bx, by, bz;      // tiles per batch along x, y, z
+    int nbx, nby, nbz;   // batches along x, y, z
+    int kx, ky, kz;      // knots per batch footprint = b? + 3
+    int slots;           // 1: footprint layout part[batch][knot][3];
+                         // 64: per-tile slot layout part[slot][tile][3]
+};
+
+cudaError_t launch_mse_fp32 (const BspGeom& g, int grad_mode,
+    const float* fimg, const float* mimg, const float* mgrad,
+    const float* coeff, const float* luts, float* part, double* score_part,
+    int* count_part, cudaStream_t st);
+size_t mse_fp32_smem_bytes (const BspGeom& g);
+
+// Tensor-core form (mse_tc.cu).
+struct TcPlan {
+    int bx;              // tiles per CTA batch along x
+    int nbatches;
+    int n_mma;           // N of the forward MMA = 3 * bx rounded up
+    int mblk;            // 128-row M blocks covering one tile's voxels
+    size_t smem;         // dynamic shared memory per CTA
+    int tmem_cols;
+    int threads;
+    int grid;
+};
+bool tc_plan (const BspGeom& g, TcPlan* plan, int ctas_per_sm, int sm_count);
+int tc_build_tables (const BspGeom& g, const TcPlan& plan, void** d_qlut);
+cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
+    int grad_mode, const float* fimg, const float* mimg, const float* mgrad,
+    const float* coeff, const void* qlut_bf16, float* part,
+    double* score_part, int* count_part, int* err_flag, cudaStream_t st);
+
+cudaError_t launch_reduce_score (const double* score_part,
+    const int* count_part, int n, DevResult* res, int mode,
+    cudaStream_t st);
+cudaError_t launch_gather_grad (const BspGeom& g, const PartLayout& lay,
+    const float* part, const DevResult* res, int mode, float* grad_out,
+    double* grad64_out, float* score_out, double* score64_out,
+    long long* nvox_out, cudaStream_t st);
+cudaError_t launch_volume_grad (const int dim[3], const float spacing[3],
+    const float inv_dc[9], const float* img, float* grad, cudaStream_t st);
+
+} // namespace b200

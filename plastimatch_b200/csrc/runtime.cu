@@ -1,0 +1,796 @@
+// Host runtime of libplastimatch_b200: the C ABI declared in
+// include/plastimatch_b200.h.
+//
+// A context owns every device buffer one registration stage needs
+// (allocated in b200bsp_create / b200bsp_set_images, none afterwards), the
+// geometry in the reference's float arithmetic, and a CUDA stream.  One
+// evaluation is a short fixed sequence of kernel launches on that stream:
+//   [H2D coefficients] -> tile kernel (FP32 or tensor-core form)
+//   -> reduce_score -> gather_grad -> [D2H score + gradient]
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/plastimatch_b200.h"
+#include "kernels.cuh"
+#include "mi.cuh"
+#include "regularize.cuh"
+
+using namespace b200;
+
+static thread_local std::string g_create_error;
+
+struct b200bsp_ctx {
+    int device = 0;
+    b200bsp_opts opts;
+    b200bsp_volume fixed, moving;
+    b200bsp_grid grid;
+    BspGeom geom;
+    int64_t num_coeff = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+
+    float* d_fixed = nullptr;
+    float* d_moving = nullptr;
+    float* d_mgrad = nullptr;
+    float* d_coeff = nullptr;
+    float* d_luts = nullptr;
+    float* d_grad = nullptr;
+    double* d_grad64 = nullptr;
+    float* d_part = nullptr;
+    double* d_score_part = nullptr;
+    int* d_count_part = nullptr;
+    DevResult* d_res = nullptr;
+    int* d_err = nullptr;
+    void* d_qlut = nullptr;
+    float* d_inv_dc = nullptr;
+    DevResult* h_res = nullptr;
+    float* h_scalar = nullptr;
+
+    PartLayout lay;
+    TcPlan plan;
+    int nscore_parts = 0;
+    bool images_set = false;
+
+    MiState mi;
+    RegState reg;
+
+    bool timing = false;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    float last_total_ms = 0.f, last_main_ms = 0.f;
+    int last_launches = 0;
+    std::string err;
+};
+
+// ------------------------------------------------------------------ util --
+
+static int
+fail (b200bsp_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start (ap, fmt);
+    vsnprintf (buf, sizeof buf, fmt, ap);
+    va_end (ap);
+    if (c) c->err = buf; else g_create_error = buf;
+    return code;
+}
+
+#define CK(call)                                                        \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) {                                        \
+            return fail (c, e_ == cudaErrorMemoryAllocation             \
+                ? B200BSP_E_OOM : B200BSP_E_CUDA, "%s: %s", #call,      \
+                cudaGetErrorString (e_));                               \
+        }                                                               \
+    } while (0)
+
+static bool
+is_device_ptr (const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes (&a, p) != cudaSuccess) {
+        cudaGetLastError ();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Cofactor inverse in float (Plastimatch src/base/direction_cosines.cxx:
+// 135-158); the caller rejects |det| < 1e-8 as the reference does.
+static bool
+inv3f (float* out, const float* m)
+{
+    float det = m[0]*(m[4]*m[8]-m[5]*m[7]) - m[1]*(m[3]*m[8]-m[5]*m[6])
+        + m[2]*(m[3]*m[7]-m[4]*m[6]);
+    if (std::fabs (det) < 1e-8) return false;
+    out[0] =  (m[4]*m[8]-m[5]*m[7]) / det;
+    out[1] = -(m[1]*m[8]-m[2]*m[7]) / det;
+    out[2] =  (m[1]*m[5]-m[2]*m[4]) / det;
+    out[3] = -(m[3]*m[8]-m[5]*m[6]) / det;
+    out[4] =  (m[0]*m[8]-m[2]*m[6]) / det;
+    out[5] = -(m[0]*m[5]-m[2]*m[3]) / det;
+    out[6] =  (m[3]*m[7]-m[4]*m[6]) / det;
+    out[7] = -(m[0]*m[7]-m[1]*m[6]) / det;
+    out[8] =  (m[0]*m[4]-m[1]*m[3]) / det;
+    return true;
+}
+
+// Cubic B-spline basis table bx/by/bz_lut[vpr*4] as Bspline_xform::allocate
+// builds it (src/base/bspline_xform.cxx:73-99, 468-482): float argument,
+// double evaluation, rounded to float.
+static void
+basis_lut (float* lut, int vpr)
+{
+    for (int j = 0; j < 4; j++) {
+        for (int v = 0; v < vpr; v++) {
+            float i = (float) v / vpr;
+            double r = 0;
+            switch (j) {
+            case 0: r = (1.0/6.0) * (- 1.0 * i*i*i + 3.0 * i*i - 3.0 * i + 1.0); break;
+            case 1: r = (1.0/6.0) * (+ 3.0 * i*i*i - 6.0 * i*i + 4.0); break;
+            case 2: r = (1.0/6.0) * (- 3.0 * i*i*i + 3.0 * i*i + 3.0 * i + 1.0); break;
+            case 3: r = (1.0/6.0) * (+ 1.0 * i*i*i); break;
+            }
+            lut[v*4+j] = (float) r;
+        }
+    }
+}
+
+// ------------------------------------------------------------- lifecycle --
+
+extern "C" void
+b200bsp_default_opts (b200bsp_opts* o)
+{
+    memset (o, 0, sizeof *o);
+    o->form = B200BSP_FORM_TC;
+    o->mse_grad = B200BSP_MSE_GRAD_NEAREST;
+    o->mi_bins = 32;
+    o->device = 0;
+}
+
+extern "C" const char*
+b200bsp_version (void)
+{
+    return "plastimatch_b200 0.1 (sm_100a)";
+}
+
+static int
+check_volume (const b200bsp_volume* v, const char* what)
+{
+    long long n = 1;
+    for (int d = 0; d < 3; d++) {
+        if (v->dim[d] < 2) {
+            return fail (nullptr, B200BSP_E_BADARG,
+                "%s: dim[%d] = %lld, need >= 2", what, d, (long long) v->dim[d]);
+        }
+        if (!(v->spacing[d] != 0.f) || !std::isfinite (v->spacing[d])) {
+            return fail (nullptr, B200BSP_E_BADARG, "%s: bad spacing", what);
+        }
+        n *= v->dim[d];
+    }
+    if (n >= (1LL << 31)) {
+        return fail (nullptr, B200BSP_E_UNSUPPORTED,
+            "%s: %lld voxels; volumes must have < 2^31 voxels", what, n);
+    }
+    return B200BSP_OK;
+}
+
+static void
+free_all (b200bsp_ctx* c)
+{
+    cudaFree (c->d_fixed); cudaFree (c->d_moving); cudaFree (c->d_mgrad);
+    cudaFree (c->d_coeff); cudaFree (c->d_luts); cudaFree (c->d_grad);
+    cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
+    cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
+    cudaFree (c->d_qlut); cudaFree (c->d_inv_dc);
+    cudaFreeHost (c->h_res); cudaFreeHost (c->h_scalar);
+    mi_free (&c->mi);
+    reg_free (&c->reg);
+    for (auto& e : c->ev) if (e) cudaEventDestroy (e);
+    if (c->own_stream) cudaStreamDestroy (c->own_stream);
+}
+
+extern "C" int
+b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
+    const b200bsp_grid* grid, const b200bsp_opts* opts, b200bsp_ctx** out)
+{
+    b200bsp_ctx* c = nullptr;
+    if (!fixed || !moving || !grid || !out) {
+        return fail (nullptr, B200BSP_E_BADARG, "null argument");
+    }
+    *out = nullptr;
+    int rc = check_volume (fixed, "fixed");
+    if (rc) return rc;
+    rc = check_volume (moving, "moving");
+    if (rc) return rc;
+    b200bsp_opts o;
+    if (opts) o = *opts; else b200bsp_default_opts (&o);
+    if (o.form != B200BSP_FORM_TC && o.form != B200BSP_FORM_FP32) {
+        return fail (nullptr, B200BSP_E_BADARG, "unknown form %d", o.form);
+    }
+    if (o.mse_grad != 0 && o.mse_grad != 1) {
+        return fail (nullptr, B200BSP_E_BADARG, "unknown mse_grad %d", o.mse_grad);
+    }
+    if (o.mi_bins < 2 || o.mi_bins > MI_MAX_BINS) {
+        return fail (nullptr, B200BSP_E_BADARG, "mi_bins must be in [2, %d]",
+            MI_MAX_BINS);
+    }
+    for (int d = 0; d < 3; d++) {
+        if (grid->vox_per_rgn[d] < 1 || grid->vox_per_rgn[d] > 64
+            || grid->roi_dim[d] < 1 || grid->roi_offset[d] < 0
+            || grid->roi_offset[d] + grid->roi_dim[d] > fixed->dim[d]) {
+            return fail (nullptr, B200BSP_E_BADARG,
+                "grid axis %d: need 1 <= vox_per_rgn <= 64 and the ROI "
+                "inside the fixed image", d);
+        }
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount (&ndev) != cudaSuccess || o.device < 0
+        || o.device >= ndev) {
+        cudaGetLastError ();
+        return fail (nullptr, B200BSP_E_CUDA, "no CUDA device %d", o.device);
+    }
+
+    c = new b200bsp_ctx ();
+    c->opts = o;
+    c->fixed = *fixed;
+    c->moving = *moving;
+    c->grid = *grid;
+    c->device = o.device;
+    if (cudaSetDevice (o.device) != cudaSuccess) {
+        delete c;
+        return fail (nullptr, B200BSP_E_CUDA, "cudaSetDevice failed");
+    }
+
+    // Geometry in the reference's float arithmetic.
+    BspGeom& g = c->geom;
+    float finv[9], minv[9];
+    if (!inv3f (finv, fixed->dcos) || !inv3f (minv, moving->dcos)) {
+        delete c;
+        return fail (nullptr, B200BSP_E_BADARG,
+            "singular matrix of direction cosines");
+    }
+    long long ntiles = 1, nknots = 1;
+    for (int d = 0; d < 3; d++) {
+        g.fdim[d] = (int) fixed->dim[d];
+        g.img_origin[d] = fixed->origin[d];
+        g.mdim[d] = (int) moving->dim[d];
+        g.morigin[d] = moving->origin[d];
+        g.minv_spacing[d] = (float) (1.0 / moving->spacing[d]);
+        g.roi_off[d] = (int) grid->roi_offset[d];
+        g.roi_dim[d] = (int) grid->roi_dim[d];
+        g.vpr[d] = (int) grid->vox_per_rgn[d];
+        g.rdims[d] = 1 + (g.roi_dim[d] - 1) / g.vpr[d];
+        g.cdims[d] = g.rdims[d] + 3;
+        ntiles *= g.rdims[d];
+        nknots *= g.cdims[d];
+    }
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            g.fstep[3*i+j] = fixed->dcos[3*i+j] * fixed->spacing[j];
+            g.mproj[3*i+j] = minv[3*i+j] / moving->spacing[i];
+        }
+    }
+    g.ntiles = (int) ntiles;
+    g.nknots = (int) nknots;
+    c->num_coeff = 3 * nknots;
+
+    // Device buffers that do not depend on the form.
+    size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
+    size_t nm = (size_t) g.mdim[0] * g.mdim[1] * g.mdim[2];
+    int rc2 = B200BSP_OK;
+    auto alloc = [&](void** p, size_t bytes) {
+        if (rc2) return;
+        cudaError_t e = cudaMalloc (p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError ();
+            rc2 = fail (c, B200BSP_E_OOM, "cudaMalloc(%zu): %s", bytes,
+                cudaGetErrorString (e));
+        }
+    };
+    alloc ((void**) &c->d_fixed, nf * sizeof (float));
+    alloc ((void**) &c->d_moving, nm * sizeof (float));
+    if (o.mse_grad == 0) alloc ((void**) &c->d_mgrad, 3 * nm * sizeof (float));
+    alloc ((void**) &c->d_coeff, c->num_coeff * sizeof (float));
+    alloc ((void**) &c->d_grad, c->num_coeff * sizeof (float));
+    alloc ((void**) &c->d_grad64, c->num_coeff * sizeof (double));
+    alloc ((void**) &c->d_res, sizeof (DevResult));
+    alloc ((void**) &c->d_err, sizeof (int));
+    alloc ((void**) &c->d_inv_dc, 9 * sizeof (float));
+    int nlut = 4 * (g.vpr[0] + g.vpr[1] + g.vpr[2]);
+    alloc ((void**) &c->d_luts, nlut * sizeof (float));
+    if (!rc2 && (cudaMallocHost ((void**) &c->h_res, sizeof (DevResult)) != cudaSuccess
+        || cudaMallocHost ((void**) &c->h_scalar, 64) != cudaSuccess)) {
+        cudaGetLastError ();
+        rc2 = fail (c, B200BSP_E_OOM, "cudaMallocHost failed");
+    }
+
+    // Tile partial-gradient layout of the chosen form.
+    int sm_count = 148;
+    cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount, o.device);
+    size_t part_elems = 0;
+    if (!rc2 && o.form == B200BSP_FORM_TC) {
+        if (!tc_plan (g, &c->plan, 2, sm_count)) {
+            rc2 = fail (c, B200BSP_E_UNSUPPORTED,
+                "tensor-core form: grid with vox_per_rgn (%d,%d,%d) not "
+                "supported; use B200BSP_FORM_FP32", g.vpr[0], g.vpr[1], g.vpr[2]);
+        } else {
+            PartLayout& L = c->lay;
+            L.bx = c->plan.bx; L.by = 1; L.bz = 1;
+            L.nbx = (g.rdims[0] + L.bx - 1) / L.bx;
+            L.nby = g.rdims[1];
+            L.nbz = g.rdims[2];
+            L.kx = L.bx + 3; L.ky = 4; L.kz = 4;
+            L.slots = 1;
+            part_elems = (size_t) c->plan.nbatches * L.kx * L.ky * L.kz * 3;
+            c->nscore_parts = c->plan.nbatches;
+        }
+    } else if (!rc2) {
+        if (mse_fp32_smem_bytes (g) > 200 * 1024) {
+            rc2 = fail (c, B200BSP_E_UNSUPPORTED, "tile too large");
+        }
+        PartLayout& L = c->lay;
+        L.bx = L.by = L.bz = 1;
+        L.nbx = g.rdims[0]; L.nby = g.rdims[1]; L.nbz = g.rdims[2];
+        L.kx = L.ky = L.kz = 4;
+        L.slots = 64;
+        part_elems = (size_t) 64 * g.ntiles * 3;
+        c->nscore_parts = g.ntiles;
+    }
+    alloc ((void**) &c->d_part, part_elems * sizeof (float));
+    alloc ((void**) &c->d_score_part, (size_t) std::max (c->nscore_parts, 1) * sizeof (double));
+    alloc ((void**) &c->d_count_part, (size_t) std::max (c->nscore_parts, 1) * sizeof (int));
+    if (!rc2 && o.form == B200BSP_FORM_TC) {
+        rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
+        if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
+    }
+    if (!rc2) rc2 = mi_alloc (&c->mi, c->geom, o.mi_bins, c->opts.form, c->plan, c->lay,
+        c->nscore_parts);
+    if (!rc2) rc2 = reg_alloc (&c->reg, c->geom);
+    if (rc2) {
+        g_create_error = c->err;
+        free_all (c);
+        delete c;
+        return rc2;
+    }
+
+    if (cudaStreamCreateWithFlags (&c->own_stream, cudaStreamNonBlocking)
+        != cudaSuccess) {
+        cudaGetLastError ();
+        free_all (c);
+        delete c;
+        return fail (nullptr, B200BSP_E_CUDA, "stream create failed");
+    }
+    c->stream = c->own_stream;
+
+    std::vector<float> luts (nlut);
+    basis_lut (luts.data (), g.vpr[0]);
+    basis_lut (luts.data () + 4 * g.vpr[0], g.vpr[1]);
+    basis_lut (luts.data () + 4 * (g.vpr[0] + g.vpr[1]), g.vpr[2]);
+    cudaMemcpy (c->d_luts, luts.data (), nlut * sizeof (float),
+        cudaMemcpyHostToDevice);
+    cudaMemcpy (c->d_inv_dc, minv, 9 * sizeof (float), cudaMemcpyHostToDevice);
+    cudaMemset (c->d_err, 0, sizeof (int));
+    if (cudaDeviceSynchronize () != cudaSuccess) {
+        std::string e = cudaGetErrorString (cudaGetLastError ());
+        free_all (c);
+        delete c;
+        return fail (nullptr, B200BSP_E_CUDA, "setup: %s", e.c_str ());
+    }
+    *out = c;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_destroy (b200bsp_ctx* c)
+{
+    if (!c) return B200BSP_OK;
+    cudaSetDevice (c->device);
+    if (c->stream) cudaStreamSynchronize (c->stream);
+    free_all (c);
+    delete c;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_grid_info (const b200bsp_ctx* c, int64_t rdims[3], int64_t cdims[3],
+    int64_t* num_coeff)
+{
+    if (!c) return B200BSP_E_BADARG;
+    for (int d = 0; d < 3; d++) {
+        if (rdims) rdims[d] = c->geom.rdims[d];
+        if (cdims) cdims[d] = c->geom.cdims[d];
+    }
+    if (num_coeff) *num_coeff = c->num_coeff;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_set_stream (b200bsp_ctx* c, void* stream)
+{
+    if (!c) return B200BSP_E_BADARG;
+    c->stream = stream ? (cudaStream_t) stream : c->own_stream;
+    return B200BSP_OK;
+}
+
+static cudaMemcpyKind
+kind_to_dev (const void* src)
+{
+    return is_device_ptr (src) ? cudaMemcpyDeviceToDevice
+                               : cudaMemcpyHostToDevice;
+}
+
+extern "C" int
+b200bsp_set_images (b200bsp_ctx* c, const float* fixed_img,
+    const float* moving_img, const float* moving_grad)
+{
+    if (!c || !fixed_img || !moving_img) {
+        return fail (c, B200BSP_E_BADARG, "null image");
+    }
+    CK (cudaSetDevice (c->device));
+    const BspGeom& g = c->geom;
+    size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
+    size_t nm = (size_t) g.mdim[0] * g.mdim[1] * g.mdim[2];
+    CK (cudaMemcpyAsync (c->d_fixed, fixed_img, nf * sizeof (float),
+        kind_to_dev (fixed_img), c->stream));
+    CK (cudaMemcpyAsync (c->d_moving, moving_img, nm * sizeof (float),
+        kind_to_dev (moving_img), c->stream));
+    if (c->opts.mse_grad == 0) {
+        if (moving_grad) {
+            CK (cudaMemcpyAsync (c->d_mgrad, moving_grad, 3 * nm * sizeof (float),
+                kind_to_dev (moving_grad), c->stream));
+        } else {
+            float sp[3] = {c->moving.spacing[0], c->moving.spacing[1],
+                c->moving.spacing[2]};
+            CK (launch_volume_grad (g.mdim, sp, c->d_inv_dc, c->d_moving,
+                c->d_mgrad, c->stream));
+        }
+    }
+    int rc = mi_set_images (&c->mi, g, c->d_fixed, c->d_moving, nf, nm,
+        c->stream);
+    if (rc) return fail (c, rc, "MI histogram setup failed");
+    CK (cudaStreamSynchronize (c->stream));
+    c->images_set = true;
+    return B200BSP_OK;
+}
+
+// ------------------------------------------------------------ evaluation --
+
+struct OutPtrs {
+    bool dev;
+    float* grad;
+    double* grad64;
+    float* score;
+    double* score64;
+    long long* nvox;
+};
+
+static int
+begin_eval (b200bsp_ctx* c, const float* coeff, const float** dcoeff)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (!c->images_set) return fail (c, B200BSP_E_STATE, "images not set");
+    if (!coeff) return fail (c, B200BSP_E_BADARG, "null coefficients");
+    CK (cudaSetDevice (c->device));
+    if (is_device_ptr (coeff)) {
+        *dcoeff = coeff;
+    } else {
+        CK (cudaMemcpyAsync (c->d_coeff, coeff, c->num_coeff * sizeof (float),
+            cudaMemcpyHostToDevice, c->stream));
+        *dcoeff = c->d_coeff;
+    }
+    if (c->timing) {
+        if (!c->ev[0]) {
+            for (auto& e : c->ev) CK (cudaEventCreate (&e));
+        }
+        CK (cudaEventRecord (c->ev[0], c->stream));
+    }
+    c->last_launches = 0;
+    return B200BSP_OK;
+}
+
+static int
+mark_main_done (b200bsp_ctx* c)
+{
+    if (c->timing) CK (cudaEventRecord (c->ev[1], c->stream));
+    return B200BSP_OK;
+}
+
+static int
+end_eval (b200bsp_ctx* c, bool wait)
+{
+    if (c->timing) CK (cudaEventRecord (c->ev[2], c->stream));
+    if (wait) CK (cudaStreamSynchronize (c->stream));
+    if (c->timing && wait) {
+        cudaEventElapsedTime (&c->last_main_ms, c->ev[0], c->ev[1]);
+        cudaEventElapsedTime (&c->last_total_ms, c->ev[0], c->ev[2]);
+    }
+    return B200BSP_OK;
+}
+
+// The MSE tile pass + reductions, results left in d_res and the given
+// gradient outputs (device pointers).
+static int
+run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
+    double* grad64_out, float* score_out, double* score64_out,
+    long long* nvox_out)
+{
+    const BspGeom& g = c->geom;
+    if (c->opts.form == B200BSP_FORM_FP32) {
+        CK (launch_mse_fp32 (g, c->opts.mse_grad, c->d_fixed, c->d_moving,
+            c->d_mgrad, dcoeff, c->d_luts, c->d_part, c->d_score_part,
+            c->d_count_part, c->stream));
+    } else {
+        CK (launch_mse_tc (g, c->plan, c->opts.mse_grad, c->d_fixed,
+            c->d_moving, c->d_mgrad, dcoeff, c->d_qlut, c->d_part,
+            c->d_score_part, c->d_count_part, c->d_err, c->stream));
+    }
+    c->last_launches++;
+    int rc = mark_main_done (c);
+    if (rc) return rc;
+    CK (launch_reduce_score (c->d_score_part, c->d_count_part,
+        c->nscore_parts, c->d_res, 0, c->stream));
+    CK (launch_gather_grad (g, c->lay, c->d_part, c->d_res, 0, grad_out,
+        grad64_out, score_out, score64_out, nvox_out, c->stream));
+    c->last_launches += 2;
+    return B200BSP_OK;
+}
+
+static int
+check_device_error (b200bsp_ctx* c)
+{
+    if (c->opts.form != B200BSP_FORM_TC) return B200BSP_OK;
+    int e = 0;
+    CK (cudaMemcpy (&e, c->d_err, sizeof (int), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset (c->d_err, 0, sizeof (int));
+        return fail (c, B200BSP_E_TIMEOUT,
+            "a bounded device-side wait gave up (code %d)", e);
+    }
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_score_mse (b200bsp_ctx* c, const float* coeff, float* score,
+    float* grad, int64_t* num_vox)
+{
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    bool dev_out = is_device_ptr (grad) && (!score || is_device_ptr (score))
+        && (!num_vox || is_device_ptr (num_vox));
+    if (dev_out && is_device_ptr (coeff)) {
+        rc = run_mse (c, dcoeff, grad, nullptr, score, nullptr,
+            (long long*) num_vox);
+        if (rc) return rc;
+        return end_eval (c, false);
+    }
+    float* g_dev = is_device_ptr (grad) ? grad : c->d_grad;
+    rc = run_mse (c, dcoeff, g_dev, nullptr, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
+        cudaMemcpyDeviceToHost, c->stream));
+    if (grad && g_dev == c->d_grad) {
+        CK (cudaMemcpyAsync (grad, c->d_grad, c->num_coeff * sizeof (float),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    rc = end_eval (c, true);
+    if (rc) return rc;
+    if (score) *score = c->h_res->score_f;
+    if (num_vox) *num_vox = c->h_res->num_vox;
+    return check_device_error (c);
+}
+
+extern "C" int
+b200bsp_score_mse_f64 (b200bsp_ctx* c, const float* coeff, double* score,
+    double* grad, int64_t* num_vox)
+{
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    rc = run_mse (c, dcoeff, nullptr, c->d_grad64, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
+        cudaMemcpyDeviceToHost, c->stream));
+    if (grad) {
+        CK (cudaMemcpyAsync (grad, c->d_grad64, c->num_coeff * sizeof (double),
+            is_device_ptr (grad) ? cudaMemcpyDeviceToDevice
+                                 : cudaMemcpyDeviceToHost, c->stream));
+    }
+    rc = end_eval (c, true);
+    if (rc) return rc;
+    if (score) *score = c->h_res->score;
+    if (num_vox) *num_vox = c->h_res->num_vox;
+    return check_device_error (c);
+}
+
+extern "C" int
+b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
+    float* grad, int64_t* num_vox, double* f_hist, double* m_hist,
+    double* j_hist)
+{
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    float* g_dev = is_device_ptr (grad) ? grad : c->d_grad;
+    rc = mi_run (&c->mi, c->geom, c->opts.form, c->plan, c->lay, c->d_fixed,
+        c->d_moving, dcoeff, c->d_luts, c->d_qlut, c->d_part, c->d_score_part,
+        c->d_count_part, c->d_err, g_dev, nullptr, c->stream, &c->last_launches);
+    if (rc) return fail (c, rc, "MI evaluation failed: %s",
+        cudaGetErrorString (cudaGetLastError ()));
+    mark_main_done (c);
+    MiResult mr;
+    rc = mi_fetch (&c->mi, &mr, f_hist, m_hist, j_hist, c->stream);
+    if (rc) return fail (c, rc, "MI fetch failed");
+    if (grad && g_dev == c->d_grad) {
+        CK (cudaMemcpyAsync (grad, c->d_grad, c->num_coeff * sizeof (float),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    rc = end_eval (c, true);
+    if (rc) return rc;
+    mi_finish (&c->mi, &mr);
+    if (score) *score = mr.score_f;
+    if (num_vox) *num_vox = mr.num_vox;
+    return check_device_error (c);
+}
+
+extern "C" int
+b200bsp_regularize (b200bsp_ctx* c, const float* coeff,
+    const b200bsp_reg_parms* parms, float* rmetric, float* grad)
+{
+    if (!parms) return fail (c, B200BSP_E_BADARG, "null parms");
+    const float* dcoeff = nullptr;
+    if (!c) return B200BSP_E_BADARG;
+    CK (cudaSetDevice (c->device));
+    if (!coeff) return fail (c, B200BSP_E_BADARG, "null coefficients");
+    if (is_device_ptr (coeff)) {
+        dcoeff = coeff;
+    } else {
+        CK (cudaMemcpyAsync (c->d_coeff, coeff, c->num_coeff * sizeof (float),
+            cudaMemcpyHostToDevice, c->stream));
+        dcoeff = c->d_coeff;
+    }
+    bool dev_grad = is_device_ptr (grad);
+    if (grad && !dev_grad) {
+        CK (cudaMemcpyAsync (c->d_grad, grad, c->num_coeff * sizeof (float),
+            cudaMemcpyHostToDevice, c->stream));
+    }
+    float* g_dev = grad ? (dev_grad ? grad : c->d_grad) : nullptr;
+    int rc = reg_run (&c->reg, c->geom, parms, dcoeff, g_dev, c->stream);
+    if (rc) return fail (c, rc, "regulariser failed: %s",
+        cudaGetErrorString (cudaGetLastError ()));
+    if (grad && !dev_grad) {
+        CK (cudaMemcpyAsync (grad, c->d_grad, c->num_coeff * sizeof (float),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    double S = 0;
+    rc = reg_fetch (&c->reg, &S, c->stream);
+    if (rc) return fail (c, rc, "regulariser fetch failed");
+    if (rmetric) *rmetric = (float) S;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_score (b200bsp_ctx* c, const float* coeff, int metric_type,
+    float lambda, const b200bsp_reg_parms* reg, float* total_score,
+    float* total_grad, float* smetric, int64_t* num_vox)
+{
+    if (!c || !total_grad) return fail (c, B200BSP_E_BADARG, "null argument");
+    std::vector<float> g ((size_t) c->num_coeff);
+    float s = 0.f;
+    int64_t nv = 0;
+    int rc = metric_type == 0
+        ? b200bsp_score_mse (c, coeff, &s, g.data (), &nv)
+        : b200bsp_score_mi (c, coeff, &s, g.data (), &nv, nullptr, nullptr,
+            nullptr);
+    if (rc) return rc;
+    // Bspline_score::accumulate (src/register/bspline_score.cxx:63-74)
+    float total = 0.f;
+    total += lambda * s;
+    for (int64_t i = 0; i < c->num_coeff; i++) g[i] = 0.f + lambda * g[i];
+    if (reg) {
+        float r = 0.f;
+        rc = b200bsp_regularize (c, coeff, reg, &r, g.data ());
+        if (rc) return rc;
+        total += r;
+    }
+    if (is_device_ptr (total_grad)) {
+        CK (cudaMemcpy (total_grad, g.data (), c->num_coeff * sizeof (float),
+            cudaMemcpyHostToDevice));
+    } else {
+        memcpy (total_grad, g.data (), c->num_coeff * sizeof (float));
+    }
+    if (total_score) *total_score = total;
+    if (smetric) *smetric = s;
+    if (num_vox) *num_vox = nv;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_interpolate_vf (b200bsp_ctx* c, const float* coeff, float* vf)
+{
+    if (!c) return B200BSP_E_BADARG;
+    return fail (c, B200BSP_E_UNSUPPORTED, "interpolate_vf not built yet");
+}
+
+extern "C" int
+b200bsp_warp (b200bsp_ctx* c, const float* coeff, float default_value,
+    float* warped)
+{
+    if (!c) return B200BSP_E_BADARG;
+    return fail (c, B200BSP_E_UNSUPPORTED, "warp not built yet");
+}
+
+extern "C" int
+b200bsp_volume_grad (const b200bsp_volume* vol, const float* img,
+    float* grad_out, int device)
+{
+    b200bsp_ctx* c = nullptr;
+    if (!vol || !img || !grad_out) return fail (c, B200BSP_E_BADARG, "null argument");
+    int rc = check_volume (vol, "volume");
+    if (rc) return rc;
+    float inv[9];
+    if (!inv3f (inv, vol->dcos)) {
+        return fail (c, B200BSP_E_BADARG, "singular direction cosines");
+    }
+    CK (cudaSetDevice (device));
+    int dim[3] = {(int) vol->dim[0], (int) vol->dim[1], (int) vol->dim[2]};
+    size_t n = (size_t) dim[0] * dim[1] * dim[2];
+    float *d_img = nullptr, *d_grad = nullptr, *d_inv = nullptr;
+    bool in_dev = is_device_ptr (img), out_dev = is_device_ptr (grad_out);
+    if (!in_dev) CK (cudaMalloc (&d_img, n * sizeof (float)));
+    if (!out_dev) CK (cudaMalloc (&d_grad, 3 * n * sizeof (float)));
+    CK (cudaMalloc (&d_inv, 9 * sizeof (float)));
+    if (!in_dev) CK (cudaMemcpy (d_img, img, n * sizeof (float), cudaMemcpyHostToDevice));
+    CK (cudaMemcpy (d_inv, inv, 9 * sizeof (float), cudaMemcpyHostToDevice));
+    float sp[3] = {vol->spacing[0], vol->spacing[1], vol->spacing[2]};
+    CK (launch_volume_grad (dim, sp, d_inv, in_dev ? img : d_img,
+        out_dev ? grad_out : d_grad, 0));
+    CK (cudaDeviceSynchronize ());
+    if (!out_dev) CK (cudaMemcpy (grad_out, d_grad, 3 * n * sizeof (float),
+        cudaMemcpyDeviceToHost));
+    cudaFree (d_img); cudaFree (d_grad); cudaFree (d_inv);
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_enable_timing (b200bsp_ctx* c, int on)
+{
+    if (!c) return B200BSP_E_BADARG;
+    c->timing = on != 0;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_last_timing (const b200bsp_ctx* c, float* ms, int* launches)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (ms) *ms = c->last_total_ms;
+    if (launches) *launches = c->last_launches;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_last_main_ms (const b200bsp_ctx* c, float* ms)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (ms) *ms = c->last_main_ms;
+    return B200BSP_OK;
+}
+
+extern "C" const char*
+b200bsp_last_error (const b200bsp_ctx* c)
+{
+    return c ? c->err.c_str () : g_create_error.c_str ();
+}

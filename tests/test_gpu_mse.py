@@ -1,0 +1,118 @@
+"""MSE score + gradient on the GPU against the oracle.
+
+Tolerances (float work, stated here as the bar):
+  score     relative 1e-5 against the double-precision oracle
+  gradient  relative 1e-3 (L2 norm of the difference over the norm of the
+            reference) against both the double oracle and the reference's
+            float flavour g / o
+  num_vox   within 0.01% (+2): a voxel whose moving position lies within
+            float rounding of a cell edge or of the inside bound may land
+            on the other side.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import plastimatch_b200 as P
+from conftest import golden_names, load_golden, rel_err
+from plastimatch_b200 import synth
+from plastimatch_b200.geometry import BsplineGrid, Volume
+
+pytestmark = pytest.mark.gpu
+
+FORMS = ["fp32", "tc"]
+
+
+def check(score, grad, nvox, f64, ref32, nv_ref):
+    assert abs(nvox - nv_ref) <= 1e-4 * nv_ref + 2, (nvox, nv_ref)
+    assert abs(score - f64.score) <= 1e-5 * abs(f64.score), (score, f64.score)
+    assert rel_err(grad, f64.grad) < 1e-3, rel_err(grad, f64.grad)
+    assert rel_err(grad, ref32) < 1e-3, rel_err(grad, ref32)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("name", golden_names("mse"))
+def test_mse_golden(form, name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images(moving_grad=rec["moving_grad"])
+        s, g, n = ctx.score_mse(coeff)
+    f64 = O.port_mse(grid, fixed, moving, coeff, moving_grad=rec["moving_grad"],
+                     precision="f64")
+    check(s, g, n, f64, rec["g_grad"], int(rec["g_num_vox"]))
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("name", [n for n in golden_names("mse") if n != "mse_roi"])
+def test_mse_trilinear_gradient_golden(form, name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    with P.Context(fixed, moving, grid, form=form, mse_grad="trilinear") as ctx:
+        ctx.set_images()
+        s, g, n = ctx.score_mse(coeff)
+    f64 = O.port_mse(grid, fixed, moving, coeff, grad_mode=1, precision="f64")
+    check(s, g, n, f64, rec["o_grad"], int(rec["o_num_vox"]))
+
+
+def test_device_moving_gradient_matches_reference():
+    for name in golden_names("mse"):
+        _, moving, _, _, rec = load_golden(name)
+        np.testing.assert_array_equal(P.volume_grad(moving), rec["moving_grad"])
+
+
+def _c1_case(seed=20261204):
+    fixed = synth.gaussian_blobs((64, 64, 64), spacing=(1, 1, 1), seed=seed)
+    g0 = BsplineGrid.for_volume(fixed, 8)
+    moving = synth.warp_trilinear(fixed, fixed, g0, synth.random_coeff(g0, 2.0, seed + 1))
+    grid = BsplineGrid.for_volume(fixed, 8)
+    coeff = synth.random_coeff(grid, 1.0, seed + 2)
+    return fixed, moving, grid, coeff
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_mse_64cubed_vpr8(form):
+    fixed, moving, grid, coeff = _c1_case()
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images()
+        s, g, n = ctx.score_mse(coeff)
+        s2, g2, n2 = ctx.score_mse(coeff)
+    mg = O.port_volume_grad(moving)
+    f64 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg, precision="f64")
+    r32 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg)
+    check(s, g, n, f64, r32.grad, r32.num_vox)
+    # deterministic: fixed reduction order, no float atomics
+    assert s == s2 and n == n2
+    np.testing.assert_array_equal(g, g2)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_mse_zero_coefficients_and_no_overlap(form):
+    fixed, moving, grid, _ = _c1_case(seed=7)
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images()
+        z = np.zeros(grid.num_coeff, np.float32)
+        s, g, n = ctx.score_mse(z)
+        assert n == fixed.npix
+        # push every voxel outside the moving image: reference returns
+        # FLT_MAX and a zero gradient
+        far = np.full(grid.num_coeff, 1e4, np.float32)
+        s, g, n = ctx.score_mse(far)
+        assert n == 0 and s == np.finfo(np.float32).max
+        assert not g.any()
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_mse_device_pointers_are_stream_ordered(form):
+    torch = pytest.importorskip("torch")
+    fixed, moving, grid, coeff = _c1_case(seed=11)
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        ctx.set_images()
+        s_h, g_h, n_h = ctx.score_mse(coeff)
+        dc = torch.from_numpy(coeff).cuda()
+        gd = torch.zeros(grid.num_coeff, device="cuda")
+        sd = torch.zeros(1, device="cuda")
+        nd = torch.zeros(1, dtype=torch.int64, device="cuda")
+        ctx.score_mse(dc, grad_out=gd, score_out=sd, nvox_out=nd)
+        torch.cuda.synchronize()
+        assert float(sd.item()) == s_h and int(nd.item()) == n_h
+        np.testing.assert_array_equal(gd.cpu().numpy(), g_h)
