@@ -1,10 +1,475 @@
+// Tensor-core (tcgen05) form of the MSE score + gradient.
+//
+// The B-spline field at the voxels of one tile is a contraction with a
+// table shared by every tile: d(v) = sum_m Q[v][m] * C_tile[m], m over the
+// tile's 64 knots, Q[v][m] = bx[lx][i] * by[ly][j] * bz[lz][k] (the
+// reference's bspline_interp_pix_c weights, src/base/bspline_interpolate.cxx:
+// 78-110).  A batch of T tiles along x turns this into one GEMM
+//     D[voxel][(c,t)] = Q[voxel][m] * C[(c,t)][m]
+// and the adjoint condense (bspline_update_sets_b, src/register/bspline.cxx:
+// 347-374) into another:
+//     G[(c,t)][m] = sum_voxel DCDV[(c,t)][voxel] * Q[voxel][m].
+// Both run on the tensor cores (kind::f16, bf16 operands, f32 accumulation
+// in TMEM).  Every bf16 operand is split x = hi + lo (two bf16), and each
+// product takes the three terms hi*hi + hi*lo + lo*hi, which keeps ~16
+// significant bits -- the error budget of the gradient (1e-3) is met with
+// margin while the voxel arithmetic (positions, trilinear samples,
+// differences) stays in f32 on the CUDA cores.
+//
+// One CTA per SM loops over batches.  Per batch:
+//   1. stage the (T+3) x 4 x 4 knot block, build C (hi/lo, 128B-swizzled)
+//   2. per 128-voxel M block: forward MMA -> D in TMEM; the voxel phase
+//      reads D, samples the moving image and writes dc/dv (hi/lo) into the
+//      adjoint operand; adjoint MMA accumulates G in TMEM
+//   3. G -> per-knot partial sums in shared memory (fixed order) -> global
+// The partial sums are combined per knot by gather_grad (deterministic).
+#include <algorithm>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "bsp_common.cuh"
 #include "kernels.cuh"
+#include "tc_ptx.cuh"
 #include "../../include/plastimatch_b200.h"
 
 namespace b200 {
-bool tc_plan (const BspGeom&, TcPlan*, int, int) { return false; }
-int tc_build_tables (const BspGeom&, const TcPlan&, void**) { return B200BSP_E_UNSUPPORTED; }
-cudaError_t launch_mse_tc (const BspGeom&, const TcPlan&, int, const float*,
-    const float*, const float*, const float*, const void*, float*, double*,
-    int*, int*, cudaStream_t) { return cudaErrorNotSupported; }
+
+constexpr int TC_THREADS = 512;
+constexpr int TC_TMAX = 32;          // tiles per batch at most
+constexpr int TC_TMEM_COLS = 256;
+constexpr int TC_D_COL = 0;          // forward accumulator [0, N)
+constexpr int TC_G_COL = 128;        // adjoint accumulator [128, 192)
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;
+
+// Shared-memory map (offsets from a 1024-byte aligned base).
+constexpr int SM_Q = 0;                           // Q hi 16 KB, lo 16 KB
+constexpr int SM_C = 32768;                       // C hi, lo: N*128 B each
+constexpr int SM_C_BYTES = 2 * 96 * 128;          // N <= 96
+constexpr int SM_DC = SM_C + SM_C_BYTES;          // DCDV hi, lo: 32 KB each
+constexpr int SM_S = SM_DC + 65536;               // knot block (float)
+constexpr int SM_KB_FLOATS = 3 * 16 * (TC_TMAX + 3);
+constexpr int SM_P = SM_S + SM_KB_FLOATS * 4;     // knot partials (float)
+constexpr int SM_TOTAL = SM_P + SM_KB_FLOATS * 4;
+
+struct TcArgs {
+    BspGeom g;
+    int T, N, mblk, V, nbx, nbatches;
+    const float* fimg;
+    const float* mimg;
+    const float* mgrad;
+    const float* coeff;
+    const uint4* qimg;
+    float* part;
+    double* score_part;
+    int* count_part;
+    int* err;
+};
+
+__device__ __forceinline__ void
+split_bf16 (float x, unsigned short& hi, unsigned short& lo)
+{
+    __nv_bfloat16 h = __float2bfloat16_rn (x);
+    __nv_bfloat16 l = __float2bfloat16_rn (x - __bfloat162float (h));
+    hi = __bfloat16_as_ushort (h);
+    lo = __bfloat16_as_ushort (l);
 }
+
+template <int GRAD_MODE>
+__global__ void __launch_bounds__ (TC_THREADS, 1)
+mse_tc_kernel (TcArgs a)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint64_t s_bar[2];
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_abort;
+    __shared__ double sh_v[TC_THREADS / 32];
+    __shared__ int sh_n[TC_THREADS / 32];
+
+    const BspGeom& g = a.g;
+    uint8_t* sm = (uint8_t*) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    const uint32_t sm_base = smem_addr (sm);
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int T = a.T, N = a.N, KX = T + 3;
+    float* S = (float*) (sm + SM_S);
+    float* P = (float*) (sm + SM_P);
+
+    if (tid == 0) {
+        mbar_init (&s_bar[0], 1);
+        mbar_init (&s_bar[1], 1);
+        fence_barrier_init ();
+        s_abort = 0;
+    }
+    if (warp == 0) {
+        tmem_alloc (&s_taddr, TC_TMEM_COLS);
+        tmem_relinquish ();
+    }
+    // Zero the adjoint operand once: rows (c, t >= T) and padding voxels
+    // that the voxel phase never writes must stay zero.
+    for (int o = tid; o < 65536 / 16; o += TC_THREADS) {
+        ((uint4*) (sm + SM_DC))[o] = make_uint4 (0, 0, 0, 0);
+    }
+    tc_fence_before ();
+    __syncthreads ();
+    tc_fence_after ();
+    const uint32_t taddr = s_taddr;
+    uint32_t ph0 = 0, ph1 = 0;
+
+    const uint32_t idesc_fwd = idesc_bf16_f32 (128, N, 0, 0);
+    const uint32_t idesc_adj = idesc_bf16_f32 (128, 64, 0, 1);
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
+    const int q = warp & 3;            // TMEM lane quarter
+    const int tg = warp >> 2;          // tile group (8 tiles)
+    const int t_begin = tg * 8;
+    const int t_end = min (T, t_begin + 8);
+
+    double sc = 0.0;
+    int cnt = 0;
+
+    if (a.mblk == 1) {
+        for (int o = tid; o < 2048; o += TC_THREADS) {
+            ((uint4*) (sm + SM_Q))[o] = a.qimg[o];
+        }
+    }
+
+    for (int b = blockIdx.x; b < a.nbatches; b += gridDim.x) {
+        const int bxi = b % a.nbx;
+        const int ty = (b / a.nbx) % g.rdims[1];
+        const int tz = b / (a.nbx * g.rdims[1]);
+        const int tx0 = bxi * T;
+
+        // 1. knot block S[c][k][j][x] and zeroed partials P
+        for (int o = tid; o < 3 * 16 * KX; o += TC_THREADS) {
+            int x = o % KX, jk = o / KX;        // jk = j + 4k
+            int j = jk & 3, k = jk >> 2;
+            int kx = tx0 + x;
+            float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+            if (o < 16 * KX && kx < g.cdims[0]) {
+                int knot = (tz + k) * g.cdims[1] * g.cdims[0]
+                    + (ty + j) * g.cdims[0] + kx;
+                v0 = __ldg (a.coeff + 3 * knot + 0);
+                v1 = __ldg (a.coeff + 3 * knot + 1);
+                v2 = __ldg (a.coeff + 3 * knot + 2);
+            }
+            if (o < 16 * KX) {
+                S[(0 * 16 + jk) * KX + x] = v0;
+                S[(1 * 16 + jk) * KX + x] = v1;
+                S[(2 * 16 + jk) * KX + x] = v2;
+            }
+            P[o] = 0.f;
+        }
+        __syncthreads ();
+
+        // C[(c,t)][m] for the forward B operand: row n = c*T + t, K = 64 slots
+        for (int o = tid; o < N * 8; o += TC_THREADS) {
+            int n = o >> 3, ch = o & 7;          // 16-byte chunk: slots 8ch..8ch+7
+            int c = n / T, t = n - c * T;
+            unsigned short hi[8], lo[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                int m = 8 * ch + e;
+                int i = m & 3, j = (m >> 2) & 3, k = m >> 4;
+                float v = (c < 3) ? S[(c * 16 + j + 4 * k) * KX + t + i] : 0.f;
+                split_bf16 (v, hi[e], lo[e]);
+            }
+            uint32_t off = sw128_offset (n, 8 * ch, N);
+            uint4 h4 = make_uint4 (hi[0] | (hi[1] << 16), hi[2] | (hi[3] << 16),
+                hi[4] | (hi[5] << 16), hi[6] | (hi[7] << 16));
+            uint4 l4 = make_uint4 (lo[0] | (lo[1] << 16), lo[2] | (lo[3] << 16),
+                lo[4] | (lo[5] << 16), lo[6] | (lo[7] << 16));
+            *(uint4*) (sm + SM_C + off) = h4;
+            *(uint4*) (sm + SM_C + N * 128 + off) = l4;
+        }
+
+        for (int mb = 0; mb < a.mblk; mb++) {
+            if (a.mblk > 1) {
+                const uint4* src = a.qimg + (size_t) mb * 2048;
+                for (int o = tid; o < 2048; o += TC_THREADS) {
+                    ((uint4*) (sm + SM_Q))[o] = src[o];
+                }
+            }
+            fence_proxy_async_smem ();
+            __syncthreads ();
+
+            // 2a. forward: D = Q * C^T (three split terms, K = 64)
+            if (tid == 0) {
+                tc_fence_after ();
+                const uint32_t qa[2] = {sm_base + SM_Q, sm_base + SM_Q + 16384};
+                const uint32_t cb[2] = {sm_base + SM_C, sm_base + SM_C + (uint32_t) N * 128};
+                const int ta[3] = {0, 0, 1}, tb[3] = {0, 1, 0};
+                uint32_t acc = 0;
+                for (int term = 0; term < 3; term++) {
+                    for (int ks = 0; ks < 4; ks++) {
+                        uint64_t ad = smem_desc_sw128 (qa[ta[term]] + ks * 32, 16, 1024);
+                        uint64_t bd = smem_desc_sw128 (cb[tb[term]] + ks * 32, 16, 1024);
+                        tc_mma_bf16 (taddr + TC_D_COL, ad, bd, idesc_fwd, acc);
+                        acc = 1;
+                    }
+                }
+                tc_commit (&s_bar[0]);
+                if (!mbar_wait_bounded (&s_bar[0], ph0, TC_WAIT_LIMIT)) {
+                    s_abort = 1;
+                    atomicExch (a.err, 1);
+                }
+                ph0 ^= 1;
+            }
+            __syncthreads ();
+            if (s_abort) goto done;
+            tc_fence_after ();
+
+            // 2b. voxel phase: thread = (voxel 32q+lane of this M block,
+            // tiles [t_begin, t_end))
+            if (t_begin < T) {
+                const int vl = 32 * q + lane;
+                const int v = 128 * mb + vl;
+                const bool vok = v < a.V;
+                const int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
+                float dv[24];
+                const uint32_t lane_base = (uint32_t) (32 * q) << 16;
+                tmem_ld8x3_wait (taddr + lane_base + TC_D_COL + 0 * T + t_begin,
+                    taddr + lane_base + TC_D_COL + 1 * T + t_begin,
+                    taddr + lane_base + TC_D_COL + 2 * T + t_begin, dv);
+                const int fj = g.roi_off[1] + vy * ty + ly;
+                const int fk = g.roi_off[2] + vz * tz + lz;
+                const bool yz_ok = vok && fj < g.roi_off[1] + g.roi_dim[1]
+                    && fk < g.roi_off[2] + g.roi_dim[2];
+#pragma unroll 2
+                for (int tt = 0; tt < 8; tt++) {
+                    const int t = t_begin + tt;
+                    if (t >= t_end) break;
+                    const int tx = tx0 + t;
+                    const int fi = g.roi_off[0] + vx * tx + lx;
+                    float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
+                    if (yz_ok && tx < g.rdims[0]
+                        && fi < g.roi_off[0] + g.roi_dim[0]) {
+                        float fxyz[3], d[3] = {dv[tt], dv[8 + tt], dv[16 + tt]};
+                        fixed_position (g, fi, fj, fk, fxyz);
+                        Sample s;
+                        if (locate (g, fxyz, d, s)) {
+                            Corners cr = load_corners (a.mimg, s.mvf, dxm, dxym);
+                            float mval = trilinear (s, cr);
+                            int fidx = fi + g.fdim[0] * (fj + g.fdim[1] * fk);
+                            float diff = mval - __ldg (a.fimg + fidx);
+                            sc += (double) (diff * diff);
+                            cnt++;
+                            if (GRAD_MODE == 0) {
+                                dc0 = diff * __ldg (a.mgrad + 3 * s.mvr + 0);
+                                dc1 = diff * __ldg (a.mgrad + 3 * s.mvr + 1);
+                                dc2 = diff * __ldg (a.mgrad + 3 * s.mvr + 2);
+                            } else {
+                                float gr[3];
+                                trilinear_grad (g, s, cr, gr);
+                                dc0 = diff * gr[0];
+                                dc1 = diff * gr[1];
+                                dc2 = diff * gr[2];
+                            }
+                        }
+                    }
+                    unsigned short h, l;
+                    uint8_t* dch = sm + SM_DC;
+                    uint8_t* dcl = sm + SM_DC + 32768;
+                    uint32_t o0 = sw128_offset (0 * 32 + t, vl, 128);
+                    uint32_t o1 = sw128_offset (1 * 32 + t, vl, 128);
+                    uint32_t o2 = sw128_offset (2 * 32 + t, vl, 128);
+                    split_bf16 (dc0, h, l);
+                    *(unsigned short*) (dch + o0) = h;
+                    *(unsigned short*) (dcl + o0) = l;
+                    split_bf16 (dc1, h, l);
+                    *(unsigned short*) (dch + o1) = h;
+                    *(unsigned short*) (dcl + o1) = l;
+                    split_bf16 (dc2, h, l);
+                    *(unsigned short*) (dch + o2) = h;
+                    *(unsigned short*) (dcl + o2) = l;
+                }
+            }
+            tc_fence_before ();
+            fence_proxy_async_smem ();
+            __syncthreads ();
+
+            // 2c. adjoint: G += DCDV * Q (K = 128 voxels of this block)
+            if (tid == 0) {
+                tc_fence_after ();
+                const uint32_t da[2] = {sm_base + SM_DC, sm_base + SM_DC + 32768};
+                const uint32_t qb[2] = {sm_base + SM_Q, sm_base + SM_Q + 16384};
+                const int ta[3] = {0, 1, 0}, tb[3] = {0, 0, 1};
+                for (int term = 0; term < 3; term++) {
+                    for (int s = 0; s < 8; s++) {
+                        uint64_t ad = smem_desc_sw128 (
+                            da[ta[term]] + (s >> 2) * 16384 + (s & 3) * 32, 16, 1024);
+                        uint64_t bd = smem_desc_sw128 (qb[tb[term]] + s * 2048,
+                            16384, 1024);
+                        uint32_t acc = (mb > 0 || term > 0 || s > 0) ? 1u : 0u;
+                        tc_mma_bf16 (taddr + TC_G_COL, ad, bd, idesc_adj, acc);
+                    }
+                }
+                tc_commit (&s_bar[1]);
+                if (!mbar_wait_bounded (&s_bar[1], ph1, TC_WAIT_LIMIT)) {
+                    s_abort = 1;
+                    atomicExch (a.err, 2);
+                }
+                ph1 ^= 1;
+            }
+            __syncthreads ();
+            if (s_abort) goto done;
+            tc_fence_after ();
+        }
+
+        // 3. G rows (c, t) = 32c + t, columns = 64 slots; warps of quarter
+        // q = c read slots [16 tg, 16 tg + 16) (k = tg) and add them to the
+        // knots (t + i, j, k) in slot order.
+        if (q < 3) {
+            float gv[16];
+            tmem_ld16_wait (taddr + ((uint32_t) (32 * q) << 16) + TC_G_COL + 16 * tg,
+                gv);
+            // lanes t and t+1 touch the same knot in consecutive i steps:
+            // __syncwarp keeps each (j, i) step complete before the next
+            const int t = lane;
+            const bool tv = t < T;
+            float* Pc = P + ((q * 4 + tg) * 4) * KX;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (tv) Pc[j * KX + t + i] += gv[4 * j + i];
+                    __syncwarp ();
+                }
+            }
+        }
+        tc_fence_before ();
+        __syncthreads ();
+        {
+            const int KF = 16 * KX;
+            float* dst = a.part + (size_t) b * KF * 3;
+            for (int o = tid; o < KF * 3; o += TC_THREADS) {
+                int kk = o / 3, c = o - 3 * kk;      // kk = x + KX (j + 4k)
+                dst[o] = P[(c * 16) * KX + kk];
+            }
+        }
+        block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
+        if (tid == 0) {
+            a.score_part[b] = sc;
+            a.count_part[b] = cnt;
+        }
+        sc = 0.0;
+        cnt = 0;
+        __syncthreads ();
+    }
+
+done:
+    tc_fence_before ();
+    __syncthreads ();
+    if (warp == 0) {
+        tmem_dealloc (taddr, TC_TMEM_COLS);
+    }
+}
+
+bool
+tc_plan (const BspGeom& g, TcPlan* p, int ctas_per_sm, int sm_count)
+{
+    int V = g.vpr[0] * g.vpr[1] * g.vpr[2];
+    int mblk = (V + 127) / 128;
+    if (mblk > 4) return false;
+    int nb_row = (g.rdims[0] + TC_TMAX - 1) / TC_TMAX;
+    int T = (g.rdims[0] + nb_row - 1) / nb_row;      // balanced batches
+    p->bx = T;
+    p->mblk = mblk;
+    p->n_mma = ((3 * T + 15) / 16) * 16;
+    p->nbatches = nb_row * g.rdims[1] * g.rdims[2];
+    p->smem = SM_TOTAL + 1024;
+    p->tmem_cols = TC_TMEM_COLS;
+    p->threads = TC_THREADS;
+    p->grid = std::min (p->nbatches, sm_count);
+    (void) ctas_per_sm;
+    return true;
+}
+
+// Q image in global memory: per M block, hi then lo, each the exact
+// 128-row x 64-slot 128B-swizzled shared-memory image (16 KB).
+int
+tc_build_tables (const BspGeom& g, const TcPlan& p, void** d_qlut)
+{
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int V = vx * vy * vz;
+    std::vector<float> lut[3];
+    for (int d = 0; d < 3; d++) {
+        int n = g.vpr[d];
+        lut[d].resize (4 * n);
+        for (int j = 0; j < 4; j++) {
+            for (int v = 0; v < n; v++) {
+                float i = (float) v / n;
+                double r = 0;
+                switch (j) {
+                case 0: r = (1.0/6.0) * (- 1.0 * i*i*i + 3.0 * i*i - 3.0 * i + 1.0); break;
+                case 1: r = (1.0/6.0) * (+ 3.0 * i*i*i - 6.0 * i*i + 4.0); break;
+                case 2: r = (1.0/6.0) * (- 3.0 * i*i*i + 3.0 * i*i + 3.0 * i + 1.0); break;
+                case 3: r = (1.0/6.0) * (+ 1.0 * i*i*i); break;
+                }
+                lut[d][v * 4 + j] = (float) r;
+            }
+        }
+    }
+    size_t bytes = (size_t) p.mblk * 32768;
+    std::vector<uint8_t> img (bytes, 0);
+    for (int v = 0; v < p.mblk * 128; v++) {
+        int mb = v / 128, vl = v % 128;
+        uint8_t* hi = img.data () + (size_t) mb * 32768;
+        uint8_t* lo = hi + 16384;
+        for (int m = 0; m < 64; m++) {
+            float qv = 0.f;
+            if (v < V) {
+                int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
+                int i = m & 3, j = (m >> 2) & 3, k = m >> 4;
+                float C = lut[2][lz * 4 + k];
+                float B = lut[1][ly * 4 + j] * C;
+                qv = lut[0][lx * 4 + i] * B;
+            }
+            __nv_bfloat16 h = __float2bfloat16_rn (qv);
+            __nv_bfloat16 l = __float2bfloat16_rn (qv - __bfloat162float (h));
+            uint32_t off = sw128_offset (vl, m, 128);
+            *(unsigned short*) (hi + off) = __bfloat16_as_ushort (h);
+            *(unsigned short*) (lo + off) = __bfloat16_as_ushort (l);
+        }
+    }
+    if (cudaMalloc (d_qlut, bytes) != cudaSuccess) return B200BSP_E_OOM;
+    if (cudaMemcpy (*d_qlut, img.data (), bytes, cudaMemcpyHostToDevice)
+        != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    return B200BSP_OK;
+}
+
+cudaError_t
+launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
+    const float* fimg, const float* mimg, const float* mgrad,
+    const float* coeff, const void* qimg, float* part, double* score_part,
+    int* count_part, int* err, cudaStream_t st)
+{
+    TcArgs a;
+    a.g = g;
+    a.T = p.bx;
+    a.N = p.n_mma;
+    a.mblk = p.mblk;
+    a.V = g.vpr[0] * g.vpr[1] * g.vpr[2];
+    a.nbx = (g.rdims[0] + p.bx - 1) / p.bx;
+    a.nbatches = p.nbatches;
+    a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;
+    a.qimg = (const uint4*) qimg;
+    a.part = part; a.score_part = score_part; a.count_part = count_part;
+    a.err = err;
+    if (grad_mode == 0) {
+        auto k = mse_tc_kernel<0>;
+        cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) p.smem);
+        k<<<p.grid, TC_THREADS, p.smem, st>>> (a);
+    } else {
+        auto k = mse_tc_kernel<1>;
+        cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) p.smem);
+        k<<<p.grid, TC_THREADS, p.smem, st>>> (a);
+    }
+    return cudaGetLastError ();
+}
+
+} // namespace b200
