@@ -27,7 +27,7 @@ def test_tc_forward_and_adjoint_gemm(N):
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     f = P.lib().b200bsp_internal_tc_selftest
     f.restype = C.c_int
-    f.argtypes = [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 3
+    f.argtypes = [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 3
     rc = f(tq.data_ptr(), tc_.data_ptr(), td.data_ptr(), N, d_out.data_ptr(),
            g_out.data_ptr(), err.data_ptr())
     assert rc == 0 and int(err.item()) == 0
