@@ -49,8 +49,9 @@ constexpr int SM_C_BYTES = 2 * 96 * 128;          // N <= 96
 constexpr int SM_DC = SM_C + SM_C_BYTES;          // DCDV hi, lo: 32 KB each
 constexpr int SM_S = SM_DC + 65536;               // knot block (float)
 constexpr int SM_KB_FLOATS = 3 * 16 * (TC_TMAX + 3);
-constexpr int SM_P = SM_S + SM_KB_FLOATS * 4;     // knot partials (float)
-constexpr int SM_TOTAL = SM_P + SM_KB_FLOATS * 4;
+constexpr int SM_P = SM_S + SM_KB_FLOATS * 4;     // knot partials (float) x2
+constexpr int SM_P2 = SM_P + SM_KB_FLOATS * 4;
+constexpr int SM_TOTAL = SM_P2 + SM_KB_FLOATS * 4;
 
 struct TcArgs {
     BspGeom g;
@@ -75,6 +76,276 @@ split_bf16 (float x, unsigned short& hi, unsigned short& lo)
     lo = __bfloat16_as_ushort (l);
 }
 
+// ---------------------------------------------------------------------------
+// Phases of one batch, shared by the pipelined and the serial schedule.
+
+struct TcCtx {
+    uint8_t* sm;
+    uint32_t sm_base;
+    uint32_t taddr;
+    int tid, warp, lane, q, tg, t_lo, t_hi;
+};
+
+// Knot block S[c][k][j][x] of batch (tx0, ty, tz); zero the partials P.
+__device__ __forceinline__ void
+stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz,
+    float* P)
+{
+    const BspGeom& g = a.g;
+    const int KX = a.T + 3;
+    float* S = (float*) (x.sm + SM_S);
+    for (int o = x.tid; o < 3 * 16 * KX; o += TC_THREADS) {
+        if (o < 16 * KX) {
+            int xx = o % KX, jk = o / KX;       // jk = j + 4k
+            int j = jk & 3, k = jk >> 2;
+            int kx = tx0 + xx;
+            float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+            if (kx < g.cdims[0]) {
+                int knot = (tz + k) * g.cdims[1] * g.cdims[0]
+                    + (ty + j) * g.cdims[0] + kx;
+                v0 = __ldg (a.coeff + 3 * knot + 0);
+                v1 = __ldg (a.coeff + 3 * knot + 1);
+                v2 = __ldg (a.coeff + 3 * knot + 2);
+            }
+            S[(0 * 16 + jk) * KX + xx] = v0;
+            S[(1 * 16 + jk) * KX + xx] = v1;
+            S[(2 * 16 + jk) * KX + xx] = v2;
+        }
+        P[o] = 0.f;
+    }
+}
+
+// C[(c,t)][m] for the forward B operand: row n = c*T + t, K = 64 slots,
+// hi/lo bf16, 128B-swizzled K-major.
+__device__ __forceinline__ void
+build_c (const TcArgs& a, const TcCtx& x)
+{
+    const int T = a.T, N = a.N, KX = T + 3;
+    const float* S = (const float*) (x.sm + SM_S);
+    for (int o = x.tid; o < N * 8; o += TC_THREADS) {
+        int n = o >> 3, ch = o & 7;          // 16-byte chunk: slots 8ch..8ch+7
+        int c = n / T, t = n - c * T;
+        // slots 8ch + e: i = e & 3, j = (2ch + (e >> 2)) & 3, k = ch >> 1
+        const float* r0 = S + (c * 16 + ((2 * ch) & 3) + 4 * (ch >> 1)) * KX + t;
+        const float* r1 = r0 + KX;
+        unsigned short hi[8], lo[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            float v = (c < 3) ? ((e < 4) ? r0[e] : r1[e - 4]) : 0.f;
+            split_bf16 (v, hi[e], lo[e]);
+        }
+        uint32_t off = sw128_offset (n, 8 * ch, N);
+        *(uint4*) (x.sm + SM_C + off) = make_uint4 (hi[0] | (hi[1] << 16),
+            hi[2] | (hi[3] << 16), hi[4] | (hi[5] << 16), hi[6] | (hi[7] << 16));
+        *(uint4*) (x.sm + SM_C + N * 128 + off) = make_uint4 (lo[0] | (lo[1] << 16),
+            lo[2] | (lo[3] << 16), lo[4] | (lo[5] << 16), lo[6] | (lo[7] << 16));
+    }
+}
+
+// Forward D = Q * C^T (three split terms, K = 64); caller is one thread.
+__device__ __forceinline__ void
+issue_forward (const TcArgs& a, const TcCtx& x, uint64_t* bar)
+{
+    const uint32_t idesc = idesc_bf16_f32 (128, a.N, 0, 0);
+    const uint32_t q0 = x.sm_base + SM_Q, c0 = x.sm_base + SM_C;
+    const uint32_t cl = c0 + (uint32_t) a.N * 128;
+    tc_fence_after ();
+#pragma unroll
+    for (int term = 0; term < 3; term++) {
+        uint32_t qa = term == 2 ? q0 + 16384 : q0;     // hi, hi, lo
+        uint32_t cb = term == 1 ? cl : c0;             // hi, lo, hi
+#pragma unroll
+        for (int ks = 0; ks < 4; ks++) {
+            tc_mma_bf16 (x.taddr + TC_D_COL,
+                smem_desc_sw128 (qa + ks * 32, 16, 1024),
+                smem_desc_sw128 (cb + ks * 32, 16, 1024), idesc,
+                (term > 0 || ks > 0) ? 1u : 0u);
+        }
+    }
+    tc_commit (bar);
+}
+
+// Adjoint G (+)= DCDV * Q over the 128 voxels of one M block (A K-major,
+// B = the Q bytes read MN-major); caller is one thread.
+__device__ __forceinline__ void
+issue_adjoint (const TcCtx& x, bool accumulate, uint64_t* bar)
+{
+    const uint32_t idesc = idesc_bf16_f32 (128, 64, 0, 1);
+    const uint32_t d0 = x.sm_base + SM_DC, q0 = x.sm_base + SM_Q;
+    tc_fence_after ();
+#pragma unroll
+    for (int term = 0; term < 3; term++) {
+        uint32_t da = term == 1 ? d0 + 32768 : d0;     // hi, lo, hi
+        uint32_t qb = term == 2 ? q0 + 16384 : q0;     // hi, hi, lo
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+            tc_mma_bf16 (x.taddr + TC_G_COL,
+                smem_desc_sw128 (da + (s >> 2) * 16384 + (s & 3) * 32, 16, 1024),
+                smem_desc_sw128 (qb + s * 2048, 16384, 1024), idesc,
+                (accumulate || term > 0 || s > 0) ? 1u : 0u);
+        }
+    }
+    tc_commit (bar);
+}
+
+// Voxel phase for one M block: thread (quarter q, lane) owns voxel
+// 128 mb + 32 q + lane of every tile in [t_lo, t_hi) (at most 8).  Tiles
+// go four at a time: all four correspondences first, then all gathers
+// (8 corners, fixed value, moving gradient), then the arithmetic, so up to
+// 48 loads per thread are in flight.
+template <int GRAD_MODE>
+__device__ __forceinline__ void
+voxel_phase (const TcArgs& a, const TcCtx& x, int mb, int tx0, int ty, int tz,
+    double& sc, int& cnt)
+{
+    const BspGeom& g = a.g;
+    const int T = a.T;
+    const int vl = 32 * x.q + x.lane, v = 128 * mb + vl;
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
+    float dv[24];
+    const uint32_t lb = x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_D_COL;
+    tmem_ld8x3_wait (lb + x.t_lo, lb + T + x.t_lo, lb + 2 * T + x.t_lo, dv);
+    const int fj = g.roi_off[1] + vy * ty + ly;
+    const int fk = g.roi_off[2] + vz * tz + lz;
+    const bool yz_ok = v < a.V && fj < g.roi_off[1] + g.roi_dim[1]
+        && fk < g.roi_off[2] + g.roi_dim[2];
+    float pj[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        pj[d] = g.img_origin[d] + fj * g.fstep[3 * d + 1] + fk * g.fstep[3 * d + 2];
+    }
+    const int frow = g.fdim[0] * (fj + g.fdim[1] * fk);
+    const int fi_end = g.roi_off[0] + g.roi_dim[0];
+    const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
+    const uint32_t vpart = (vl >> 6) * 16384u + (vl & 7) * 2u;
+    const uint32_t vunit = (vl & 63) >> 3;
+    uint8_t* dch = x.sm + SM_DC;
+    float scf = 0.f;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        bool ok[4];
+        Sample s[4];
+        int fidx[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int tt = 4 * h + u;
+            const int t = x.t_lo + tt;
+            const int tx = tx0 + t;
+            const int fi = g.roi_off[0] + vx * tx + lx;
+            ok[u] = yz_ok && t < x.t_hi && tx < g.rdims[0] && fi < fi_end;
+            fidx[u] = fi + frow;
+            if (ok[u]) {
+                float fxyz[3] = {pj[0] + fi * g.fstep[0], pj[1] + fi * g.fstep[3],
+                    pj[2] + fi * g.fstep[6]};
+                float d[3] = {dv[tt], dv[8 + tt], dv[16 + tt]};
+                ok[u] = locate (g, fxyz, d, s[u]);
+            }
+        }
+        Corners cr[4];
+        float fv[4], gx[4], gy[4], gz[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (ok[u]) {
+                cr[u] = load_corners (a.mimg, s[u].mvf, dxm, dxym);
+                fv[u] = __ldg (a.fimg + fidx[u]);
+                if (GRAD_MODE == 0) {
+                    gx[u] = __ldg (a.mgrad + 3 * s[u].mvr + 0);
+                    gy[u] = __ldg (a.mgrad + 3 * s[u].mvr + 1);
+                    gz[u] = __ldg (a.mgrad + 3 * s[u].mvr + 2);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int t = x.t_lo + 4 * h + u;
+            float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
+            if (ok[u]) {
+                float diff = trilinear (s[u], cr[u]) - fv[u];
+                scf += diff * diff;
+                cnt++;
+                if (GRAD_MODE == 0) {
+                    dc0 = diff * gx[u]; dc1 = diff * gy[u]; dc2 = diff * gz[u];
+                } else {
+                    float gr[3];
+                    trilinear_grad (g, s[u], cr[u], gr);
+                    dc0 = diff * gr[0]; dc1 = diff * gr[1]; dc2 = diff * gr[2];
+                }
+            }
+            if (t < x.t_hi) {
+                // rows r = 32c + t: (r >> 3) * 1024 = 4096 c + (t >> 3) * 1024
+                uint32_t o = vpart + (t >> 3) * 1024u + (t & 7) * 128u
+                    + ((vunit ^ (uint32_t) (t & 7)) << 4);
+                unsigned short hh, ll;
+                split_bf16 (dc0, hh, ll);
+                *(unsigned short*) (dch + o) = hh;
+                *(unsigned short*) (dch + 32768 + o) = ll;
+                split_bf16 (dc1, hh, ll);
+                *(unsigned short*) (dch + 4096 + o) = hh;
+                *(unsigned short*) (dch + 32768 + 4096 + o) = ll;
+                split_bf16 (dc2, hh, ll);
+                *(unsigned short*) (dch + 8192 + o) = hh;
+                *(unsigned short*) (dch + 32768 + 8192 + o) = ll;
+            }
+        }
+    }
+    sc += (double) scf;
+}
+
+// G rows (c, t) = 32c + t, columns = 64 slots.  Warps of quarter q = c read
+// slots [16 tg, 16 tg + 16) (k = tg) and add them to knots (t + i, j, k) in
+// slot order.
+__device__ __forceinline__ void
+readout (const TcArgs& a, const TcCtx& x, float* P)
+{
+    if (x.q >= 3) return;
+    const int T = a.T, KX = T + 3;
+    float gv[16];
+    tmem_ld16_wait (x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_G_COL + 16 * x.tg,
+        gv);
+    // lanes t and t+1 touch the same knot in consecutive i steps:
+    // __syncwarp keeps each (j, i) step complete before the next
+    const int t = x.lane;
+    const bool tv = t < T;
+    float* Pc = P + ((x.q * 4 + x.tg) * 4) * KX;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (tv) Pc[j * KX + t + i] += gv[4 * j + i];
+            __syncwarp ();
+        }
+    }
+}
+
+__device__ __forceinline__ void
+write_partials (const TcArgs& a, const TcCtx& x, int b, const float* P)
+{
+    const int KX = a.T + 3, KF = 16 * KX;
+    float* dst = a.part + (size_t) b * KF * 3;
+    for (int o = x.tid; o < KF * 3; o += TC_THREADS) {
+        int kk = o / 3, c = o - 3 * kk;      // kk = x + KX (j + 4k)
+        dst[o] = P[(c * 16) * KX + kk];
+    }
+}
+
+// Thread 0 waits on `bar` (bounded); everyone learns whether it gave up.
+__device__ __forceinline__ bool
+sync_wait (const TcArgs& a, const TcCtx& x, uint64_t* bar, uint32_t& ph,
+    int* s_abort, int code)
+{
+    if (x.tid == 0) {
+        if (!mbar_wait_bounded (bar, ph, TC_WAIT_LIMIT)) {
+            *s_abort = 1;
+            atomicExch (a.err, code);
+        }
+    }
+    ph ^= 1;
+    __syncthreads ();
+    tc_fence_after ();
+    return *s_abort == 0;
+}
+
 template <int GRAD_MODE>
 __global__ void __launch_bounds__ (TC_THREADS, 1)
 mse_tc_kernel (TcArgs a)
@@ -87,281 +358,147 @@ mse_tc_kernel (TcArgs a)
     __shared__ int sh_n[TC_THREADS / 32];
 
     const BspGeom& g = a.g;
-    uint8_t* sm = (uint8_t*) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
-    const uint32_t sm_base = smem_addr (sm);
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
-    const int T = a.T, N = a.N, KX = T + 3;
-    float* S = (float*) (sm + SM_S);
-    float* P = (float*) (sm + SM_P);
+    TcCtx x;
+    x.sm = (uint8_t*) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    x.sm_base = smem_addr (x.sm);
+    x.tid = threadIdx.x;
+    x.warp = x.tid >> 5;
+    x.lane = x.tid & 31;
+    x.q = x.warp & 3;                  // TMEM lane quarter
+    x.tg = x.warp >> 2;                // tile group
+    x.t_lo = (a.T * x.tg) / 4;         // balanced contiguous tile ranges
+    x.t_hi = (a.T * (x.tg + 1)) / 4;
+    auto pbuf = [&](int i) {
+        return (float*) (x.sm + ((i & 1) ? SM_P2 : SM_P));
+    };
 
-    if (tid == 0) {
+    if (x.tid == 0) {
         mbar_init (&s_bar[0], 1);
         mbar_init (&s_bar[1], 1);
         fence_barrier_init ();
         s_abort = 0;
     }
-    if (warp == 0) {
+    if (x.warp == 0) {
         tmem_alloc (&s_taddr, TC_TMEM_COLS);
         tmem_relinquish ();
     }
-    // Zero the adjoint operand once: rows (c, t >= T) and padding voxels
-    // that the voxel phase never writes must stay zero.
-    for (int o = tid; o < 65536 / 16; o += TC_THREADS) {
-        ((uint4*) (sm + SM_DC))[o] = make_uint4 (0, 0, 0, 0);
+    // Adjoint rows (c, t >= T) and padding voxels are never written by the
+    // voxel phase; start them at zero.
+    for (int o = x.tid; o < 65536 / 16; o += TC_THREADS) {
+        ((uint4*) (x.sm + SM_DC))[o] = make_uint4 (0, 0, 0, 0);
+    }
+    if (a.mblk == 1) {
+        for (int o = x.tid; o < 2048; o += TC_THREADS) {
+            ((uint4*) (x.sm + SM_Q))[o] = a.qimg[o];
+        }
     }
     tc_fence_before ();
     __syncthreads ();
     tc_fence_after ();
-    const uint32_t taddr = s_taddr;
-    uint32_t ph0 = 0, ph1 = 0;
-
-    const uint32_t idesc_fwd = idesc_bf16_f32 (128, N, 0, 0);
-    const uint32_t idesc_adj = idesc_bf16_f32 (128, 64, 0, 1);
-    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
-    const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
-    const int q = warp & 3;            // TMEM lane quarter
-    const int tg = warp >> 2;          // tile group (8 tiles)
-    const int t_begin = tg * 8;
-    const int t_end = min (T, t_begin + 8);
-
+    x.taddr = s_taddr;
+    uint32_t ph_f = 0, ph_a = 0;
     double sc = 0.0;
     int cnt = 0;
+    const int nb_local = (a.nbatches - (int) blockIdx.x + (int) gridDim.x - 1)
+        / (int) gridDim.x;
 
-    if (a.mblk == 1) {
-        for (int o = tid; o < 2048; o += TC_THREADS) {
-            ((uint4*) (sm + SM_Q))[o] = a.qimg[o];
-        }
-    }
+    auto coords = [&](int b, int& tx0, int& ty, int& tz) {
+        tx0 = (b % a.nbx) * a.T;
+        ty = (b / a.nbx) % g.rdims[1];
+        tz = b / (a.nbx * g.rdims[1]);
+    };
 
-    for (int b = blockIdx.x; b < a.nbatches; b += gridDim.x) {
-        const int bxi = b % a.nbx;
-        const int ty = (b / a.nbx) % g.rdims[1];
-        const int tz = b / (a.nbx * g.rdims[1]);
-        const int tx0 = bxi * T;
-
-        // 1. knot block S[c][k][j][x] and zeroed partials P
-        for (int o = tid; o < 3 * 16 * KX; o += TC_THREADS) {
-            int x = o % KX, jk = o / KX;        // jk = j + 4k
-            int j = jk & 3, k = jk >> 2;
-            int kx = tx0 + x;
-            float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-            if (o < 16 * KX && kx < g.cdims[0]) {
-                int knot = (tz + k) * g.cdims[1] * g.cdims[0]
-                    + (ty + j) * g.cdims[0] + kx;
-                v0 = __ldg (a.coeff + 3 * knot + 0);
-                v1 = __ldg (a.coeff + 3 * knot + 1);
-                v2 = __ldg (a.coeff + 3 * knot + 2);
-            }
-            if (o < 16 * KX) {
-                S[(0 * 16 + jk) * KX + x] = v0;
-                S[(1 * 16 + jk) * KX + x] = v1;
-                S[(2 * 16 + jk) * KX + x] = v2;
-            }
-            P[o] = 0.f;
-        }
+    if (a.mblk == 1 && nb_local > 0) {
+        // Pipelined: adjoint(b) runs while batch b+1 is staged; forward(b+1)
+        // runs while batch b is read out.
+        int tx0, ty, tz;
+        coords (blockIdx.x, tx0, ty, tz);
+        stage_batch (a, x, tx0, ty, tz, pbuf (0));
         __syncthreads ();
-
-        // C[(c,t)][m] for the forward B operand: row n = c*T + t, K = 64 slots
-        for (int o = tid; o < N * 8; o += TC_THREADS) {
-            int n = o >> 3, ch = o & 7;          // 16-byte chunk: slots 8ch..8ch+7
-            int c = n / T, t = n - c * T;
-            unsigned short hi[8], lo[8];
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-                int m = 8 * ch + e;
-                int i = m & 3, j = (m >> 2) & 3, k = m >> 4;
-                float v = (c < 3) ? S[(c * 16 + j + 4 * k) * KX + t + i] : 0.f;
-                split_bf16 (v, hi[e], lo[e]);
-            }
-            uint32_t off = sw128_offset (n, 8 * ch, N);
-            uint4 h4 = make_uint4 (hi[0] | (hi[1] << 16), hi[2] | (hi[3] << 16),
-                hi[4] | (hi[5] << 16), hi[6] | (hi[7] << 16));
-            uint4 l4 = make_uint4 (lo[0] | (lo[1] << 16), lo[2] | (lo[3] << 16),
-                lo[4] | (lo[5] << 16), lo[6] | (lo[7] << 16));
-            *(uint4*) (sm + SM_C + off) = h4;
-            *(uint4*) (sm + SM_C + N * 128 + off) = l4;
-        }
-
-        for (int mb = 0; mb < a.mblk; mb++) {
-            if (a.mblk > 1) {
-                const uint4* src = a.qimg + (size_t) mb * 2048;
-                for (int o = tid; o < 2048; o += TC_THREADS) {
-                    ((uint4*) (sm + SM_Q))[o] = src[o];
-                }
-            }
-            fence_proxy_async_smem ();
-            __syncthreads ();
-
-            // 2a. forward: D = Q * C^T (three split terms, K = 64)
-            if (tid == 0) {
-                tc_fence_after ();
-                const uint32_t qa[2] = {sm_base + SM_Q, sm_base + SM_Q + 16384};
-                const uint32_t cb[2] = {sm_base + SM_C, sm_base + SM_C + (uint32_t) N * 128};
-                const int ta[3] = {0, 0, 1}, tb[3] = {0, 1, 0};
-                uint32_t acc = 0;
-                for (int term = 0; term < 3; term++) {
-                    for (int ks = 0; ks < 4; ks++) {
-                        uint64_t ad = smem_desc_sw128 (qa[ta[term]] + ks * 32, 16, 1024);
-                        uint64_t bd = smem_desc_sw128 (cb[tb[term]] + ks * 32, 16, 1024);
-                        tc_mma_bf16 (taddr + TC_D_COL, ad, bd, idesc_fwd, acc);
-                        acc = 1;
-                    }
-                }
-                tc_commit (&s_bar[0]);
-                if (!mbar_wait_bounded (&s_bar[0], ph0, TC_WAIT_LIMIT)) {
-                    s_abort = 1;
-                    atomicExch (a.err, 1);
-                }
-                ph0 ^= 1;
-            }
-            __syncthreads ();
-            if (s_abort) goto done;
-            tc_fence_after ();
-
-            // 2b. voxel phase: thread = (voxel 32q+lane of this M block,
-            // tiles [t_begin, t_end))
-            if (t_begin < T) {
-                const int vl = 32 * q + lane;
-                const int v = 128 * mb + vl;
-                const bool vok = v < a.V;
-                const int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
-                float dv[24];
-                const uint32_t lane_base = (uint32_t) (32 * q) << 16;
-                tmem_ld8x3_wait (taddr + lane_base + TC_D_COL + 0 * T + t_begin,
-                    taddr + lane_base + TC_D_COL + 1 * T + t_begin,
-                    taddr + lane_base + TC_D_COL + 2 * T + t_begin, dv);
-                const int fj = g.roi_off[1] + vy * ty + ly;
-                const int fk = g.roi_off[2] + vz * tz + lz;
-                const bool yz_ok = vok && fj < g.roi_off[1] + g.roi_dim[1]
-                    && fk < g.roi_off[2] + g.roi_dim[2];
-#pragma unroll 2
-                for (int tt = 0; tt < 8; tt++) {
-                    const int t = t_begin + tt;
-                    if (t >= t_end) break;
-                    const int tx = tx0 + t;
-                    const int fi = g.roi_off[0] + vx * tx + lx;
-                    float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
-                    if (yz_ok && tx < g.rdims[0]
-                        && fi < g.roi_off[0] + g.roi_dim[0]) {
-                        float fxyz[3], d[3] = {dv[tt], dv[8 + tt], dv[16 + tt]};
-                        fixed_position (g, fi, fj, fk, fxyz);
-                        Sample s;
-                        if (locate (g, fxyz, d, s)) {
-                            Corners cr = load_corners (a.mimg, s.mvf, dxm, dxym);
-                            float mval = trilinear (s, cr);
-                            int fidx = fi + g.fdim[0] * (fj + g.fdim[1] * fk);
-                            float diff = mval - __ldg (a.fimg + fidx);
-                            sc += (double) (diff * diff);
-                            cnt++;
-                            if (GRAD_MODE == 0) {
-                                dc0 = diff * __ldg (a.mgrad + 3 * s.mvr + 0);
-                                dc1 = diff * __ldg (a.mgrad + 3 * s.mvr + 1);
-                                dc2 = diff * __ldg (a.mgrad + 3 * s.mvr + 2);
-                            } else {
-                                float gr[3];
-                                trilinear_grad (g, s, cr, gr);
-                                dc0 = diff * gr[0];
-                                dc1 = diff * gr[1];
-                                dc2 = diff * gr[2];
-                            }
-                        }
-                    }
-                    unsigned short h, l;
-                    uint8_t* dch = sm + SM_DC;
-                    uint8_t* dcl = sm + SM_DC + 32768;
-                    uint32_t o0 = sw128_offset (0 * 32 + t, vl, 128);
-                    uint32_t o1 = sw128_offset (1 * 32 + t, vl, 128);
-                    uint32_t o2 = sw128_offset (2 * 32 + t, vl, 128);
-                    split_bf16 (dc0, h, l);
-                    *(unsigned short*) (dch + o0) = h;
-                    *(unsigned short*) (dcl + o0) = l;
-                    split_bf16 (dc1, h, l);
-                    *(unsigned short*) (dch + o1) = h;
-                    *(unsigned short*) (dcl + o1) = l;
-                    split_bf16 (dc2, h, l);
-                    *(unsigned short*) (dch + o2) = h;
-                    *(unsigned short*) (dcl + o2) = l;
-                }
-            }
+        build_c (a, x);
+        fence_proxy_async_smem ();
+        __syncthreads ();
+        if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
+        for (int i = 0; i < nb_local; i++) {
+            const int b = blockIdx.x + i * gridDim.x;
+            float* P = pbuf (i);
+            coords (b, tx0, ty, tz);
+            if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
+            voxel_phase<GRAD_MODE> (a, x, 0, tx0, ty, tz, sc, cnt);
             tc_fence_before ();
             fence_proxy_async_smem ();
             __syncthreads ();
-
-            // 2c. adjoint: G += DCDV * Q (K = 128 voxels of this block)
-            if (tid == 0) {
-                tc_fence_after ();
-                const uint32_t da[2] = {sm_base + SM_DC, sm_base + SM_DC + 32768};
-                const uint32_t qb[2] = {sm_base + SM_Q, sm_base + SM_Q + 16384};
-                const int ta[3] = {0, 1, 0}, tb[3] = {0, 0, 1};
-                for (int term = 0; term < 3; term++) {
-                    for (int s = 0; s < 8; s++) {
-                        uint64_t ad = smem_desc_sw128 (
-                            da[ta[term]] + (s >> 2) * 16384 + (s & 3) * 32, 16, 1024);
-                        uint64_t bd = smem_desc_sw128 (qb[tb[term]] + s * 2048,
-                            16384, 1024);
-                        uint32_t acc = (mb > 0 || term > 0 || s > 0) ? 1u : 0u;
-                        tc_mma_bf16 (taddr + TC_G_COL, ad, bd, idesc_adj, acc);
-                    }
-                }
-                tc_commit (&s_bar[1]);
-                if (!mbar_wait_bounded (&s_bar[1], ph1, TC_WAIT_LIMIT)) {
-                    s_abort = 1;
-                    atomicExch (a.err, 2);
-                }
-                ph1 ^= 1;
+            if (x.tid == 0) issue_adjoint (x, false, &s_bar[1]);
+            if (i + 1 < nb_local) {
+                int nx0, ny, nz;
+                coords (b + gridDim.x, nx0, ny, nz);
+                stage_batch (a, x, nx0, ny, nz, pbuf (i + 1));
+                __syncthreads ();
+                build_c (a, x);
+                fence_proxy_async_smem ();
+                __syncthreads ();
+                if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
             }
+            if (!sync_wait (a, x, &s_bar[1], ph_a, &s_abort, 2)) goto done;
+            readout (a, x, P);
+            tc_fence_before ();
             __syncthreads ();
-            if (s_abort) goto done;
-            tc_fence_after ();
+            write_partials (a, x, b, P);
+            block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
+            if (x.tid == 0) {
+                a.score_part[b] = sc;
+                a.count_part[b] = cnt;
+            }
+            sc = 0.0;
+            cnt = 0;
         }
-
-        // 3. G rows (c, t) = 32c + t, columns = 64 slots; warps of quarter
-        // q = c read slots [16 tg, 16 tg + 16) (k = tg) and add them to the
-        // knots (t + i, j, k) in slot order.
-        if (q < 3) {
-            float gv[16];
-            tmem_ld16_wait (taddr + ((uint32_t) (32 * q) << 16) + TC_G_COL + 16 * tg,
-                gv);
-            // lanes t and t+1 touch the same knot in consecutive i steps:
-            // __syncwarp keeps each (j, i) step complete before the next
-            const int t = lane;
-            const bool tv = t < T;
-            float* Pc = P + ((q * 4 + tg) * 4) * KX;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    if (tv) Pc[j * KX + t + i] += gv[4 * j + i];
-                    __syncwarp ();
+    } else {
+        // Serial schedule for tiles of more than 128 voxels: Q is reloaded
+        // per 128-voxel block, so batches cannot overlap.
+        for (int i = 0; i < nb_local; i++) {
+            const int b = blockIdx.x + i * gridDim.x;
+            int tx0, ty, tz;
+            coords (b, tx0, ty, tz);
+            float* P = pbuf (0);
+            stage_batch (a, x, tx0, ty, tz, P);
+            __syncthreads ();
+            build_c (a, x);
+            for (int mb = 0; mb < a.mblk; mb++) {
+                const uint4* src = a.qimg + (size_t) mb * 2048;
+                for (int o = x.tid; o < 2048; o += TC_THREADS) {
+                    ((uint4*) (x.sm + SM_Q))[o] = src[o];
                 }
+                fence_proxy_async_smem ();
+                __syncthreads ();
+                if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
+                if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
+                voxel_phase<GRAD_MODE> (a, x, mb, tx0, ty, tz, sc, cnt);
+                tc_fence_before ();
+                fence_proxy_async_smem ();
+                __syncthreads ();
+                if (x.tid == 0) issue_adjoint (x, mb > 0, &s_bar[1]);
+                if (!sync_wait (a, x, &s_bar[1], ph_a, &s_abort, 2)) goto done;
             }
-        }
-        tc_fence_before ();
-        __syncthreads ();
-        {
-            const int KF = 16 * KX;
-            float* dst = a.part + (size_t) b * KF * 3;
-            for (int o = tid; o < KF * 3; o += TC_THREADS) {
-                int kk = o / 3, c = o - 3 * kk;      // kk = x + KX (j + 4k)
-                dst[o] = P[(c * 16) * KX + kk];
+            readout (a, x, P);
+            tc_fence_before ();
+            __syncthreads ();
+            write_partials (a, x, b, P);
+            block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
+            if (x.tid == 0) {
+                a.score_part[b] = sc;
+                a.count_part[b] = cnt;
             }
+            sc = 0.0;
+            cnt = 0;
+            __syncthreads ();
         }
-        block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
-        if (tid == 0) {
-            a.score_part[b] = sc;
-            a.count_part[b] = cnt;
-        }
-        sc = 0.0;
-        cnt = 0;
-        __syncthreads ();
     }
 
 done:
     tc_fence_before ();
     __syncthreads ();
-    if (warp == 0) {
-        tmem_dealloc (taddr, TC_TMEM_COLS);
+    if (x.warp == 0) {
+        tmem_dealloc (x.taddr, TC_TMEM_COLS);
     }
 }
 
