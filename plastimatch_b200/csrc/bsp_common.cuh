@@ -35,6 +35,8 @@ struct BspGeom {
     int cdims[3];         // knots per axis = rdims + 3
     int ntiles;
     int nknots;
+    float m_hi[3];        // dim - 0.5: strict upper bound of the inside test
+    float m_fmax[3];      // dim - 2: largest floor corner after clamping
 };
 
 // Where one fixed voxel lands in the moving image.
@@ -89,6 +91,73 @@ locate (const BspGeom& g, const float fxyz[3], const float dxyz[3], Sample& s)
     s.mvf = f[0] + g.mdim[0] * (f[1] + g.mdim[1] * f[2]);
     s.mvr = r[0] + g.mdim[0] * (r[1] + g.mdim[1] * r[2]);
     return true;
+}
+
+// Branch-free form of locate(): the same inside test, and the clamp of
+// li_clamp written as floor -> clamp to [0, dim-2] -> fraction saturated to
+// [0, 1], which reproduces all three of li_clamp's cases exactly
+// (ma < 0: corner 0, fraction 0; ma >= dim-1: corner dim-2, fraction 1;
+// otherwise floor and ma - floor).  Round index = corner + (fraction >= .5).
+__device__ __forceinline__ bool
+locate_fast (const BspGeom& g, const float fxyz[3], const float dxyz[3],
+    int& mvf, int& mvr, float w2[3])
+{
+    float t0 = (fxyz[0] + dxyz[0]) - g.morigin[0];
+    float t1 = (fxyz[1] + dxyz[1]) - g.morigin[1];
+    float t2 = (fxyz[2] + dxyz[2]) - g.morigin[2];
+    bool in = true;
+    int f[3], r[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        float ma = t0 * g.mproj[3*d+0] + t1 * g.mproj[3*d+1]
+            + t2 * g.mproj[3*d+2];
+        in = in && (ma > -0.5f) && (ma < g.m_hi[d]);
+        float fc = fminf (fmaxf (floorf (ma), 0.f), g.m_fmax[d]);
+        float w = __saturatef (ma - fc);
+        w2[d] = w;
+        f[d] = (int) fc;
+        r[d] = f[d] + (w >= 0.5f ? 1 : 0);
+    }
+    mvf = f[0] + g.mdim[0] * (f[1] + g.mdim[1] * f[2]);
+    mvr = r[0] + g.mdim[0] * (r[1] + g.mdim[1] * r[2]);
+    return in;
+}
+
+// Trilinear value as nested linear interpolation (x, then y, then z).
+__device__ __forceinline__ float
+trilinear_lerp (const float w2[3], const float m[8])
+{
+    float c00 = fmaf (w2[0], m[1] - m[0], m[0]);
+    float c10 = fmaf (w2[0], m[3] - m[2], m[2]);
+    float c01 = fmaf (w2[0], m[5] - m[4], m[4]);
+    float c11 = fmaf (w2[0], m[7] - m[6], m[6]);
+    float c0 = fmaf (w2[1], c10 - c00, c00);
+    float c1 = fmaf (w2[1], c11 - c01, c01);
+    return fmaf (w2[2], c1 - c0, c0);
+}
+
+// Gradient of the trilinear interpolant (index space, scaled by 1/spacing).
+__device__ __forceinline__ void
+trilinear_lerp_grad (const BspGeom& g, const float w2[3], const float m[8],
+    float out[3])
+{
+    float c00 = fmaf (w2[0], m[1] - m[0], m[0]);
+    float c10 = fmaf (w2[0], m[3] - m[2], m[2]);
+    float c01 = fmaf (w2[0], m[5] - m[4], m[4]);
+    float c11 = fmaf (w2[0], m[7] - m[6], m[6]);
+    float c0 = fmaf (w2[1], c10 - c00, c00);
+    float c1 = fmaf (w2[1], c11 - c01, c01);
+    out[2] = g.minv_spacing[2] * (c1 - c0);
+    float e0 = fmaf (w2[2], c01 - c00, c00);     // y = 0 face
+    float e1 = fmaf (w2[2], c11 - c10, c10);     // y = 1 face
+    out[1] = g.minv_spacing[1] * (e1 - e0);
+    float a0 = fmaf (w2[1], m[2] - m[0], m[0]);  // x = 0 edge, z = 0
+    float a1 = fmaf (w2[1], m[6] - m[4], m[4]);  // x = 0 edge, z = 1
+    float b0 = fmaf (w2[1], m[3] - m[1], m[1]);  // x = 1 edge, z = 0
+    float b1 = fmaf (w2[1], m[7] - m[5], m[5]);  // x = 1 edge, z = 1
+    float x0 = fmaf (w2[2], a1 - a0, a0);
+    float x1 = fmaf (w2[2], b1 - b0, b0);
+    out[0] = g.minv_spacing[0] * (x1 - x0);
 }
 
 // The eight corner values of a trilinear cell, in li_value's order.

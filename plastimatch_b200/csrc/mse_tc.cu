@@ -87,6 +87,8 @@ struct TcCtx {
 };
 
 // Knot block S[c][k][j][x] of batch (tx0, ty, tz); zero the partials P.
+// Thread (row = tid / 32, lane) covers knot row jk = row, x = lane and
+// x = lane + 32: no division.
 __device__ __forceinline__ void
 stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz,
     float* P)
@@ -94,24 +96,28 @@ stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz,
     const BspGeom& g = a.g;
     const int KX = a.T + 3;
     float* S = (float*) (x.sm + SM_S);
-    for (int o = x.tid; o < 3 * 16 * KX; o += TC_THREADS) {
-        if (o < 16 * KX) {
-            int xx = o % KX, jk = o / KX;       // jk = j + 4k
-            int j = jk & 3, k = jk >> 2;
-            int kx = tx0 + xx;
+    const int jk = x.tid >> 5;                 // 0..15 = j + 4k
+    const int j = jk & 3, k = jk >> 2;
+    const int row = (tz + k) * g.cdims[1] * g.cdims[0] + (ty + j) * g.cdims[0];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int xx = x.lane + 32 * h;
+        if (xx < KX) {
+            const int kx = tx0 + xx;
             float v0 = 0.f, v1 = 0.f, v2 = 0.f;
             if (kx < g.cdims[0]) {
-                int knot = (tz + k) * g.cdims[1] * g.cdims[0]
-                    + (ty + j) * g.cdims[0] + kx;
-                v0 = __ldg (a.coeff + 3 * knot + 0);
-                v1 = __ldg (a.coeff + 3 * knot + 1);
-                v2 = __ldg (a.coeff + 3 * knot + 2);
+                const float* cp = a.coeff + 3 * (row + kx);
+                v0 = __ldg (cp + 0);
+                v1 = __ldg (cp + 1);
+                v2 = __ldg (cp + 2);
             }
             S[(0 * 16 + jk) * KX + xx] = v0;
             S[(1 * 16 + jk) * KX + xx] = v1;
             S[(2 * 16 + jk) * KX + xx] = v2;
+            P[(0 * 16 + jk) * KX + xx] = 0.f;
+            P[(1 * 16 + jk) * KX + xx] = 0.f;
+            P[(2 * 16 + jk) * KX + xx] = 0.f;
         }
-        P[o] = 0.f;
     }
 }
 
@@ -123,22 +129,27 @@ build_c (const TcArgs& a, const TcCtx& x)
     const int T = a.T, N = a.N, KX = T + 3;
     const float* S = (const float*) (x.sm + SM_S);
     for (int o = x.tid; o < N * 8; o += TC_THREADS) {
-        int n = o >> 3, ch = o & 7;          // 16-byte chunk: slots 8ch..8ch+7
-        int c = n / T, t = n - c * T;
+        const int n = o >> 3, ch = o & 7;    // 16-byte chunk: slots 8ch..8ch+7
+        const int c = (n >= T) + (n >= 2 * T);
+        const int t = n - c * T;
         // slots 8ch + e: i = e & 3, j = (2ch + (e >> 2)) & 3, k = ch >> 1
         const float* r0 = S + (c * 16 + ((2 * ch) & 3) + 4 * (ch >> 1)) * KX + t;
         const float* r1 = r0 + KX;
-        unsigned short hi[8], lo[8];
+        const bool live = c < 3;
+        uint32_t hw[4], lw[4];
 #pragma unroll
-        for (int e = 0; e < 8; e++) {
-            float v = (c < 3) ? ((e < 4) ? r0[e] : r1[e - 4]) : 0.f;
-            split_bf16 (v, hi[e], lo[e]);
+        for (int e = 0; e < 8; e += 2) {
+            float v0 = live ? ((e < 4) ? r0[e] : r1[e - 4]) : 0.f;
+            float v1 = live ? ((e < 4) ? r0[e + 1] : r1[e - 3]) : 0.f;
+            unsigned short h0, l0, h1, l1;
+            split_bf16 (v0, h0, l0);
+            split_bf16 (v1, h1, l1);
+            hw[e >> 1] = (uint32_t) h0 | ((uint32_t) h1 << 16);
+            lw[e >> 1] = (uint32_t) l0 | ((uint32_t) l1 << 16);
         }
-        uint32_t off = sw128_offset (n, 8 * ch, N);
-        *(uint4*) (x.sm + SM_C + off) = make_uint4 (hi[0] | (hi[1] << 16),
-            hi[2] | (hi[3] << 16), hi[4] | (hi[5] << 16), hi[6] | (hi[7] << 16));
-        *(uint4*) (x.sm + SM_C + N * 128 + off) = make_uint4 (lo[0] | (lo[1] << 16),
-            lo[2] | (lo[3] << 16), lo[4] | (lo[5] << 16), lo[6] | (lo[7] << 16));
+        const uint32_t off = sw128_offset (n, 8 * ch, N);
+        *(uint4*) (x.sm + SM_C + off) = make_uint4 (hw[0], hw[1], hw[2], hw[3]);
+        *(uint4*) (x.sm + SM_C + N * 128 + off) = make_uint4 (lw[0], lw[1], lw[2], lw[3]);
     }
 }
 
@@ -188,27 +199,49 @@ issue_adjoint (const TcCtx& x, bool accumulate, uint64_t* bar)
     tc_commit (bar);
 }
 
-// Voxel phase for one M block: thread (quarter q, lane) owns voxel
-// 128 mb + 32 q + lane of every tile in [t_lo, t_hi) (at most 8).  Tiles
-// go four at a time: all four correspondences first, then all gathers
-// (8 corners, fixed value, moving gradient), then the arithmetic, so up to
-// 48 loads per thread are in flight.
+// Per-thread voxel constants of one 128-voxel M block.
+struct VoxelSlot {
+    int lx, ly, lz;
+    bool live;           // voxel index < voxels per tile
+    uint32_t vpart;      // adjoint-operand byte offset part from the voxel
+    uint32_t vunit;      // 16-byte unit of the voxel within its 128-B row
+};
+
+__device__ __forceinline__ VoxelSlot
+voxel_slot (const TcArgs& a, const TcCtx& x, int mb)
+{
+    const BspGeom& g = a.g;
+    VoxelSlot s;
+    const int vl = 32 * x.q + x.lane, v = 128 * mb + vl;
+    const int vx = g.vpr[0], vy = g.vpr[1];
+    s.lx = v % vx;
+    s.ly = (v / vx) % vy;
+    s.lz = v / (vx * vy);
+    s.live = v < a.V;
+    s.vpart = (vl >> 6) * 16384u + (vl & 7) * 2u;
+    s.vunit = (vl & 63) >> 3;
+    return s;
+}
+
+// Voxel phase for one M block: thread (quarter q, lane) owns one voxel of
+// every tile in [t_lo, t_hi) (at most 8).  Tiles go four at a time: all four
+// correspondences first, then all gathers (8 corners, fixed value, moving
+// gradient), then the arithmetic, so up to 48 loads per thread are in
+// flight.  Sample indices are clamped inside the moving image even when
+// the sample is rejected, so only the fixed-image load needs a guard.
 template <int GRAD_MODE>
 __device__ __forceinline__ void
-voxel_phase (const TcArgs& a, const TcCtx& x, int mb, int tx0, int ty, int tz,
-    double& sc, int& cnt)
+voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
+    int ty, int tz, double& sc, int& cnt)
 {
     const BspGeom& g = a.g;
     const int T = a.T;
-    const int vl = 32 * x.q + x.lane, v = 128 * mb + vl;
-    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
-    const int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
     float dv[24];
     const uint32_t lb = x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_D_COL;
     tmem_ld8x3_wait (lb + x.t_lo, lb + T + x.t_lo, lb + 2 * T + x.t_lo, dv);
-    const int fj = g.roi_off[1] + vy * ty + ly;
-    const int fk = g.roi_off[2] + vz * tz + lz;
-    const bool yz_ok = v < a.V && fj < g.roi_off[1] + g.roi_dim[1]
+    const int fj = g.roi_off[1] + g.vpr[1] * ty + vs.ly;
+    const int fk = g.roi_off[2] + g.vpr[2] * tz + vs.lz;
+    const bool yz_ok = vs.live && fj < g.roi_off[1] + g.roi_dim[1]
         && fk < g.roi_off[2] + g.roi_dim[2];
     float pj[3];
 #pragma unroll
@@ -217,43 +250,45 @@ voxel_phase (const TcArgs& a, const TcCtx& x, int mb, int tx0, int ty, int tz,
     }
     const int frow = g.fdim[0] * (fj + g.fdim[1] * fk);
     const int fi_end = g.roi_off[0] + g.roi_dim[0];
+    const int fi0 = g.roi_off[0] + g.vpr[0] * (tx0 + x.t_lo) + vs.lx;
+    const int t_cnt = min (x.t_hi - x.t_lo, g.rdims[0] - tx0 - x.t_lo);
     const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
-    const uint32_t vpart = (vl >> 6) * 16384u + (vl & 7) * 2u;
-    const uint32_t vunit = (vl & 63) >> 3;
-    uint8_t* dch = x.sm + SM_DC;
+    uint8_t* dch = x.sm + SM_DC + vs.vpart;
     float scf = 0.f;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         bool ok[4];
-        Sample s[4];
-        int fidx[4];
+        int mvf[4], mvr[4];
+        float w2[4][3];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const int tt = 4 * h + u;
-            const int t = x.t_lo + tt;
-            const int tx = tx0 + t;
-            const int fi = g.roi_off[0] + vx * tx + lx;
-            ok[u] = yz_ok && t < x.t_hi && tx < g.rdims[0] && fi < fi_end;
-            fidx[u] = fi + frow;
-            if (ok[u]) {
-                float fxyz[3] = {pj[0] + fi * g.fstep[0], pj[1] + fi * g.fstep[3],
-                    pj[2] + fi * g.fstep[6]};
-                float d[3] = {dv[tt], dv[8 + tt], dv[16 + tt]};
-                ok[u] = locate (g, fxyz, d, s[u]);
-            }
+            const int fi = fi0 + g.vpr[0] * tt;
+            const float ffi = (float) fi;
+            float fxyz[3] = {fmaf (ffi, g.fstep[0], pj[0]),
+                fmaf (ffi, g.fstep[3], pj[1]), fmaf (ffi, g.fstep[6], pj[2])};
+            float d[3] = {dv[tt], dv[8 + tt], dv[16 + tt]};
+            bool in = locate_fast (g, fxyz, d, mvf[u], mvr[u], w2[u]);
+            ok[u] = in && yz_ok && tt < t_cnt && fi < fi_end;
         }
-        Corners cr[4];
-        float fv[4], gx[4], gy[4], gz[4];
+        float cr[4][8], fv[4], gx[4], gy[4], gz[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            if (ok[u]) {
-                cr[u] = load_corners (a.mimg, s[u].mvf, dxm, dxym);
-                fv[u] = __ldg (a.fimg + fidx[u]);
-                if (GRAD_MODE == 0) {
-                    gx[u] = __ldg (a.mgrad + 3 * s[u].mvr + 0);
-                    gy[u] = __ldg (a.mgrad + 3 * s[u].mvr + 1);
-                    gz[u] = __ldg (a.mgrad + 3 * s[u].mvr + 2);
-                }
+            const float* mp = a.mimg + mvf[u];
+            cr[u][0] = __ldg (mp);
+            cr[u][1] = __ldg (mp + 1);
+            cr[u][2] = __ldg (mp + dxm);
+            cr[u][3] = __ldg (mp + dxm + 1);
+            cr[u][4] = __ldg (mp + dxym);
+            cr[u][5] = __ldg (mp + dxym + 1);
+            cr[u][6] = __ldg (mp + dxym + dxm);
+            cr[u][7] = __ldg (mp + dxym + dxm + 1);
+            fv[u] = ok[u] ? __ldg (a.fimg + frow + fi0 + g.vpr[0] * (4 * h + u)) : 0.f;
+            if (GRAD_MODE == 0) {
+                const float* gp = a.mgrad + 3 * mvr[u];
+                gx[u] = __ldg (gp + 0);
+                gy[u] = __ldg (gp + 1);
+                gz[u] = __ldg (gp + 2);
             }
         }
 #pragma unroll
@@ -261,21 +296,21 @@ voxel_phase (const TcArgs& a, const TcCtx& x, int mb, int tx0, int ty, int tz,
             const int t = x.t_lo + 4 * h + u;
             float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
             if (ok[u]) {
-                float diff = trilinear (s[u], cr[u]) - fv[u];
-                scf += diff * diff;
+                const float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
+                scf = fmaf (diff, diff, scf);
                 cnt++;
                 if (GRAD_MODE == 0) {
                     dc0 = diff * gx[u]; dc1 = diff * gy[u]; dc2 = diff * gz[u];
                 } else {
                     float gr[3];
-                    trilinear_grad (g, s[u], cr[u], gr);
+                    trilinear_lerp_grad (g, w2[u], cr[u], gr);
                     dc0 = diff * gr[0]; dc1 = diff * gr[1]; dc2 = diff * gr[2];
                 }
             }
             if (t < x.t_hi) {
                 // rows r = 32c + t: (r >> 3) * 1024 = 4096 c + (t >> 3) * 1024
-                uint32_t o = vpart + (t >> 3) * 1024u + (t & 7) * 128u
-                    + ((vunit ^ (uint32_t) (t & 7)) << 4);
+                const uint32_t o = (t >> 3) * 1024u + (t & 7) * 128u
+                    + ((vs.vunit ^ (uint32_t) (t & 7)) << 4);
                 unsigned short hh, ll;
                 split_bf16 (dc0, hh, ll);
                 *(unsigned short*) (dch + o) = hh;
@@ -323,9 +358,10 @@ write_partials (const TcArgs& a, const TcCtx& x, int b, const float* P)
 {
     const int KX = a.T + 3, KF = 16 * KX;
     float* dst = a.part + (size_t) b * KF * 3;
-    for (int o = x.tid; o < KF * 3; o += TC_THREADS) {
-        int kk = o / 3, c = o - 3 * kk;      // kk = x + KX (j + 4k)
-        dst[o] = P[(c * 16) * KX + kk];
+    for (int kk = x.tid; kk < KF; kk += TC_THREADS) {    // kk = x + KX (j + 4k)
+        dst[3 * kk + 0] = P[0 * 16 * KX + kk];
+        dst[3 * kk + 1] = P[1 * 16 * KX + kk];
+        dst[3 * kk + 2] = P[2 * 16 * KX + kk];
     }
 }
 
@@ -409,6 +445,7 @@ mse_tc_kernel (TcArgs a)
     };
 
     if (a.mblk == 1 && nb_local > 0) {
+        const VoxelSlot vs0 = voxel_slot (a, x, 0);
         // Pipelined: adjoint(b) runs while batch b+1 is staged; forward(b+1)
         // runs while batch b is read out.
         int tx0, ty, tz;
@@ -424,7 +461,7 @@ mse_tc_kernel (TcArgs a)
             float* P = pbuf (i);
             coords (b, tx0, ty, tz);
             if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
-            voxel_phase<GRAD_MODE> (a, x, 0, tx0, ty, tz, sc, cnt);
+            voxel_phase<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
             tc_fence_before ();
             fence_proxy_async_smem ();
             __syncthreads ();
@@ -472,7 +509,8 @@ mse_tc_kernel (TcArgs a)
                 __syncthreads ();
                 if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
                 if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
-                voxel_phase<GRAD_MODE> (a, x, mb, tx0, ty, tz, sc, cnt);
+                voxel_phase<GRAD_MODE> (a, x, voxel_slot (a, x, mb), tx0, ty,
+                    tz, sc, cnt);
                 tc_fence_before ();
                 fence_proxy_async_smem ();
                 __syncthreads ();

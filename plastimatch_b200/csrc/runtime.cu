@@ -273,6 +273,8 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         g.vpr[d] = (int) grid->vox_per_rgn[d];
         g.rdims[d] = 1 + (g.roi_dim[d] - 1) / g.vpr[d];
         g.cdims[d] = g.rdims[d] + 3;
+        g.m_hi[d] = (float) moving->dim[d] - 0.5f;
+        g.m_fmax[d] = (float) (moving->dim[d] - 2);
         ntiles *= g.rdims[d];
         nknots *= g.cdims[d];
     }
