@@ -113,8 +113,8 @@ gather_grad_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
                     int lx = kx - bi * lay.bx;
                     int b = bi + lay.nbx * (bj + lay.nby * bk);
                     int kk = lx + lay.kx * (ly + lay.ky * lz);
-                    const float* p = part + ((size_t) b * KF + kk) * 3;
-                    s0 += p[0]; s1 += p[1]; s2 += p[2];
+                    const float* p = part + (size_t) b * 3 * KF + kk;
+                    s0 += p[0]; s1 += p[KF]; s2 += p[2 * KF];
                 }
             }
         }

@@ -23,7 +23,7 @@ struct PartLayout {
     int bx, by, bz;      // tiles per batch along x, y, z
     int nbx, nby, nbz;   // batches along x, y, z
     int kx, ky, kz;      // knots per batch footprint = b? + 3
-    int slots;           // 1: footprint layout part[batch][knot][3];
+    int slots;           // 1: footprint layout part[batch][c][knot];
                          // 64: per-tile slot layout part[slot][tile][3]
 };
 

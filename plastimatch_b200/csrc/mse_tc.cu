@@ -16,13 +16,19 @@
 // margin while the voxel arithmetic (positions, trilinear samples,
 // differences) stays in f32 on the CUDA cores.
 //
-// One CTA per SM loops over batches.  Per batch:
+// Two CTAs share an SM (about 111 KB of shared memory and 256 TMEM columns
+// each), so one CTA's tensor-core and synchronisation phases hide behind
+// the other's voxel work.  Each CTA loops over batches of T <= 26 tiles:
 //   1. stage the (T+3) x 4 x 4 knot block, build C (hi/lo, 128B-swizzled)
-//   2. per 128-voxel M block: forward MMA -> D in TMEM; the voxel phase
-//      reads D, samples the moving image and writes dc/dv (hi/lo) into the
-//      adjoint operand; adjoint MMA accumulates G in TMEM
-//   3. G -> per-knot partial sums in shared memory (fixed order) -> global
-// The partial sums are combined per knot by gather_grad (deterministic).
+//   2. forward MMA -> D in TMEM; the voxel phase reads D, samples the moving
+//      image and writes dc/dv (hi/lo) into the adjoint operand; adjoint MMA
+//      accumulates G in TMEM (per 128-voxel block when a tile has more)
+//   3. G is copied to shared memory and every knot of the batch footprint
+//      sums its (at most four) contributions in a fixed order -> global.
+// With one 128-voxel block per tile the batches are software-pipelined:
+// the adjoint of batch b runs while batch b+1 is staged and the forward of
+// batch b+1 runs while batch b is gathered.  The per-batch partial sums
+// are combined per knot by gather_grad (deterministic, no atomics).
 #include <algorithm>
 #include <vector>
 
@@ -35,23 +41,34 @@
 
 namespace b200 {
 
-constexpr int TC_THREADS = 512;
-constexpr int TC_TMAX = 32;          // tiles per batch at most
+constexpr int TC_THREADS = 256;
+constexpr int TC_WARPS = TC_THREADS / 32;
+constexpr int TC_TMAX = 26;          // tiles per batch at most
 constexpr int TC_TMEM_COLS = 256;
 constexpr int TC_D_COL = 0;          // forward accumulator [0, N)
 constexpr int TC_G_COL = 128;        // adjoint accumulator [128, 192)
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;
 
+// Adjoint-operand rows: (c, t) -> r = 8 (3 (t >> 3) + c) + (t & 7), so the
+// three components of one tile sit at the same place in consecutive 8-row
+// groups.  T <= 26 needs 12 groups = 96 rows; the MMA reads 128 rows per
+// K chunk, and rows 96..127 alias the next chunk (their G rows are never
+// read).
+constexpr int DC_CHUNK = 96 * 128;                 // one 64-voxel K chunk
+constexpr int DC_HALF = 2 * DC_CHUNK;              // 128 voxels, hi or lo
+constexpr int DC_TAIL = 32 * 128;                  // rows 96..127 over-read
+
 // Shared-memory map (offsets from a 1024-byte aligned base).
-constexpr int SM_Q = 0;                           // Q hi 16 KB, lo 16 KB
-constexpr int SM_C = 32768;                       // C hi, lo: N*128 B each
-constexpr int SM_C_BYTES = 2 * 96 * 128;          // N <= 96
-constexpr int SM_DC = SM_C + SM_C_BYTES;          // DCDV hi, lo: 32 KB each
-constexpr int SM_S = SM_DC + 65536;               // knot block (float)
-constexpr int SM_KB_FLOATS = 3 * 16 * (TC_TMAX + 3);
-constexpr int SM_P = SM_S + SM_KB_FLOATS * 4;     // knot partials (float) x2
-constexpr int SM_P2 = SM_P + SM_KB_FLOATS * 4;
-constexpr int SM_TOTAL = SM_P2 + SM_KB_FLOATS * 4;
+constexpr int SM_Q = 0;                            // Q hi 16 KB, lo 16 KB
+constexpr int SM_C = 32768;                        // C hi, lo: N*128 B each
+constexpr int SM_C_BYTES = 2 * 80 * 128;           // N <= 80
+constexpr int SM_DC = SM_C + SM_C_BYTES;           // DCDV hi, lo (+ tail);
+                                                   // G copy after the adjoint
+constexpr int SM_S = SM_DC + 2 * DC_HALF + DC_TAIL; // knot block (float)
+constexpr int SM_S_FLOATS = 3 * 16 * (TC_TMAX + 3);
+constexpr int SM_TOTAL = SM_S + SM_S_FLOATS * 4;
+static_assert (3 * TC_TMAX * 64 * 4 <= 2 * DC_HALF, "G copy fits the DCDV area");
+static_assert (3 * TC_TMAX <= 80, "N fits the C area");
 
 struct TcArgs {
     BspGeom g;
@@ -61,7 +78,7 @@ struct TcArgs {
     const float* mgrad;
     const float* coeff;
     const uint4* qimg;
-    float* part;
+    float* part;          // [batch][c][knot of the (T+3) x 4 x 4 footprint]
     double* score_part;
     int* count_part;
     int* err;
@@ -76,9 +93,6 @@ split_bf16 (float x, unsigned short& hi, unsigned short& lo)
     lo = __bfloat16_as_ushort (l);
 }
 
-// ---------------------------------------------------------------------------
-// Phases of one batch, shared by the pipelined and the serial schedule.
-
 struct TcCtx {
     uint8_t* sm;
     uint32_t sm_base;
@@ -86,37 +100,36 @@ struct TcCtx {
     int tid, warp, lane, q, tg, t_lo, t_hi;
 };
 
-// Knot block S[c][k][j][x] of batch (tx0, ty, tz); zero the partials P.
-// Thread (row = tid / 32, lane) covers knot row jk = row, x = lane and
-// x = lane + 32: no division.
+// Knot block S[c][k][j][x] of batch (tx0, ty, tz).  Warp w covers knot
+// rows jk = w, w + 8 (jk = j + 4k), lane x and x + 32.
 __device__ __forceinline__ void
-stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz,
-    float* P)
+stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz)
 {
     const BspGeom& g = a.g;
     const int KX = a.T + 3;
     float* S = (float*) (x.sm + SM_S);
-    const int jk = x.tid >> 5;                 // 0..15 = j + 4k
-    const int j = jk & 3, k = jk >> 2;
-    const int row = (tz + k) * g.cdims[1] * g.cdims[0] + (ty + j) * g.cdims[0];
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-        const int xx = x.lane + 32 * h;
-        if (xx < KX) {
-            const int kx = tx0 + xx;
-            float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-            if (kx < g.cdims[0]) {
-                const float* cp = a.coeff + 3 * (row + kx);
-                v0 = __ldg (cp + 0);
-                v1 = __ldg (cp + 1);
-                v2 = __ldg (cp + 2);
+    for (int r = 0; r < 2; r++) {
+        const int jk = x.warp + TC_WARPS * r;
+        const int j = jk & 3, k = jk >> 2;
+        const int row = (tz + k) * g.cdims[1] * g.cdims[0]
+            + (ty + j) * g.cdims[0];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int xx = x.lane + 32 * h;
+            if (xx < KX) {
+                const int kx = tx0 + xx;
+                float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+                if (kx < g.cdims[0]) {
+                    const float* cp = a.coeff + 3 * (row + kx);
+                    v0 = __ldg (cp + 0);
+                    v1 = __ldg (cp + 1);
+                    v2 = __ldg (cp + 2);
+                }
+                S[(0 * 16 + jk) * KX + xx] = v0;
+                S[(1 * 16 + jk) * KX + xx] = v1;
+                S[(2 * 16 + jk) * KX + xx] = v2;
             }
-            S[(0 * 16 + jk) * KX + xx] = v0;
-            S[(1 * 16 + jk) * KX + xx] = v1;
-            S[(2 * 16 + jk) * KX + xx] = v2;
-            P[(0 * 16 + jk) * KX + xx] = 0.f;
-            P[(1 * 16 + jk) * KX + xx] = 0.f;
-            P[(2 * 16 + jk) * KX + xx] = 0.f;
         }
     }
 }
@@ -176,8 +189,8 @@ issue_forward (const TcArgs& a, const TcCtx& x, uint64_t* bar)
     tc_commit (bar);
 }
 
-// Adjoint G (+)= DCDV * Q over the 128 voxels of one M block (A K-major,
-// B = the Q bytes read MN-major); caller is one thread.
+// Adjoint G (+)= DCDV * Q over the 128 voxels of one M block (A K-major in
+// 96-row chunks, B = the Q bytes read MN-major); caller is one thread.
 __device__ __forceinline__ void
 issue_adjoint (const TcCtx& x, bool accumulate, uint64_t* bar)
 {
@@ -186,12 +199,12 @@ issue_adjoint (const TcCtx& x, bool accumulate, uint64_t* bar)
     tc_fence_after ();
 #pragma unroll
     for (int term = 0; term < 3; term++) {
-        uint32_t da = term == 1 ? d0 + 32768 : d0;     // hi, lo, hi
+        uint32_t da = term == 1 ? d0 + DC_HALF : d0;   // hi, lo, hi
         uint32_t qb = term == 2 ? q0 + 16384 : q0;     // hi, hi, lo
 #pragma unroll
         for (int s = 0; s < 8; s++) {
             tc_mma_bf16 (x.taddr + TC_G_COL,
-                smem_desc_sw128 (da + (s >> 2) * 16384 + (s & 3) * 32, 16, 1024),
+                smem_desc_sw128 (da + (s >> 2) * DC_CHUNK + (s & 3) * 32, 16, 1024),
                 smem_desc_sw128 (qb + s * 2048, 16384, 1024), idesc,
                 (accumulate || term > 0 || s > 0) ? 1u : 0u);
         }
@@ -218,17 +231,17 @@ voxel_slot (const TcArgs& a, const TcCtx& x, int mb)
     s.ly = (v / vx) % vy;
     s.lz = v / (vx * vy);
     s.live = v < a.V;
-    s.vpart = (vl >> 6) * 16384u + (vl & 7) * 2u;
+    s.vpart = (vl >> 6) * (uint32_t) DC_CHUNK + (vl & 7) * 2u;
     s.vunit = (vl & 63) >> 3;
     return s;
 }
 
 // Voxel phase for one M block: thread (quarter q, lane) owns one voxel of
-// every tile in [t_lo, t_hi) (at most 8).  Tiles go four at a time: all four
-// correspondences first, then all gathers (8 corners, fixed value, moving
-// gradient), then the arithmetic, so up to 48 loads per thread are in
-// flight.  Sample indices are clamped inside the moving image even when
-// the sample is rejected, so only the fixed-image load needs a guard.
+// every tile in [t_lo, t_hi).  Tiles go four at a time: the field values
+// come from TMEM, then all four correspondences, then all gathers (8
+// corners, fixed value, moving gradient), then the arithmetic.  Sample
+// indices are clamped inside the moving image even when the sample is
+// rejected, so only the fixed-image load needs a guard.
 template <int GRAD_MODE>
 __device__ __forceinline__ void
 voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
@@ -236,40 +249,42 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
 {
     const BspGeom& g = a.g;
     const int T = a.T;
-    float dv[24];
     const uint32_t lb = x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_D_COL;
-    tmem_ld8x3_wait (lb + x.t_lo, lb + T + x.t_lo, lb + 2 * T + x.t_lo, dv);
     const int fj = g.roi_off[1] + g.vpr[1] * ty + vs.ly;
     const int fk = g.roi_off[2] + g.vpr[2] * tz + vs.lz;
     const bool yz_ok = vs.live && fj < g.roi_off[1] + g.roi_dim[1]
         && fk < g.roi_off[2] + g.roi_dim[2];
+    const int fi0 = g.roi_off[0] + g.vpr[0] * (tx0 + x.t_lo) + vs.lx;
     float pj[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        pj[d] = g.img_origin[d] + fj * g.fstep[3 * d + 1] + fk * g.fstep[3 * d + 2];
+        pj[d] = g.img_origin[d] + fi0 * g.fstep[3 * d] + fj * g.fstep[3 * d + 1]
+            + fk * g.fstep[3 * d + 2];
     }
-    const int frow = g.fdim[0] * (fj + g.fdim[1] * fk);
-    const int fi_end = g.roi_off[0] + g.roi_dim[0];
-    const int fi0 = g.roi_off[0] + g.vpr[0] * (tx0 + x.t_lo) + vs.lx;
+    const float xstep[3] = {g.vpr[0] * g.fstep[0], g.vpr[0] * g.fstep[3],
+        g.vpr[0] * g.fstep[6]};
+    const int frow = g.fdim[0] * (fj + g.fdim[1] * fk) + fi0;
+    const int fi_room = g.roi_off[0] + g.roi_dim[0] - fi0;   // fi - fi0 < room
     const int t_cnt = min (x.t_hi - x.t_lo, g.rdims[0] - tx0 - x.t_lo);
     const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
     uint8_t* dch = x.sm + SM_DC + vs.vpart;
     float scf = 0.f;
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
+    for (int t4 = 0; t4 < x.t_hi - x.t_lo; t4 += 4) {
+        float dv[12];
+        tmem_ld4x3_wait (lb + x.t_lo + t4, lb + T + x.t_lo + t4,
+            lb + 2 * T + x.t_lo + t4, dv);
         bool ok[4];
         int mvf[4], mvr[4];
         float w2[4][3];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const int tt = 4 * h + u;
-            const int fi = fi0 + g.vpr[0] * tt;
-            const float ffi = (float) fi;
-            float fxyz[3] = {fmaf (ffi, g.fstep[0], pj[0]),
-                fmaf (ffi, g.fstep[3], pj[1]), fmaf (ffi, g.fstep[6], pj[2])};
-            float d[3] = {dv[tt], dv[8 + tt], dv[16 + tt]};
+            const int tt = t4 + u;
+            const float ft = (float) tt;
+            float fxyz[3] = {fmaf (ft, xstep[0], pj[0]), fmaf (ft, xstep[1], pj[1]),
+                fmaf (ft, xstep[2], pj[2])};
+            float d[3] = {dv[u], dv[4 + u], dv[8 + u]};
             bool in = locate_fast (g, fxyz, d, mvf[u], mvr[u], w2[u]);
-            ok[u] = in && yz_ok && tt < t_cnt && fi < fi_end;
+            ok[u] = in && yz_ok && tt < t_cnt && g.vpr[0] * tt < fi_room;
         }
         float cr[4][8], fv[4], gx[4], gy[4], gz[4];
 #pragma unroll
@@ -283,7 +298,7 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
             cr[u][5] = __ldg (mp + dxym + 1);
             cr[u][6] = __ldg (mp + dxym + dxm);
             cr[u][7] = __ldg (mp + dxym + dxm + 1);
-            fv[u] = ok[u] ? __ldg (a.fimg + frow + fi0 + g.vpr[0] * (4 * h + u)) : 0.f;
+            fv[u] = ok[u] ? __ldg (a.fimg + frow + g.vpr[0] * (t4 + u)) : 0.f;
             if (GRAD_MODE == 0) {
                 const float* gp = a.mgrad + 3 * mvr[u];
                 gx[u] = __ldg (gp + 0);
@@ -293,7 +308,7 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const int t = x.t_lo + 4 * h + u;
+            const int t = x.t_lo + t4 + u;
             float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
             if (ok[u]) {
                 const float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
@@ -308,60 +323,73 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
                 }
             }
             if (t < x.t_hi) {
-                // rows r = 32c + t: (r >> 3) * 1024 = 4096 c + (t >> 3) * 1024
-                const uint32_t o = (t >> 3) * 1024u + (t & 7) * 128u
+                // row r = 8 (3 (t >> 3) + c) + (t & 7)
+                const uint32_t o = (3 * (t >> 3)) * 1024u + (t & 7) * 128u
                     + ((vs.vunit ^ (uint32_t) (t & 7)) << 4);
                 unsigned short hh, ll;
                 split_bf16 (dc0, hh, ll);
                 *(unsigned short*) (dch + o) = hh;
-                *(unsigned short*) (dch + 32768 + o) = ll;
+                *(unsigned short*) (dch + DC_HALF + o) = ll;
                 split_bf16 (dc1, hh, ll);
-                *(unsigned short*) (dch + 4096 + o) = hh;
-                *(unsigned short*) (dch + 32768 + 4096 + o) = ll;
+                *(unsigned short*) (dch + 1024 + o) = hh;
+                *(unsigned short*) (dch + DC_HALF + 1024 + o) = ll;
                 split_bf16 (dc2, hh, ll);
-                *(unsigned short*) (dch + 8192 + o) = hh;
-                *(unsigned short*) (dch + 32768 + 8192 + o) = ll;
+                *(unsigned short*) (dch + 2048 + o) = hh;
+                *(unsigned short*) (dch + DC_HALF + 2048 + o) = ll;
             }
         }
     }
     sc += (double) scf;
 }
 
-// G rows (c, t) = 32c + t, columns = 64 slots.  Warps of quarter q = c read
-// slots [16 tg, 16 tg + 16) (k = tg) and add them to knots (t + i, j, k) in
-// slot order.
+// Copy G (rows r -> (c, t), 64 slot columns) from TMEM to shared memory as
+// Gs[(c*T + t)*64 + slot].  Warp (quarter q, group tg) takes rows 32q..+31,
+// slots 32tg..+31.
 __device__ __forceinline__ void
-readout (const TcArgs& a, const TcCtx& x, float* P)
+dump_g (const TcArgs& a, const TcCtx& x)
 {
-    if (x.q >= 3) return;
-    const int T = a.T, KX = T + 3;
+    const int r = 32 * x.q + x.lane, gi = r >> 3;
+    const int c = gi % 3, t = 8 * (gi / 3) + (r & 7);
+    float* Gs = (float*) (x.sm + SM_DC);
+    const bool live = gi < 12 && t < a.T;
     float gv[16];
-    tmem_ld16_wait (x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_G_COL + 16 * x.tg,
-        gv);
-    // lanes t and t+1 touch the same knot in consecutive i steps:
-    // __syncwarp keeps each (j, i) step complete before the next
-    const int t = x.lane;
-    const bool tv = t < T;
-    float* Pc = P + ((x.q * 4 + x.tg) * 4) * KX;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int h = 0; h < 2; h++) {
+        const int col = 32 * x.tg + 16 * h;
+        tmem_ld16_wait (x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_G_COL + col,
+            gv);
+        if (live) {
+            float4* dst = (float4*) (Gs + (c * a.T + t) * 64 + col);
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            if (tv) Pc[j * KX + t + i] += gv[4 * j + i];
-            __syncwarp ();
+            for (int e = 0; e < 4; e++) {
+                dst[e] = make_float4 (gv[4 * e], gv[4 * e + 1], gv[4 * e + 2],
+                    gv[4 * e + 3]);
+            }
         }
     }
 }
 
+// Every knot (x, j, k) of the batch footprint sums slot (i, j, k) of the
+// tiles t = x - i, i = 0..3 (slot order, as the reference's condense), and
+// writes part[b][c][x + KX (j + 4k)].
 __device__ __forceinline__ void
-write_partials (const TcArgs& a, const TcCtx& x, int b, const float* P)
+gather_knots (const TcArgs& a, const TcCtx& x, int b)
 {
-    const int KX = a.T + 3, KF = 16 * KX;
-    float* dst = a.part + (size_t) b * KF * 3;
-    for (int kk = x.tid; kk < KF; kk += TC_THREADS) {    // kk = x + KX (j + 4k)
-        dst[3 * kk + 0] = P[0 * 16 * KX + kk];
-        dst[3 * kk + 1] = P[1 * 16 * KX + kk];
-        dst[3 * kk + 2] = P[2 * 16 * KX + kk];
+    const int T = a.T, KX = T + 3, KF = 16 * KX;
+    const float* Gs = (const float*) (x.sm + SM_DC);
+    float* dst = a.part + (size_t) b * 3 * KF;
+    for (int row = x.warp; row < 48; row += TC_WARPS) {     // row = 16c + jk
+        const int c = row >> 4, jk = row & 15;
+        const int xx = x.lane;
+        if (xx < KX) {
+            float s = 0.f;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int t = xx - i;
+                if (t >= 0 && t < T) s += Gs[(c * T + t) * 64 + i + 4 * jk];
+            }
+            dst[c * KF + jk * KX + xx] = s;
+        }
     }
 }
 
@@ -383,15 +411,15 @@ sync_wait (const TcArgs& a, const TcCtx& x, uint64_t* bar, uint32_t& ph,
 }
 
 template <int GRAD_MODE>
-__global__ void __launch_bounds__ (TC_THREADS, 1)
+__global__ void __launch_bounds__ (TC_THREADS, 2)
 mse_tc_kernel (TcArgs a)
 {
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t s_bar[2];
     __shared__ uint32_t s_taddr;
     __shared__ int s_abort;
-    __shared__ double sh_v[TC_THREADS / 32];
-    __shared__ int sh_n[TC_THREADS / 32];
+    __shared__ double sh_v[TC_WARPS];
+    __shared__ int sh_n[TC_WARPS];
 
     const BspGeom& g = a.g;
     TcCtx x;
@@ -400,13 +428,10 @@ mse_tc_kernel (TcArgs a)
     x.tid = threadIdx.x;
     x.warp = x.tid >> 5;
     x.lane = x.tid & 31;
-    x.q = x.warp & 3;                  // TMEM lane quarter
-    x.tg = x.warp >> 2;                // tile group
-    x.t_lo = (a.T * x.tg) / 4;         // balanced contiguous tile ranges
-    x.t_hi = (a.T * (x.tg + 1)) / 4;
-    auto pbuf = [&](int i) {
-        return (float*) (x.sm + ((i & 1) ? SM_P2 : SM_P));
-    };
+    x.q = x.warp & 3;                          // TMEM lane quarter
+    x.tg = x.warp >> 2;                        // tile group (2)
+    x.t_lo = (a.T * x.tg) / 2;                 // balanced contiguous ranges
+    x.t_hi = (a.T * (x.tg + 1)) / 2;
 
     if (x.tid == 0) {
         mbar_init (&s_bar[0], 1);
@@ -418,9 +443,10 @@ mse_tc_kernel (TcArgs a)
         tmem_alloc (&s_taddr, TC_TMEM_COLS);
         tmem_relinquish ();
     }
-    // Adjoint rows (c, t >= T) and padding voxels are never written by the
-    // voxel phase; start them at zero.
-    for (int o = x.tid; o < 65536 / 16; o += TC_THREADS) {
+    // Adjoint entries the voxel phase never writes (rows of tiles >= T,
+    // padding voxels) start at zero; the G copy only overwrites the rows of
+    // live tiles, which the voxel phase rewrites every batch.
+    for (int o = x.tid; o < (2 * DC_HALF + DC_TAIL) / 16; o += TC_THREADS) {
         ((uint4*) (x.sm + SM_DC))[o] = make_uint4 (0, 0, 0, 0);
     }
     if (a.mblk == 1) {
@@ -443,14 +469,25 @@ mse_tc_kernel (TcArgs a)
         ty = (b / a.nbx) % g.rdims[1];
         tz = b / (a.nbx * g.rdims[1]);
     };
+    auto finish_batch = [&](int b) {
+        gather_knots (a, x, b);
+        block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
+        if (x.tid == 0) {
+            a.score_part[b] = sc;
+            a.count_part[b] = cnt;
+        }
+        sc = 0.0;
+        cnt = 0;
+        __syncthreads ();
+    };
 
     if (a.mblk == 1 && nb_local > 0) {
         const VoxelSlot vs0 = voxel_slot (a, x, 0);
         // Pipelined: adjoint(b) runs while batch b+1 is staged; forward(b+1)
-        // runs while batch b is read out.
+        // runs while batch b is gathered.
         int tx0, ty, tz;
         coords (blockIdx.x, tx0, ty, tz);
-        stage_batch (a, x, tx0, ty, tz, pbuf (0));
+        stage_batch (a, x, tx0, ty, tz);
         __syncthreads ();
         build_c (a, x);
         fence_proxy_async_smem ();
@@ -458,7 +495,6 @@ mse_tc_kernel (TcArgs a)
         if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
         for (int i = 0; i < nb_local; i++) {
             const int b = blockIdx.x + i * gridDim.x;
-            float* P = pbuf (i);
             coords (b, tx0, ty, tz);
             if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
             voxel_phase<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
@@ -469,7 +505,7 @@ mse_tc_kernel (TcArgs a)
             if (i + 1 < nb_local) {
                 int nx0, ny, nz;
                 coords (b + gridDim.x, nx0, ny, nz);
-                stage_batch (a, x, nx0, ny, nz, pbuf (i + 1));
+                stage_batch (a, x, nx0, ny, nz);
                 __syncthreads ();
                 build_c (a, x);
                 fence_proxy_async_smem ();
@@ -477,17 +513,10 @@ mse_tc_kernel (TcArgs a)
                 if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
             }
             if (!sync_wait (a, x, &s_bar[1], ph_a, &s_abort, 2)) goto done;
-            readout (a, x, P);
+            dump_g (a, x);
             tc_fence_before ();
             __syncthreads ();
-            write_partials (a, x, b, P);
-            block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
-            if (x.tid == 0) {
-                a.score_part[b] = sc;
-                a.count_part[b] = cnt;
-            }
-            sc = 0.0;
-            cnt = 0;
+            finish_batch (b);
         }
     } else {
         // Serial schedule for tiles of more than 128 voxels: Q is reloaded
@@ -496,8 +525,7 @@ mse_tc_kernel (TcArgs a)
             const int b = blockIdx.x + i * gridDim.x;
             int tx0, ty, tz;
             coords (b, tx0, ty, tz);
-            float* P = pbuf (0);
-            stage_batch (a, x, tx0, ty, tz, P);
+            stage_batch (a, x, tx0, ty, tz);
             __syncthreads ();
             build_c (a, x);
             for (int mb = 0; mb < a.mblk; mb++) {
@@ -517,18 +545,10 @@ mse_tc_kernel (TcArgs a)
                 if (x.tid == 0) issue_adjoint (x, mb > 0, &s_bar[1]);
                 if (!sync_wait (a, x, &s_bar[1], ph_a, &s_abort, 2)) goto done;
             }
-            readout (a, x, P);
+            dump_g (a, x);
             tc_fence_before ();
             __syncthreads ();
-            write_partials (a, x, b, P);
-            block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
-            if (x.tid == 0) {
-                a.score_part[b] = sc;
-                a.count_part[b] = cnt;
-            }
-            sc = 0.0;
-            cnt = 0;
-            __syncthreads ();
+            finish_batch (b);
         }
     }
 
@@ -555,8 +575,7 @@ tc_plan (const BspGeom& g, TcPlan* p, int ctas_per_sm, int sm_count)
     p->smem = SM_TOTAL + 1024;
     p->tmem_cols = TC_TMEM_COLS;
     p->threads = TC_THREADS;
-    p->grid = std::min (p->nbatches, sm_count);
-    (void) ctas_per_sm;
+    p->grid = std::min (p->nbatches, std::max (1, ctas_per_sm) * sm_count);
     return true;
 }
 

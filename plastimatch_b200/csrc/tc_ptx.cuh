@@ -183,6 +183,24 @@ tmem_ld8x3_wait (uint32_t a0, uint32_t a1, uint32_t a2, float* v)
     for (int i = 0; i < 24; i++) v[i] = __uint_as_float (r[i]);
 }
 
+// Three 4-column loads and the wait in one statement.
+__device__ __forceinline__ void
+tmem_ld4x3_wait (uint32_t a0, uint32_t a1, uint32_t a2, float* v)
+{
+    uint32_t r[12];
+    asm volatile (
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%12];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%4, %5, %6, %7}, [%13];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%8, %9, %10, %11}, [%14];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]),
+          "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11])
+        : "r"(a0), "r"(a1), "r"(a2) : "memory");
+#pragma unroll
+    for (int i = 0; i < 12; i++) v[i] = __uint_as_float (r[i]);
+}
+
 __device__ __forceinline__ void
 tmem_ld16_wait (uint32_t taddr, float* v)
 {
