@@ -41,8 +41,10 @@
 
 namespace b200 {
 
-constexpr int TC_THREADS = 256;
+constexpr int TC_THREADS = 256;               // compute warps
 constexpr int TC_WARPS = TC_THREADS / 32;
+constexpr int TC_BLOCK = TC_THREADS + 32;      // + one tensor-core issuing warp
+constexpr int GS_STRIDE = 65;                  // odd: conflict-free G copy
 constexpr int TC_TMAX = 26;          // tiles per batch at most
 constexpr int TC_TMEM_COLS = 256;
 constexpr int TC_D_COL = 0;          // forward accumulator [0, N)
@@ -67,7 +69,7 @@ constexpr int SM_DC = SM_C + SM_C_BYTES;           // DCDV hi, lo (+ tail);
 constexpr int SM_S = SM_DC + 2 * DC_HALF + DC_TAIL; // knot block (float)
 constexpr int SM_S_FLOATS = 3 * 16 * (TC_TMAX + 3);
 constexpr int SM_TOTAL = SM_S + SM_S_FLOATS * 4;
-static_assert (3 * TC_TMAX * 64 * 4 <= 2 * DC_HALF, "G copy fits the DCDV area");
+static_assert (3 * TC_TMAX * GS_STRIDE * 4 <= 2 * DC_HALF, "G copy fits the DCDV area");
 static_assert (3 * TC_TMAX <= 80, "N fits the C area");
 
 struct TcArgs {
@@ -343,8 +345,9 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
 }
 
 // Copy G (rows r -> (c, t), 64 slot columns) from TMEM to shared memory as
-// Gs[(c*T + t)*64 + slot].  Warp (quarter q, group tg) takes rows 32q..+31,
-// slots 32tg..+31.
+// Gs[(c*T + t)*65 + slot] (odd row stride: the per-lane rows land in
+// distinct banks).  Warp (quarter q, group tg) takes rows 32q..+31, slots
+// 32tg..+31.
 __device__ __forceinline__ void
 dump_g (const TcArgs& a, const TcCtx& x)
 {
@@ -359,12 +362,9 @@ dump_g (const TcArgs& a, const TcCtx& x)
         tmem_ld16_wait (x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_G_COL + col,
             gv);
         if (live) {
-            float4* dst = (float4*) (Gs + (c * a.T + t) * 64 + col);
+            float* dst = Gs + (c * a.T + t) * GS_STRIDE + col;
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-                dst[e] = make_float4 (gv[4 * e], gv[4 * e + 1], gv[4 * e + 2],
-                    gv[4 * e + 3]);
-            }
+            for (int e = 0; e < 16; e++) dst[e] = gv[e];
         }
     }
 }
@@ -386,36 +386,113 @@ gather_knots (const TcArgs& a, const TcCtx& x, int b)
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const int t = xx - i;
-                if (t >= 0 && t < T) s += Gs[(c * T + t) * 64 + i + 4 * jk];
+                if (t >= 0 && t < T) s += Gs[(c * T + t) * GS_STRIDE + i + 4 * jk];
             }
             dst[c * KF + jk * KX + xx] = s;
         }
     }
 }
 
-// Thread 0 waits on `bar` (bounded); everyone learns whether it gave up.
-__device__ __forceinline__ bool
-sync_wait (const TcArgs& a, const TcCtx& x, uint64_t* bar, uint32_t& ph,
-    int* s_abort, int code)
+// Compute-warp barrier (named barrier 1 over the 256 compute threads).
+__device__ __forceinline__ void
+cbar ()
 {
-    if (x.tid == 0) {
-        if (!mbar_wait_bounded (bar, ph, TC_WAIT_LIMIT)) {
+    named_bar_sync (1, TC_THREADS);
+}
+
+// Compute warps wait for a tensor-core phase: lane 0 of each warp polls
+// (bounded, and gives up early once another wait has failed), then all
+// compute warps meet, so they leave the batch loop together on failure.
+__device__ __forceinline__ bool
+cwait (const TcArgs& a, const TcCtx& x, uint64_t* bar, uint32_t& ph,
+    volatile int* s_abort, int code)
+{
+    if (x.lane == 0) {
+        bool ok = false;
+        for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
+            if (mbar_try_wait (bar, ph)) { ok = true; break; }
+        }
+        if (!ok) {
             *s_abort = 1;
             atomicExch (a.err, code);
         }
     }
     ph ^= 1;
-    __syncthreads ();
+    __syncwarp ();
+    cbar ();
     tc_fence_after ();
     return *s_abort == 0;
 }
 
+// One arrival per compute warp, after the warp's shared-memory writes are
+// made visible to the tensor cores.
+__device__ __forceinline__ void
+warp_arrive (const TcCtx& x, uint64_t* bar)
+{
+    fence_proxy_async_smem ();
+    tc_fence_before ();
+    __syncwarp ();
+    if (x.lane == 0) mbar_arrive (bar);
+}
+
+// Deterministic sum over the compute warps (fixed tree order).
+__device__ __forceinline__ void
+cblock_sum (double& v, int& n, double* sh_v, int* sh_n, const TcCtx& x)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_down_sync (0xffffffffu, v, o);
+        n += __shfl_down_sync (0xffffffffu, n, o);
+    }
+    if (x.lane == 0) { sh_v[x.warp] = v; sh_n[x.warp] = n; }
+    cbar ();
+    if (x.warp == 0) {
+        v = (x.lane < TC_WARPS) ? sh_v[x.lane] : 0.0;
+        n = (x.lane < TC_WARPS) ? sh_n[x.lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v += __shfl_down_sync (0xffffffffu, v, o);
+            n += __shfl_down_sync (0xffffffffu, n, o);
+        }
+    }
+}
+
+// Tensor-core warp: for every batch and 128-voxel block, wait for the
+// forward operands, issue the forward GEMM, wait for dc/dv, issue the
+// adjoint.  Bounded waits; gives up when a compute wait failed.
+__device__ __forceinline__ void
+mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, uint64_t* bars,
+    volatile int* s_abort)
+{
+    uint32_t ph_c = 0, ph_dc = 0;
+    for (int i = 0; i < nb_local && !*s_abort; i++) {
+        for (int mb = 0; mb < a.mblk; mb++) {
+            bool ok = false;
+            for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
+                if (mbar_try_wait (&bars[0], ph_c)) { ok = true; break; }
+            }
+            if (!ok) { *s_abort = 1; atomicExch (a.err, 3); return; }
+            ph_c ^= 1;
+            issue_forward (a, x, &bars[2]);
+            ok = false;
+            for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
+                if (mbar_try_wait (&bars[1], ph_dc)) { ok = true; break; }
+            }
+            if (!ok) { *s_abort = 1; atomicExch (a.err, 4); return; }
+            ph_dc ^= 1;
+            issue_adjoint (x, mb > 0, &bars[3]);
+        }
+    }
+}
+
 template <int GRAD_MODE>
-__global__ void __launch_bounds__ (TC_THREADS, 2)
+__global__ void __launch_bounds__ (TC_BLOCK, 2)
 mse_tc_kernel (TcArgs a)
 {
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t s_bar[2];
+    // bars: 0 C ready (8 arrivals), 1 dc/dv ready (8), 2 D full (commit),
+    // 3 G full (commit)
+    __shared__ uint64_t s_bar[4];
     __shared__ uint32_t s_taddr;
     __shared__ int s_abort;
     __shared__ double sh_v[TC_WARPS];
@@ -429,133 +506,128 @@ mse_tc_kernel (TcArgs a)
     x.warp = x.tid >> 5;
     x.lane = x.tid & 31;
     x.q = x.warp & 3;                          // TMEM lane quarter
-    x.tg = x.warp >> 2;                        // tile group (2)
+    x.tg = (x.warp >> 2) & 1;                  // tile group (2)
     x.t_lo = (a.T * x.tg) / 2;                 // balanced contiguous ranges
     x.t_hi = (a.T * (x.tg + 1)) / 2;
+    const bool mma_warp = x.warp == TC_WARPS;
 
     if (x.tid == 0) {
-        mbar_init (&s_bar[0], 1);
-        mbar_init (&s_bar[1], 1);
+        mbar_init (&s_bar[0], TC_WARPS);
+        mbar_init (&s_bar[1], TC_WARPS);
+        mbar_init (&s_bar[2], 1);
+        mbar_init (&s_bar[3], 1);
         fence_barrier_init ();
         s_abort = 0;
     }
-    if (x.warp == 0) {
+    if (mma_warp) {
         tmem_alloc (&s_taddr, TC_TMEM_COLS);
         tmem_relinquish ();
-    }
-    // Adjoint entries the voxel phase never writes (rows of tiles >= T,
-    // padding voxels) start at zero; the G copy only overwrites the rows of
-    // live tiles, which the voxel phase rewrites every batch.
-    for (int o = x.tid; o < (2 * DC_HALF + DC_TAIL) / 16; o += TC_THREADS) {
-        ((uint4*) (x.sm + SM_DC))[o] = make_uint4 (0, 0, 0, 0);
-    }
-    if (a.mblk == 1) {
-        for (int o = x.tid; o < 2048; o += TC_THREADS) {
-            ((uint4*) (x.sm + SM_Q))[o] = a.qimg[o];
+    } else {
+        // Adjoint entries the voxel phase never writes (rows of tiles >= T)
+        // only feed G rows that are never read; start them at zero anyway.
+        for (int o = x.tid; o < (2 * DC_HALF + DC_TAIL) / 16; o += TC_THREADS) {
+            ((uint4*) (x.sm + SM_DC))[o] = make_uint4 (0, 0, 0, 0);
+        }
+        if (a.mblk == 1) {
+            for (int o = x.tid; o < 2048; o += TC_THREADS) {
+                ((uint4*) (x.sm + SM_Q))[o] = a.qimg[o];
+            }
         }
     }
     tc_fence_before ();
     __syncthreads ();
     tc_fence_after ();
     x.taddr = s_taddr;
-    uint32_t ph_f = 0, ph_a = 0;
-    double sc = 0.0;
-    int cnt = 0;
     const int nb_local = (a.nbatches - (int) blockIdx.x + (int) gridDim.x - 1)
         / (int) gridDim.x;
+    volatile int* abort_flag = &s_abort;
 
-    auto coords = [&](int b, int& tx0, int& ty, int& tz) {
-        tx0 = (b % a.nbx) * a.T;
-        ty = (b / a.nbx) % g.rdims[1];
-        tz = b / (a.nbx * g.rdims[1]);
-    };
-    auto finish_batch = [&](int b) {
-        gather_knots (a, x, b);
-        block_sum<TC_THREADS> (sc, cnt, sh_v, sh_n);
-        if (x.tid == 0) {
-            a.score_part[b] = sc;
-            a.count_part[b] = cnt;
-        }
-        sc = 0.0;
-        cnt = 0;
-        __syncthreads ();
-    };
-
-    if (a.mblk == 1 && nb_local > 0) {
-        const VoxelSlot vs0 = voxel_slot (a, x, 0);
-        // Pipelined: adjoint(b) runs while batch b+1 is staged; forward(b+1)
-        // runs while batch b is gathered.
-        int tx0, ty, tz;
-        coords (blockIdx.x, tx0, ty, tz);
-        stage_batch (a, x, tx0, ty, tz);
-        __syncthreads ();
-        build_c (a, x);
-        fence_proxy_async_smem ();
-        __syncthreads ();
-        if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
-        for (int i = 0; i < nb_local; i++) {
-            const int b = blockIdx.x + i * gridDim.x;
-            coords (b, tx0, ty, tz);
-            if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
-            voxel_phase<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
-            tc_fence_before ();
-            fence_proxy_async_smem ();
-            __syncthreads ();
-            if (x.tid == 0) issue_adjoint (x, false, &s_bar[1]);
-            if (i + 1 < nb_local) {
-                int nx0, ny, nz;
-                coords (b + gridDim.x, nx0, ny, nz);
-                stage_batch (a, x, nx0, ny, nz);
-                __syncthreads ();
-                build_c (a, x);
-                fence_proxy_async_smem ();
-                __syncthreads ();
-                if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
-            }
-            if (!sync_wait (a, x, &s_bar[1], ph_a, &s_abort, 2)) goto done;
-            dump_g (a, x);
-            tc_fence_before ();
-            __syncthreads ();
-            finish_batch (b);
-        }
+    if (mma_warp) {
+        if (x.lane == 0) mma_loop (a, x, nb_local, s_bar, abort_flag);
+        __syncwarp ();
     } else {
-        // Serial schedule for tiles of more than 128 voxels: Q is reloaded
-        // per 128-voxel block, so batches cannot overlap.
-        for (int i = 0; i < nb_local; i++) {
-            const int b = blockIdx.x + i * gridDim.x;
-            int tx0, ty, tz;
-            coords (b, tx0, ty, tz);
-            stage_batch (a, x, tx0, ty, tz);
-            __syncthreads ();
-            build_c (a, x);
-            for (int mb = 0; mb < a.mblk; mb++) {
-                const uint4* src = a.qimg + (size_t) mb * 2048;
-                for (int o = x.tid; o < 2048; o += TC_THREADS) {
-                    ((uint4*) (x.sm + SM_Q))[o] = src[o];
-                }
-                fence_proxy_async_smem ();
-                __syncthreads ();
-                if (x.tid == 0) issue_forward (a, x, &s_bar[0]);
-                if (!sync_wait (a, x, &s_bar[0], ph_f, &s_abort, 1)) goto done;
-                voxel_phase<GRAD_MODE> (a, x, voxel_slot (a, x, mb), tx0, ty,
-                    tz, sc, cnt);
-                tc_fence_before ();
-                fence_proxy_async_smem ();
-                __syncthreads ();
-                if (x.tid == 0) issue_adjoint (x, mb > 0, &s_bar[1]);
-                if (!sync_wait (a, x, &s_bar[1], ph_a, &s_abort, 2)) goto done;
-            }
+        uint32_t ph_d = 0, ph_g = 0;
+        double sc = 0.0;
+        int cnt = 0;
+        auto coords = [&](int b, int& tx0, int& ty, int& tz) {
+            tx0 = (b % a.nbx) * a.T;
+            ty = (b / a.nbx) % g.rdims[1];
+            tz = b / (a.nbx * g.rdims[1]);
+        };
+        auto finish_batch = [&](int b) {
             dump_g (a, x);
             tc_fence_before ();
-            __syncthreads ();
-            finish_batch (b);
+            cbar ();
+            gather_knots (a, x, b);
+            cblock_sum (sc, cnt, sh_v, sh_n, x);
+            if (x.tid == 0) {
+                a.score_part[b] = sc;
+                a.count_part[b] = cnt;
+            }
+            sc = 0.0;
+            cnt = 0;
+            cbar ();
+        };
+        if (a.mblk == 1 && nb_local > 0) {
+            const VoxelSlot vs0 = voxel_slot (a, x, 0);
+            // Pipelined: the adjoint of batch b runs while batch b+1 is
+            // staged; the forward of b+1 runs while batch b is gathered.
+            int tx0, ty, tz;
+            coords (blockIdx.x, tx0, ty, tz);
+            stage_batch (a, x, tx0, ty, tz);
+            cbar ();
+            build_c (a, x);
+            warp_arrive (x, &s_bar[0]);
+            for (int i = 0; i < nb_local; i++) {
+                const int b = blockIdx.x + i * gridDim.x;
+                coords (b, tx0, ty, tz);
+                if (!cwait (a, x, &s_bar[2], ph_d, abort_flag, 1)) break;
+                voxel_phase<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                warp_arrive (x, &s_bar[1]);
+                if (i + 1 < nb_local) {
+                    int nx0, ny, nz;
+                    coords (b + gridDim.x, nx0, ny, nz);
+                    stage_batch (a, x, nx0, ny, nz);
+                    cbar ();
+                    build_c (a, x);
+                    warp_arrive (x, &s_bar[0]);
+                }
+                if (!cwait (a, x, &s_bar[3], ph_g, abort_flag, 2)) break;
+                finish_batch (b);
+            }
+        } else {
+            // Tiles of more than 128 voxels: Q is reloaded per 128-voxel
+            // block, so batches run one after another.
+            for (int i = 0; i < nb_local; i++) {
+                const int b = blockIdx.x + i * gridDim.x;
+                int tx0, ty, tz;
+                coords (b, tx0, ty, tz);
+                stage_batch (a, x, tx0, ty, tz);
+                cbar ();
+                build_c (a, x);
+                bool ok = true;
+                for (int mb = 0; mb < a.mblk && ok; mb++) {
+                    const uint4* src = a.qimg + (size_t) mb * 2048;
+                    for (int o = x.tid; o < 2048; o += TC_THREADS) {
+                        ((uint4*) (x.sm + SM_Q))[o] = src[o];
+                    }
+                    warp_arrive (x, &s_bar[0]);
+                    ok = cwait (a, x, &s_bar[2], ph_d, abort_flag, 1);
+                    if (!ok) break;
+                    voxel_phase<GRAD_MODE> (a, x, voxel_slot (a, x, mb), tx0,
+                        ty, tz, sc, cnt);
+                    warp_arrive (x, &s_bar[1]);
+                    ok = cwait (a, x, &s_bar[3], ph_g, abort_flag, 2);
+                }
+                if (!ok) break;
+                finish_batch (b);
+            }
         }
     }
 
-done:
     tc_fence_before ();
     __syncthreads ();
-    if (x.warp == 0) {
+    if (mma_warp) {
         tmem_dealloc (x.taddr, TC_TMEM_COLS);
     }
 }
@@ -574,7 +646,7 @@ tc_plan (const BspGeom& g, TcPlan* p, int ctas_per_sm, int sm_count)
     p->nbatches = nb_row * g.rdims[1] * g.rdims[2];
     p->smem = SM_TOTAL + 1024;
     p->tmem_cols = TC_TMEM_COLS;
-    p->threads = TC_THREADS;
+    p->threads = TC_BLOCK;
     p->grid = std::min (p->nbatches, std::max (1, ctas_per_sm) * sm_count);
     return true;
 }
@@ -656,12 +728,12 @@ launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
         auto k = mse_tc_kernel<0>;
         cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int) p.smem);
-        k<<<p.grid, TC_THREADS, p.smem, st>>> (a);
+        k<<<p.grid, TC_BLOCK, p.smem, st>>> (a);
     } else {
         auto k = mse_tc_kernel<1>;
         cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int) p.smem);
-        k<<<p.grid, TC_THREADS, p.smem, st>>> (a);
+        k<<<p.grid, TC_BLOCK, p.smem, st>>> (a);
     }
     return cudaGetLastError ();
 }

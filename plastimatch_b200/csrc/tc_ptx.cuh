@@ -49,6 +49,21 @@ mbar_wait_bounded (uint64_t* bar, uint32_t parity, uint32_t limit)
     return false;
 }
 
+// Arrive once on `bar` (count-based phase completion).
+__device__ __forceinline__ void
+mbar_arrive (uint64_t* bar)
+{
+    asm volatile ("mbarrier.arrive.shared::cta.b64 _, [%0];"
+        :: "r"(smem_addr (bar)) : "memory");
+}
+
+// Named barrier over `nthreads` threads (a multiple of 32).
+__device__ __forceinline__ void
+named_bar_sync (int id, int nthreads)
+{
+    asm volatile ("bar.sync %0, %1;" :: "r"(id), "r"(nthreads) : "memory");
+}
+
 __device__ __forceinline__ void
 fence_barrier_init ()
 {
