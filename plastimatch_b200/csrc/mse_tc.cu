@@ -102,6 +102,13 @@ struct TcCtx {
     int tid, warp, lane, q, tg, t_lo, t_hi;
 };
 
+// Compute-warp barrier (named barrier 1 over the 256 compute threads).
+__device__ __forceinline__ void
+cbar ()
+{
+    named_bar_sync (1, TC_THREADS);
+}
+
 // Knot block S[c][k][j][x] of batch (tx0, ty, tz).  Warp w covers knot
 // rows jk = w, w + 8 (jk = j + 4k), lane x and x + 32.
 __device__ __forceinline__ void
@@ -344,6 +351,175 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
     sc += (double) scf;
 }
 
+// Voxel phase in x-line order (tiles of at most 128 voxels).  The batch is
+// done in two rounds of at most 13 tiles.  In each round the compute warps
+// first copy the field values D from TMEM (lane = voxel of a tile) into
+// Dt[c][rho * W + x] in the idle C area, where rho = ly + vy lz is the row
+// of the tile and x = vx * tile + lx runs along the whole round (W = vx *
+// tiles); then thread s of the round takes sample s = rho * W + x, so a
+// warp's 32 lanes are 32 consecutive x of one (or two) rows: every gather
+// touches one or two cache lines and the fixed image is read coalesced.
+template <int GRAD_MODE>
+__device__ __forceinline__ void
+voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
+    int tx0, int ty, int tz, double& sc, int& cnt)
+{
+    const BspGeom& g = a.g;
+    const int T = a.T;
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int nrho = vy * vz;
+    const float inv_vx = 1.f / (float) vx, inv_vy = 1.f / (float) vy;
+    const int T0 = (T + 1) >> 1;                   // tiles of round 0
+    float* Dt = (float*) (x.sm + SM_C);
+    const uint32_t lb = x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_D_COL;
+    const int rho_v = vs.ly + vy * vs.lz;           // this lane's tile row
+    const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
+    const int fi_base = g.roi_off[0] + vx * tx0;
+    const int fj_base = g.roi_off[1] + vy * ty;
+    const int fk_base = g.roi_off[2] + vz * tz;
+    const int fi_end = g.roi_off[0] + g.roi_dim[0];
+    const int fj_end = g.roi_off[1] + g.roi_dim[1];
+    const int fk_end = g.roi_off[2] + g.roi_dim[2];
+    const int tx_room = g.rdims[0] - tx0;          // live tiles of the batch
+    uint8_t* dch = x.sm + SM_DC;
+    float scf = 0.f;
+
+    // Padding voxels (V..127) carry no samples; their adjoint columns must be
+    // zero in the rows of live tiles (the G copy of the previous batch
+    // overwrote this area, and a non-finite bf16 there times Q = 0 would
+    // still poison the accumulation).
+    const int npad = 128 - a.V;
+    for (int o = x.tid; o < npad * T; o += TC_THREADS) {
+        const int tb = o / npad, v = a.V + (o - tb * npad);
+        uint8_t* p = dch + (v >> 6) * DC_CHUNK + (3 * (tb >> 3)) * 1024
+            + (tb & 7) * 128 + ((((v & 63) >> 3) ^ (tb & 7)) << 4) + (v & 7) * 2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            *(unsigned short*) (p + 1024 * c) = 0;
+            *(unsigned short*) (p + DC_HALF + 1024 * c) = 0;
+        }
+    }
+
+    for (int r = 0; r < 2; r++) {
+        const int rt0 = r * T0;                    // first tile of the round
+        const int Tr = min (T0, T - rt0);
+        if (Tr <= 0) break;
+        const int W = vx * Tr, plane = nrho * W;
+        // 1. D -> Dt: warp group tg copies tiles [tg*h, tg*h + h) of the round
+        {
+            const int h = (Tr + 1) >> 1;
+            const int u0 = x.tg * h, u1 = min (Tr, u0 + h);
+            for (int t4 = u0; t4 < u1; t4 += 4) {
+                float dv[12];
+                tmem_ld4x3_wait (lb + rt0 + t4, lb + T + rt0 + t4,
+                    lb + 2 * T + rt0 + t4, dv);
+                if (vs.live) {
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int tt = t4 + u;
+                        if (tt < u1) {
+                            const int o = rho_v * W + tt * vx + vs.lx;
+                            Dt[o] = dv[u];
+                            Dt[plane + o] = dv[4 + u];
+                            Dt[2 * plane + o] = dv[8 + u];
+                        }
+                    }
+                }
+            }
+        }
+        cbar ();
+        // 2. samples s = tid + 256 k of the round, four at a time
+        const int total = plane;
+        for (int s0 = x.tid; s0 < total; s0 += 4 * TC_THREADS) {
+            bool ok[4];
+            int mvf[4], mvr[4], fidx[4];
+            uint32_t doff[4];
+            float w2[4][3];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int sidx = s0 + u * TC_THREADS;
+                const bool in_round = sidx < total;
+                const int sc_ = in_round ? sidx : 0;
+                const int rho = (int) (((float) sc_ + 0.5f) * (1.f / (float) W));
+                const int xx = sc_ - rho * W;
+                const int tt = (int) (((float) xx + 0.5f) * inv_vx);
+                const int lx = xx - tt * vx;
+                const int lz = (int) (((float) rho + 0.5f) * inv_vy);
+                const int ly = rho - lz * vy;
+                const int fi = fi_base + vx * rt0 + xx;
+                const int fj = fj_base + ly, fk = fk_base + lz;
+                const int tb = rt0 + tt;                  // tile within batch
+                const bool live = in_round && tb < tx_room && fi < fi_end
+                    && fj < fj_end && fk < fk_end;
+                float fxyz[3];
+                fixed_position (g, fi, fj, fk, fxyz);
+                float d[3] = {Dt[sc_], Dt[plane + sc_], Dt[2 * plane + sc_]};
+                bool in = locate_fast (g, fxyz, d, mvf[u], mvr[u], w2[u]);
+                ok[u] = in && live;
+                fidx[u] = fi + g.fdim[0] * (fj + g.fdim[1] * fk);
+                // adjoint operand offset: row r(c, tb), column v
+                const int v = lx + vx * rho;
+                doff[u] = in_round
+                    ? (uint32_t) ((v >> 6) * DC_CHUNK + (3 * (tb >> 3)) * 1024
+                        + (tb & 7) * 128 + ((((v & 63) >> 3) ^ (tb & 7)) << 4)
+                        + (v & 7) * 2)
+                    : 0xffffffffu;
+            }
+            float cr[4][8], fv[4], gx[4], gy[4], gz[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float* mp = a.mimg + mvf[u];
+                cr[u][0] = __ldg (mp);
+                cr[u][1] = __ldg (mp + 1);
+                cr[u][2] = __ldg (mp + dxm);
+                cr[u][3] = __ldg (mp + dxm + 1);
+                cr[u][4] = __ldg (mp + dxym);
+                cr[u][5] = __ldg (mp + dxym + 1);
+                cr[u][6] = __ldg (mp + dxym + dxm);
+                cr[u][7] = __ldg (mp + dxym + dxm + 1);
+                fv[u] = ok[u] ? __ldg (a.fimg + fidx[u]) : 0.f;
+                if (GRAD_MODE == 0) {
+                    const float* gp = a.mgrad + 3 * mvr[u];
+                    gx[u] = __ldg (gp + 0);
+                    gy[u] = __ldg (gp + 1);
+                    gz[u] = __ldg (gp + 2);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
+                if (ok[u]) {
+                    const float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
+                    scf = fmaf (diff, diff, scf);
+                    cnt++;
+                    if (GRAD_MODE == 0) {
+                        dc0 = diff * gx[u]; dc1 = diff * gy[u]; dc2 = diff * gz[u];
+                    } else {
+                        float gr[3];
+                        trilinear_lerp_grad (g, w2[u], cr[u], gr);
+                        dc0 = diff * gr[0]; dc1 = diff * gr[1]; dc2 = diff * gr[2];
+                    }
+                }
+                if (doff[u] != 0xffffffffu) {
+                    uint8_t* p = dch + doff[u];
+                    unsigned short hh, ll;
+                    split_bf16 (dc0, hh, ll);
+                    *(unsigned short*) (p) = hh;
+                    *(unsigned short*) (p + DC_HALF) = ll;
+                    split_bf16 (dc1, hh, ll);
+                    *(unsigned short*) (p + 1024) = hh;
+                    *(unsigned short*) (p + DC_HALF + 1024) = ll;
+                    split_bf16 (dc2, hh, ll);
+                    *(unsigned short*) (p + 2048) = hh;
+                    *(unsigned short*) (p + DC_HALF + 2048) = ll;
+                }
+            }
+        }
+        cbar ();                                   // Dt reused by the next round
+    }
+    sc += (double) scf;
+}
+
 // Copy G (rows r -> (c, t), 64 slot columns) from TMEM to shared memory as
 // Gs[(c*T + t)*65 + slot] (odd row stride: the per-lane rows land in
 // distinct banks).  Warp (quarter q, group tg) takes rows 32q..+31, slots
@@ -391,13 +567,6 @@ gather_knots (const TcArgs& a, const TcCtx& x, int b)
             dst[c * KF + jk * KX + xx] = s;
         }
     }
-}
-
-// Compute-warp barrier (named barrier 1 over the 256 compute threads).
-__device__ __forceinline__ void
-cbar ()
-{
-    named_bar_sync (1, TC_THREADS);
 }
 
 // Compute warps wait for a tensor-core phase: lane 0 of each warp polls
@@ -582,7 +751,7 @@ mse_tc_kernel (TcArgs a)
                 const int b = blockIdx.x + i * gridDim.x;
                 coords (b, tx0, ty, tz);
                 if (!cwait (a, x, &s_bar[2], ph_d, abort_flag, 1)) break;
-                voxel_phase<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                voxel_phase_xline<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
                 warp_arrive (x, &s_bar[1]);
                 if (i + 1 < nb_local) {
                     int nx0, ny, nz;
