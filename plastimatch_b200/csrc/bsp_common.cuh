@@ -123,6 +123,49 @@ locate_fast (const BspGeom& g, const float fxyz[3], const float dxyz[3],
     return in;
 }
 
+// Conversion-free variants for the hot loops: the XU pipe (int <-> float,
+// floor, float -> bf16) is narrow, so the per-sample path uses integer and
+// FMA-pipe arithmetic instead.  The magic constant 2^23 = 8388608 puts an
+// integer-valued float's value in the low mantissa bits.
+
+// (float) i for 0 <= i < 2^23.
+__device__ __forceinline__ float
+i2f_small (int i)
+{
+    return __int_as_float (i + 0x4B000000) - 8388608.f;
+}
+
+// As locate_fast, without XU instructions: floor(max(ma, 0)) comes from an
+// add with round-down to 2^23 (ma is first clamped to [0, 2^22]).  Same
+// results as locate() / li_clamp for every input.
+__device__ __forceinline__ bool
+locate_nx (const BspGeom& g, const float fxyz[3], const float dxyz[3],
+    int& mvf, int& mvr, float w2[3])
+{
+    float t0 = (fxyz[0] + dxyz[0]) - g.morigin[0];
+    float t1 = (fxyz[1] + dxyz[1]) - g.morigin[1];
+    float t2 = (fxyz[2] + dxyz[2]) - g.morigin[2];
+    bool in = true;
+    int f[3], r[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        float ma = t0 * g.mproj[3*d+0] + t1 * g.mproj[3*d+1]
+            + t2 * g.mproj[3*d+2];
+        in = in && (ma > -0.5f) && (ma < g.m_hi[d]);
+        float mc = fminf (fmaxf (ma, 0.f), 4194304.f);
+        float big = __fadd_rd (mc, 8388608.f);            // 2^23 + floor(mc)
+        int fi = min (__float_as_int (big) - 0x4B000000, g.mdim[d] - 2);
+        float fc = fminf (big - 8388608.f, g.m_fmax[d]);
+        float w = __saturatef (ma - fc);
+        w2[d] = w;
+        f[d] = fi;
+        r[d] = fi + (w >= 0.5f ? 1 : 0);
+    }
+    mvf = f[0] + g.mdim[0] * (f[1] + g.mdim[1] * f[2]);
+    mvr = r[0] + g.mdim[0] * (r[1] + g.mdim[1] * r[2]);
+    return in;
+}
+
 // Trilinear value as nested linear interpolation (x, then y, then z).
 __device__ __forceinline__ float
 trilinear_lerp (const float w2[3], const float m[8])

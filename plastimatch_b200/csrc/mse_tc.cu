@@ -95,6 +95,19 @@ split_bf16 (float x, unsigned short& hi, unsigned short& lo)
     lo = __bfloat16_as_ushort (l);
 }
 
+// Split two floats into bf16 hi/lo pairs with packed conversions:
+// hi = bf16(a) | bf16(b) << 16, lo likewise for the remainders.
+__device__ __forceinline__ void
+split_bf16x2 (float a, float b, uint32_t& hi, uint32_t& lo)
+{
+    __nv_bfloat162 h = __floats2bfloat162_rn (a, b);
+    float ha = __uint_as_float ((uint32_t) __bfloat16_as_ushort (h.x) << 16);
+    float hb = __uint_as_float ((uint32_t) __bfloat16_as_ushort (h.y) << 16);
+    __nv_bfloat162 l = __floats2bfloat162_rn (a - ha, b - hb);
+    hi = *(uint32_t*) &h;
+    lo = *(uint32_t*) &l;
+}
+
 struct TcCtx {
     uint8_t* sm;
     uint32_t sm_base;
@@ -368,7 +381,8 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
     const int T = a.T;
     const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
     const int nrho = vy * vz;
-    const float inv_vx = 1.f / (float) vx, inv_vy = 1.f / (float) vy;
+    const unsigned mvx = 0xFFFFFFFFu / (unsigned) vx + 1u;
+    const unsigned mvy = 0xFFFFFFFFu / (unsigned) vy + 1u;
     const int T0 = (T + 1) >> 1;                   // tiles of round 0
     float* Dt = (float*) (x.sm + SM_C);
     const uint32_t lb = x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_D_COL;
@@ -405,6 +419,10 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
         const int Tr = min (T0, T - rt0);
         if (Tr <= 0) break;
         const int W = vx * Tr, plane = nrho * W;
+        // multiply-high reciprocals: floor(n / d) = umulhi(n, ceil(2^32 / d))
+        // exactly for the n < 2^16 and 2 <= d <= 1024 used here (d = 1 is
+        // the identity)
+        const unsigned mW = 0xFFFFFFFFu / (unsigned) W + 1u;
         // 1. D -> Dt: warp group tg copies tiles [tg*h, tg*h + h) of the round
         {
             const int h = (Tr + 1) >> 1;
@@ -440,21 +458,28 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                 const int sidx = s0 + u * TC_THREADS;
                 const bool in_round = sidx < total;
                 const int sc_ = in_round ? sidx : 0;
-                const int rho = (int) (((float) sc_ + 0.5f) * (1.f / (float) W));
+                // exact small-range divisions by multiply-high (no XU)
+                const int rho = W > 1 ? (int) __umulhi ((unsigned) sc_, mW) : sc_;
                 const int xx = sc_ - rho * W;
-                const int tt = (int) (((float) xx + 0.5f) * inv_vx);
+                const int tt = vx > 1 ? (int) __umulhi ((unsigned) xx, mvx) : xx;
                 const int lx = xx - tt * vx;
-                const int lz = (int) (((float) rho + 0.5f) * inv_vy);
+                const int lz = vy > 1 ? (int) __umulhi ((unsigned) rho, mvy) : rho;
                 const int ly = rho - lz * vy;
                 const int fi = fi_base + vx * rt0 + xx;
                 const int fj = fj_base + ly, fk = fk_base + lz;
                 const int tb = rt0 + tt;                  // tile within batch
                 const bool live = in_round && tb < tx_room && fi < fi_end
                     && fj < fj_end && fk < fk_end;
+                const float ffi = i2f_small (fi), ffj = i2f_small (fj);
+                const float ffk = i2f_small (fk);
                 float fxyz[3];
-                fixed_position (g, fi, fj, fk, fxyz);
+#pragma unroll
+                for (int dd = 0; dd < 3; dd++) {
+                    fxyz[dd] = g.img_origin[dd] + ffi * g.fstep[3 * dd]
+                        + ffj * g.fstep[3 * dd + 1] + ffk * g.fstep[3 * dd + 2];
+                }
                 float d[3] = {Dt[sc_], Dt[plane + sc_], Dt[2 * plane + sc_]};
-                bool in = locate_fast (g, fxyz, d, mvf[u], mvr[u], w2[u]);
+                bool in = locate_nx (g, fxyz, d, mvf[u], mvr[u], w2[u]);
                 ok[u] = in && live;
                 fidx[u] = fi + g.fdim[0] * (fj + g.fdim[1] * fk);
                 // adjoint operand offset: row r(c, tb), column v
@@ -502,16 +527,15 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                 }
                 if (doff[u] != 0xffffffffu) {
                     uint8_t* p = dch + doff[u];
-                    unsigned short hh, ll;
-                    split_bf16 (dc0, hh, ll);
-                    *(unsigned short*) (p) = hh;
-                    *(unsigned short*) (p + DC_HALF) = ll;
-                    split_bf16 (dc1, hh, ll);
-                    *(unsigned short*) (p + 1024) = hh;
-                    *(unsigned short*) (p + DC_HALF + 1024) = ll;
-                    split_bf16 (dc2, hh, ll);
-                    *(unsigned short*) (p + 2048) = hh;
-                    *(unsigned short*) (p + DC_HALF + 2048) = ll;
+                    uint32_t h01, l01, h2, l2;
+                    split_bf16x2 (dc0, dc1, h01, l01);
+                    split_bf16x2 (dc2, 0.f, h2, l2);
+                    *(unsigned short*) (p) = (unsigned short) h01;
+                    *(unsigned short*) (p + DC_HALF) = (unsigned short) l01;
+                    *(unsigned short*) (p + 1024) = (unsigned short) (h01 >> 16);
+                    *(unsigned short*) (p + DC_HALF + 1024) = (unsigned short) (l01 >> 16);
+                    *(unsigned short*) (p + 2048) = (unsigned short) h2;
+                    *(unsigned short*) (p + DC_HALF + 2048) = (unsigned short) l2;
                 }
             }
         }
