@@ -92,10 +92,14 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device),
                  f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE,
+                 "-lms", "20"], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the first sample marks the sampler as live before timing starts
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self
@@ -205,7 +209,7 @@ def run_reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--form", default="tc", choices=["tc", "fp32"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])

@@ -1,17 +1,438 @@
-#include "mi.cuh"
+// Mattes mutual information with partial-volume (PVI-8) histograms,
+// flavour g semantics (Plastimatch src/register/bspline_mi.cxx:1505-1750):
+//
+//   set_images  EQSP bin ranges from the image min/max
+//               (bspline_initialize_mi_hist_eqsp, src/register/
+//               joint_histogram.cxx:115-139) and a one-byte bin image per
+//               volume: bin = floor((v - offset) / delta), the reference's
+//               binning arithmetic, evaluated once instead of per access.
+//   pass 1      per voxel: the eight trilinear corner weights are added to
+//               the moving and joint histograms, 1 to the fixed histogram
+//               (Joint_histogram::add_pvi_8, joint_histogram.cxx:423-486).
+//               Each CTA accumulates in shared memory; weights are summed as
+//               64-bit fixed point (2^-32 units), so the result is exact up
+//               to one rounding per weight and independent of the order in
+//               which threads add -- deterministic without float atomics.
+//   score       S = -sum_j j log(N j / (f m)) / N over j > 0.001/bins^2
+//               (mi_hist_score_omp, src/register/bspline_mi.cxx:285-309), and
+//               the per-joint-bin factor log(N j / (f m)) - S used by pass 2
+//               for j > 0.0001.
+//   pass 2      dc/dv = -sum_pv dw_pv (factor) / N, rotated by proj with the
+//               reference's in-place projection (bspline_mi_pvi_8_dc_dv_dcos,
+//               src/register/bspline_mi.txx:9-120), then the tile adjoint.
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
 #include "../../include/plastimatch_b200.h"
+#include "fp32_tile.cuh"
+#include "mi.cuh"
 
 namespace b200 {
-int mi_alloc (MiState* s, const BspGeom&, int bins, int, const TcPlan&,
-    const PartLayout&, int) { s->bins = bins; return 0; }
-void mi_free (MiState*) {}
-int mi_set_images (MiState*, const BspGeom&, const float*, const float*,
-    size_t, size_t, cudaStream_t) { return 0; }
-int mi_run (MiState*, const BspGeom&, int, const TcPlan&, const PartLayout&,
-    const float*, const float*, const float*, const float*, const void*,
-    float*, double*, int*, int*, float*, double*, cudaStream_t, int*)
-{ return B200BSP_E_UNSUPPORTED; }
-int mi_fetch (MiState*, MiResult*, double*, double*, double*, cudaStream_t)
-{ return B200BSP_E_UNSUPPORTED; }
-void mi_finish (MiState*, MiResult*) {}
+
+constexpr float MI_FIX = 4294967296.0f;       // 2^32: one unit of weight
+
+// ---- ranges and bin images -------------------------------------------------
+
+__global__ void
+minmax_kernel (const float* __restrict__ img, long long n, float* out)
+{
+    __shared__ float smn[256], smx[256];
+    float mn = FLT_MAX, mx = -FLT_MAX;
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        float v = img[i];
+        mn = fminf (mn, v);
+        mx = fmaxf (mx, v);
+    }
+    smn[threadIdx.x] = mn;
+    smx[threadIdx.x] = mx;
+    __syncthreads ();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            smn[threadIdx.x] = fminf (smn[threadIdx.x], smn[threadIdx.x + o]);
+            smx[threadIdx.x] = fmaxf (smx[threadIdx.x], smx[threadIdx.x + o]);
+        }
+        __syncthreads ();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * blockIdx.x] = smn[0];
+        out[2 * blockIdx.x + 1] = smx[0];
+    }
 }
+
+__global__ void
+bin_image_kernel (const float* __restrict__ img, long long n, float offset,
+    float delta, int bins, uint8_t* __restrict__ out)
+{
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        // (v - offset) / delta in float, IEEE division, then floor
+        float b = floorf (__fdiv_rn (img[i] - offset, delta));
+        int bi = (int) fminf (fmaxf (b, 0.f), (float) (bins - 1));
+        out[i] = (uint8_t) bi;
+    }
+}
+
+static int
+eqsp_range (const float* d_img, size_t n, int bins, float* d_scratch,
+    float* offset, float* delta, cudaStream_t st)
+{
+    const int blocks = 296;
+    minmax_kernel<<<blocks, 256, 0, st>>> (d_img, (long long) n, d_scratch);
+    std::vector<float> mm (2 * blocks);
+    if (cudaMemcpyAsync (mm.data (), d_scratch, mm.size () * sizeof (float),
+            cudaMemcpyDeviceToHost, st) != cudaSuccess
+        || cudaStreamSynchronize (st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    float mn = FLT_MAX, mx = -FLT_MAX;
+    for (int b = 0; b < blocks; b++) {
+        mn = std::fmin (mn, mm[2 * b]);
+        mx = std::fmax (mx, mm[2 * b + 1]);
+    }
+    // delta = (max - min) / (bins - 1); offset = min - 0.5 * delta
+    *delta = (mx - mn) / (float) (bins - 1);
+    *offset = (float) (mn - 0.5 * (double) *delta);
+    if (!(*delta > 0.f)) {
+        *delta = 1.f;      // constant image: every voxel in bin 0
+    }
+    return B200BSP_OK;
+}
+
+int
+mi_alloc (MiState* s, const BspGeom& g, int bins)
+{
+    s->bins = bins;
+    size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
+    size_t nm = (size_t) g.mdim[0] * g.mdim[1] * g.mdim[2];
+    size_t nh = 2 * bins + bins * bins + 1;
+    if (cudaMalloc (&s->d_fbin, nf) != cudaSuccess
+        || cudaMalloc (&s->d_mbin, nm) != cudaSuccess
+        || cudaMalloc (&s->d_hist, nh * sizeof (unsigned long long)) != cudaSuccess
+        || cudaMalloc (&s->d_histd, nh * sizeof (double)) != cudaSuccess
+        || cudaMalloc (&s->d_lut, bins * bins * sizeof (float)) != cudaSuccess
+        || cudaMalloc (&s->d_nvf, sizeof (float)) != cudaSuccess
+        || cudaMalloc (&s->d_minmax, 2 * 296 * sizeof (float)) != cudaSuccess
+        || cudaMalloc (&s->d_part, (size_t) 64 * 3 * g.ntiles * sizeof (float))
+            != cudaSuccess
+        || cudaMalloc (&s->d_score_part, g.ntiles * sizeof (double)) != cudaSuccess
+        || cudaMalloc (&s->d_count_part, g.ntiles * sizeof (int)) != cudaSuccess
+        || cudaMallocHost (&s->h_histd, nh * sizeof (double)) != cudaSuccess
+        || cudaMallocHost (&s->h_res, sizeof (DevResult)) != cudaSuccess) {
+        cudaGetLastError ();
+        return B200BSP_E_OOM;
+    }
+    return B200BSP_OK;
+}
+
+void
+mi_free (MiState* s)
+{
+    cudaFree (s->d_fbin); cudaFree (s->d_mbin); cudaFree (s->d_hist);
+    cudaFree (s->d_histd); cudaFree (s->d_lut); cudaFree (s->d_nvf);
+    cudaFree (s->d_minmax); cudaFree (s->d_part); cudaFree (s->d_score_part);
+    cudaFree (s->d_count_part);
+    cudaFreeHost (s->h_histd); cudaFreeHost (s->h_res);
+    *s = MiState ();
+}
+
+int
+mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
+    const float* d_moving, size_t nf, size_t nm, cudaStream_t st)
+{
+    int rc = eqsp_range (d_fixed, nf, s->bins, s->d_minmax, &s->f_offset,
+        &s->f_delta, st);
+    if (rc) return rc;
+    rc = eqsp_range (d_moving, nm, s->bins, s->d_minmax, &s->m_offset,
+        &s->m_delta, st);
+    if (rc) return rc;
+    bin_image_kernel<<<1184, 256, 0, st>>> (d_fixed, (long long) nf,
+        s->f_offset, s->f_delta, s->bins, s->d_fbin);
+    bin_image_kernel<<<1184, 256, 0, st>>> (d_moving, (long long) nm,
+        s->m_offset, s->m_delta, s->bins, s->d_mbin);
+    if (cudaGetLastError () != cudaSuccess) return B200BSP_E_CUDA;
+    s->ready = true;
+    return B200BSP_OK;
+}
+
+// ---- pass 1: histograms ----------------------------------------------------
+
+constexpr int MIH_THREADS = 256;
+
+__global__ void __launch_bounds__ (MIH_THREADS)
+mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
+    const float* __restrict__ luts, const uint8_t* __restrict__ fbin,
+    const uint8_t* __restrict__ mbin, int B,
+    unsigned long long* __restrict__ ghist)
+{
+    extern __shared__ unsigned long long hsm[];   // f[B], m[B], j[B*B]
+    __shared__ float sC[192];
+    __shared__ float slut[4 * 3 * 64];
+    const int nh = 2 * B + B * B;
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int V = vx * vy * vz;
+    unsigned long long* hf = hsm;
+    unsigned long long* hm = hsm + B;
+    unsigned long long* hj = hsm + 2 * B;
+    for (int i = threadIdx.x; i < nh; i += MIH_THREADS) hsm[i] = 0ull;
+    for (int o = threadIdx.x; o < 4 * (vx + vy + vz); o += MIH_THREADS) {
+        slut[o] = luts[o];
+    }
+    const float* sbx = slut;
+    const float* sby = slut + 4 * vx;
+    const float* sbz = sby + 4 * vy;
+    const int dx = g.mdim[0], dxy = g.mdim[0] * g.mdim[1];
+    unsigned long long cnt = 0;
+    __syncthreads ();
+    for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+        const int tx = t % g.rdims[0];
+        const int ty = (t / g.rdims[0]) % g.rdims[1];
+        const int tz = t / (g.rdims[0] * g.rdims[1]);
+        for (int o = threadIdx.x; o < 192; o += MIH_THREADS) {
+            int m = o / 3, c = o - 3 * m;
+            int i = m & 3, j = (m >> 2) & 3, k = m >> 4;
+            sC[o] = coeff[3 * ((tz + k) * g.cdims[1] * g.cdims[0]
+                + (ty + j) * g.cdims[0] + (tx + i)) + c];
+        }
+        __syncthreads ();
+        for (int v = threadIdx.x; v < V; v += MIH_THREADS) {
+            int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
+            int fi = g.roi_off[0] + vx * tx + lx;
+            int fj = g.roi_off[1] + vy * ty + ly;
+            int fk = g.roi_off[2] + vz * tz + lz;
+            if (fi >= g.roi_off[0] + g.roi_dim[0]
+                || fj >= g.roi_off[1] + g.roi_dim[1]
+                || fk >= g.roi_off[2] + g.roi_dim[2]) continue;
+            float fxyz[3], d[3] = {0.f, 0.f, 0.f};
+            fixed_position (g, fi, fj, fk, fxyz);
+            int m = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                float C = sbz[lz * 4 + k];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    float Bv = sby[ly * 4 + j] * C;
+#pragma unroll
+                    for (int i = 0; i < 4; i++, m++) {
+                        float A = sbx[lx * 4 + i] * Bv;
+                        d[0] += A * sC[3 * m + 0];
+                        d[1] += A * sC[3 * m + 1];
+                        d[2] += A * sC[3 * m + 2];
+                    }
+                }
+            }
+            Sample s;
+            if (!locate (g, fxyz, d, s)) continue;
+            const float* l1 = s.w1;
+            const float* l2 = s.w2;
+            float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
+                l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2],
+                l1[0] * l1[1] * l2[2], l2[0] * l1[1] * l2[2],
+                l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
+            int nbr[8] = {s.mvf, s.mvf + 1, s.mvf + dx, s.mvf + dx + 1,
+                s.mvf + dxy, s.mvf + dxy + 1, s.mvf + dxy + dx,
+                s.mvf + dxy + dx + 1};
+            int fb = fbin[fi + g.fdim[0] * (fj + g.fdim[1] * fk)];
+            atomicAdd (&hf[fb], 4294967296ull);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                int mb = mbin[nbr[k]];
+                unsigned long long q = __float2ull_rn (w[k] * MI_FIX);
+                atomicAdd (&hm[mb], q);
+                atomicAdd (&hj[fb * B + mb], q);
+            }
+            cnt++;
+        }
+        __syncthreads ();
+    }
+    for (int i = threadIdx.x; i < nh; i += MIH_THREADS) {
+        if (hsm[i]) atomicAdd (&ghist[i], hsm[i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync (0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd (&ghist[nh], cnt);
+}
+
+// ---- score and pass-2 factor table -----------------------------------------
+
+__global__ void __launch_bounds__ (1024)
+mi_score_kernel (const unsigned long long* __restrict__ ghist, int B,
+    double* __restrict__ histd, float* __restrict__ lut,
+    float* __restrict__ nvf, DevResult* __restrict__ res)
+{
+    __shared__ double sh_v[32];
+    __shared__ int sh_n[32];
+    __shared__ float s_score;
+    const int nh = 2 * B + B * B;
+    const double inv = 1.0 / 4294967296.0;
+    for (int i = threadIdx.x; i < nh; i += blockDim.x) {
+        histd[i] = (double) ghist[i] * inv;
+    }
+    __syncthreads ();
+    const long long N = (long long) ghist[nh];
+    const double fnv = (double) N;
+    const double thresh = 0.001 / (B * B);
+    const double* f = histd;
+    const double* m = histd + B;
+    const double* j = histd + 2 * B;
+    double acc = 0.0;
+    for (int jb = threadIdx.x; jb < B * B; jb += blockDim.x) {
+        int mb = jb % B, fb = jb / B;
+        if (j[jb] > thresh) {
+            acc -= j[jb] * (double) logf ((float) (fnv * j[jb] / (m[mb] * f[fb])));
+        }
+    }
+    int dummy = 0;
+    block_sum<1024> (acc, dummy, sh_v, sh_n);
+    if (threadIdx.x == 0) {
+        double S = N > 0 ? acc / fnv : (double) FLT_MAX;
+        res->raw = acc;
+        res->score = S;
+        res->score_f = N > 0 ? (float) S : FLT_MAX;
+        res->num_vox = N;
+        res->error = 0;
+        s_score = res->score_f;
+        *nvf = (float) N;
+    }
+    __syncthreads ();
+    const float num_vox_f = (float) N;
+    for (int jb = threadIdx.x; jb < B * B; jb += blockDim.x) {
+        int mb = jb % B, fb = jb / B;
+        float val = 0.f;
+        if (N > 0 && j[jb] > 0.0001) {
+            val = logf ((float) (((double) num_vox_f * j[jb]) / (f[fb] * m[mb])))
+                - s_score;
+        }
+        lut[jb] = val;
+    }
+}
+
+// ---- pass 2: gradient --------------------------------------------------------
+
+struct MiGradVoxel {
+    static constexpr bool kNeedCorners = false;
+    const uint8_t* fbin;
+    const uint8_t* mbin;
+    const float* lut;
+    const float* nvf;
+    int B;
+    __device__ __forceinline__ bool
+    voxel (const BspGeom& g, int fidx, const Sample& s, const Corners&,
+        float dc[3], double&) const
+    {
+        const float* l1 = s.w1;
+        const float* l2 = s.w2;
+        // derivative of each corner weight along x, y, z (reference order)
+        const float dw[24] = {
+            (-1) * l1[1] * l1[2], l1[0] * (-1) * l1[2], l1[0] * l1[1] * (-1),
+            (+1) * l1[1] * l1[2], l2[0] * (-1) * l1[2], l2[0] * l1[1] * (-1),
+            (-1) * l2[1] * l1[2], l1[0] * (+1) * l1[2], l1[0] * l2[1] * (-1),
+            (+1) * l2[1] * l1[2], l2[0] * (+1) * l1[2], l2[0] * l2[1] * (-1),
+            (-1) * l1[1] * l2[2], l1[0] * (-1) * l2[2], l1[0] * l1[1] * (+1),
+            (+1) * l1[1] * l2[2], l2[0] * (-1) * l2[2], l2[0] * l1[1] * (+1),
+            (-1) * l2[1] * l2[2], l1[0] * (+1) * l2[2], l1[0] * l2[1] * (+1),
+            (+1) * l2[1] * l2[2], l2[0] * (+1) * l2[2], l2[0] * l2[1] * (+1)};
+        const int dx = g.mdim[0], dxy = g.mdim[0] * g.mdim[1];
+        const int nbr[8] = {s.mvf, s.mvf + 1, s.mvf + dx, s.mvf + dx + 1,
+            s.mvf + dxy, s.mvf + dxy + 1, s.mvf + dxy + dx,
+            s.mvf + dxy + dx + 1};
+        const int off = (int) __ldg (fbin + fidx) * B;
+        float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            float f = __ldg (lut + off + __ldg (mbin + nbr[k]));
+            d0 -= dw[3 * k + 0] * f;
+            d1 -= dw[3 * k + 1] * f;
+            d2 -= dw[3 * k + 2] * f;
+        }
+        const float nv = *nvf;
+        d0 = d0 / nv;
+        d1 = d1 / nv;
+        d2 = d2 / nv;
+        // the reference projects in place: each row sees the updated rows above
+        const float* p = g.mproj;
+        d0 = d0 * p[0] + d1 * p[1] + d2 * p[2];
+        d1 = d0 * p[3] + d1 * p[4] + d2 * p[5];
+        d2 = d0 * p[6] + d1 * p[7] + d2 * p[8];
+        dc[0] = d0;
+        dc[1] = d1;
+        dc[2] = d2;
+        return true;
+    }
+};
+
+int
+mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
+    const float* d_luts, DevResult* d_res, float* grad_out,
+    double* grad64_out, cudaStream_t st, int* launches)
+{
+    if (!s->ready) return B200BSP_E_STATE;
+    const int B = s->bins;
+    const int nh = 2 * B + B * B;
+    if (cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
+            st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    size_t hsmem = (size_t) nh * sizeof (unsigned long long);
+    auto hk = mi_hist_kernel;
+    if (hsmem > 48 * 1024) {
+        cudaFuncSetAttribute (hk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) hsmem);
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, 0);
+    int grid = std::min (g.ntiles, 4 * sms);
+    hk<<<grid, MIH_THREADS, hsmem, st>>> (g, d_coeff, d_luts, s->d_fbin,
+        s->d_mbin, B, s->d_hist);
+    mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd, s->d_lut,
+        s->d_nvf, d_res);
+    MiGradVoxel f{s->d_fbin, s->d_mbin, s->d_lut, s->d_nvf, B};
+    if (launch_fp32_tile (g, f, nullptr, d_coeff, d_luts, s->d_part,
+            s->d_score_part, s->d_count_part, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    PartLayout lay;
+    lay.bx = lay.by = lay.bz = 1;
+    lay.nbx = g.rdims[0]; lay.nby = g.rdims[1]; lay.nbz = g.rdims[2];
+    lay.kx = lay.ky = lay.kz = 4;
+    lay.slots = 64;
+    if (launch_gather_grad (g, lay, s->d_part, d_res, 1, grad_out, grad64_out,
+            nullptr, nullptr, nullptr, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    if (launches) *launches += 4;
+    return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+}
+
+int
+mi_fetch (MiState* s, const DevResult* d_res, double* f_hist, double* m_hist,
+    double* j_hist, cudaStream_t st)
+{
+    const int B = s->bins;
+    const int nh = 2 * B + B * B;
+    if (cudaMemcpyAsync (s->h_res, d_res, sizeof (DevResult),
+            cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    if (f_hist || m_hist || j_hist) {
+        if (cudaMemcpyAsync (s->h_histd, s->d_histd, nh * sizeof (double),
+                cudaMemcpyDeviceToHost, st) != cudaSuccess
+            || cudaStreamSynchronize (st) != cudaSuccess) {
+            return B200BSP_E_CUDA;
+        }
+        if (f_hist) memcpy (f_hist, s->h_histd, B * sizeof (double));
+        if (m_hist) memcpy (m_hist, s->h_histd + B, B * sizeof (double));
+        if (j_hist) memcpy (j_hist, s->h_histd + 2 * B, B * B * sizeof (double));
+    }
+    return B200BSP_OK;
+}
+
+void
+mi_finish (MiState* s, MiResult* r)
+{
+    r->score_f = s->h_res->score_f;
+    r->score = s->h_res->score;
+    r->num_vox = s->h_res->num_vox;
+}
+
+} // namespace b200

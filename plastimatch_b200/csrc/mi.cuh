@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -20,27 +21,29 @@ struct MiState {
     int bins = 0;
     bool ready = false;
     float f_offset = 0.f, f_delta = 1.f, m_offset = 0.f, m_delta = 1.f;
-    unsigned long long* d_hist = nullptr;   // fixed-point histograms
-    double* d_histd = nullptr;              // f, m, j histograms (double)
-    float* d_lut = nullptr;                 // dS/dP per joint bin
-    double* d_scal = nullptr;               // score, N
-    double* h_scal = nullptr;
-    double* h_hist = nullptr;
-    float* d_minmax = nullptr;
+    uint8_t* d_fbin = nullptr;                // fixed-image bin per voxel
+    uint8_t* d_mbin = nullptr;                // moving-image bin per voxel
+    unsigned long long* d_hist = nullptr;     // f[B], m[B], j[B*B], N (fixed point)
+    double* d_histd = nullptr;                // f, m, j as doubles
+    float* d_lut = nullptr;                   // dS/dP per joint bin (0 = skip)
+    float* d_nvf = nullptr;                   // num_vox as float
+    float* d_minmax = nullptr;                // per-block min/max scratch
+    float* d_part = nullptr;                  // pass-2 tile partials, 64 slots
+    double* d_score_part = nullptr;
+    int* d_count_part = nullptr;
+    double* h_histd = nullptr;
+    DevResult* h_res = nullptr;
 };
 
-int mi_alloc (MiState* s, const BspGeom& g, int bins, int form,
-    const TcPlan& plan, const PartLayout& lay, int nparts);
+int mi_alloc (MiState* s, const BspGeom& g, int bins);
 void mi_free (MiState* s);
 int mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
     const float* d_moving, size_t nf, size_t nm, cudaStream_t st);
-int mi_run (MiState* s, const BspGeom& g, int form, const TcPlan& plan,
-    const PartLayout& lay, const float* d_fixed, const float* d_moving,
-    const float* d_coeff, const float* d_luts, const void* d_qlut,
-    float* d_part, double* d_score_part, int* d_count_part, int* d_err,
-    float* grad_out, double* grad64_out, cudaStream_t st, int* launches);
-int mi_fetch (MiState* s, MiResult* r, double* f_hist, double* m_hist,
-    double* j_hist, cudaStream_t st);
+int mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
+    const float* d_luts, DevResult* d_res, float* grad_out,
+    double* grad64_out, cudaStream_t st, int* launches);
+int mi_fetch (MiState* s, const DevResult* d_res, double* f_hist,
+    double* m_hist, double* j_hist, cudaStream_t st);
 void mi_finish (MiState* s, MiResult* r);
 
 } // namespace b200

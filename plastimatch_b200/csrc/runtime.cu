@@ -357,9 +357,19 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
         if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
     }
-    if (!rc2) rc2 = mi_alloc (&c->mi, c->geom, o.mi_bins, c->opts.form, c->plan, c->lay,
-        c->nscore_parts);
-    if (!rc2) rc2 = reg_alloc (&c->reg, c->geom);
+    if (!rc2 && mi_alloc (&c->mi, c->geom, o.mi_bins)) {
+        rc2 = fail (c, B200BSP_E_OOM, "MI buffers: out of device memory");
+    }
+    if (!rc2) {
+        // Bspline_xform::grid_spac = vox_per_rgn * |spacing| (float)
+        float gsp[3];
+        for (int d = 0; d < 3; d++) {
+            gsp[d] = (float) g.vpr[d] * std::fabs (c->fixed.spacing[d]);
+        }
+        if (reg_alloc (&c->reg, c->geom, gsp)) {
+            rc2 = fail (c, B200BSP_E_OOM, "regulariser buffers");
+        }
+    }
     if (rc2) {
         g_create_error = c->err;
         free_all (c);
@@ -622,18 +632,27 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     float* grad, int64_t* num_vox, double* f_hist, double* m_hist,
     double* j_hist)
 {
+    if (!c) return B200BSP_E_BADARG;
+    for (int d = 0; d < 3; d++) {
+        if (c->geom.roi_off[d] != 0 || c->geom.roi_dim[d] != c->geom.fdim[d]) {
+            // The reference's histogram pass scans the whole fixed image
+            // while its gradient pass scans the ROI; the two agree only
+            // when the ROI is the whole image.
+            return fail (c, B200BSP_E_UNSUPPORTED,
+                "MI needs the ROI to cover the whole fixed image");
+        }
+    }
     const float* dcoeff = nullptr;
     int rc = begin_eval (c, coeff, &dcoeff);
     if (rc) return rc;
     float* g_dev = is_device_ptr (grad) ? grad : c->d_grad;
-    rc = mi_run (&c->mi, c->geom, c->opts.form, c->plan, c->lay, c->d_fixed,
-        c->d_moving, dcoeff, c->d_luts, c->d_qlut, c->d_part, c->d_score_part,
-        c->d_count_part, c->d_err, g_dev, nullptr, c->stream, &c->last_launches);
+    rc = mi_run (&c->mi, c->geom, dcoeff, c->d_luts, c->d_res, g_dev, nullptr,
+        c->stream, &c->last_launches);
     if (rc) return fail (c, rc, "MI evaluation failed: %s",
         cudaGetErrorString (cudaGetLastError ()));
     mark_main_done (c);
     MiResult mr;
-    rc = mi_fetch (&c->mi, &mr, f_hist, m_hist, j_hist, c->stream);
+    rc = mi_fetch (&c->mi, c->d_res, f_hist, m_hist, j_hist, c->stream);
     if (rc) return fail (c, rc, "MI fetch failed");
     if (grad && g_dev == c->d_grad) {
         CK (cudaMemcpyAsync (grad, c->d_grad, c->num_coeff * sizeof (float),
