@@ -1,9 +1,462 @@
+// Analytic regulariser (Plastimatch src/register/
+// bspline_regularize_analytic.cxx:166-337 and 637-1059, implementation 'c'):
+// S = sum over tiles and terms of c^T V c with 32 weighted 64x64 matrices V
+// per tile, and dS/dc condensed per knot.
+//
+// Every V is a Kronecker product X (x) Y (x) Z of three 4x4 one-dimensional
+// integrals (get_Vmatrix, :282-337): X, built from grid spacing 0, acts on
+// the tile's z knot digit, Y on the y digit and Z, built from grid
+// spacing 2, on the x digit.  The tiles form a full Cartesian product, so
+// the sum of the tile operators over the grid is again a Kronecker product
+// of three banded (7-diagonal) knot-axis operators.  The device applies
+// those separably instead of forming 64x64 matrices per tile:
+//   pass 1  knot-x bands applied to each coefficient component
+//   pass 2  knot-y bands applied to the pass-1 fields
+//   pass 3  weighted knot-z bands, summed into the nine outputs below; the
+//           gradient and the per-knot score follow, and the score is
+//           reduced per block in a fixed order.
+// Outputs of pass 3 (input component in brackets):
+//   Dx[x] Dy[y] Dz[z]   same-component terms: V0..V8, V21..V31 on every
+//                       component, V15..V20 on the components the elastic
+//                       group gives them (region_smoothness_elastic_omp,
+//                       :516-600)
+//   Cxy[x] Cxz[x] Cyx[y] Cyz[y] Czx[z] Czy[z]   the elastic cross terms
+//                       (V9+V10, V11+V12, V13+V14)
+//   grad_x = 2 Dx + Cyx + Czx, grad_y = 2 Dy + Cxy + Czy,
+//   grad_z = 2 Dz + Cxz + Cyz,
+//   S = sum over knots of cx Dx + cy Dy + cz Dz + cy Cxy + cz Cxz + cz Cyz.
+// All arithmetic is double; the gradient is added into the float gradient
+// once per knot component.
+#include <cstring>
+#include <map>
+
 #include "regularize.cuh"
 
 namespace b200 {
-int reg_alloc (RegState*, const BspGeom&) { return 0; }
-void reg_free (RegState*) {}
-int reg_run (RegState*, const BspGeom&, const b200bsp_reg_parms*,
-    const float*, float*, cudaStream_t) { return B200BSP_E_UNSUPPORTED; }
-int reg_fetch (RegState*, double*, cudaStream_t) { return B200BSP_E_UNSUPPORTED; }
+
+constexpr int REG_THREADS = 256;
+
+// ---- one-dimensional integrals (host, double) ---------------------------------
+
+// Uniform cubic B-spline pieces in power form: row j holds the coefficients
+// of 1, u, u^2, u^3 of the basis function that weights knot j of a tile.
+static const double BSPL[16] = {
+    1.0 / 6.0, -1.0 / 2.0, 1.0 / 2.0, -1.0 / 6.0,
+    2.0 / 3.0, 0.0, -1.0, 1.0 / 2.0,
+    1.0 / 6.0, 1.0 / 2.0, 1.0 / 2.0, -1.0 / 2.0,
+    0.0, 0.0, 0.0, 1.0 / 6.0};
+
+// Polynomial coefficients of derivative `order` of the four pieces, in the
+// physical coordinate (u / grid spacing).
+static void
+pieces (double out[16], double gs, int order)
+{
+    double r = 1.0 / gs;
+    double scale[4] = {1.0, r, r * r, r * r * r};
+    for (int j = 0; j < 4; j++) {
+        for (int p = 0; p < 4; p++) {
+            // d^order/dx^order of x^p = p!/(p-order)! x^(p-order)
+            double v = 0.0;
+            int q = p - order;                 // resulting power
+            if (q >= 0) {
+                double f = 1.0;
+                for (int m = p; m > q; m--) f *= m;
+                v = BSPL[4 * j + p] * scale[p] * f;
+            }
+            // stored at the power it multiplies after differentiation
+            if (q >= 0) out[4 * j + q] = v;
+        }
+        for (int q = 4 - order; q < 4; q++) out[4 * j + q] = 0.0;
+    }
 }
+
+// F[j][i] = integral over [0, gs] of piece_j^(p) * piece_i^(q).
+static void
+integral (double F[16], const double P[16], const double Qm[16], double gs)
+{
+    double I[7];
+    double g = gs;
+    for (int n = 0; n < 7; n++) {
+        I[n] = g / (n + 1);
+        g *= gs;
+    }
+    for (int j = 0; j < 4; j++) {
+        for (int i = 0; i < 4; i++) {
+            double s = 0.0;
+            for (int a = 0; a < 4; a++) {
+                for (int b = 0; b < 4; b++) {
+                    s += P[4 * j + a] * Qm[4 * i + b] * I[a + b];
+                }
+            }
+            F[4 * j + i] = s;
+        }
+    }
+}
+
+// Derivative-order pairs (row, column) of the factors the 32 terms use.
+static const int PAIRS[6][2] = {{0, 0}, {1, 1}, {2, 2}, {3, 3}, {1, 0}, {0, 1}};
+
+static int
+pair_index (int a, int b)
+{
+    for (int k = 0; k < 6; k++) {
+        if (PAIRS[k][0] == a && PAIRS[k][1] == b) return k;
+    }
+    return -1;
+}
+
+// Banded knot-axis operator: sum over tiles t of F[k - t][k' - t]; stored as
+// band[k][d + 3] = G[k][k + d].
+static void
+assemble (double* band, const double F[16], int n, int ntiles)
+{
+    for (int k = 0; k < n; k++) {
+        for (int d = -3; d <= 3; d++) {
+            double s = 0.0;
+            int k2 = k + d;
+            if (k2 >= 0 && k2 < n) {
+                int t0 = std::max (0, std::max (k - 3, k2 - 3));
+                int t1 = std::min (ntiles - 1, std::min (k, k2));
+                for (int t = t0; t <= t1; t++) s += F[4 * (k - t) + (k2 - t)];
+            }
+            band[7 * k + d + 3] = s;
+        }
+    }
+}
+
+// The 32 terms of analytic_init (:637-940): derivative orders of the X
+// (knot z), Y (knot y) and Z (knot x) factors and the weight selector.
+struct RegTerm { int xa, xb, ya, yb, za, zb, w; };
+static const RegTerm TERMS[32] = {
+    {2, 2, 0, 0, 0, 0, 0}, {0, 0, 2, 2, 0, 0, 0}, {0, 0, 0, 0, 2, 2, 0},
+    {1, 1, 1, 1, 0, 0, 1}, {1, 1, 0, 0, 1, 1, 1}, {0, 0, 1, 1, 1, 1, 1},
+    {1, 1, 0, 0, 0, 0, 2}, {0, 0, 1, 1, 0, 0, 2}, {0, 0, 0, 0, 1, 1, 2},
+    {1, 0, 0, 1, 0, 0, 3}, {0, 1, 1, 0, 0, 0, 4}, {1, 0, 0, 0, 0, 1, 3},
+    {0, 1, 0, 0, 1, 0, 4}, {0, 0, 1, 0, 0, 1, 3}, {0, 0, 0, 1, 1, 0, 4},
+    {1, 1, 0, 0, 0, 0, 5}, {0, 0, 1, 1, 0, 0, 5}, {0, 0, 0, 0, 1, 1, 5},
+    {1, 1, 0, 0, 0, 0, 6}, {0, 0, 1, 1, 0, 0, 6}, {0, 0, 0, 0, 1, 1, 6},
+    {0, 0, 0, 0, 0, 0, 7},
+    {3, 3, 0, 0, 0, 0, 8}, {0, 0, 3, 3, 0, 0, 8}, {0, 0, 0, 0, 3, 3, 8},
+    {2, 2, 1, 1, 0, 0, 8}, {2, 2, 0, 0, 1, 1, 8}, {0, 0, 2, 2, 1, 1, 8},
+    {1, 1, 2, 2, 0, 0, 8}, {1, 1, 0, 0, 2, 2, 8}, {0, 0, 1, 1, 2, 2, 8},
+    {1, 1, 1, 1, 1, 1, 8},
+};
+
+// Term weights, in float arithmetic as the reference scales its V matrices.
+static float
+term_weight (int sel, const b200bsp_reg_parms* p)
+{
+    float lem = p->linear_elastic_multiplier;
+    switch (sel) {
+    case 0: return p->curvature_penalty;
+    case 1: return p->curvature_penalty * p->curvature_mixed_weight;
+    case 2: return p->diffusion_penalty;
+    case 3: return p->lame_coefficient_1 * lem;
+    case 4: return p->lame_coefficient_2 * lem;
+    case 5: return lem * (2 * p->lame_coefficient_1 + p->lame_coefficient_2) / 2;
+    case 6: return lem * (p->lame_coefficient_1) / 2;
+    case 7: return p->total_displacement_penalty;
+    case 8: return p->third_order_penalty;
+    }
+    return 0.f;
+}
+
+// Outputs of pass 3 and the coefficient component each one reads.
+enum { O_DX, O_DY, O_DZ, O_CXY, O_CXZ, O_CYX, O_CYZ, O_CZX, O_CZY, O_N };
+static const int OUT_COMP[O_N] = {0, 1, 2, 0, 0, 1, 1, 2, 2};
+
+// Which outputs term t feeds.
+static int
+term_outputs (int t, int out[3])
+{
+    if (t <= 8 || t >= 21) {
+        out[0] = O_DX; out[1] = O_DY; out[2] = O_DZ;
+        return 3;
+    }
+    switch (t) {
+    case 9: case 10: out[0] = O_CXY; out[1] = O_CYX; return 2;
+    case 11: case 12: out[0] = O_CXZ; out[1] = O_CZX; return 2;
+    case 13: case 14: out[0] = O_CYZ; out[1] = O_CZY; return 2;
+    case 15: out[0] = O_DX; return 1;
+    case 16: out[0] = O_DY; return 1;
+    case 17: out[0] = O_DZ; return 1;
+    case 18: out[0] = O_DY; out[1] = O_DZ; return 2;
+    case 19: out[0] = O_DX; out[1] = O_DZ; return 2;
+    case 20: out[0] = O_DX; out[1] = O_DY; return 2;
+    }
+    return 0;
+}
+
+// ---- device passes ----------------------------------------------------------
+
+__global__ void __launch_bounds__ (REG_THREADS)
+reg_pass_x (RegPlan plan, int cx, int nk, const double* __restrict__ gx,
+    const float* __restrict__ coeff, double* __restrict__ t1)
+{
+    int knot = blockIdx.x * REG_THREADS + threadIdx.x;
+    if (knot >= nk) return;
+    int kx = knot % cx;
+    for (int s = 0; s < plan.n1; s++) {
+        int c = plan.t1_c[s];
+        const double* band = gx + ((size_t) plan.t1_xf[s] * cx + kx) * 7;
+        double acc = 0.0;
+#pragma unroll
+        for (int d = -3; d <= 3; d++) {
+            if (kx + d >= 0 && kx + d < cx) {
+                acc += band[d + 3] * (double) coeff[3 * (knot + d) + c];
+            }
+        }
+        t1[(size_t) s * nk + knot] = acc;
+    }
+}
+
+__global__ void __launch_bounds__ (REG_THREADS)
+reg_pass_y (RegPlan plan, int cx, int cy, int nk,
+    const double* __restrict__ gy, const double* __restrict__ t1,
+    double* __restrict__ t2)
+{
+    int knot = blockIdx.x * REG_THREADS + threadIdx.x;
+    if (knot >= nk) return;
+    int ky = (knot / cx) % cy;
+    for (int s = 0; s < plan.n2; s++) {
+        const double* src = t1 + (size_t) plan.t2_src[s] * nk;
+        const double* band = gy + ((size_t) plan.t2_yf[s] * cy + ky) * 7;
+        double acc = 0.0;
+#pragma unroll
+        for (int d = -3; d <= 3; d++) {
+            if (ky + d >= 0 && ky + d < cy) {
+                acc += band[d + 3] * src[knot + d * cx];
+            }
+        }
+        t2[(size_t) s * nk + knot] = acc;
+    }
+}
+
+__global__ void __launch_bounds__ (REG_THREADS)
+reg_pass_z (RegPlan plan, int cx, int cy, int cz, int nk,
+    const double* __restrict__ hz, const double* __restrict__ t2,
+    const float* __restrict__ coeff, float* __restrict__ grad,
+    double* __restrict__ part)
+{
+    __shared__ double sh_v[REG_THREADS / 32];
+    __shared__ int sh_n[REG_THREADS / 32];
+    int knot = blockIdx.x * REG_THREADS + threadIdx.x;
+    double S = 0.0;
+    if (knot < nk) {
+        int kz = knot / (cx * cy);
+        int plane = cx * cy;
+        double out[O_N];
+#pragma unroll
+        for (int o = 0; o < O_N; o++) out[o] = 0.0;
+        for (int e = 0; e < plan.ne; e++) {
+            const double* src = t2 + (size_t) plan.e_src[e] * nk;
+            const double* band = hz + ((size_t) e * cz + kz) * 7;
+            double acc = 0.0;
+#pragma unroll
+            for (int d = -3; d <= 3; d++) {
+                if (kz + d >= 0 && kz + d < cz) {
+                    acc += band[d + 3] * src[knot + d * plane];
+                }
+            }
+            // out[e_out] += acc, with a compile-time index
+#pragma unroll
+            for (int o = 0; o < O_N; o++) {
+                if (plan.e_out[e] == o) out[o] += acc;
+            }
+        }
+        double c0 = coeff[3 * knot + 0], c1 = coeff[3 * knot + 1];
+        double c2 = coeff[3 * knot + 2];
+        S = c0 * out[O_DX] + c1 * out[O_DY] + c2 * out[O_DZ]
+            + c1 * out[O_CXY] + c2 * out[O_CXZ] + c2 * out[O_CYZ];
+        if (grad) {
+            double g0 = 2.0 * out[O_DX] + out[O_CYX] + out[O_CZX];
+            double g1 = 2.0 * out[O_DY] + out[O_CXY] + out[O_CZY];
+            double g2 = 2.0 * out[O_DZ] + out[O_CXZ] + out[O_CYZ];
+            grad[3 * knot + 0] = (float) ((double) grad[3 * knot + 0] + g0);
+            grad[3 * knot + 1] = (float) ((double) grad[3 * knot + 1] + g1);
+            grad[3 * knot + 2] = (float) ((double) grad[3 * knot + 2] + g2);
+        }
+    }
+    int dummy = 0;
+    block_sum<REG_THREADS> (S, dummy, sh_v, sh_n);
+    if (threadIdx.x == 0) part[blockIdx.x] = S;
+}
+
+__global__ void __launch_bounds__ (1024)
+reg_reduce (const double* __restrict__ part, int n, double* __restrict__ out)
+{
+    __shared__ double sh_v[32];
+    __shared__ int sh_n[32];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += 1024) v += part[i];
+    int dummy = 0;
+    block_sum<1024> (v, dummy, sh_v, sh_n);
+    if (threadIdx.x == 0) *out = v;
+}
+
+// ---- host -------------------------------------------------------------------
+
+int
+reg_alloc (RegState* s, const BspGeom& g, const float grid_spac[3])
+{
+    for (int d = 0; d < 3; d++) {
+        s->cdims[d] = g.cdims[d];
+        s->gs[d] = (double) grid_spac[d];
+    }
+    s->nknots = g.nknots;
+    s->nblocks = (g.nknots + REG_THREADS - 1) / REG_THREADS;
+    const int cx = g.cdims[0], cy = g.cdims[1], cz = g.cdims[2];
+    if (cudaMalloc (&s->d_gx, sizeof (double) * 6 * cx * 7) != cudaSuccess
+        || cudaMalloc (&s->d_gy, sizeof (double) * 6 * cy * 7) != cudaSuccess
+        || cudaMalloc (&s->d_hz, sizeof (double) * REG_E_MAX * cz * 7) != cudaSuccess
+        || cudaMalloc (&s->d_t1, sizeof (double) * REG_T1_MAX * (size_t) g.nknots)
+            != cudaSuccess
+        || cudaMalloc (&s->d_t2, sizeof (double) * REG_T2_MAX * (size_t) g.nknots)
+            != cudaSuccess
+        || cudaMalloc (&s->d_part, sizeof (double) * s->nblocks) != cudaSuccess
+        || cudaMalloc (&s->d_score, sizeof (double)) != cudaSuccess
+        || cudaMallocHost (&s->h_score, sizeof (double)) != cudaSuccess) {
+        cudaGetLastError ();
+        return B200BSP_E_OOM;
+    }
+    // Unweighted knot-axis bands for the six factor kinds.  Knot x takes
+    // the Z factor (grid spacing 2), knot y the Y factor (spacing 1), knot
+    // z the X factor (spacing 0).
+    std::vector<double> gxh (6 * cx * 7), gyh (6 * cy * 7);
+    s->gz_host.assign (6 * cz * 7, 0.0);
+    for (int f = 0; f < 6; f++) {
+        double P[16], Qm[16], F[16];
+        pieces (P, s->gs[2], PAIRS[f][0]);
+        pieces (Qm, s->gs[2], PAIRS[f][1]);
+        integral (F, P, Qm, s->gs[2]);
+        assemble (&gxh[f * cx * 7], F, cx, g.rdims[0]);
+        pieces (P, s->gs[1], PAIRS[f][0]);
+        pieces (Qm, s->gs[1], PAIRS[f][1]);
+        integral (F, P, Qm, s->gs[1]);
+        assemble (&gyh[f * cy * 7], F, cy, g.rdims[1]);
+        pieces (P, s->gs[0], PAIRS[f][0]);
+        pieces (Qm, s->gs[0], PAIRS[f][1]);
+        integral (F, P, Qm, s->gs[0]);
+        assemble (&s->gz_host[f * cz * 7], F, cz, g.rdims[2]);
+    }
+    if (cudaMemcpy (s->d_gx, gxh.data (), gxh.size () * sizeof (double),
+            cudaMemcpyHostToDevice) != cudaSuccess
+        || cudaMemcpy (s->d_gy, gyh.data (), gyh.size () * sizeof (double),
+            cudaMemcpyHostToDevice) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    return B200BSP_OK;
+}
+
+void
+reg_free (RegState* s)
+{
+    cudaFree (s->d_gx); cudaFree (s->d_gy); cudaFree (s->d_hz);
+    cudaFree (s->d_t1); cudaFree (s->d_t2); cudaFree (s->d_part);
+    cudaFree (s->d_score); cudaFreeHost (s->h_score);
+    *s = RegState ();
+}
+
+// Build the pass plan and the weighted z bands for one set of weights.
+static int
+reg_prepare (RegState* s, const b200bsp_reg_parms* p, cudaStream_t st)
+{
+    RegPlan plan;
+    memset (&plan, 0, sizeof plan);
+    std::map<int, int> t1_of, t2_of, e_of;       // keys -> slot
+    const int cz = s->cdims[2];
+    std::vector<double> hz;
+    for (int t = 0; t < 32; t++) {
+        const RegTerm& T = TERMS[t];
+        float w = term_weight (T.w, p);
+        if (w == 0.f) continue;
+        int xf = pair_index (T.za, T.zb);        // knot-x factor
+        int yf = pair_index (T.ya, T.yb);        // knot-y factor
+        int zf = pair_index (T.xa, T.xb);        // knot-z factor
+        int outs[3];
+        int no = term_outputs (t, outs);
+        for (int q = 0; q < no; q++) {
+            int o = outs[q], c = OUT_COMP[o];
+            int k1 = c * 8 + xf;
+            if (!t1_of.count (k1)) {
+                int id = plan.n1++;
+                plan.t1_c[id] = (unsigned char) c;
+                plan.t1_xf[id] = (unsigned char) xf;
+                t1_of[k1] = id;
+            }
+            int s1 = t1_of[k1];
+            int k2 = s1 * 8 + yf;
+            if (!t2_of.count (k2)) {
+                int id = plan.n2++;
+                plan.t2_src[id] = (unsigned char) s1;
+                plan.t2_yf[id] = (unsigned char) yf;
+                t2_of[k2] = id;
+            }
+            int s2 = t2_of[k2];
+            int k3 = s2 * 16 + o;
+            if (!e_of.count (k3)) {
+                int id = plan.ne++;
+                plan.e_src[id] = (unsigned char) s2;
+                plan.e_out[id] = (unsigned char) o;
+                e_of[k3] = id;
+                hz.resize ((size_t) plan.ne * cz * 7, 0.0);
+            }
+            double* dst = &hz[(size_t) e_of[k3] * cz * 7];
+            const double* src = &s->gz_host[(size_t) zf * cz * 7];
+            for (int i = 0; i < cz * 7; i++) dst[i] += (double) w * src[i];
+            if (plan.n1 > REG_T1_MAX || plan.n2 > REG_T2_MAX
+                || plan.ne > REG_E_MAX) {
+                return B200BSP_E_UNSUPPORTED;   // cannot happen: 32 terms
+            }
+        }
+    }
+    if (!hz.empty ()
+        && cudaMemcpyAsync (s->d_hz, hz.data (), hz.size () * sizeof (double),
+            cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    // a pageable source is staged before cudaMemcpyAsync returns; the
+    // synchronisation keeps the plan update ordered for every caller
+    if (cudaStreamSynchronize (st) != cudaSuccess) return B200BSP_E_CUDA;
+    s->plan = plan;
+    s->parms = *p;
+    s->have_parms = true;
+    return B200BSP_OK;
+}
+
+int
+reg_run (RegState* s, const BspGeom& g, const b200bsp_reg_parms* p,
+    const float* d_coeff, float* d_grad, cudaStream_t st)
+{
+    if (!s->have_parms || memcmp (&s->parms, p, sizeof *p) != 0) {
+        int rc = reg_prepare (s, p, st);
+        if (rc) return rc;
+    }
+    const int cx = g.cdims[0], cy = g.cdims[1], cz = g.cdims[2];
+    const int nk = g.nknots;
+    const int nb = s->nblocks;
+    if (s->plan.n1) {
+        reg_pass_x<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, nk, s->d_gx,
+            d_coeff, s->d_t1);
+        reg_pass_y<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, cy, nk, s->d_gy,
+            s->d_t1, s->d_t2);
+    }
+    reg_pass_z<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, cy, cz, nk, s->d_hz,
+        s->d_t2, d_coeff, d_grad, s->d_part);
+    reg_reduce<<<1, 1024, 0, st>>> (s->d_part, nb, s->d_score);
+    return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+}
+
+int
+reg_fetch (RegState* s, double* score, cudaStream_t st)
+{
+    if (cudaMemcpyAsync (s->h_score, s->d_score, sizeof (double),
+            cudaMemcpyDeviceToHost, st) != cudaSuccess
+        || cudaStreamSynchronize (st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    *score = *s->h_score;
+    return B200BSP_OK;
+}
+
+} // namespace b200
