@@ -199,6 +199,27 @@ int b200bsp_last_timing (const b200bsp_ctx* ctx, float* ms, int* launches);
 /* Device time of the last evaluation's main tile kernel alone (ms). */
 int b200bsp_last_main_ms (const b200bsp_ctx* ctx, float* ms);
 
+/* Largest tile count b200bsp_score_mse_static accepts (its fixed scratch:
+ * about 6.4 MB of static device memory per device). */
+#define B200BSP_STATIC_MAX_TILES 8192
+
+/* No counterpart in the reference.  MSE score and gradient as
+ * b200bsp_score_mse with the FP32 form, for callers that may not allocate
+ * device memory: no context, no allocation; partial sums live in one
+ * static device array of the library.  All pointers are device memory on
+ * the current device (moving_grad only for B200BSP_MSE_GRAD_NEAREST;
+ * score and num_vox may be NULL); the call is ordered on `stream` and
+ * returns without waiting.  Grids of more than B200BSP_STATIC_MAX_TILES
+ * tiles are rejected (B200BSP_E_UNSUPPORTED).  The first call on each
+ * device looks up the array's address; make it before any stream capture.
+ * Calls whose device work overlaps race on the shared array: issue them on
+ * one stream.  Errors are reported through b200bsp_last_error (NULL). */
+int b200bsp_score_mse_static (const b200bsp_volume* fixed,
+    const b200bsp_volume* moving, const b200bsp_grid* grid, int mse_grad,
+    const float* fixed_img, const float* moving_img, const float* moving_grad,
+    const float* coeff, float* score, float* grad, int64_t* num_vox,
+    void* stream);
+
 /* Text of the last error on this context (or the last create failure when
  * ctx is NULL). */
 const char* b200bsp_last_error (const b200bsp_ctx* ctx);

@@ -99,6 +99,8 @@ _SIGS = {
     "b200bsp_last_timing": (C.c_int, [_VP, _VP, _VP]),
     "b200bsp_last_main_ms": (C.c_int, [_VP, _VP]),
     "b200bsp_last_error": (C.c_char_p, [_VP]),
+    "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
+                                           _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 
@@ -148,6 +150,24 @@ def volume_grad(vol: Volume, device: int = 0) -> np.ndarray:
     _check(lib().b200bsp_volume_grad(C.byref(d), _ptr(vol.img), _ptr(out),
                                      device))
     return out
+
+
+def score_mse_static(fixed: Volume, moving: Volume, grid: BsplineGrid,
+                     fixed_img, moving_img, coeff, grad, score=None,
+                     nvox=None, moving_grad=None, mse_grad: str = "nearest",
+                     stream: int | None = None) -> None:
+    """b200bsp_score_mse_static: MSE score + gradient without a context and
+    without allocating; every buffer is a device tensor the caller owns
+    (grad: num_coeff float32, score: 1 float32, nvox: 1 int64).  Ordered on
+    `stream` (a cudaStream_t handle; None = the legacy default stream)."""
+    fd, md = _vol_desc(fixed), _vol_desc(moving)
+    gd = GridDesc((C.c_int64 * 3)(*grid.roi_offset),
+                  (C.c_int64 * 3)(*grid.roi_dim),
+                  (C.c_int64 * 3)(*grid.vox_per_rgn))
+    _check(lib().b200bsp_score_mse_static(
+        C.byref(fd), C.byref(md), C.byref(gd), MSE_GRAD[mse_grad],
+        _ptr(fixed_img), _ptr(moving_img), _ptr(moving_grad), _ptr(coeff),
+        _ptr(score), _ptr(grad), _ptr(nvox), stream))
 
 
 class Context:

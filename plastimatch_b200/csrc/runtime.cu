@@ -201,6 +201,75 @@ free_all (b200bsp_ctx* c)
     if (c->own_stream) cudaStreamDestroy (c->own_stream);
 }
 
+namespace b200 {
+
+// The checks and geometry of b200bsp_create for the context-free
+// b200bsp_score_mse_static: fills g and the three basis tables (x, y, z
+// back to back, *nlut floats).  Errors go to the no-context error text.
+int
+static_geometry (const b200bsp_volume* fixed, const b200bsp_volume* moving,
+    const b200bsp_grid* grid, BspGeom* out, float* luts, int* nlut)
+{
+    int rc = check_volume (fixed, "fixed");
+    if (rc) return rc;
+    rc = check_volume (moving, "moving");
+    if (rc) return rc;
+    for (int d = 0; d < 3; d++) {
+        if (grid->vox_per_rgn[d] < 1 || grid->vox_per_rgn[d] > 64
+            || grid->roi_dim[d] < 1 || grid->roi_offset[d] < 0
+            || grid->roi_offset[d] + grid->roi_dim[d] > fixed->dim[d]) {
+            return fail (nullptr, B200BSP_E_BADARG,
+                "grid axis %d: need 1 <= vox_per_rgn <= 64 and the ROI "
+                "inside the fixed image", d);
+        }
+    }
+    float finv[9], minv[9];
+    if (!inv3f (finv, fixed->dcos) || !inv3f (minv, moving->dcos)) {
+        return fail (nullptr, B200BSP_E_BADARG,
+            "singular matrix of direction cosines");
+    }
+    BspGeom g;
+    long long ntiles = 1, nknots = 1;
+    for (int d = 0; d < 3; d++) {
+        g.fdim[d] = (int) fixed->dim[d];
+        g.img_origin[d] = fixed->origin[d];
+        g.mdim[d] = (int) moving->dim[d];
+        g.morigin[d] = moving->origin[d];
+        g.minv_spacing[d] = (float) (1.0 / moving->spacing[d]);
+        g.roi_off[d] = (int) grid->roi_offset[d];
+        g.roi_dim[d] = (int) grid->roi_dim[d];
+        g.vpr[d] = (int) grid->vox_per_rgn[d];
+        g.rdims[d] = 1 + (g.roi_dim[d] - 1) / g.vpr[d];
+        g.cdims[d] = g.rdims[d] + 3;
+        g.m_hi[d] = (float) moving->dim[d] - 0.5f;
+        g.m_fmax[d] = (float) (moving->dim[d] - 2);
+        ntiles *= g.rdims[d];
+        nknots *= g.cdims[d];
+    }
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            g.fstep[3*i+j] = fixed->dcos[3*i+j] * fixed->spacing[j];
+            g.mproj[3*i+j] = minv[3*i+j] / moving->spacing[i];
+        }
+    }
+    g.ntiles = (int) ntiles;
+    g.nknots = (int) nknots;
+    basis_lut (luts, g.vpr[0]);
+    basis_lut (luts + 4 * g.vpr[0], g.vpr[1]);
+    basis_lut (luts + 4 * (g.vpr[0] + g.vpr[1]), g.vpr[2]);
+    *nlut = 4 * (g.vpr[0] + g.vpr[1] + g.vpr[2]);
+    *out = g;
+    return B200BSP_OK;
+}
+
+int
+static_fail (int code, const char* msg)
+{
+    return fail (nullptr, code, "%s", msg);
+}
+
+} // namespace b200
+
 extern "C" int
 b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     const b200bsp_grid* grid, const b200bsp_opts* opts, b200bsp_ctx** out)
