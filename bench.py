@@ -206,10 +206,57 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
+                  evals=50):
+    """The same workload with the curvature regulariser added (lambda 0.005)
+    and with Mattes MI (PVI-8, 32 bins) instead of MSE: device time per
+    evaluation (CUDA events on the context stream, L2 flushed before each),
+    reported beside the headline MSE number."""
+    import ctypes as C
+    import torch
+    lib = P.lib()
+    reg = P.reg_parms(curvature=0.005)
+    s_c, n_c, r_c = C.c_float(), C.c_int64(), C.c_float()
+
+    def mse_reg():
+        ctx.score_mse(d_coeff, grad_out=d_grad)
+        rc = lib.b200bsp_regularize(ctx._h, d_coeff.data_ptr(), C.byref(reg),
+                                    C.addressof(r_c), d_grad.data_ptr())
+        if rc:
+            raise RuntimeError(lib.b200bsp_last_error(ctx._h))
+
+    def mi():
+        rc = lib.b200bsp_score_mi(ctx._h, d_coeff.data_ptr(), C.addressof(s_c),
+                                  d_grad.data_ptr(), C.addressof(n_c), None,
+                                  None, None)
+        if rc:
+            raise RuntimeError(lib.b200bsp_last_error(ctx._h))
+
+    out = {}
+    for name, fn in (("mse_plus_curvature_regularizer", mse_reg),
+                     ("mattes_mi_pvi8_32bins", mi)):
+        ts = []
+        for i in range(warmup + evals):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            if i >= warmup:
+                ts.append(a.elapsed_time(b))
+        ms = float(np.median(ts))
+        out[name] = {"value": nvox / (ms * 1e-3) / 1e9, "unit": "Gvox/s",
+                     "ms_per_eval": ms, "evals": evals}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--form", default="tc", choices=["tc", "fp32"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
@@ -291,6 +338,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dev_ms = float(t.item())
 
+    extra = extra_metrics(P, ctx, stream, flush, d_coeff, d_grad,
+                          grid.num_roi_voxels, args.warmup)
+
     # end to end through the C ABI with pinned host buffers
     h_coeff = torch.from_numpy(coeff).pin_memory()
     h_grad = torch.zeros(grid.num_coeff).pin_memory()
@@ -342,6 +392,10 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": dict(WORKLOAD, form=args.form,
+                           arithmetic="voxel work f32; tensor-core products "
+                                      "as 3-term bf16 splits with f32 "
+                                      "accumulation" if args.form == "tc"
+                                      else "f32 SIMT",
                            l2="inputs 167 MB > L2 and 256 MiB flush write "
                               "before every timed step (excluded)",
                            parallelism=f"replicas x{world}"),
@@ -355,6 +409,7 @@ def main():
                          "algorithmic_bytes_per_launch":
                              ALGO_BYTES_PER_VOXEL * nvox},
             "cpu_baseline": cpu,
+            "also_measured": extra,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
             "score": s_h, "num_vox": n_h,
