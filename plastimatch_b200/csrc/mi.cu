@@ -10,8 +10,8 @@
 //               the moving and joint histograms, 1 to the fixed histogram
 //               (Joint_histogram::add_pvi_8, joint_histogram.cxx:423-486).
 //               Each CTA accumulates in shared memory; weights are summed as
-//               64-bit fixed point (2^-32 units), so the result is exact up
-//               to one rounding per weight and independent of the order in
+//               64-bit integers in 2^-24 units, so the result is exact up to
+//               one rounding per weight and independent of the order in
 //               which threads add -- deterministic without float atomics.
 //   score       S = -sum_j j log(N j / (f m)) / N over j > 0.001/bins^2
 //               (mi_hist_score_omp, src/register/bspline_mi.cxx:285-309), and
@@ -30,7 +30,6 @@
 
 namespace b200 {
 
-constexpr float MI_FIX = 4294967296.0f;       // 2^32: one unit of weight
 
 // ---- ranges and bin images -------------------------------------------------
 
@@ -157,8 +156,18 @@ mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
 }
 
 // ---- pass 1: histograms ----------------------------------------------------
+//
+// Weights are summed as integers in units of 2^-24 (one rounding per
+// weight), so the histograms do not depend on the order of the additions.
+// Voxels of a warp mostly fall into the same few bins (smooth regions), and
+// same-address atomics of one warp are serialised; each voxel therefore
+// first merges its eight corners by moving bin, and lanes whose corners all
+// share one bin are combined across the warp (match + reduce) so that one
+// lane per distinct (fixed, moving) bin pair updates shared memory.
 
-constexpr int MIH_THREADS = 256;
+constexpr int MIH_THREADS = 128;
+constexpr float MI_WUNIT = 16777216.0f;      // 2^24
+constexpr double MI_WUNIT_INV = 1.0 / 16777216.0;
 
 __global__ void __launch_bounds__ (MIH_THREADS)
 mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
@@ -172,6 +181,7 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
     const int nh = 2 * B + B * B;
     const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
     const int V = vx * vy * vz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long* hf = hsm;
     unsigned long long* hm = hsm + B;
     unsigned long long* hj = hsm + 2 * B;
@@ -183,7 +193,7 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
     const float* sby = slut + 4 * vx;
     const float* sbz = sby + 4 * vy;
     const int dx = g.mdim[0], dxy = g.mdim[0] * g.mdim[1];
-    unsigned long long cnt = 0;
+    unsigned int cnt = 0;
     __syncthreads ();
     for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
         const int tx = t % g.rdims[0];
@@ -196,53 +206,103 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
                 + (ty + j) * g.cdims[0] + (tx + i)) + c];
         }
         __syncthreads ();
-        for (int v = threadIdx.x; v < V; v += MIH_THREADS) {
-            int lx = v % vx, ly = (v / vx) % vy, lz = v / (vx * vy);
+        // warp-uniform trip count: every lane reaches the warp collectives
+        for (int v0 = 32 * warp; v0 < V; v0 += MIH_THREADS) {
+            const int v = v0 + lane;
+            const int vv = v < V ? v : 0;
+            int lx = vv % vx, ly = (vv / vx) % vy, lz = vv / (vx * vy);
             int fi = g.roi_off[0] + vx * tx + lx;
             int fj = g.roi_off[1] + vy * ty + ly;
             int fk = g.roi_off[2] + vz * tz + lz;
-            if (fi >= g.roi_off[0] + g.roi_dim[0]
-                || fj >= g.roi_off[1] + g.roi_dim[1]
-                || fk >= g.roi_off[2] + g.roi_dim[2]) continue;
-            float fxyz[3], d[3] = {0.f, 0.f, 0.f};
-            fixed_position (g, fi, fj, fk, fxyz);
-            int m = 0;
+            bool live = v < V && fi < g.roi_off[0] + g.roi_dim[0]
+                && fj < g.roi_off[1] + g.roi_dim[1]
+                && fk < g.roi_off[2] + g.roi_dim[2];
+            int fb = 0, mb[8];
+            unsigned int q[8];
+            if (live) {
+                float fxyz[3], d[3] = {0.f, 0.f, 0.f};
+                fixed_position (g, fi, fj, fk, fxyz);
+                int m = 0;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                float C = sbz[lz * 4 + k];
+                for (int k = 0; k < 4; k++) {
+                    float C = sbz[lz * 4 + k];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    float Bv = sby[ly * 4 + j] * C;
+                    for (int j = 0; j < 4; j++) {
+                        float Bv = sby[ly * 4 + j] * C;
 #pragma unroll
-                    for (int i = 0; i < 4; i++, m++) {
-                        float A = sbx[lx * 4 + i] * Bv;
-                        d[0] += A * sC[3 * m + 0];
-                        d[1] += A * sC[3 * m + 1];
-                        d[2] += A * sC[3 * m + 2];
+                        for (int i = 0; i < 4; i++, m++) {
+                            float A = sbx[lx * 4 + i] * Bv;
+                            d[0] += A * sC[3 * m + 0];
+                            d[1] += A * sC[3 * m + 1];
+                            d[2] += A * sC[3 * m + 2];
+                        }
+                    }
+                }
+                Sample s;
+                live = locate (g, fxyz, d, s);
+                if (live) {
+                    const float* l1 = s.w1;
+                    const float* l2 = s.w2;
+                    const float w[8] = {l1[0] * l1[1] * l1[2],
+                        l2[0] * l1[1] * l1[2], l1[0] * l2[1] * l1[2],
+                        l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
+                        l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2],
+                        l2[0] * l2[1] * l2[2]};
+                    const int nbr[8] = {s.mvf, s.mvf + 1, s.mvf + dx,
+                        s.mvf + dx + 1, s.mvf + dxy, s.mvf + dxy + 1,
+                        s.mvf + dxy + dx, s.mvf + dxy + dx + 1};
+                    fb = fbin[fi + g.fdim[0] * (fj + g.fdim[1] * fk)];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        mb[k] = mbin[nbr[k]];
+                        q[k] = __float2uint_rn (w[k] * MI_WUNIT);
                     }
                 }
             }
-            Sample s;
-            if (!locate (g, fxyz, d, s)) continue;
-            const float* l1 = s.w1;
-            const float* l2 = s.w2;
-            float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
-                l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2],
-                l1[0] * l1[1] * l2[2], l2[0] * l1[1] * l2[2],
-                l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
-            int nbr[8] = {s.mvf, s.mvf + 1, s.mvf + dx, s.mvf + dx + 1,
-                s.mvf + dxy, s.mvf + dxy + 1, s.mvf + dxy + dx,
-                s.mvf + dxy + dx + 1};
-            int fb = fbin[fi + g.fdim[0] * (fj + g.fdim[1] * fk)];
-            atomicAdd (&hf[fb], 4294967296ull);
+            // merge corners with equal moving bins into the first of them
+            bool first[8];
+            bool single = true;
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                int mb = mbin[nbr[k]];
-                unsigned long long q = __float2ull_rn (w[k] * MI_FIX);
-                atomicAdd (&hm[mb], q);
-                atomicAdd (&hj[fb * B + mb], q);
+            for (int k = 0; k < 8; k++) first[k] = live;
+#pragma unroll
+            for (int k = 1; k < 8; k++) {
+#pragma unroll
+                for (int k2 = 0; k2 < k; k2++) {
+                    if (first[k] && first[k2] && mb[k2] == mb[k]) {
+                        q[k2] += q[k];
+                        first[k] = false;
+                    }
+                }
+                single = single && !first[k];
             }
-            cnt++;
+            const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+            if (live) {
+                // fixed histogram: one count per voxel
+                unsigned peers = __match_any_sync (live_mask, fb);
+                if (lane == __ffs (peers) - 1) {
+                    atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
+                }
+                cnt++;
+            }
+            const unsigned single_mask = __ballot_sync (0xffffffffu,
+                live && single);
+            if (live && single) {
+                const int key = fb * B + mb[0];
+                unsigned peers = __match_any_sync (single_mask, key);
+                unsigned sum = __reduce_add_sync (peers, q[0]);
+                if (lane == __ffs (peers) - 1) {
+                    atomicAdd (&hm[mb[0]], (unsigned long long) sum);
+                    atomicAdd (&hj[key], (unsigned long long) sum);
+                }
+            } else if (live) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    if (first[k]) {
+                        atomicAdd (&hm[mb[k]], (unsigned long long) q[k]);
+                        atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
+                    }
+                }
+            }
         }
         __syncthreads ();
     }
@@ -250,7 +310,7 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
         if (hsm[i]) atomicAdd (&ghist[i], hsm[i]);
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync (0xffffffffu, cnt, o);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd (&ghist[nh], cnt);
+    if (lane == 0 && cnt) atomicAdd (&ghist[nh], (unsigned long long) cnt);
 }
 
 // ---- score and pass-2 factor table -----------------------------------------
@@ -264,9 +324,9 @@ mi_score_kernel (const unsigned long long* __restrict__ ghist, int B,
     __shared__ int sh_n[32];
     __shared__ float s_score;
     const int nh = 2 * B + B * B;
-    const double inv = 1.0 / 4294967296.0;
     for (int i = threadIdx.x; i < nh; i += blockDim.x) {
-        histd[i] = (double) ghist[i] * inv;
+        histd[i] = i < B ? (double) ghist[i]
+                         : (double) ghist[i] * MI_WUNIT_INV;
     }
     __syncthreads ();
     const long long N = (long long) ghist[nh];
@@ -381,7 +441,7 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     }
     int sms = 148;
     cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, 0);
-    int grid = std::min (g.ntiles, 4 * sms);
+    int grid = std::min (g.ntiles, 8 * sms);
     hk<<<grid, MIH_THREADS, hsmem, st>>> (g, d_coeff, d_luts, s->d_fbin,
         s->d_mbin, B, s->d_hist);
     mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd, s->d_lut,

@@ -6,7 +6,7 @@ Tolerances (float work, stated here as the bar):
              reference) against the double oracle and the reference's float
              flavour g (golden record)
   histograms relative 1e-5 (L2) against the reference's pass-1 histograms;
-             the device sums corner weights as 64-bit fixed point, and its
+             the device sums corner weights as integers in 2^-24 units, and its
              pass 1 takes world positions as origin + step * index where the
              reference accumulates x positions step by step
   num_vox    within 0.01% (+2), as for MSE
