@@ -203,4 +203,22 @@ launch_volume_grad (const int dim[3], const float spacing[3],
     return cudaGetLastError ();
 }
 
+__global__ void
+pad_grad4_kernel (const float* __restrict__ g3, float4* __restrict__ g4,
+    long long n)
+{
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        g4[i] = make_float4 (g3[3 * i], g3[3 * i + 1], g3[3 * i + 2], 0.f);
+    }
+}
+
+cudaError_t
+launch_pad_grad4 (const float* grad3, float4* grad4, long long n,
+    cudaStream_t st)
+{
+    pad_grad4_kernel<<<1184, 256, 0, st>>> (grad3, grad4, n);
+    return cudaGetLastError ();
+}
+
 } // namespace b200

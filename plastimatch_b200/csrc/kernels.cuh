@@ -48,8 +48,12 @@ bool tc_plan (const BspGeom& g, TcPlan* plan, int ctas_per_sm, int sm_count);
 int tc_build_tables (const BspGeom& g, const TcPlan& plan, void** d_qlut);
 cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
     int grad_mode, const float* fimg, const float* mimg, const float* mgrad,
-    const float* coeff, const void* qlut_bf16, float* part,
-    double* score_part, int* count_part, int* err_flag, cudaStream_t st);
+    const float4* mgrad4, const float* coeff, const void* qlut_bf16,
+    float* part, double* score_part, int* count_part, int* err_flag,
+    cudaStream_t st);
+// Moving gradient xyz-interleaved -> float4 (w = 0), for 16-byte loads.
+cudaError_t launch_pad_grad4 (const float* grad3, float4* grad4, long long n,
+    cudaStream_t st);
 
 cudaError_t launch_reduce_score (const double* score_part,
     const int* count_part, int n, DevResult* res, int mode,

@@ -75,6 +75,12 @@ static_assert (3 * TC_TMAX <= 80, "N fits the C area");
 struct TcArgs {
     BspGeom g;
     int T, N, mblk, V, nbx, nbatches;
+    // x-line voxel phase with axis-aligned geometry (see voxel_phase_axis):
+    // T0 tiles per round, W = vx * T0 voxels per round row, plane = W * vy * vz
+    // samples per round, multiply-high reciprocals of W and vx
+    int axis, T0, W, plane;
+    unsigned mW, mvx;
+    const float4* mgrad4;     // moving gradient padded to float4
     const float* fimg;
     const float* mimg;
     const float* mgrad;
@@ -544,6 +550,200 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
     sc += (double) scf;
 }
 
+// Voxel phase for axis-aligned geometry (step and projection matrices
+// diagonal), in the x-line order of voxel_phase_xline with the per-sample
+// work cut to what a sample needs: world positions come from per-batch
+// tables (x along the batch, y and z per tile row, with the fixed-image row
+// index), the field is read back as one (x, y) pair and one z, the clamp
+// runs without conversions, every index stays inside its image so no load
+// is guarded, and the moving gradient is one 16-byte load.  Both rounds use
+// W = vx * T0 voxels per row so one sample -> (row, x) mapping serves every
+// batch; a round-1 tile slot past the batch's last tile is dead.
+template <int GRAD_MODE>
+__device__ __forceinline__ void
+voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
+    int tx0, int ty, int tz, double& sc, int& cnt)
+{
+    const BspGeom& g = a.g;
+    const int T = a.T, T0 = a.T0, W = a.W, plane = a.plane;
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int nrho = vy * vz;
+    float2* Dxy = (float2*) (x.sm + SM_C);
+    float* Dz = (float*) (x.sm + SM_C + 8 * plane);
+    uint4* rowtab = (uint4*) (x.sm + SM_S);
+    float* posx = (float*) (x.sm + SM_S + 16 * nrho);
+    uint8_t* dch = x.sm + SM_DC;
+    const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
+    const int fi_base = g.roi_off[0] + vx * tx0;
+    const int fj_base = g.roi_off[1] + vy * ty;
+    const int fk_base = g.roi_off[2] + vz * tz;
+    // batch x index X = vx * (batch tile) + lx is live below xlim
+    const int xlim = min (min (g.rdims[0] - tx0, T) * vx,
+        g.roi_off[0] + g.roi_dim[0] - fi_base);
+    float scf = 0.f;
+
+    // Padding voxels (V..127) carry no samples; zero their adjoint columns
+    // in the rows of live tiles (see voxel_phase_xline).
+    const int npad = 128 - a.V;
+    for (int o = x.tid; o < npad * T; o += TC_THREADS) {
+        const int tb = o / npad, v = a.V + (o - tb * npad);
+        uint8_t* p = dch + (v >> 6) * DC_CHUNK + (3 * (tb >> 3)) * 1024
+            + (tb & 7) * 128 + ((((v & 63) >> 3) ^ (tb & 7)) << 4) + (v & 7) * 2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            *(unsigned short*) (p + 1024 * c) = 0;
+            *(unsigned short*) (p + DC_HALF + 1024 * c) = 0;
+        }
+    }
+    // Position tables: x over both rounds, (y, z, fixed row, live) per row.
+    // origin + step * index with the step's zero off-diagonal terms dropped
+    // (they add exact zeros).
+    for (int i = x.tid; i < 2 * W; i += TC_THREADS) {
+        posx[i] = fmaf (i2f_small (fi_base + i), g.fstep[0], g.img_origin[0]);
+    }
+    for (int rho = x.tid; rho < nrho; rho += TC_THREADS) {
+        const int lz = rho / vy, ly = rho - lz * vy;
+        const int fj = fj_base + ly, fk = fk_base + lz;
+        const bool live = fj < g.roi_off[1] + g.roi_dim[1]
+            && fk < g.roi_off[2] + g.roi_dim[2];
+        const float py = fmaf (i2f_small (fj), g.fstep[4], g.img_origin[1]);
+        const float pz = fmaf (i2f_small (fk), g.fstep[8], g.img_origin[2]);
+        const int row = g.fdim[0] * (min (fj, g.fdim[1] - 1)
+            + g.fdim[1] * min (fk, g.fdim[2] - 1));
+        rowtab[rho] = make_uint4 (__float_as_uint (py), __float_as_uint (pz),
+            (uint32_t) row, live ? 1u : 0u);
+    }
+
+    const uint32_t lb = x.taddr + ((uint32_t) (32 * x.q) << 16) + TC_D_COL;
+    const int rho_v = vs.ly + vy * vs.lz;
+    for (int r = 0; r < 2; r++) {
+        const int rt0 = r * T0;
+        const int Tr = min (T0, T - rt0);
+        if (Tr <= 0) break;
+        // 1. field values of the round's tiles: TMEM -> (Dxy, Dz)[rho W + x]
+        {
+            const int h = (Tr + 1) >> 1;
+            const int u0 = x.tg * h, u1 = min (Tr, u0 + h);
+            for (int t4 = u0; t4 < u1; t4 += 4) {
+                float dv[12];
+                tmem_ld4x3_wait (lb + rt0 + t4, lb + T + rt0 + t4,
+                    lb + 2 * T + rt0 + t4, dv);
+                if (vs.live) {
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int tt = t4 + u;
+                        if (tt < u1) {
+                            const int o = rho_v * W + tt * vx + vs.lx;
+                            Dxy[o] = make_float2 (dv[u], dv[4 + u]);
+                            Dz[o] = dv[8 + u];
+                        }
+                    }
+                }
+            }
+        }
+        cbar ();
+        // 2. samples s and s + 256, s = tid + 512 k
+        const int X0 = r * W;
+        for (int s0 = x.tid; s0 < plane; s0 += 2 * TC_THREADS) {
+            bool ok[2];
+            int mvf[2], mvr[2], fidx[2];
+            uint32_t doff[2];
+            float w2[2][3];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int sv = s0 + u * TC_THREADS;
+                const bool in_plane = sv < plane;
+                const int sc_ = in_plane ? sv : 0;
+                const int rho = (int) __umulhi ((unsigned) sc_, a.mW);
+                const int xx = sc_ - rho * W;
+                const int tt = (int) __umulhi ((unsigned) xx, a.mvx);
+                const int lx = xx - tt * vx;
+                const int X = X0 + xx;
+                const uint4 rw = rowtab[rho];
+                const float2 dxy = Dxy[sc_];
+                const float dz = Dz[sc_];
+                const float ma[3] = {
+                    ((posx[X] + dxy.x) - g.morigin[0]) * g.mproj[0],
+                    ((__uint_as_float (rw.x) + dxy.y) - g.morigin[1]) * g.mproj[4],
+                    ((__uint_as_float (rw.y) + dz) - g.morigin[2]) * g.mproj[8]};
+                bool in = in_plane && rw.w != 0u && X < xlim;
+                int f[3];
+                bool up[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    in = in && ma[d] > -0.5f && ma[d] < g.m_hi[d];
+                    // floor(max(ma, 0)) in the low mantissa bits of
+                    // max(ma, 0) + 2^23 rounded down; corner clamped to
+                    // dim - 2, fraction saturated to [0, 1] (li_clamp)
+                    const float big = __fadd_rd (fmaxf (ma[d], 0.f), 8388608.f);
+                    f[d] = min (__float_as_int (big) - 0x4B000000, g.mdim[d] - 2);
+                    const float fc = fminf (big - 8388608.f, g.m_fmax[d]);
+                    const float w = __saturatef (ma[d] - fc);
+                    w2[u][d] = w;
+                    up[d] = w >= 0.5f;
+                }
+                ok[u] = in;
+                mvf[u] = f[0] + dxm * (f[1] + g.mdim[1] * f[2]);
+                mvr[u] = mvf[u] + (up[0] ? 1 : 0) + (up[1] ? dxm : 0)
+                    + (up[2] ? dxym : 0);
+                fidx[u] = (int) rw.z + min (fi_base + X, g.fdim[0] - 1);
+                const int v = lx + vx * rho;
+                const int tb = rt0 + tt;
+                doff[u] = in_plane
+                    ? (uint32_t) ((v >> 6) * DC_CHUNK + (3 * (tb >> 3)) * 1024
+                        + (tb & 7) * 128 + ((((v >> 3) ^ tb) & 7) << 4)
+                        + (v & 7) * 2)
+                    : 0xffffffffu;
+            }
+            float cr[2][8], fv[2];
+            float4 gr[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const float* mp = a.mimg + mvf[u];
+                cr[u][0] = __ldg (mp);
+                cr[u][1] = __ldg (mp + 1);
+                cr[u][2] = __ldg (mp + dxm);
+                cr[u][3] = __ldg (mp + dxm + 1);
+                cr[u][4] = __ldg (mp + dxym);
+                cr[u][5] = __ldg (mp + dxym + 1);
+                cr[u][6] = __ldg (mp + dxym + dxm);
+                cr[u][7] = __ldg (mp + dxym + dxm + 1);
+                fv[u] = __ldg (a.fimg + fidx[u]);
+                if (GRAD_MODE == 0) gr[u] = __ldg (a.mgrad4 + mvr[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
+                diff = ok[u] ? diff : 0.f;
+                scf = fmaf (diff, diff, scf);
+                cnt += ok[u] ? 1 : 0;
+                float dc0, dc1, dc2;
+                if (GRAD_MODE == 0) {
+                    dc0 = diff * gr[u].x; dc1 = diff * gr[u].y; dc2 = diff * gr[u].z;
+                } else {
+                    float grd[3];
+                    trilinear_lerp_grad (g, w2[u], cr[u], grd);
+                    dc0 = diff * grd[0]; dc1 = diff * grd[1]; dc2 = diff * grd[2];
+                }
+                if (doff[u] != 0xffffffffu) {
+                    uint8_t* p = dch + doff[u];
+                    uint32_t h01, l01, h2, l2;
+                    split_bf16x2 (dc0, dc1, h01, l01);
+                    split_bf16x2 (dc2, 0.f, h2, l2);
+                    *(unsigned short*) (p) = (unsigned short) h01;
+                    *(unsigned short*) (p + DC_HALF) = (unsigned short) l01;
+                    *(unsigned short*) (p + 1024) = (unsigned short) (h01 >> 16);
+                    *(unsigned short*) (p + DC_HALF + 1024) = (unsigned short) (l01 >> 16);
+                    *(unsigned short*) (p + 2048) = (unsigned short) h2;
+                    *(unsigned short*) (p + DC_HALF + 2048) = (unsigned short) l2;
+                }
+            }
+        }
+        cbar ();                                   // Dxy/Dz reused next round
+    }
+    sc += (double) scf;
+}
+
 // Copy G (rows r -> (c, t), 64 slot columns) from TMEM to shared memory as
 // Gs[(c*T + t)*65 + slot] (odd row stride: the per-lane rows land in
 // distinct banks).  Warp (quarter q, group tg) takes rows 32q..+31, slots
@@ -693,7 +893,9 @@ mse_tc_kernel (TcArgs a)
 
     const BspGeom& g = a.g;
     TcCtx x;
-    x.sm = (uint8_t*) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+    // Round up to 1024 B by offsetting smem_raw itself, so every access
+    // through x.sm stays a shared-memory access (32-bit addresses).
+    x.sm = smem_raw + ((1024u - (smem_addr (smem_raw) & 1023u)) & 1023u);
     x.sm_base = smem_addr (x.sm);
     x.tid = threadIdx.x;
     x.warp = x.tid >> 5;
@@ -775,7 +977,11 @@ mse_tc_kernel (TcArgs a)
                 const int b = blockIdx.x + i * gridDim.x;
                 coords (b, tx0, ty, tz);
                 if (!cwait (a, x, &s_bar[2], ph_d, abort_flag, 1)) break;
-                voxel_phase_xline<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                if (a.axis) {
+                    voxel_phase_axis<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                } else {
+                    voxel_phase_xline<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                }
                 warp_arrive (x, &s_bar[1]);
                 if (i + 1 < nb_local) {
                     int nx0, ny, nz;
@@ -902,8 +1108,8 @@ tc_build_tables (const BspGeom& g, const TcPlan& p, void** d_qlut)
 cudaError_t
 launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
     const float* fimg, const float* mimg, const float* mgrad,
-    const float* coeff, const void* qimg, float* part, double* score_part,
-    int* count_part, int* err, cudaStream_t st)
+    const float4* mgrad4, const float* coeff, const void* qimg, float* part,
+    double* score_part, int* count_part, int* err, cudaStream_t st)
 {
     TcArgs a;
     a.g = g;
@@ -911,6 +1117,28 @@ launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
     a.N = p.n_mma;
     a.mblk = p.mblk;
     a.V = g.vpr[0] * g.vpr[1] * g.vpr[2];
+    // The axis-aligned voxel phase: diagonal step and projection, one
+    // 128-voxel block per tile, rounds whose field copy and position tables
+    // fit the C and knot-block areas, and divisors >= 2 for the
+    // multiply-high reciprocals.
+    a.T0 = (a.T + 1) / 2;
+    a.W = g.vpr[0] * a.T0;
+    a.plane = a.W * g.vpr[1] * g.vpr[2];
+    bool diag = true;
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            if (i != j && (g.fstep[3 * i + j] != 0.f || g.mproj[3 * i + j] != 0.f)) {
+                diag = false;
+            }
+        }
+    }
+    a.axis = diag && p.mblk == 1 && g.vpr[0] >= 2 && a.W >= 2
+        && 12 * a.plane <= SM_C_BYTES
+        && 2 * a.W + 4 * g.vpr[1] * g.vpr[2] <= SM_S_FLOATS
+        && (grad_mode == 1 || mgrad4 != nullptr);
+    a.mW = a.W >= 2 ? 0xFFFFFFFFu / (unsigned) a.W + 1u : 0u;
+    a.mvx = g.vpr[0] >= 2 ? 0xFFFFFFFFu / (unsigned) g.vpr[0] + 1u : 0u;
+    a.mgrad4 = mgrad4;
     a.nbx = (g.rdims[0] + p.bx - 1) / p.bx;
     a.nbatches = p.nbatches;
     a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;

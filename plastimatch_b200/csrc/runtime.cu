@@ -41,6 +41,7 @@ struct b200bsp_ctx {
     float* d_fixed = nullptr;
     float* d_moving = nullptr;
     float* d_mgrad = nullptr;
+    float4* d_mgrad4 = nullptr;       // TC form, nearest gradient: padded copy
     float* d_coeff = nullptr;
     float* d_luts = nullptr;
     float* d_grad = nullptr;
@@ -190,6 +191,7 @@ static void
 free_all (b200bsp_ctx* c)
 {
     cudaFree (c->d_fixed); cudaFree (c->d_moving); cudaFree (c->d_mgrad);
+    cudaFree (c->d_mgrad4);
     cudaFree (c->d_coeff); cudaFree (c->d_luts); cudaFree (c->d_grad);
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
     cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
@@ -373,6 +375,9 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     alloc ((void**) &c->d_fixed, nf * sizeof (float));
     alloc ((void**) &c->d_moving, nm * sizeof (float));
     if (o.mse_grad == 0) alloc ((void**) &c->d_mgrad, 3 * nm * sizeof (float));
+    if (o.mse_grad == 0 && o.form == B200BSP_FORM_TC) {
+        alloc ((void**) &c->d_mgrad4, nm * sizeof (float4));
+    }
     alloc ((void**) &c->d_coeff, c->num_coeff * sizeof (float));
     alloc ((void**) &c->d_grad, c->num_coeff * sizeof (float));
     alloc ((void**) &c->d_grad64, c->num_coeff * sizeof (double));
@@ -537,6 +542,10 @@ b200bsp_set_images (b200bsp_ctx* c, const float* fixed_img,
             CK (launch_volume_grad (g.mdim, sp, c->d_inv_dc, c->d_moving,
                 c->d_mgrad, c->stream));
         }
+        if (c->d_mgrad4) {
+            CK (launch_pad_grad4 (c->d_mgrad, c->d_mgrad4, (long long) nm,
+                c->stream));
+        }
     }
     int rc = mi_set_images (&c->mi, g, c->d_fixed, c->d_moving, nf, nm,
         c->stream);
@@ -614,8 +623,9 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
             c->d_count_part, c->stream));
     } else {
         CK (launch_mse_tc (g, c->plan, c->opts.mse_grad, c->d_fixed,
-            c->d_moving, c->d_mgrad, dcoeff, c->d_qlut, c->d_part,
-            c->d_score_part, c->d_count_part, c->d_err, c->stream));
+            c->d_moving, c->d_mgrad, c->d_mgrad4, dcoeff, c->d_qlut,
+            c->d_part, c->d_score_part, c->d_count_part, c->d_err,
+            c->stream));
     }
     c->last_launches++;
     int rc = mark_main_done (c);
