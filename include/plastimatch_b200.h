@@ -104,7 +104,9 @@ const char* b200bsp_version (void);
  * (src/register/bspline_state.cxx:165-212, bspline_cuda.h:124-140).
  * Computes rdims/cdims and the basis tables as Bspline_xform::allocate does
  * (src/base/bspline_xform.cxx:361-488).  Allocates all device memory the
- * evaluations need; later calls allocate nothing. */
+ * score and regulariser evaluations need; later scoring calls allocate
+ * nothing (b200bsp_interpolate_vf / b200bsp_warp with host outputs allocate
+ * one staging buffer on first use, see there). */
 int b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     const b200bsp_grid* grid, const b200bsp_opts* opts, b200bsp_ctx** out);
 
@@ -173,12 +175,18 @@ int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
 /* Dense displacement field over the ROI (bspline_interpolate_vf,
  * src/base/bspline_interpolate.cxx:112-142): vf is dim[0]*dim[1]*dim[2]*3
  * floats of the fixed image, xyz interleaved; voxels outside the ROI are
- * zero. */
+ * zero.  coeff and vf may be host or device memory; with a host vf the
+ * first call allocates a device staging buffer of 12 bytes per fixed voxel,
+ * kept until b200bsp_destroy. */
 int b200bsp_interpolate_vf (b200bsp_ctx* ctx, const float* coeff, float* vf);
 
 /* Warp the moving image onto the fixed grid with trilinear interpolation
- * and `default_value` outside (bspline_warp, src/base/bspline_warp.cxx:
- * 171-227, linear interpolation, no vector-field output). */
+ * and `default_value` outside (bspline_warp with linear interpolation,
+ * src/base/bspline_warp.cxx:28-227; no vector-field output).  The reference
+ * takes each voxel's tile from its absolute index, so the warp is defined
+ * when the grid's ROI is the whole fixed image: B200BSP_E_UNSUPPORTED
+ * otherwise.  Host or device pointers; a host `warped` uses the staging
+ * buffer of b200bsp_interpolate_vf. */
 int b200bsp_warp (b200bsp_ctx* ctx, const float* coeff, float default_value,
     float* warped);
 

@@ -236,6 +236,36 @@ def port_reg(grid, fixed, coeff, pen, precision="f32") -> Result:
     return Result(s.value, gr)
 
 
+def port_interpolate_vf(grid, fixed, coeff) -> np.ndarray:
+    """bspline_interpolate_vf restated: field over the ROI, zero elsewhere;
+    shape (nz, ny, nx, 3)."""
+    vf = np.zeros(fixed.npix * 3, np.float32)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = port().orc_interpolate_vf(C.byref(orc_grid(grid, fixed)),
+                                   C.byref(orc_vol(fixed)), _p(coeff), _p(vf))
+    if rc:
+        raise RuntimeError("oracle interpolate_vf failed")
+    nx, ny, nz = fixed.dim
+    return vf.reshape(nz, ny, nx, 3)
+
+
+def port_warp(grid, fixed, moving, coeff, default=0.0, with_vf=False):
+    """bspline_warp (linear) restated: warped moving image on the fixed grid
+    (and the field when with_vf)."""
+    out = np.zeros(fixed.npix, np.float32)
+    vf = np.zeros(fixed.npix * 3, np.float32) if with_vf else None
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = port().orc_warp(C.byref(orc_grid(grid, fixed)),
+                         C.byref(orc_vol(fixed)), C.byref(orc_vol(moving)),
+                         _p(moving.img), _p(coeff), C.c_float(default),
+                         _p(out), _p(vf))
+    if rc:
+        raise RuntimeError(f"oracle warp failed rc={rc}")
+    nx, ny, nz = fixed.dim
+    out = out.reshape(nz, ny, nx)
+    return (out, vf.reshape(nz, ny, nx, 3)) if with_vf else out
+
+
 # ----------------------------------------------------------- reference ---
 
 def _ref_geom(v) -> RefGeom:
@@ -318,3 +348,25 @@ def ref_luts(grid, fixed):
     ref().ref_luts(C.byref(_ref_geom(fixed)), C.byref(_ref_grid(grid)),
                    _p(bx), _p(by), _p(bz), _p(q))
     return bx, by, bz, q
+
+
+def ref_interpolate_vf(grid, fixed, coeff) -> np.ndarray:
+    vf = np.zeros(fixed.npix * 3, np.float32)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    ref().ref_interpolate_vf(C.byref(_ref_geom(fixed)),
+                             C.byref(_ref_grid(grid)), _p(coeff), _p(vf))
+    nx, ny, nz = fixed.dim
+    return vf.reshape(nz, ny, nx, 3)
+
+
+def ref_warp(grid, fixed, moving, coeff, default=0.0, linear=True):
+    """The reference's bspline_warp: (warped image, field)."""
+    out = np.zeros(fixed.npix, np.float32)
+    vf = np.zeros(fixed.npix * 3, np.float32)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    ref().ref_warp(C.byref(_ref_geom(fixed)), C.byref(_ref_geom(moving)),
+                   _p(moving.img), C.byref(_ref_grid(grid)), _p(coeff),
+                   C.c_int(1 if linear else 0), C.c_float(default), _p(out),
+                   _p(vf))
+    nx, ny, nz = fixed.dim
+    return out.reshape(nz, ny, nx), vf.reshape(nz, ny, nx, 3)

@@ -1409,3 +1409,119 @@ orc_reg_f64 (const orc_grid* g, const float* coeff, const float pen[8],
     memset (grad, 0, sizeof(double) * g->num_coeff);
     return reg_common (g, coeff, pen, rmetric, 0, grad);
 }
+
+/* ------------------------------------------------------------------ */
+/* Dense vector field and warp                                          */
+/* ------------------------------------------------------------------ */
+
+/* Field at one voxel from the q_lut weights of its offset in the tile:
+ * bspline_interp_pix / bspline_interp_pix_b
+ * (src/base/bspline_interpolate.cxx:21-76), knots in (k, j, i) order. */
+static inline void
+interp_pix_q (float out[3], const orc_grid* g, const float* coeff,
+    const int64_t p[3], const float* q)
+{
+    const int64_t* cd = g->cdims;
+    int m = 0;
+    out[0] = out[1] = out[2] = 0;
+    for (int k = 0; k < 4; k++)
+        for (int j = 0; j < 4; j++)
+            for (int i = 0; i < 4; i++, m++) {
+                int64_t cidx = 3 * ((p[2] + k) * cd[1] * cd[0]
+                    + (p[1] + j) * cd[0] + (p[0] + i));
+                out[0] += q[m] * coeff[cidx+0];
+                out[1] += q[m] * coeff[cidx+1];
+                out[2] += q[m] * coeff[cidx+2];
+            }
+}
+
+/* bspline_interpolate_vf (src/base/bspline_interpolate.cxx:112-142): the
+ * field at every ROI voxel (tile and offset counted from the ROI corner),
+ * zero elsewhere; vf is xyz-interleaved over the fixed image. */
+int
+orc_interpolate_vf (const orc_grid* g, const orc_vol* fixed,
+    const float* coeff, float* vf)
+{
+    const int64_t* vpr = g->vox_per_rgn;
+    const int64_t* dim = fixed->dim;
+    float* q_lut = (float*) malloc (sizeof(float) * 64 * vpr[0] * vpr[1] * vpr[2]);
+    if (!q_lut) return -1;
+    orc_q_lut (q_lut, vpr);
+    memset (vf, 0, sizeof(float) * 3 * dim[0] * dim[1] * dim[2]);
+    for (int64_t k = 0; k < g->roi_dim[2]; k++)
+    for (int64_t j = 0; j < g->roi_dim[1]; j++)
+    for (int64_t i = 0; i < g->roi_dim[0]; i++) {
+        int64_t p[3] = {i / vpr[0], j / vpr[1], k / vpr[2]};
+        int64_t qidx = (i % vpr[0]) + vpr[0] * ((j % vpr[1])
+            + vpr[1] * (k % vpr[2]));
+        int64_t v = (k + g->roi_offset[2]) * dim[0] * dim[1]
+            + (j + g->roi_offset[1]) * dim[0] + (i + g->roi_offset[0]);
+        interp_pix_q (&vf[3*v], g, coeff, p, &q_lut[qidx*64]);
+    }
+    free (q_lut);
+    return 0;
+}
+
+/* bspline_warp_dcos with linear interpolation on a float image
+ * (src/base/bspline_warp.cxx:28-160): every fixed voxel gets the trilinear
+ * moving value at its displaced position, or default_val outside the
+ * moving image; positions advance along x as LOOP_X does.  The reference
+ * takes the tile from the absolute voxel index, so this is defined only
+ * when the ROI is the whole image (returns -2 otherwise).  vf_out (may be
+ * NULL) receives the field. */
+int
+orc_warp (const orc_grid* g, const orc_vol* fx, const orc_vol* mv,
+    const float* m_img, const float* coeff, float default_val, float* out,
+    float* vf_out)
+{
+    const int64_t* vpr = g->vox_per_rgn;
+    const int64_t* dim = fx->dim;
+    for (int d = 0; d < 3; d++)
+        if (g->roi_offset[d] != 0 || g->roi_dim[d] != dim[d]) return -2;
+    float* q_lut = (float*) malloc (sizeof(float) * 64 * vpr[0] * vpr[1] * vpr[2]);
+    if (!q_lut) return -1;
+    orc_q_lut (q_lut, vpr);
+    int64_t npix = dim[0] * dim[1] * dim[2];
+    for (int64_t v = 0; v < npix; v++) out[v] = default_val;
+    if (vf_out) memset (vf_out, 0, sizeof(float) * 3 * npix);
+    const float* st = fx->step;
+    const float* org = fx->origin;
+    int64_t fijk[3];
+    float fxyz[3];
+    for (fijk[2] = 0; fijk[2] < dim[2]; fijk[2]++) {
+        fxyz[2] = org[2] + fijk[2] * st[2*3+2];
+        for (fijk[1] = 0, fxyz[1] = org[1] + fijk[2] * st[1*3+2];
+             fijk[1] < dim[1];
+             ++fijk[1],
+             fxyz[2] = org[2] + fijk[2] * st[2*3+2] + fijk[1] * st[2*3+1],
+             fxyz[1] = org[1] + fijk[2] * st[1*3+2] + fijk[1] * st[1*3+1]) {
+            for (fijk[0] = 0,
+                 fxyz[0] = org[0] + fijk[2] * st[0*3+2] + fijk[1] * st[0*3+1];
+                 fijk[0] < dim[0];
+                 ++fijk[0], fxyz[0] += st[0], fxyz[1] += st[3],
+                 fxyz[2] += st[6]) {
+                int64_t p[3], qidx;
+                float dxyz[3], mijk[3], li1[3], li2[3];
+                int64_t mf[3], mr[3];
+                for (int d = 0; d < 3; d++) p[d] = fijk[d] / vpr[d];
+                qidx = (fijk[0] % vpr[0]) + vpr[0] * ((fijk[1] % vpr[1])
+                    + vpr[1] * (fijk[2] % vpr[2]));
+                interp_pix_q (dxyz, g, coeff, p, &q_lut[qidx*64]);
+                int64_t fv = vidx (dim, fijk[0], fijk[1], fijk[2]);
+                if (vf_out) {
+                    vf_out[3*fv+0] = dxyz[0];
+                    vf_out[3*fv+1] = dxyz[1];
+                    vf_out[3*fv+2] = dxyz[2];
+                }
+                if (!correspond_f (mijk, fxyz, dxyz, mv)) continue;
+                for (int d = 0; d < 3; d++)
+                    li_clamp_f (mijk[d], mv->dim[d] - 1, &mf[d], &mr[d],
+                        &li1[d], &li2[d]);
+                out[fv] = li_value_f (li1, li2,
+                    vidx (mv->dim, mf[0], mf[1], mf[2]), m_img, mv->dim);
+            }
+        }
+    }
+    free (q_lut);
+    return 0;
+}

@@ -95,6 +95,15 @@ int orc_reg_f32 (const orc_grid* g, const float* coeff,
 int orc_reg_f64 (const orc_grid* g, const float* coeff,
     const float penalties[8], double* rmetric, double* grad);
 
+/* Dense vector field over the ROI (bspline_interpolate_vf) and the warped
+ * moving image (bspline_warp, linear interpolation; ROI must be the whole
+ * image, returns -2 otherwise). */
+int orc_interpolate_vf (const orc_grid* g, const orc_vol* fixed,
+    const float* coeff, float* vf);
+int orc_warp (const orc_grid* g, const orc_vol* fixed, const orc_vol* moving,
+    const float* m_img, const float* coeff, float default_val, float* out,
+    float* vf_out);
+
 #ifdef __cplusplus
 }
 #endif

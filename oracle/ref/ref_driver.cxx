@@ -18,12 +18,14 @@
 #include <omp.h>
 
 #include "bspline.h"
+#include "bspline_interpolate.h"
 #include "bspline_mi.h"
 #include "bspline_mse.h"
 #include "bspline_optimize.h"
 #include "bspline_parms.h"
 #include "bspline_regularize.h"
 #include "bspline_state.h"
+#include "bspline_warp.h"
 #include "bspline_xform.h"
 #include "joint_histogram.h"
 #include "metric_state.h"
@@ -260,6 +262,63 @@ ref_volume_grad (const ref_geom* g, const float* img, float* grad_out)
     Volume::Pointer v = make_volume (g, img, 1);
     Volume::Pointer gr = volume_gradient (v);
     memcpy (grad_out, gr->img, sizeof(float) * 3 * gr->npix);
+    return 0;
+}
+
+static void
+init_xform (Bspline_xform* bxf, const ref_geom* fg, const ref_grid* grid,
+    const float* coeff)
+{
+    float origin[3], spacing[3], dcos[9];
+    plm_long dim[3], roi_offset[3], roi_dim[3], vpr[3];
+    for (int d = 0; d < 3; d++) {
+        origin[d] = fg->origin[d]; spacing[d] = fg->spacing[d];
+        dim[d] = fg->dim[d]; roi_offset[d] = grid->roi_offset[d];
+        roi_dim[d] = grid->roi_dim[d]; vpr[d] = grid->vox_per_rgn[d];
+    }
+    memcpy (dcos, fg->dcos, sizeof dcos);
+    bxf->initialize (origin, spacing, dim, roi_offset, roi_dim, vpr, dcos);
+    if (coeff) memcpy (bxf->coeff, coeff, sizeof(float) * bxf->num_coeff);
+}
+
+/* bspline_interpolate_vf (src/base/bspline_interpolate.cxx:112-142) into a
+ * vector-field volume over the fixed image (xyz interleaved). */
+int
+ref_interpolate_vf (const ref_geom* fg, const ref_grid* grid,
+    const float* coeff, float* vf)
+{
+    Quiet q;
+    Bspline_xform bxf;
+    init_xform (&bxf, fg, grid, coeff);
+    Volume::Pointer v = Volume::New (fg->dim, fg->origin, fg->spacing,
+        fg->dcos, PT_VF_FLOAT_INTERLEAVED, 3);
+    bspline_interpolate_vf (v.get (), &bxf);
+    memcpy (vf, v->img, sizeof(float) * 3 * v->npix);
+    return 0;
+}
+
+/* bspline_warp (src/base/bspline_warp.cxx:162-227) of a float moving image
+ * onto the fixed grid; vf_out (may be NULL) receives the field. */
+int
+ref_warp (const ref_geom* fg, const ref_geom* mg, const float* mimg,
+    const ref_grid* grid, const float* coeff, int linear, float default_val,
+    float* out, float* vf_out)
+{
+    Quiet q;
+    Bspline_xform bxf;
+    init_xform (&bxf, fg, grid, coeff);
+    Volume::Pointer moving = make_volume (mg, mimg, 1);
+    Volume::Pointer vout = Volume::New (fg->dim, fg->origin, fg->spacing,
+        fg->dcos, PT_FLOAT, 1);
+    Volume::Pointer vf;
+    if (vf_out) {
+        vf = Volume::New (fg->dim, fg->origin, fg->spacing, fg->dcos,
+            PT_VF_FLOAT_INTERLEAVED, 3);
+    }
+    bspline_warp (vout.get (), vf ? vf.get () : 0, &bxf, moving.get (),
+        linear, default_val);
+    memcpy (out, vout->img, sizeof(float) * vout->npix);
+    if (vf_out) memcpy (vf_out, vf->img, sizeof(float) * 3 * vf->npix);
     return 0;
 }
 

@@ -55,6 +55,12 @@ cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
 cudaError_t launch_pad_grad4 (const float* grad3, float4* grad4, long long n,
     cudaStream_t st);
 
+// Dense field (vf, may be NULL) and/or warped moving image (warped, may be
+// NULL) over the ROI's voxels (warp.cu).
+cudaError_t launch_field_warp (const BspGeom& g, const float* coeff,
+    const float* luts, const float* mimg, float default_value, float* vf,
+    float* warped, cudaStream_t st);
+
 cudaError_t launch_reduce_score (const double* score_part,
     const int* count_part, int n, DevResult* res, int mode,
     cudaStream_t st);

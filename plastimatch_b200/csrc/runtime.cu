@@ -41,6 +41,7 @@ struct b200bsp_ctx {
     float* d_fixed = nullptr;
     float* d_moving = nullptr;
     float* d_mgrad = nullptr;
+    float* d_out = nullptr;           // field / warp staging (host outputs)
     float4* d_mgrad4 = nullptr;       // TC form, nearest gradient: padded copy
     float* d_coeff = nullptr;
     float* d_luts = nullptr;
@@ -191,6 +192,7 @@ static void
 free_all (b200bsp_ctx* c)
 {
     cudaFree (c->d_fixed); cudaFree (c->d_moving); cudaFree (c->d_mgrad);
+    cudaFree (c->d_out);
     cudaFree (c->d_mgrad4);
     cudaFree (c->d_coeff); cudaFree (c->d_luts); cudaFree (c->d_grad);
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
@@ -817,11 +819,57 @@ b200bsp_score (b200bsp_ctx* c, const float* coeff, int metric_type,
     return B200BSP_OK;
 }
 
+// Field and warp share one path: coefficients to the device, outputs
+// either written in place (device pointers) or through the staging buffer.
+static int
+field_warp (b200bsp_ctx* c, const float* coeff, float* vf, float* warped,
+    float default_value)
+{
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    const BspGeom& g = c->geom;
+    const size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
+    float* out = vf ? vf : warped;
+    const size_t bytes = (vf ? 3 : 1) * nf * sizeof (float);
+    const bool dev_out = is_device_ptr (out);
+    float* target = out;
+    if (!dev_out) {
+        if (!c->d_out) {
+            cudaError_t e = cudaMalloc ((void**) &c->d_out,
+                3 * nf * sizeof (float));
+            if (e != cudaSuccess) {
+                cudaGetLastError ();
+                c->d_out = nullptr;
+                return fail (c, B200BSP_E_OOM, "staging buffer: %s",
+                    cudaGetErrorString (e));
+            }
+        }
+        target = c->d_out;
+    }
+    bool whole = true;
+    for (int d = 0; d < 3; d++) {
+        whole = whole && g.roi_off[d] == 0 && g.roi_dim[d] == g.fdim[d];
+    }
+    if (vf && !whole) CK (cudaMemsetAsync (target, 0, bytes, c->stream));
+    CK (launch_field_warp (g, dcoeff, c->d_luts, c->d_moving, default_value,
+        vf ? target : nullptr, vf ? nullptr : target, c->stream));
+    c->last_launches = 1;
+    rc = mark_main_done (c);
+    if (rc) return rc;
+    if (!dev_out) {
+        CK (cudaMemcpyAsync (out, target, bytes, cudaMemcpyDeviceToHost,
+            c->stream));
+    }
+    return end_eval (c, !dev_out);
+}
+
 extern "C" int
 b200bsp_interpolate_vf (b200bsp_ctx* c, const float* coeff, float* vf)
 {
     if (!c) return B200BSP_E_BADARG;
-    return fail (c, B200BSP_E_UNSUPPORTED, "interpolate_vf not built yet");
+    if (!vf) return fail (c, B200BSP_E_BADARG, "null output");
+    return field_warp (c, coeff, vf, nullptr, 0.f);
 }
 
 extern "C" int
@@ -829,7 +877,14 @@ b200bsp_warp (b200bsp_ctx* c, const float* coeff, float default_value,
     float* warped)
 {
     if (!c) return B200BSP_E_BADARG;
-    return fail (c, B200BSP_E_UNSUPPORTED, "warp not built yet");
+    if (!warped) return fail (c, B200BSP_E_BADARG, "null output");
+    for (int d = 0; d < 3; d++) {
+        if (c->geom.roi_off[d] != 0 || c->geom.roi_dim[d] != c->geom.fdim[d]) {
+            return fail (c, B200BSP_E_UNSUPPORTED,
+                "warp needs the grid's ROI to be the whole fixed image");
+        }
+    }
+    return field_warp (c, coeff, nullptr, warped, default_value);
 }
 
 extern "C" int

@@ -3,7 +3,9 @@
 Run where the reference tree is available and oracle/_ref/libplmref.so has
 been built (oracle/build_ref.sh):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--force]
+
+(existing fixtures are kept unless --force)
 
 Each fixture holds the inputs (images, geometry, grid, coefficients) and
 the outputs of the compiled reference on them, so parity is pinned even
@@ -54,10 +56,20 @@ CASES = {
 }
 
 
-def main():
+# Dense vector field / warp fixtures: the inputs of an MSE case and the
+# reference's bspline_interpolate_vf and bspline_warp (linear, default -7)
+# on them.  Warp needs the ROI to be the whole image.
+WARP_CASES = {"warp_small": "mse_small", "warp_dcos": "mse_dcos",
+              "vf_roi": "mse_roi"}
+WARP_DEFAULT = -7.0
+
+
+def main(force=False):
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libplmref.so missing; run oracle/build_ref.sh")
     for name, (dim, sp, vpr, roff, rdim, seed, dcos, remap, csig) in CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
         fixed, moving = make_pair(dim, sp, seed, dcos, remap)
         grid = BsplineGrid.for_volume(fixed, vpr, roi_offset=roff,
                                       roi_dim=rdim)
@@ -99,7 +111,31 @@ def main():
             rec["f_hist"], rec["m_hist"], rec["j_hist"] = r.f_hist, r.m_hist, r.j_hist
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **rec)
         print("wrote", name)
+    for name, base in WARP_CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
+        dim, sp, vpr, roff, rdim, seed, dcos, remap, csig = CASES[base]
+        fixed, moving = make_pair(dim, sp, seed, dcos, remap)
+        grid = BsplineGrid.for_volume(fixed, vpr, roi_offset=roff,
+                                      roi_dim=rdim)
+        coeff = synth.random_coeff(grid, csig, seed=seed + 3)
+        rec = dict(
+            fixed=fixed.img, moving=moving.img,
+            f_origin=np.array(fixed.origin, np.float32),
+            f_spacing=np.array(fixed.spacing, np.float32),
+            m_origin=np.array(moving.origin, np.float32),
+            m_spacing=np.array(moving.spacing, np.float32),
+            dcos=np.array(fixed.dcos, np.float32),
+            roi_offset=np.array(grid.roi_offset), roi_dim=np.array(grid.roi_dim),
+            vpr=np.array(grid.vox_per_rgn), coeff=coeff,
+            vf=O.ref_interpolate_vf(grid, fixed, coeff),
+            default=np.float32(WARP_DEFAULT))
+        if rdim is None:
+            rec["warped"], rec["warp_vf"] = O.ref_warp(grid, fixed, moving,
+                                                       coeff, WARP_DEFAULT)
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **rec)
+        print("wrote", name)
 
 
 if __name__ == "__main__":
-    main()
+    main(force="--force" in sys.argv)

@@ -94,3 +94,30 @@ def test_reference_reproduces_golden(name):
     r = O.ref_metric(grid, fixed, moving, coeff, flavor="g",
                      moving_grad=rec["moving_grad"])
     np.testing.assert_array_equal(r.grad, rec["g_grad"])
+
+
+WARP_GOLDEN = golden_names("warp") + golden_names("vf")
+
+
+@pytest.mark.parametrize("name", WARP_GOLDEN)
+def test_port_interpolate_vf_bit_exact(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    np.testing.assert_array_equal(O.port_interpolate_vf(grid, fixed, coeff),
+                                  rec["vf"])
+
+
+@pytest.mark.parametrize("name", golden_names("warp"))
+def test_port_warp_bit_exact(name):
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    w, vf = O.port_warp(grid, fixed, moving, coeff, float(rec["default"]),
+                        with_vf=True)
+    np.testing.assert_array_equal(w, rec["warped"])
+    np.testing.assert_array_equal(vf, rec["warp_vf"])
+    # some voxels land outside the moving image and keep the default
+    assert (w == rec["default"]).any() and (w != rec["default"]).any()
+
+
+def test_port_warp_rejects_partial_roi():
+    fixed, moving, grid, coeff, rec = load_golden("vf_roi")
+    with pytest.raises(RuntimeError):
+        O.port_warp(grid, fixed, moving, coeff)
