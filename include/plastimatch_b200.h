@@ -207,6 +207,32 @@ int b200bsp_last_timing (const b200bsp_ctx* ctx, float* ms, int* launches);
 /* Device time of the last evaluation's main tile kernel alone (ms). */
 int b200bsp_last_main_ms (const b200bsp_ctx* ctx, float* ms);
 
+/* Resample types of registration_resample_volume
+ * (src/register/registration_resample.cxx:12-59). */
+#define B200BSP_RESAMPLE_VOXEL         0  /* rate = voxels per output voxel */
+#define B200BSP_RESAMPLE_VOXEL_LEGACY  1  /* same, legacy_subsampling grid */
+#define B200BSP_RESAMPLE_MM            2  /* rate = output spacing (mm) */
+#define B200BSP_RESAMPLE_PERCENT       3  /* rate = fraction of the voxels */
+
+/* The output grid of one pyramid level: volume_subsample_vox,
+ * volume_subsample_vox_legacy, volume_resample_spacing or
+ * volume_resample_percent (src/base/volume_resample.cxx:297-413) by type.
+ * out keeps in's direction cosines.  *is_copy (may be NULL) is 1 when the
+ * reference clones the input instead (voxel types, rate 1 on every axis).
+ * Host only. */
+int b200bsp_resample_geometry (const b200bsp_volume* in, int type,
+    const float rate[3], b200bsp_volume* out, int* is_copy);
+
+/* Trilinear resampling of a float image onto the grid `out`
+ * (volume_resample_float_li, src/base/volume_resample.cxx:70-136):
+ * positions step by out's spacing from out's origin, direction cosines are
+ * not used (as in the reference), voxels whose rounded input index lies
+ * outside the input are 0.  Bit-identical to the reference.  Images may be
+ * host or device memory; allocates temporary device buffers and waits for
+ * the result. */
+int b200bsp_resample (const b200bsp_volume* in, const float* in_img,
+    const b200bsp_volume* out, float* out_img, int device);
+
 /* Largest tile count b200bsp_score_mse_static accepts (its fixed scratch:
  * about 6.4 MB of static device memory per device). */
 #define B200BSP_STATIC_MAX_TILES 8192

@@ -266,6 +266,39 @@ def port_warp(grid, fixed, moving, coeff, default=0.0, with_vf=False):
     return (out, vf.reshape(nz, ny, nx, 3)) if with_vf else out
 
 
+RESAMPLE_MODES = {"voxel": 0, "voxel_legacy": 1, "mm": 2, "percent": 3}
+
+
+def port_resample_geometry(vol, mode, rate):
+    """(dim, origin, spacing, is_copy) of registration_resample_volume."""
+    od = (C.c_int64 * 3)()
+    oo = (C.c_float * 3)()
+    osp = (C.c_float * 3)()
+    copy = port().orc_resample_geometry(
+        (C.c_int64 * 3)(*vol.dim), (C.c_float * 3)(*vol.origin),
+        (C.c_float * 3)(*vol.spacing), C.c_int(RESAMPLE_MODES[mode]),
+        (C.c_float * 3)(*rate), od, oo, osp)
+    return tuple(od), tuple(oo), tuple(osp), bool(copy)
+
+
+def port_resample(vol, mode, rate):
+    """registration_resample_volume on a float image: a Volume."""
+    from plastimatch_b200.geometry import Volume
+    od, oo, osp, copy = port_resample_geometry(vol, mode, rate)
+    if copy:
+        return Volume(vol.img.copy(), origin=vol.origin, spacing=vol.spacing,
+                      dcos=vol.dcos)
+    out = np.zeros(od[0] * od[1] * od[2], np.float32)
+    img = np.ascontiguousarray(vol.img, np.float32)
+    port().orc_resample_li((C.c_int64 * 3)(*vol.dim),
+                           (C.c_float * 3)(*vol.origin),
+                           (C.c_float * 3)(*vol.spacing), _p(img),
+                           (C.c_int64 * 3)(*od), (C.c_float * 3)(*oo),
+                           (C.c_float * 3)(*osp), _p(out))
+    return Volume(out.reshape(od[2], od[1], od[0]), origin=oo, spacing=osp,
+                  dcos=vol.dcos)
+
+
 # ----------------------------------------------------------- reference ---
 
 def _ref_geom(v) -> RefGeom:
@@ -370,3 +403,22 @@ def ref_warp(grid, fixed, moving, coeff, default=0.0, linear=True):
                    _p(vf))
     nx, ny, nz = fixed.dim
     return out.reshape(nz, ny, nx), vf.reshape(nz, ny, nx, 3)
+
+
+def ref_resample(vol, mode, rate):
+    """The reference's resampling (registration_resample_volume): a Volume."""
+    from plastimatch_b200.geometry import Volume
+    ref().ref_resample.restype = C.c_int64
+    od = (C.c_int64 * 3)()
+    oo = (C.c_float * 3)()
+    osp = (C.c_float * 3)()
+    img = np.ascontiguousarray(vol.img, np.float32)
+    g = _ref_geom(vol)
+    rate3 = (C.c_float * 3)(*rate)
+    n = ref().ref_resample(C.byref(g), _p(img), C.c_int(RESAMPLE_MODES[mode]),
+                           rate3, od, oo, osp, None, C.c_int64(0))
+    out = np.zeros(n, np.float32)
+    ref().ref_resample(C.byref(g), _p(img), C.c_int(RESAMPLE_MODES[mode]),
+                       rate3, od, oo, osp, _p(out), C.c_int64(n))
+    return Volume(out.reshape(od[2], od[1], od[0]), origin=tuple(oo),
+                  spacing=tuple(osp), dcos=vol.dcos)

@@ -1525,3 +1525,99 @@ orc_warp (const orc_grid* g, const orc_vol* fx, const orc_vol* mv,
     free (q_lut);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Pyramid resampling                                                   */
+/* ------------------------------------------------------------------ */
+
+static int64_t
+round_long (double x)       /* ROUND_PLM_LONG (src/sys/plm_math.h:53-54) */
+{
+    return (x >= 0) ? (int64_t) (x + 0.5) : (int64_t) (-(-x + 0.5));
+}
+
+/* Output geometry of registration_resample_volume
+ * (src/register/registration_resample.cxx:12-59) for resample type mode:
+ * 0 voxel rate (volume_subsample_vox, src/base/volume_resample.cxx:297-315),
+ * 1 voxel rate, legacy (volume_subsample_vox_legacy, :337-357),
+ * 2 millimetres (volume_resample_spacing, :381-393),
+ * 3 percent (volume_resample_percent, :395-413).
+ * Returns 1 when the reference clones the input instead (voxel rate 1). */
+int
+orc_resample_geometry (const int64_t dim[3], const float origin[3],
+    const float spacing[3], int mode, const float rate[3],
+    int64_t odim[3], float oorigin[3], float ospacing[3])
+{
+    if ((mode == 0 || mode == 1) && rate[0] == 1.0f && rate[1] == 1.0f
+        && rate[2] == 1.0f) {
+        for (int d = 0; d < 3; d++) {
+            odim[d] = dim[d]; oorigin[d] = origin[d]; ospacing[d] = spacing[d];
+        }
+        return 1;
+    }
+    for (int d = 0; d < 3; d++) {
+        if (mode == 0) {
+            int64_t r = round_long (rate[d]);
+            odim[d] = (dim[d] + r - 1) / r;
+            oorigin[d] = origin[d];
+            ospacing[d] = spacing[d] * r;
+        } else if (mode == 1) {
+            float in_size = dim[d] * spacing[d];
+            odim[d] = dim[d] / (int64_t) rate[d];
+            if (odim[d] < 1) odim[d] = 1;
+            ospacing[d] = in_size / odim[d];
+            oorigin[d] = (float) (origin[d] - 0.5 * spacing[d]
+                + 0.5 * ospacing[d]);
+        } else if (mode == 2) {
+            float in_size = (dim[d] - 1) * spacing[d];
+            odim[d] = 1 + round_long (in_size / rate[d]);
+            oorigin[d] = origin[d];
+            ospacing[d] = rate[d];
+        } else {
+            float in_size = (dim[d] - 1) * spacing[d];
+            odim[d] = 1 + round_long (rate[d] * (dim[d] - 1));
+            ospacing[d] = odim[d] == 1 ? in_size : in_size / (odim[d] - 1);
+            oorigin[d] = origin[d];
+        }
+    }
+    return 0;
+}
+
+/* volume_resample_float_li (src/base/volume_resample.cxx:70-136): output
+ * positions advance by the output spacing from the output origin (direction
+ * cosines ignored, as the reference does), the input index is
+ * (position - origin) / spacing, a voxel whose rounded index falls outside
+ * the input is 0, the rest are trilinear (li_clamp, LI_VALUE). */
+void
+orc_resample_li (const int64_t idim[3], const float iorigin[3],
+    const float ispacing[3], const float* in, const int64_t odim[3],
+    const float oorigin[3], const float ospacing[3], float* out)
+{
+    int64_t v = 0;
+    float x, y, z, ijk[3];
+    int64_t k, j, i;
+    for (k = 0, z = oorigin[2]; k < odim[2]; k++, z += ospacing[2]) {
+        ijk[2] = (z - iorigin[2]) / ispacing[2];
+        int64_t zi = round_long (ijk[2]);
+        for (j = 0, y = oorigin[1]; j < odim[1]; j++, y += ospacing[1]) {
+            ijk[1] = (y - iorigin[1]) / ispacing[1];
+            int64_t yi = round_long (ijk[1]);
+            for (i = 0, x = oorigin[0]; i < odim[0]; i++, x += ospacing[0], v++) {
+                ijk[0] = (x - iorigin[0]) / ispacing[0];
+                int64_t xi = round_long (ijk[0]);
+                if (zi < 0 || zi >= idim[2] || yi < 0 || yi >= idim[1]
+                    || xi < 0 || xi >= idim[0]) {
+                    out[v] = 0.0f;
+                    continue;
+                }
+                int64_t f[3], r[3];
+                float l1[3], l2[3];
+                for (int d = 0; d < 3; d++)
+                    li_clamp_f (ijk[d], idim[d] - 1, &f[d], &r[d], &l1[d],
+                        &l2[d]);
+                out[v] = li_value_f (l1, l2, vidx (idim, f[0], f[1], f[2]),
+                    in, idim);
+            }
+        }
+    }
+}

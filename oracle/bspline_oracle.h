@@ -104,6 +104,16 @@ int orc_warp (const orc_grid* g, const orc_vol* fixed, const orc_vol* moving,
     const float* m_img, const float* coeff, float default_val, float* out,
     float* vf_out);
 
+/* Pyramid resampling: the output geometry of a resample type (0 voxel
+ * rate, 1 voxel rate legacy, 2 mm, 3 percent; returns 1 for a plain copy)
+ * and the trilinear resampler. */
+int orc_resample_geometry (const int64_t dim[3], const float origin[3],
+    const float spacing[3], int mode, const float rate[3],
+    int64_t odim[3], float oorigin[3], float ospacing[3]);
+void orc_resample_li (const int64_t idim[3], const float iorigin[3],
+    const float ispacing[3], const float* in, const int64_t odim[3],
+    const float oorigin[3], const float ospacing[3], float* out);
+
 #ifdef __cplusplus
 }
 #endif

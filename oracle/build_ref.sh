@@ -38,7 +38,7 @@ CXXFLAGS="-std=c++11 $OPT -fopenmp -fPIC -w -include $HERE/ref/prelude.h \
 UNITS="
 base/volume base/direction_cosines base/direction_matrices base/interpolate
 base/bspline_interpolate base/bspline_warp base/bspline_xform base/bspline_header base/volume_grad
-base/volume_header base/xpm base/pointset
+base/volume_header base/volume_resample base/xpm base/pointset
 util/bspline_correspond
 register/bspline register/bspline_mse register/bspline_score
 register/bspline_state register/bspline_parms register/bspline_mi

@@ -32,6 +32,7 @@
 #include "regularization_parms.h"
 #include "volume.h"
 #include "volume_grad.h"
+#include "volume_resample.h"
 
 extern "C" {
 
@@ -320,6 +321,36 @@ ref_warp (const ref_geom* fg, const ref_geom* mg, const float* mimg,
     memcpy (out, vout->img, sizeof(float) * vout->npix);
     if (vf_out) memcpy (vf_out, vf->img, sizeof(float) * 3 * vf->npix);
     return 0;
+}
+
+/* The resampling step of registration_resample_volume
+ * (src/register/registration_resample.cxx:12-59) for resample type mode
+ * (0 voxel rate, 1 voxel rate legacy, 2 mm, 3 percent), on a float image.
+ * Writes the output geometry; writes the image when out_cap (floats) is
+ * large enough.  Returns the output voxel count. */
+int64_t
+ref_resample (const ref_geom* g, const float* img, int mode,
+    const float rate[3], int64_t odim[3], float oorigin[3], float ospacing[3],
+    float* out, int64_t out_cap)
+{
+    Quiet q;
+    Volume::Pointer v = make_volume (g, img, 1);
+    Volume::Pointer r;
+    bool unit = rate[0] == 1.0f && rate[1] == 1.0f && rate[2] == 1.0f;
+    if ((mode == 0 || mode == 1) && unit) r = v->clone ();
+    else if (mode == 0) r = volume_subsample_vox (v, rate);
+    else if (mode == 1) r = volume_subsample_vox_legacy (v, rate);
+    else if (mode == 2) r = volume_resample_spacing (v, rate);
+    else r = volume_resample_percent (v, rate);
+    for (int d = 0; d < 3; d++) {
+        odim[d] = r->dim[d];
+        oorigin[d] = r->origin[d];
+        ospacing[d] = r->spacing[d];
+    }
+    if (out && out_cap >= r->npix) {
+        memcpy (out, r->img, sizeof(float) * r->npix);
+    }
+    return r->npix;
 }
 
 /* B-spline grid sizes the reference derives (Bspline_header::set,

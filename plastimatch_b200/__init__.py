@@ -99,6 +99,8 @@ _SIGS = {
     "b200bsp_last_timing": (C.c_int, [_VP, _VP, _VP]),
     "b200bsp_last_main_ms": (C.c_int, [_VP, _VP]),
     "b200bsp_last_error": (C.c_char_p, [_VP]),
+    "b200bsp_resample_geometry": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP]),
+    "b200bsp_resample": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int]),
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
 }
@@ -150,6 +152,47 @@ def volume_grad(vol: Volume, device: int = 0) -> np.ndarray:
     _check(lib().b200bsp_volume_grad(C.byref(d), _ptr(vol.img), _ptr(out),
                                      device))
     return out
+
+
+RESAMPLE = {"voxel": 0, "voxel_legacy": 1, "mm": 2, "percent": 3}
+
+
+def resample_geometry(vol: Volume, mode: str, rate):
+    """(dim, origin, spacing, is_copy) of one pyramid level
+    (b200bsp_resample_geometry)."""
+    d = _vol_desc(vol)
+    o = VolumeDesc()
+    cp = C.c_int()
+    _check(lib().b200bsp_resample_geometry(C.byref(d), RESAMPLE[mode],
+                                           (C.c_float * 3)(*rate), C.byref(o),
+                                           C.byref(cp)))
+    return tuple(o.dim), tuple(o.origin), tuple(o.spacing), bool(cp.value)
+
+
+def resample(vol: Volume, dim, origin, spacing, out=None,
+             device: int = 0) -> Volume:
+    """Trilinear resampling onto the grid (dim, origin, spacing)
+    (b200bsp_resample).  vol.img and `out` may be numpy arrays or device
+    tensors; returns a Volume holding the numpy result when out is None."""
+    d = _vol_desc(vol)
+    o = VolumeDesc((C.c_int64 * 3)(*dim), (C.c_float * 3)(*origin),
+                   (C.c_float * 3)(*spacing), (C.c_float * 9)(*vol.dcos))
+    res = np.zeros(dim[0] * dim[1] * dim[2], np.float32) if out is None else out
+    _check(lib().b200bsp_resample(C.byref(d), _ptr(vol.img), C.byref(o),
+                                  _ptr(res), device))
+    if out is not None:
+        return out
+    return Volume(res.reshape(dim[2], dim[1], dim[0]), origin=origin,
+                  spacing=spacing, dcos=vol.dcos)
+
+
+def pyramid_level(vol: Volume, mode: str, rate, device: int = 0) -> Volume:
+    """registration_resample_volume: the image of one pyramid level."""
+    dim, origin, spacing, copy = resample_geometry(vol, mode, rate)
+    if copy:
+        return Volume(vol.img.copy(), origin=vol.origin, spacing=vol.spacing,
+                      dcos=vol.dcos)
+    return resample(vol, dim, origin, spacing, device=device)
 
 
 def score_mse_static(fixed: Volume, moving: Volume, grid: BsplineGrid,

@@ -64,6 +64,22 @@ WARP_CASES = {"warp_small": "mse_small", "warp_dcos": "mse_dcos",
 WARP_DEFAULT = -7.0
 
 
+# Pyramid resampling fixtures: one float image (odd sizes, anisotropic
+# spacing, off-origin) through registration_resample_volume per type.
+RESAMPLE_CASES = {
+    "resample_voxel": ("voxel", (2.0, 3.0, 1.0)),
+    "resample_voxel4": ("voxel", (4.0, 4.0, 2.0)),
+    "resample_legacy": ("voxel_legacy", (2.0, 2.0, 3.0)),
+    "resample_mm": ("mm", (2.3, 1.7, 3.1)),
+    "resample_percent": ("percent", (0.5, 0.37, 0.8)),
+}
+
+
+def resample_input():
+    v = synth.gaussian_blobs((37, 30, 23), spacing=(0.9, 1.1, 2.5), seed=71)
+    return Volume(v.img, origin=(-11.3, 4.2, 7.7), spacing=v.spacing)
+
+
 def main(force=False):
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libplmref.so missing; run oracle/build_ref.sh")
@@ -134,6 +150,21 @@ def main(force=False):
             rec["warped"], rec["warp_vf"] = O.ref_warp(grid, fixed, moving,
                                                        coeff, WARP_DEFAULT)
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **rec)
+        print("wrote", name)
+
+    for name, (mode, rate) in RESAMPLE_CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
+        v = resample_input()
+        r = O.ref_resample(v, mode, rate)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"), img=v.img,
+            origin=np.array(v.origin, np.float32),
+            spacing=np.array(v.spacing, np.float32),
+            mode=np.array(mode), rate=np.array(rate, np.float32),
+            out=r.img, out_dim=np.array(r.dim),
+            out_origin=np.array(r.origin, np.float32),
+            out_spacing=np.array(r.spacing, np.float32))
         print("wrote", name)
 
 

@@ -121,3 +121,23 @@ def test_port_warp_rejects_partial_roi():
     fixed, moving, grid, coeff, rec = load_golden("vf_roi")
     with pytest.raises(RuntimeError):
         O.port_warp(grid, fixed, moving, coeff)
+
+
+def _resample_case(name):
+    from plastimatch_b200.geometry import Volume
+    import os
+    from conftest import GOLDEN
+    r = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+    v = Volume(r["img"], origin=tuple(float(x) for x in r["origin"]),
+               spacing=tuple(float(x) for x in r["spacing"]))
+    return v, str(r["mode"]), tuple(float(x) for x in r["rate"]), r
+
+
+@pytest.mark.parametrize("name", golden_names("resample"))
+def test_port_resample_bit_exact(name):
+    v, mode, rate, rec = _resample_case(name)
+    out = O.port_resample(v, mode, rate)
+    assert out.dim == tuple(int(x) for x in rec["out_dim"])
+    np.testing.assert_array_equal(np.float32(out.origin), rec["out_origin"])
+    np.testing.assert_array_equal(np.float32(out.spacing), rec["out_spacing"])
+    np.testing.assert_array_equal(out.img, rec["out"])
