@@ -38,6 +38,7 @@ extern "C" {
 #define B200BSP_E_TIMEOUT      -4   /* a bounded device-side wait gave up */
 #define B200BSP_E_STATE        -5   /* call out of order (e.g. no images) */
 #define B200BSP_E_UNSUPPORTED  -6   /* valid request this build cannot do */
+#define B200BSP_E_IO           -7   /* file missing, unreadable or malformed */
 
 /* Kernel forms. */
 #define B200BSP_FORM_TC    0   /* tcgen05 tensor-core field + adjoint (default) */
@@ -232,6 +233,34 @@ int b200bsp_resample_geometry (const b200bsp_volume* in, int type,
  * the result. */
 int b200bsp_resample (const b200bsp_volume* in, const float* in_img,
     const b200bsp_volume* out, float* out_img, int device);
+
+/* Save the grid over `fixed` with its coefficients in the reference's
+ * B-spline coefficient file format (Bspline_xform::save,
+ * src/base/bspline_xform.cxx:101-148); Plastimatch reads the file back with
+ * bspline_xform_load.  Host memory. */
+int b200bsp_xform_save (const char* path, const b200bsp_volume* fixed,
+    const b200bsp_grid* grid, const float* coeff);
+
+/* Read a B-spline coefficient file (bspline_xform_load,
+ * src/base/bspline_xform.cxx:150-279): the fixed image geometry, the grid
+ * and num_coeff always; the coefficients (xyz interleaved per knot) when
+ * coeff is non-NULL and coeff_cap >= num_coeff.  Host memory. */
+int b200bsp_xform_load (const char* path, b200bsp_volume* fixed,
+    b200bsp_grid* grid, float* coeff, int64_t coeff_cap, int64_t* num_coeff);
+
+/* Write a float image (channels 1) or an interleaved vector field
+ * (channels 3) as MetaImage, byte for byte as write_mha
+ * (src/base/mha_io.cxx:25-103).  Host memory. */
+int b200bsp_mha_write (const char* path, const b200bsp_volume* geom,
+    int channels, const float* data);
+
+/* Read a MetaImage as read_mha does (src/base/mha_io.cxx:105-241): float,
+ * short or unsigned char samples, either byte order, converted to float;
+ * `channels` is 3 for a vector field.  With data NULL only the header is
+ * read; otherwise cap (floats) must hold dim[0]*dim[1]*dim[2]*channels.
+ * Host memory. */
+int b200bsp_mha_read (const char* path, b200bsp_volume* geom, int* channels,
+    float* data, int64_t cap);
 
 /* Largest tile count b200bsp_score_mse_static accepts (its fixed scratch:
  * about 6.4 MB of static device memory per device). */

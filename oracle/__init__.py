@@ -422,3 +422,43 @@ def ref_resample(vol, mode, rate):
                        rate3, od, oo, osp, _p(out), C.c_int64(n))
     return Volume(out.reshape(od[2], od[1], od[0]), origin=tuple(oo),
                   spacing=tuple(osp), dcos=vol.dcos)
+
+
+def ref_xform_save(path, grid, fixed, coeff):
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    ref().ref_xform_save(os.fsencode(str(path)), C.byref(_ref_geom(fixed)),
+                         C.byref(_ref_grid(grid)), _p(coeff))
+
+
+def ref_xform_load(path):
+    """(RefGeom, RefGrid, coeff) as bspline_xform_load reads them."""
+    r = ref()
+    r.ref_xform_load.restype = C.c_int64
+    g, gr = RefGeom(), RefGrid()
+    n = r.ref_xform_load(os.fsencode(str(path)), C.byref(g), C.byref(gr), None,
+                         C.c_int64(0))
+    if n < 0:
+        raise RuntimeError("reference rejected the file")
+    coeff = np.zeros(n, np.float32)
+    r.ref_xform_load(os.fsencode(str(path)), C.byref(g), C.byref(gr), _p(coeff),
+                     C.c_int64(n))
+    return g, gr, coeff
+
+
+def ref_write_mha(path, vol, vf=None):
+    data = vol.img if vf is None else np.ascontiguousarray(vf, np.float32)
+    ref().ref_write_mha(os.fsencode(str(path)), C.byref(_ref_geom(vol)),
+                        C.c_int(1 if vf is None else 3), _p(data))
+
+
+def ref_read_mha(path):
+    """(RefGeom, channels, float data) as read_mha reads them."""
+    r = ref()
+    r.ref_read_mha.restype = C.c_int64
+    g, ch = RefGeom(), C.c_int()
+    n = r.ref_read_mha(os.fsencode(str(path)), C.byref(g), C.byref(ch), None,
+                       C.c_int64(0))
+    data = np.zeros(n * ch.value, np.float32)
+    r.ref_read_mha(os.fsencode(str(path)), C.byref(g), C.byref(ch), _p(data),
+                   C.c_int64(data.size))
+    return g, ch.value, data

@@ -38,7 +38,7 @@ CXXFLAGS="-std=c++11 $OPT -fopenmp -fPIC -w -include $HERE/ref/prelude.h \
 UNITS="
 base/volume base/direction_cosines base/direction_matrices base/interpolate
 base/bspline_interpolate base/bspline_warp base/bspline_xform base/bspline_header base/volume_grad
-base/volume_header base/volume_resample base/xpm base/pointset
+base/volume_header base/volume_resample base/mha_io base/xpm base/pointset
 util/bspline_correspond
 register/bspline register/bspline_mse register/bspline_score
 register/bspline_state register/bspline_parms register/bspline_mi
@@ -49,7 +49,7 @@ register/bspline_landmarks register/bspline_gm register/similarity_metric_type
 register/bspline_optimize register/bspline_optimize_liblbfgs
 register/bspline_optimize_steepest
 sys/logfile sys/print_and_exit sys/plm_timer sys/string_util sys/file_util
-sys/path_util
+sys/path_util sys/plm_endian sys/plm_fwrite
 "
 OBJS=()
 pids=()

@@ -28,6 +28,7 @@
 #include "bspline_warp.h"
 #include "bspline_xform.h"
 #include "joint_histogram.h"
+#include "mha_io.h"
 #include "metric_state.h"
 #include "regularization_parms.h"
 #include "volume.h"
@@ -351,6 +352,88 @@ ref_resample (const ref_geom* g, const float* img, int mode,
         memcpy (out, r->img, sizeof(float) * r->npix);
     }
     return r->npix;
+}
+
+/* Bspline_xform::save (src/base/bspline_xform.cxx:101-148) of the grid
+ * over geometry fg with coefficients coeff. */
+int
+ref_xform_save (const char* path, const ref_geom* fg, const ref_grid* grid,
+    const float* coeff)
+{
+    Quiet q;
+    Bspline_xform bxf;
+    init_xform (&bxf, fg, grid, coeff);
+    bxf.save (path);
+    return 0;
+}
+
+/* bspline_xform_load (src/base/bspline_xform.cxx:150-279): geometry, grid
+ * and coefficients (coeff may be NULL: sizes only).  Returns num_coeff, or
+ * -1 when the reference rejects the file. */
+int64_t
+ref_xform_load (const char* path, ref_geom* fg, ref_grid* grid, float* coeff,
+    int64_t cap)
+{
+    Quiet q;
+    Bspline_xform* bxf = bspline_xform_load (path);
+    if (!bxf) return -1;
+    const float* dc = bxf->dc.get_matrix ();
+    for (int d = 0; d < 3; d++) {
+        fg->dim[d] = bxf->img_dim[d];
+        fg->origin[d] = bxf->img_origin[d];
+        fg->spacing[d] = bxf->img_spacing[d];
+        grid->roi_offset[d] = bxf->roi_offset[d];
+        grid->roi_dim[d] = bxf->roi_dim[d];
+        grid->vox_per_rgn[d] = bxf->vox_per_rgn[d];
+    }
+    for (int i = 0; i < 9; i++) fg->dcos[i] = dc[i];
+    int64_t n = bxf->num_coeff;
+    if (coeff && cap >= n) memcpy (coeff, bxf->coeff, sizeof(float) * n);
+    delete bxf;
+    return n;
+}
+
+/* write_mha (src/base/mha_io.cxx:25-103) of a float image (channels 1) or
+ * an interleaved vector field (channels 3). */
+int
+ref_write_mha (const char* path, const ref_geom* g, int channels,
+    const float* data)
+{
+    Quiet q;
+    Volume::Pointer v = make_volume (g, data, channels);
+    write_mha (path, v.get ());
+    return 0;
+}
+
+/* read_mha (src/base/mha_io.cxx:105-241) converted to float: geometry,
+ * channel count and data (data may be NULL: header only).  Returns the
+ * voxel count, or -1 when the file cannot be read. */
+int64_t
+ref_read_mha (const char* path, ref_geom* g, int* channels, float* data,
+    int64_t cap)
+{
+    Quiet q;
+    Volume* v = read_mha (path);
+    if (!v) return -1;
+    for (int d = 0; d < 3; d++) {
+        g->dim[d] = v->dim[d];
+        g->origin[d] = v->origin[d];
+        g->spacing[d] = v->spacing[d];
+    }
+    const float* dc = v->direction_cosines.get_matrix ();
+    for (int i = 0; i < 9; i++) g->dcos[i] = dc[i];
+    *channels = v->pix_type == PT_VF_FLOAT_INTERLEAVED ? 3 : 1;
+    int64_t n = v->npix;
+    if (data && cap >= n * *channels) {
+        if (v->pix_type == PT_VF_FLOAT_INTERLEAVED || v->pix_type == PT_FLOAT) {
+            memcpy (data, v->img, sizeof(float) * n * *channels);
+        } else {
+            v->convert (PT_FLOAT);
+            memcpy (data, v->img, sizeof(float) * n);
+        }
+    }
+    delete v;
+    return n;
 }
 
 /* B-spline grid sizes the reference derives (Bspline_header::set,

@@ -30,7 +30,7 @@ B200BSP_OK = 0
 FORMS = {"tc": 0, "fp32": 1}
 MSE_GRAD = {"nearest": 0, "trilinear": 1}
 ERRORS = {-1: "E_BADARG", -2: "E_OOM", -3: "E_CUDA", -4: "E_TIMEOUT",
-          -5: "E_STATE", -6: "E_UNSUPPORTED"}
+          -5: "E_STATE", -6: "E_UNSUPPORTED", -7: "E_IO"}
 
 
 class B200Error(RuntimeError):
@@ -101,6 +101,11 @@ _SIGS = {
     "b200bsp_last_error": (C.c_char_p, [_VP]),
     "b200bsp_resample_geometry": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP]),
     "b200bsp_resample": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int]),
+    "b200bsp_xform_save": (C.c_int, [C.c_char_p, _VP, _VP, _VP]),
+    "b200bsp_xform_load": (C.c_int, [C.c_char_p, _VP, _VP, _VP, C.c_int64,
+                                     _VP]),
+    "b200bsp_mha_write": (C.c_int, [C.c_char_p, _VP, C.c_int, _VP]),
+    "b200bsp_mha_read": (C.c_int, [C.c_char_p, _VP, _VP, _VP, C.c_int64]),
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
 }
@@ -152,6 +157,60 @@ def volume_grad(vol: Volume, device: int = 0) -> np.ndarray:
     _check(lib().b200bsp_volume_grad(C.byref(d), _ptr(vol.img), _ptr(out),
                                      device))
     return out
+
+
+def _path(p) -> bytes:
+    return os.fsencode(os.fspath(p))
+
+
+def xform_save(path, fixed: Volume, grid: BsplineGrid, coeff) -> None:
+    """Write a B-spline coefficient file (Bspline_xform::save format)."""
+    gd = GridDesc((C.c_int64 * 3)(*grid.roi_offset),
+                  (C.c_int64 * 3)(*grid.roi_dim),
+                  (C.c_int64 * 3)(*grid.vox_per_rgn))
+    _check(lib().b200bsp_xform_save(_path(path), C.byref(_vol_desc(fixed)),
+                                    C.byref(gd), _ptr(coeff)))
+
+
+def xform_load(path):
+    """Read a B-spline coefficient file: (geometry dict, BsplineGrid over an
+    image of that geometry, coefficients)."""
+    v, g, n = VolumeDesc(), GridDesc(), C.c_int64()
+    _check(lib().b200bsp_xform_load(_path(path), C.byref(v), C.byref(g), None,
+                                    0, C.byref(n)))
+    coeff = np.zeros(n.value, np.float32)
+    _check(lib().b200bsp_xform_load(_path(path), C.byref(v), C.byref(g),
+                                    _ptr(coeff), n.value, C.byref(n)))
+    geom = dict(dim=tuple(v.dim), origin=tuple(v.origin),
+                spacing=tuple(v.spacing), dcos=tuple(v.dcos))
+    grid = BsplineGrid(geom["origin"], geom["spacing"], geom["dim"],
+                       tuple(g.roi_offset), tuple(g.roi_dim),
+                       tuple(g.vox_per_rgn), geom["dcos"])
+    return geom, grid, coeff
+
+
+def mha_write(path, vol: Volume, vf=None) -> None:
+    """Write vol.img (or, when given, the vector field vf of vol's geometry,
+    shape (nz, ny, nx, 3)) as MetaImage (write_mha format)."""
+    data = vol.img if vf is None else np.ascontiguousarray(vf, np.float32)
+    _check(lib().b200bsp_mha_write(_path(path), C.byref(_vol_desc(vol)),
+                                   1 if vf is None else 3, _ptr(data)))
+
+
+def mha_read(path):
+    """Read a MetaImage: a Volume for one channel, else (vector field
+    (nz, ny, nx, 3), Volume of the geometry with a zero image)."""
+    v, ch = VolumeDesc(), C.c_int()
+    _check(lib().b200bsp_mha_read(_path(path), C.byref(v), C.byref(ch), None, 0))
+    nx, ny, nz = v.dim
+    data = np.zeros(nx * ny * nz * ch.value, np.float32)
+    _check(lib().b200bsp_mha_read(_path(path), C.byref(v), C.byref(ch),
+                                  _ptr(data), data.size))
+    kw = dict(origin=tuple(v.origin), spacing=tuple(v.spacing),
+              dcos=tuple(v.dcos))
+    if ch.value == 1:
+        return Volume(data.reshape(nz, ny, nx), **kw)
+    return data.reshape(nz, ny, nx, 3), Volume(np.zeros((nz, ny, nx)), **kw)
 
 
 RESAMPLE = {"voxel": 0, "voxel_legacy": 1, "mm": 2, "percent": 3}
