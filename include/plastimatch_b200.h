@@ -262,6 +262,61 @@ int b200bsp_mha_write (const char* path, const b200bsp_volume* geom,
 int b200bsp_mha_read (const char* path, b200bsp_volume* geom, int* channels,
     float* data, int64_t cap);
 
+/* Limited-memory BFGS: the optimiser of Plastimatch's "liblbfgs"
+ * implementation (src/register/bspline_optimize_liblbfgs.cxx:20-117 with
+ * liblbfgs' default parameters), restated from the published methods:
+ * two-loop recursion over m correction pairs and the More-Thuente line
+ * search.  Vectors stay in device memory (double). */
+typedef struct {
+    int m;                /* correction pairs kept (6) */
+    double epsilon;       /* stop when ||g|| / max(1, ||x||) <= epsilon (1e-5) */
+    int max_its;          /* stop after iteration k > max_its (Bspline_parms, 10) */
+    int max_feval;        /* ... or after more evaluations than this (10) */
+    int max_linesearch;   /* trials per line search (40) */
+    double min_step, max_step;   /* 1e-20, 1e20 */
+    double ftol;          /* sufficient decrease (1e-4) */
+    double gtol;          /* curvature, strong Wolfe (0.9) */
+    double xtol;          /* relative interval width (1e-16) */
+} b200bsp_lbfgs_parms;
+
+/* status values */
+#define B200BSP_LBFGS_CONVERGED          0   /* gradient test met */
+#define B200BSP_LBFGS_STOPPED            1   /* max_its / max_feval reached */
+#define B200BSP_LBFGS_ALREADY_MINIMIZED  2   /* gradient test met at x0 */
+/* negative: the line search failed (rounding, step limits, trial count);
+ * x is the last accepted point */
+
+typedef struct {
+    int status;
+    int iterations;       /* line searches completed */
+    int fevals;           /* function evaluations */
+    double score;         /* objective at the returned x */
+} b200bsp_lbfgs_result;
+
+/* Fill parms with the defaults above. */
+void b200bsp_lbfgs_default_parms (b200bsp_lbfgs_parms* parms);
+
+/* Optimise the coefficients of the context's registration: the objective is
+ * bspline_score() -- lambda * metric (0 MSE, 1 MI) plus the analytic
+ * regulariser when reg is non-NULL -- evaluated on the device.  coeff (host
+ * or device) holds x0 on entry; on return it holds what Plastimatch's
+ * transform holds after its optimiser: the last evaluated coefficients
+ * (a stop inside a line search leaves the last trial point there), and
+ * res->score the last evaluated total score.  Allocates the optimiser's
+ * device vectors ((2m + 5) doubles per coefficient) for the call. */
+int b200bsp_optimize_lbfgs (b200bsp_ctx* ctx, int metric_type, float lambda,
+    const b200bsp_reg_parms* reg, const b200bsp_lbfgs_parms* parms,
+    float* coeff, b200bsp_lbfgs_result* res);
+
+/* The same optimiser on a caller's function: fn receives host copies of x
+ * (n doubles) and writes the gradient to g, returning f.  x (host) holds x0
+ * on entry and the last accepted point on return (res->score its value). */
+typedef double (*b200bsp_eval_fn) (void* user, const double* x, double* g,
+    int64_t n);
+int b200bsp_lbfgs_minimize (int64_t n, double* x, b200bsp_eval_fn fn,
+    void* user, const b200bsp_lbfgs_parms* parms, b200bsp_lbfgs_result* res,
+    int device);
+
 /* Largest tile count b200bsp_score_mse_static accepts (its fixed scratch:
  * about 6.4 MB of static device memory per device). */
 #define B200BSP_STATIC_MAX_TILES 8192

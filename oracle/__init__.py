@@ -462,3 +462,56 @@ def ref_read_mha(path):
     r.ref_read_mha(os.fsencode(str(path)), C.byref(g), C.byref(ch), _p(data),
                    C.c_int64(data.size))
     return g, ch.value, data
+
+
+def ref_optimize(grid, fixed, moving, coeff, max_its=10, max_feval=10,
+                 flavor="g", metric="mse", bins=32, reg_impl="", curvature=0.0,
+                 threads=0):
+    """Plastimatch's bspline_optimize with implementation liblbfgs:
+    (final coefficients, last total score, iterations, evaluations)."""
+    r = ref()
+    c = np.array(coeff, np.float32)
+    res = RefResult()
+    it = r.ref_optimize(
+        C.byref(_ref_geom(fixed)), _p(fixed.img), C.byref(_ref_geom(moving)),
+        _p(moving.img), None, C.byref(_ref_grid(grid)), _p(c),
+        C.c_char(flavor.encode()), C.c_int(1 if metric == "mi" else 0),
+        C.c_int(bins), C.c_char(reg_impl.encode() if reg_impl else b"\0"),
+        C.c_float(curvature), C.c_int(max_its), C.c_int(max_feval),
+        C.c_int(threads), C.byref(res))
+    return c, float(res.total_score), int(it), int(res.num_vox)
+
+
+LBFGS_EVAL = C.CFUNCTYPE(C.c_double, C.c_void_p, C.POINTER(C.c_double),
+                         C.POINTER(C.c_double), C.c_int, C.c_double)
+LBFGS_PROGRESS = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double),
+                             C.POINTER(C.c_double), C.c_double, C.c_double,
+                             C.c_double, C.c_double, C.c_int, C.c_int, C.c_int)
+
+
+def ref_lbfgs(fn, x0, max_its=1000):
+    """liblbfgs (vendored in the reference) with default parameters on a
+    Python function fn(x) -> (f, g), stopped by Plastimatch's progress rule
+    (k > max_its; the linked liblbfgs consults it after every evaluation):
+    (x, f, status, completed iterations, evaluations)."""
+    n = len(x0)
+    x = np.array(x0, np.float64)
+    state = {"k": 0, "fe": 0}
+
+    def ev(inst, xp, gp, nn, step):
+        xa = np.ctypeslib.as_array(xp, shape=(nn,))
+        f, g = fn(xa.copy())
+        np.ctypeslib.as_array(gp, shape=(nn,))[:] = g
+        state["fe"] += 1
+        return float(f)
+
+    def pr(inst, xp, gp, fx, xn, gn, st, nn, k, ls):
+        if ls > 0:
+            state["k"] = k          # completed line searches
+        return 1 if k > max_its else 0
+
+    cb_e, cb_p = LBFGS_EVAL(ev), LBFGS_PROGRESS(pr)
+    fx = C.c_double()
+    rc = ref().lbfgs(C.c_int(n), x.ctypes.data_as(C.POINTER(C.c_double)),
+                     C.byref(fx), cb_e, cb_p, None, None)
+    return x, fx.value, rc, state["k"], state["fe"]

@@ -354,6 +354,33 @@ ref_resample (const ref_geom* g, const float* img, int mode,
     return r->npix;
 }
 
+/* Plastimatch's optimiser loop (bspline_optimize, src/register/
+ * bspline_optimize.cxx:122-153) with implementation "liblbfgs" and the
+ * given iteration / evaluation limits: coeff holds x0 and receives the
+ * result; res->total_score the last score bspline_score produced. */
+int
+ref_optimize (const ref_geom* fg, const float* fimg,
+    const ref_geom* mg, const float* mimg, const float* mgrad,
+    const ref_grid* grid, float* coeff, char flavor, int metric_mi, int bins,
+    char reg_impl, float curvature_penalty, int max_its, int max_feval,
+    int threads, ref_result* res)
+{
+    Quiet q;
+    Ref_setup s;
+    setup (&s, fg, fimg, mg, mimg, mgrad, grid, coeff, flavor, metric_mi,
+        bins, reg_impl, curvature_penalty, threads);
+    s.parms.optimization = BOPT_LIBLBFGS;
+    s.parms.max_its = max_its;
+    s.parms.max_feval = max_feval;
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    s.bod.optimize ();
+    memcpy (coeff, s.bxf.coeff, sizeof(float) * s.bxf.num_coeff);
+    res->total_score = bst->ssd.total_score;
+    res->num_vox = bst->feval;
+    res->num_coeff = s.bxf.num_coeff;
+    return bst->it;
+}
+
 /* Bspline_xform::save (src/base/bspline_xform.cxx:101-148) of the grid
  * over geometry fg with coefficients coeff. */
 int

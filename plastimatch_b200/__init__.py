@@ -74,6 +74,53 @@ def reg_parms(curvature=0.0, diffusion=0.0, lame_1=0.0, lame_2=0.0,
                     curvature_mixed_weight)
 
 
+class LbfgsParms(C.Structure):
+    _fields_ = [("m", C.c_int), ("epsilon", C.c_double), ("max_its", C.c_int),
+                ("max_feval", C.c_int), ("max_linesearch", C.c_int),
+                ("min_step", C.c_double), ("max_step", C.c_double),
+                ("ftol", C.c_double), ("gtol", C.c_double),
+                ("xtol", C.c_double)]
+
+
+class LbfgsResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int),
+                ("fevals", C.c_int), ("score", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+EVAL_FN = C.CFUNCTYPE(C.c_double, C.c_void_p, C.POINTER(C.c_double),
+                      C.POINTER(C.c_double), C.c_int64)
+
+
+def lbfgs_parms(**kw) -> LbfgsParms:
+    """Defaults of b200bsp_lbfgs_default_parms with keyword overrides."""
+    p = LbfgsParms()
+    lib().b200bsp_lbfgs_default_parms(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def lbfgs_minimize(fn, x0, device: int = 0, **parms):
+    """Minimise fn(x) -> (f, g) (numpy, double) with the device L-BFGS:
+    (x, result dict)."""
+    x = np.array(x0, np.float64)
+
+    def cb(user, xp, gp, n):
+        f, g = fn(np.ctypeslib.as_array(xp, shape=(n,)).copy())
+        np.ctypeslib.as_array(gp, shape=(n,))[:] = g
+        return float(f)
+
+    cfn = EVAL_FN(cb)
+    res = LbfgsResult()
+    p = lbfgs_parms(**parms)
+    _check(lib().b200bsp_lbfgs_minimize(x.size, _ptr(x, np.float64), cfn, None,
+                                        C.byref(p), C.byref(res), device))
+    return x, res.as_dict()
+
+
 _lib = None
 
 # Every entry point of include/plastimatch_b200.h with its ctypes signature.
@@ -106,6 +153,11 @@ _SIGS = {
                                      _VP]),
     "b200bsp_mha_write": (C.c_int, [C.c_char_p, _VP, C.c_int, _VP]),
     "b200bsp_mha_read": (C.c_int, [C.c_char_p, _VP, _VP, _VP, C.c_int64]),
+    "b200bsp_lbfgs_default_parms": (None, [_VP]),
+    "b200bsp_optimize_lbfgs": (C.c_int, [_VP, C.c_int, C.c_float, _VP, _VP,
+                                         _VP, _VP]),
+    "b200bsp_lbfgs_minimize": (C.c_int, [C.c_int64, _VP, _VP, _VP, _VP, _VP,
+                                         C.c_int]),
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
 }
@@ -404,6 +456,20 @@ class Context:
                                    C.addressof(ts), _ptr(g), C.addressof(sm),
                                    C.addressof(n)), self._h)
         return ts.value, g, sm.value, n.value
+
+    def optimize_lbfgs(self, coeff, metric="mse", lam=1.0,
+                       reg: RegParms | None = None, **parms):
+        """b200bsp_optimize_lbfgs from x0 = coeff: (coefficients, result
+        dict).  parms override the defaults (max_its, max_feval, m, ...)."""
+        c = np.array(coeff, np.float32) if not hasattr(coeff, "data_ptr") \
+            else coeff
+        res = LbfgsResult()
+        p = lbfgs_parms(**parms)
+        _check(lib().b200bsp_optimize_lbfgs(
+            self._h, 0 if metric == "mse" else 1, lam,
+            C.byref(reg) if reg is not None else None, C.byref(p), _ptr(c),
+            C.byref(res)), self._h)
+        return c, res.as_dict()
 
     def interpolate_vf(self, coeff):
         nx, ny, nz = self.fixed.dim

@@ -272,6 +272,13 @@ static_fail (int code, const char* msg)
     return fail (nullptr, code, "%s", msg);
 }
 
+// The stream a context's work is ordered on (its own or the caller's).
+cudaStream_t
+ctx_stream (const b200bsp_ctx* c)
+{
+    return c->stream;
+}
+
 } // namespace b200
 
 extern "C" int
