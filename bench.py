@@ -206,6 +206,45 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def registration_c1(P, with_cpu):
+    """The reference's CPU-runnable case: 64^3 blobs, moving = fixed under a
+    seeded B-spline warp (8-voxel spacing, N(0, 2 mm)), vox_per_rgn 8, zero
+    initial coefficients, MSE, 30 L-BFGS iterations (liblbfgs semantics,
+    max_feval 100).  Wall time of the whole optimisation on the device, and
+    of the reference's own bspline_optimize (liblbfgs) on the host cores."""
+    from plastimatch_b200 import synth
+    from plastimatch_b200.geometry import BsplineGrid
+    fixed = synth.gaussian_blobs((64, 64, 64), spacing=(1, 1, 1),
+                                 seed=20261204)
+    g0 = BsplineGrid.for_volume(fixed, 8)
+    moving = synth.warp_trilinear(fixed, fixed, g0,
+                                  synth.random_coeff(g0, 2.0, 20261205))
+    grid = BsplineGrid.for_volume(fixed, 8)
+    x0 = np.zeros(grid.num_coeff, np.float32)
+    out = {}
+    with P.Context(fixed, moving, grid) as ctx:
+        ctx.set_images()
+        ctx.optimize_lbfgs(x0, max_its=2, max_feval=4)      # warm-up
+        t0 = time.perf_counter()
+        c, res = ctx.optimize_lbfgs(x0, max_its=30, max_feval=100)
+        out["gpu_s"] = time.perf_counter() - t0
+        out["fevals"] = res["fevals"]
+        out["final_score"] = res["score"]
+        s0, _, _ = ctx.score_mse(x0)
+        out["initial_score"] = s0
+    if with_cpu:
+        import oracle as O
+        if O.ref_available():
+            t0 = time.perf_counter()
+            _, sref, _, fe = O.ref_optimize(grid, fixed, moving, x0,
+                                            max_its=30, max_feval=100,
+                                            threads=host_threads())
+            out["cpu_reference_s"] = time.perf_counter() - t0
+            out["cpu_reference_fevals"] = fe
+            out["cpu_reference_final_score"] = sref
+    return out
+
+
 def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
                   evals=50):
     """The same workload with the curvature regulariser added (lambda 0.005)
@@ -340,6 +379,9 @@ def main():
 
     extra = extra_metrics(P, ctx, stream, flush, d_coeff, d_grad,
                           grid.num_roi_voxels, args.warmup)
+    if rank == 0:
+        extra["registration_64cubed_vpr8_30_lbfgs_its"] = registration_c1(
+            P, not args.no_cpu_baseline and world == 1)
 
     # end to end through the C ABI with pinned host buffers
     h_coeff = torch.from_numpy(coeff).pin_memory()

@@ -152,6 +152,186 @@ launch_gather_grad (const BspGeom& g, const PartLayout& lay, const float* part,
     return cudaGetLastError ();
 }
 
+// Score reduction and gradient gather in one launch (MSE): every block sums
+// the per-CTA voxel counts in the same fixed order (it needs N to
+// normalise), block 0 also sums the scores and writes the result block
+// (with the tile kernel's error flag); then one thread per knot, x fastest
+// so that a warp's loads of one component run along a footprint row,
+// gathers each component's partials in the same order as
+// gather_grad_kernel and normalises by 2 / N.  The block's gradient goes
+// out through shared memory as one contiguous run (16-byte stores), which
+// also suits an output in mapped host memory.
+constexpr int FIN_THREADS = 256;
+constexpr int FIN_UNROLL = 8;
+
+template <typename T>
+__device__ __forceinline__ void
+store_run (T* __restrict__ dst, const double* __restrict__ src, int n)
+{
+    constexpr int V = 16 / sizeof (T);
+    if (((uintptr_t) dst & 15) == 0) {
+        for (int i = threadIdx.x; i < n / V; i += FIN_THREADS) {
+            __align__ (16) T v[V];
+#pragma unroll
+            for (int e = 0; e < V; e++) v[e] = (T) src[V * i + e];
+            *(uint4*) (dst + V * i) = *(const uint4*) v;
+        }
+        for (int i = (n / V) * V + threadIdx.x; i < n; i += FIN_THREADS) {
+            dst[i] = (T) src[i];
+        }
+    } else {
+        for (int i = threadIdx.x; i < n; i += FIN_THREADS) dst[i] = (T) src[i];
+    }
+}
+
+__global__ void __launch_bounds__ (FIN_THREADS)
+finish_mse_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
+    const double* __restrict__ sp, const int* __restrict__ cp, int nparts,
+    const int* __restrict__ err, DevResult* __restrict__ res,
+    DevResult* __restrict__ res_host, float* __restrict__ grad_out,
+    double* __restrict__ grad64_out, float* __restrict__ score_out,
+    double* __restrict__ score64_out, long long* __restrict__ nvox_out)
+{
+    __shared__ double sh_v[FIN_THREADS / 32];
+    __shared__ int sh_n[FIN_THREADS / 32];
+    __shared__ long long s_n;
+    __shared__ __align__ (16) double s_g[3 * FIN_THREADS];
+    const bool first = blockIdx.x == 0;
+    // the counts (and on block 0 the scores), FIN_UNROLL independent loads
+    // at a time, each thread in ascending index order, then the fixed-order
+    // block sum
+    double v = 0.0;
+    int n32 = 0;
+    for (int i0 = threadIdx.x; i0 < nparts; i0 += FIN_UNROLL * FIN_THREADS) {
+        int c8[FIN_UNROLL];
+        double s8[FIN_UNROLL];
+#pragma unroll
+        for (int u = 0; u < FIN_UNROLL; u++) {
+            const int i = i0 + u * FIN_THREADS;
+            c8[u] = i < nparts ? __ldg (cp + i) : 0;
+            s8[u] = first && i < nparts ? __ldg (sp + i) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < FIN_UNROLL; u++) {
+            n32 += c8[u];
+            v += s8[u];
+        }
+    }
+    block_sum<FIN_THREADS> (v, n32, sh_v, sh_n);
+    if (threadIdx.x == 0) {
+        s_n = n32;
+        if (first) {
+            DevResult r;
+            r.raw = v;
+            r.num_vox = n32;
+            r.error = err ? *err : 0;
+            if (n32 < 1) {
+                r.score = FLT_MAX;
+                r.score_f = FLT_MAX;
+            } else {
+                r.score = v / (double) n32;
+                r.score_f = (float) r.score;
+            }
+            *res = r;
+            if (res_host) *res_host = r;
+            if (score_out) *score_out = r.score_f;
+            if (score64_out) *score64_out = r.score;
+            if (nvox_out) *nvox_out = r.num_vox;
+        }
+    }
+    __syncthreads ();
+    const long long N = s_n;
+    const int knot0 = blockIdx.x * FIN_THREADS;
+    const int knot = knot0 + threadIdx.x;
+    const double scale = N < 1 ? 0.0 : 2.0 / (double) N;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (knot < g.nknots) {
+        const int cx = g.cdims[0], cy = g.cdims[1];
+        const int kx = knot % cx, ky = (knot / cx) % cy, kz = knot / (cx * cy);
+        if (lay.slots == 64) {
+            // slot m = i + 4j + 16k of tile (kx-i, ky-j, kz-k), ascending
+            // m; the loads of 8 slots x 3 components go out together
+#pragma unroll 1
+            for (int m0 = 0; m0 < 64; m0 += 8) {
+                const int k = m0 >> 4, tz = kz - k;
+                const bool okz = tz >= 0 && tz < g.rdims[2];
+                float val[8][3];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int i = q & 3, j = ((m0 + q) >> 2) & 3;
+                    const int tx = kx - i, ty = ky - j;
+                    const bool ok = okz && tx >= 0 && tx < g.rdims[0]
+                        && ty >= 0 && ty < g.rdims[1];
+                    const int t = tx + g.rdims[0] * (ty + g.rdims[1] * tz);
+                    const float* p = part + ((size_t) (m0 + q) * g.ntiles
+                        + (ok ? t : 0)) * 3;
+                    val[q][0] = ok ? __ldg (p) : 0.f;
+                    val[q][1] = ok ? __ldg (p + 1) : 0.f;
+                    val[q][2] = ok ? __ldg (p + 2) : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    s0 += val[q][0]; s1 += val[q][1]; s2 += val[q][2];
+                }
+            }
+        } else {
+            // batches (bi, bj, bk) whose footprint holds the knot: bk and
+            // bj from kz - 3 .. kz and ky - 3 .. ky (the tensor-core layout
+            // has one tile per batch along y and z), bi one of two (a row
+            // split into several batches gives each at least 3 tiles, so a
+            // footprint of bx + 3 knots meets at most two batches); per bk
+            // the 8 x 3 loads first, then the sums in ascending batch order
+            const int KF = lay.kx * lay.ky * lay.kz;
+            const int bi1 = min (lay.nbx - 1, kx / lay.bx);
+#pragma unroll 1
+            for (int dk = 0; dk < 4; dk++) {
+                const int bk = kz - 3 + dk, lz = kz - bk * lay.bz;
+                const bool okz = bk >= 0 && bk < lay.nbz && lz < lay.kz;
+                float val[8][3];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int dj = q >> 1, di = q & 1;
+                    const int bj = ky - 3 + dj, bi = bi1 - 1 + di;
+                    const int ly = ky - bj * lay.by, lx = kx - bi * lay.bx;
+                    const bool ok = okz && bj >= 0 && bj < lay.nby && bi >= 0
+                        && lx < lay.kx && lx >= 0 && ly < lay.ky;
+                    const int b = bi + lay.nbx * (bj + lay.nby * bk);
+                    const int kk = lx + lay.kx * (ly + lay.ky * lz);
+                    const float* p = part + (ok ? (size_t) b * 3 * KF + kk : 0);
+                    val[q][0] = ok ? __ldg (p) : 0.f;
+                    val[q][1] = ok ? __ldg (p + KF) : 0.f;
+                    val[q][2] = ok ? __ldg (p + 2 * KF) : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    s0 += val[q][0]; s1 += val[q][1]; s2 += val[q][2];
+                }
+            }
+        }
+    }
+    s_g[3 * threadIdx.x] = s0 * scale;
+    s_g[3 * threadIdx.x + 1] = s1 * scale;
+    s_g[3 * threadIdx.x + 2] = s2 * scale;
+    __syncthreads ();
+    const int n = 3 * min (FIN_THREADS, g.nknots - knot0);
+    if (grad_out) store_run<float> (grad_out + 3 * (size_t) knot0, s_g, n);
+    if (grad64_out) store_run<double> (grad64_out + 3 * (size_t) knot0, s_g, n);
+}
+
+cudaError_t
+launch_finish_mse (const BspGeom& g, const PartLayout& lay, const float* part,
+    const double* score_part, const int* count_part, int nparts,
+    const int* err, DevResult* res, DevResult* res_host, float* grad_out,
+    double* grad64_out, float* score_out, double* score64_out,
+    long long* nvox_out, cudaStream_t st)
+{
+    const int blocks = std::max (1, (g.nknots + FIN_THREADS - 1) / FIN_THREADS);
+    finish_mse_kernel<<<blocks, FIN_THREADS, 0, st>>> (g, lay, part,
+        score_part, count_part, nparts, err, res, res_host, grad_out,
+        grad64_out, score_out, score64_out, nvox_out);
+    return cudaGetLastError ();
+}
+
 // Central differences with replicated borders, divided by 2*spacing and
 // rotated by the inverse direction cosines; xyz interleaved.
 __global__ void

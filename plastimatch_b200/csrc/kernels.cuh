@@ -61,6 +61,16 @@ cudaError_t launch_field_warp (const BspGeom& g, const float* coeff,
     const float* luts, const float* mimg, float default_value, float* vf,
     float* warped, cudaStream_t st);
 
+// Score reduction + per-knot gradient gather, MSE normalisation, one
+// launch.  err (may be null): the tile kernel's error flag, copied into the
+// result block; res_host (may be null): a second copy of the result block,
+// e.g. mapped host memory.  Any output may be mapped host memory.
+cudaError_t launch_finish_mse (const BspGeom& g, const PartLayout& lay,
+    const float* part, const double* score_part, const int* count_part,
+    int nparts, const int* err, DevResult* res, DevResult* res_host,
+    float* grad_out, double* grad64_out, float* score_out,
+    double* score64_out, long long* nvox_out, cudaStream_t st);
+
 cudaError_t launch_reduce_score (const double* score_part,
     const int* count_part, int n, DevResult* res, int mode,
     cudaStream_t st);

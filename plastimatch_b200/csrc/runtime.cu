@@ -55,6 +55,7 @@ struct b200bsp_ctx {
     void* d_qlut = nullptr;
     float* d_inv_dc = nullptr;
     DevResult* h_res = nullptr;
+    DevResult* h_res_dev = nullptr;   // device alias of h_res (mapped)
     float* h_scalar = nullptr;
 
     PartLayout lay;
@@ -106,6 +107,21 @@ is_device_ptr (const void* p)
         return false;
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Device address of host memory the GPU can write in place (page-locked and
+// mapped, as cudaMallocHost / cudaHostAlloc memory is under unified
+// addressing), else nullptr.
+static void*
+mapped_alias (void* p)
+{
+    if (!p) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes (&a, p) != cudaSuccess) {
+        cudaGetLastError ();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
 // Cofactor inverse in float (Plastimatch src/base/direction_cosines.cxx:
@@ -400,6 +416,11 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         cudaGetLastError ();
         rc2 = fail (c, B200BSP_E_OOM, "cudaMallocHost failed");
     }
+    if (!rc2 && cudaHostGetDevicePointer ((void**) &c->h_res_dev, c->h_res, 0)
+        != cudaSuccess) {
+        cudaGetLastError ();
+        c->h_res_dev = nullptr;          // result block then comes by copy
+    }
 
     // Tile partial-gradient layout of the chosen form.
     int sm_count = 148;
@@ -623,7 +644,7 @@ end_eval (b200bsp_ctx* c, bool wait)
 static int
 run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     double* grad64_out, float* score_out, double* score64_out,
-    long long* nvox_out)
+    long long* nvox_out, DevResult* res_host = nullptr)
 {
     const BspGeom& g = c->geom;
     if (c->opts.form == B200BSP_FORM_FP32) {
@@ -639,20 +660,25 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     c->last_launches++;
     int rc = mark_main_done (c);
     if (rc) return rc;
-    CK (launch_reduce_score (c->d_score_part, c->d_count_part,
-        c->nscore_parts, c->d_res, 0, c->stream));
-    CK (launch_gather_grad (g, c->lay, c->d_part, c->d_res, 0, grad_out,
-        grad64_out, score_out, score64_out, nvox_out, c->stream));
-    c->last_launches += 2;
+    CK (launch_finish_mse (g, c->lay, c->d_part, c->d_score_part,
+        c->d_count_part, c->nscore_parts,
+        c->opts.form == B200BSP_FORM_TC ? c->d_err : nullptr, c->d_res,
+        res_host, grad_out, grad64_out, score_out, score64_out, nvox_out,
+        c->stream));
+    c->last_launches += 1;
     return B200BSP_OK;
 }
 
+// e: the tile kernel's error flag as the finish kernel copied it into the
+// result block; -1 reads it from the device.
 static int
-check_device_error (b200bsp_ctx* c)
+check_device_error (b200bsp_ctx* c, int e = -1)
 {
     if (c->opts.form != B200BSP_FORM_TC) return B200BSP_OK;
-    int e = 0;
-    CK (cudaMemcpy (&e, c->d_err, sizeof (int), cudaMemcpyDeviceToHost));
+    if (e < 0) {
+        e = 0;
+        CK (cudaMemcpy (&e, c->d_err, sizeof (int), cudaMemcpyDeviceToHost));
+    }
     if (e) {
         cudaMemset (c->d_err, 0, sizeof (int));
         return fail (c, B200BSP_E_TIMEOUT,
@@ -676,11 +702,18 @@ b200bsp_score_mse (b200bsp_ctx* c, const float* coeff, float* score,
         if (rc) return rc;
         return end_eval (c, false);
     }
-    float* g_dev = is_device_ptr (grad) ? grad : c->d_grad;
-    rc = run_mse (c, dcoeff, g_dev, nullptr, nullptr, nullptr, nullptr);
+    // Host outputs: the finish kernel writes the gradient and the result
+    // block straight into page-locked mapped memory when it can, else they
+    // come back by copy.
+    float* g_map = (float*) mapped_alias (grad);
+    float* g_dev = is_device_ptr (grad) ? grad : g_map ? g_map : c->d_grad;
+    rc = run_mse (c, dcoeff, g_dev, nullptr, nullptr, nullptr, nullptr,
+        c->h_res_dev);
     if (rc) return rc;
-    CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
-        cudaMemcpyDeviceToHost, c->stream));
+    if (!c->h_res_dev) {
+        CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
     if (grad && g_dev == c->d_grad) {
         CK (cudaMemcpyAsync (grad, c->d_grad, c->num_coeff * sizeof (float),
             cudaMemcpyDeviceToHost, c->stream));
@@ -689,7 +722,7 @@ b200bsp_score_mse (b200bsp_ctx* c, const float* coeff, float* score,
     if (rc) return rc;
     if (score) *score = c->h_res->score_f;
     if (num_vox) *num_vox = c->h_res->num_vox;
-    return check_device_error (c);
+    return check_device_error (c, c->h_res->error);
 }
 
 extern "C" int
@@ -699,20 +732,23 @@ b200bsp_score_mse_f64 (b200bsp_ctx* c, const float* coeff, double* score,
     const float* dcoeff = nullptr;
     int rc = begin_eval (c, coeff, &dcoeff);
     if (rc) return rc;
-    rc = run_mse (c, dcoeff, nullptr, c->d_grad64, nullptr, nullptr, nullptr);
+    double* g_out = is_device_ptr (grad) ? grad : (double*) mapped_alias (grad);
+    rc = run_mse (c, dcoeff, nullptr, g_out ? g_out : c->d_grad64, nullptr,
+        nullptr, nullptr, c->h_res_dev);
     if (rc) return rc;
-    CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
-        cudaMemcpyDeviceToHost, c->stream));
-    if (grad) {
+    if (!c->h_res_dev) {
+        CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (grad && !g_out) {
         CK (cudaMemcpyAsync (grad, c->d_grad64, c->num_coeff * sizeof (double),
-            is_device_ptr (grad) ? cudaMemcpyDeviceToDevice
-                                 : cudaMemcpyDeviceToHost, c->stream));
+            cudaMemcpyDeviceToHost, c->stream));
     }
     rc = end_eval (c, true);
     if (rc) return rc;
     if (score) *score = c->h_res->score;
     if (num_vox) *num_vox = c->h_res->num_vox;
-    return check_device_error (c);
+    return check_device_error (c, c->h_res->error);
 }
 
 extern "C" int

@@ -116,3 +116,31 @@ def test_mse_device_pointers_are_stream_ordered(form):
         torch.cuda.synchronize()
         assert float(sd.item()) == s_h and int(nd.item()) == n_h
         np.testing.assert_array_equal(gd.cpu().numpy(), g_h)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_mse_page_locked_host_outputs(form):
+    """Page-locked (mapped) host buffers are written in place by the device;
+    the results equal those through pageable buffers, float and double."""
+    import ctypes as C
+    torch = pytest.importorskip("torch")
+    fixed, moving, grid, coeff = _c1_case(seed=12)
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images()
+        s_h, g_h, n_h = ctx.score_mse(coeff)
+        hc = torch.from_numpy(coeff).pin_memory()
+        for dtype, fn in ((torch.float32, P.lib().b200bsp_score_mse),
+                          (torch.float64, P.lib().b200bsp_score_mse_f64)):
+            hg = torch.full((grid.num_coeff,), 7.0, dtype=dtype).pin_memory()
+            sc = C.c_float() if dtype == torch.float32 else C.c_double()
+            nv = C.c_int64()
+            P._check(fn(ctx._h, hc.data_ptr(), C.addressof(sc), hg.data_ptr(),
+                        C.addressof(nv)), ctx._h)
+            assert nv.value == n_h
+            if dtype == torch.float32:
+                assert sc.value == s_h
+                np.testing.assert_array_equal(hg.numpy(), g_h)
+            else:
+                s64, g64, n64 = ctx.score_mse_f64(coeff)
+                assert sc.value == s64
+                np.testing.assert_array_equal(hg.numpy(), g64)
