@@ -28,7 +28,7 @@
 // With one 128-voxel block per tile the batches are software-pipelined:
 // the adjoint of batch b runs while batch b+1 is staged and the forward of
 // batch b+1 runs while batch b is gathered.  The per-batch partial sums
-// are combined per knot by gather_grad (deterministic, no atomics).
+// are combined per knot by the finish kernel (deterministic, no atomics).
 #include <algorithm>
 #include <vector>
 
@@ -50,6 +50,11 @@ constexpr int TC_TMEM_COLS = 256;
 constexpr int TC_D_COL = 0;          // forward accumulator [0, N)
 constexpr int TC_G_COL = 128;        // adjoint accumulator [128, 192)
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;
+// Samples per thread per iteration of the axis-aligned voxel phase (their
+// loads go out together).
+#ifndef TC_SPT
+#define TC_SPT 2
+#endif
 
 // Adjoint-operand rows: (c, t) -> r = 8 (3 (t >> 3) + c) + (t & 7), so the
 // three components of one tile sit at the same place in consecutive 8-row
@@ -66,7 +71,7 @@ constexpr int SM_C = 32768;                        // C hi, lo: N*128 B each
 constexpr int SM_C_BYTES = 2 * 80 * 128;           // N <= 80
 constexpr int SM_DC = SM_C + SM_C_BYTES;           // DCDV hi, lo (+ tail);
                                                    // G copy after the adjoint
-constexpr int SM_S = SM_DC + 2 * DC_HALF + DC_TAIL; // knot block (float)
+constexpr int SM_S = SM_DC + 2 * DC_HALF + DC_TAIL; // knot block (bf16 hi|lo)
 constexpr int SM_S_FLOATS = 3 * 16 * (TC_TMAX + 3);
 constexpr int SM_TOTAL = SM_S + SM_S_FLOATS * 4;
 static_assert (3 * TC_TMAX * GS_STRIDE * 4 <= 2 * DC_HALF, "G copy fits the DCDV area");
@@ -87,8 +92,8 @@ struct TcArgs {
     const float* coeff;
     const uint4* qimg;
     float* part;          // [batch][c][knot of the (T+3) x 4 x 4 footprint]
-    double* score_part;
-    int* count_part;
+    double* score_part;   // [CTA]: sum of diff^2 over the CTA's batches
+    int* count_part;      // [CTA]: voxels counted
     int* err;
 };
 
@@ -128,14 +133,17 @@ cbar ()
     named_bar_sync (1, TC_THREADS);
 }
 
-// Knot block S[c][k][j][x] of batch (tx0, ty, tz).  Warp w covers knot
-// rows jk = w, w + 8 (jk = j + 4k), lane x and x + 32.
+// Knot block S[c][k][j][x] of batch (tx0, ty, tz), each coefficient
+// already split: bf16 hi in the low half-word, bf16 lo in the high one (the
+// forward operand repeats every coefficient four times, so it is split once
+// here).  Warp w covers knot rows jk = w, w + 8 (jk = j + 4k), lane x and
+// x + 32.
 __device__ __forceinline__ void
 stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz)
 {
     const BspGeom& g = a.g;
     const int KX = a.T + 3;
-    float* S = (float*) (x.sm + SM_S);
+    uint32_t* S = (uint32_t*) (x.sm + SM_S);
 #pragma unroll
     for (int r = 0; r < 2; r++) {
         const int jk = x.warp + TC_WARPS * r;
@@ -154,9 +162,13 @@ stage_batch (const TcArgs& a, const TcCtx& x, int tx0, int ty, int tz)
                     v1 = __ldg (cp + 1);
                     v2 = __ldg (cp + 2);
                 }
-                S[(0 * 16 + jk) * KX + xx] = v0;
-                S[(1 * 16 + jk) * KX + xx] = v1;
-                S[(2 * 16 + jk) * KX + xx] = v2;
+                unsigned short h, l;
+                split_bf16 (v0, h, l);
+                S[(0 * 16 + jk) * KX + xx] = (uint32_t) h | ((uint32_t) l << 16);
+                split_bf16 (v1, h, l);
+                S[(1 * 16 + jk) * KX + xx] = (uint32_t) h | ((uint32_t) l << 16);
+                split_bf16 (v2, h, l);
+                S[(2 * 16 + jk) * KX + xx] = (uint32_t) h | ((uint32_t) l << 16);
             }
         }
     }
@@ -168,25 +180,22 @@ __device__ __forceinline__ void
 build_c (const TcArgs& a, const TcCtx& x)
 {
     const int T = a.T, N = a.N, KX = T + 3;
-    const float* S = (const float*) (x.sm + SM_S);
+    const uint32_t* S = (const uint32_t*) (x.sm + SM_S);
     for (int o = x.tid; o < N * 8; o += TC_THREADS) {
         const int n = o >> 3, ch = o & 7;    // 16-byte chunk: slots 8ch..8ch+7
         const int c = (n >= T) + (n >= 2 * T);
         const int t = n - c * T;
         // slots 8ch + e: i = e & 3, j = (2ch + (e >> 2)) & 3, k = ch >> 1
-        const float* r0 = S + (c * 16 + ((2 * ch) & 3) + 4 * (ch >> 1)) * KX + t;
-        const float* r1 = r0 + KX;
+        const uint32_t* r0 = S + (c * 16 + ((2 * ch) & 3) + 4 * (ch >> 1)) * KX + t;
+        const uint32_t* r1 = r0 + KX;
         const bool live = c < 3;
         uint32_t hw[4], lw[4];
 #pragma unroll
         for (int e = 0; e < 8; e += 2) {
-            float v0 = live ? ((e < 4) ? r0[e] : r1[e - 4]) : 0.f;
-            float v1 = live ? ((e < 4) ? r0[e + 1] : r1[e - 3]) : 0.f;
-            unsigned short h0, l0, h1, l1;
-            split_bf16 (v0, h0, l0);
-            split_bf16 (v1, h1, l1);
-            hw[e >> 1] = (uint32_t) h0 | ((uint32_t) h1 << 16);
-            lw[e >> 1] = (uint32_t) l0 | ((uint32_t) l1 << 16);
+            const uint32_t p0 = live ? ((e < 4) ? r0[e] : r1[e - 4]) : 0u;
+            const uint32_t p1 = live ? ((e < 4) ? r0[e + 1] : r1[e - 3]) : 0u;
+            hw[e >> 1] = __byte_perm (p0, p1, 0x5410);   // the two hi halves
+            lw[e >> 1] = __byte_perm (p0, p1, 0x7632);   // the two lo halves
         }
         const uint32_t off = sw128_offset (n, 8 * ch, N);
         *(uint4*) (x.sm + SM_C + off) = make_uint4 (hw[0], hw[1], hw[2], hw[3]);
@@ -642,15 +651,15 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
             }
         }
         cbar ();
-        // 2. samples s and s + 256, s = tid + 512 k
+        // 2. samples s + 256 u (u < TC_SPT), s = tid + 256 TC_SPT k
         const int X0 = r * W;
-        for (int s0 = x.tid; s0 < plane; s0 += 2 * TC_THREADS) {
-            bool ok[2];
-            int mvf[2], mvr[2], fidx[2];
-            uint32_t doff[2];
-            float w2[2][3];
+        for (int s0 = x.tid; s0 < plane; s0 += TC_SPT * TC_THREADS) {
+            bool ok[TC_SPT];
+            int mvf[TC_SPT], mvr[TC_SPT], fidx[TC_SPT];
+            uint32_t doff[TC_SPT];
+            float w2[TC_SPT][3];
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < TC_SPT; u++) {
                 const int sv = s0 + u * TC_THREADS;
                 const bool in_plane = sv < plane;
                 const int sc_ = in_plane ? sv : 0;
@@ -695,10 +704,10 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                         + (v & 7) * 2)
                     : 0xffffffffu;
             }
-            float cr[2][8], fv[2];
-            float4 gr[2];
+            float cr[TC_SPT][8], fv[TC_SPT];
+            float4 gr[TC_SPT];
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < TC_SPT; u++) {
                 const float* mp = a.mimg + mvf[u];
                 cr[u][0] = __ldg (mp);
                 cr[u][1] = __ldg (mp + 1);
@@ -712,7 +721,7 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                 if (GRAD_MODE == 0) gr[u] = __ldg (a.mgrad4 + mvr[u]);
             }
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < TC_SPT; u++) {
                 float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
                 diff = ok[u] ? diff : 0.f;
                 scf = fmaf (diff, diff, scf);
@@ -949,19 +958,14 @@ mse_tc_kernel (TcArgs a)
             ty = (b / a.nbx) % g.rdims[1];
             tz = b / (a.nbx * g.rdims[1]);
         };
+        // G -> shared -> the batch's partial gradient (the next writer of
+        // the G copy's area, the voxel phase, starts after a compute
+        // barrier)
         auto finish_batch = [&](int b) {
             dump_g (a, x);
             tc_fence_before ();
             cbar ();
             gather_knots (a, x, b);
-            cblock_sum (sc, cnt, sh_v, sh_n, x);
-            if (x.tid == 0) {
-                a.score_part[b] = sc;
-                a.count_part[b] = cnt;
-            }
-            sc = 0.0;
-            cnt = 0;
-            cbar ();
         };
         if (a.mblk == 1 && nb_local > 0) {
             const VoxelSlot vs0 = voxel_slot (a, x, 0);
@@ -1021,6 +1025,13 @@ mse_tc_kernel (TcArgs a)
                 if (!ok) break;
                 finish_batch (b);
             }
+        }
+        // the CTA's score and voxel count (its batches in order; every
+        // compute warp gets here, also after a failed wait)
+        cblock_sum (sc, cnt, sh_v, sh_n, x);
+        if (x.tid == 0) {
+            a.score_part[blockIdx.x] = sc;
+            a.count_part[blockIdx.x] = cnt;
         }
     }
 

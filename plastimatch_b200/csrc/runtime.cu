@@ -440,7 +440,7 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
             L.kx = L.bx + 3; L.ky = 4; L.kz = 4;
             L.slots = 1;
             part_elems = (size_t) c->plan.nbatches * L.kx * L.ky * L.kz * 3;
-            c->nscore_parts = c->plan.nbatches;
+            c->nscore_parts = c->plan.grid;      // one score part per CTA
         }
     } else if (!rc2) {
         if (mse_fp32_smem_bytes (g) > 200 * 1024) {
