@@ -51,6 +51,23 @@ cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
     const float4* mgrad4, const float* coeff, const void* qlut_bf16,
     float* part, double* score_part, int* count_part, int* err_flag,
     cudaStream_t st);
+
+// Mattes MI on the tensor-core kernel (axis-aligned geometry, tiles of at
+// most 128 voxels, histograms that fit the adjoint operand's area): pass 1
+// (hist_pass: PVI-8 histograms into mi.hist, integer 2^-24 units, count
+// last) or pass 2 (dc/dv from the factor table -> per-batch partials).
+struct TcMiArgs {
+    const uint8_t* fbin;
+    const uint8_t* mbin;
+    int bins;
+    const float* lut;            // [fixed bin][moving bin] pass-2 factors
+    const float* nvf;            // voxel count as float
+    unsigned long long* hist;    // f[B], m[B], j[B*B], count
+};
+bool tc_mi_supported (const BspGeom& g, const TcPlan& p, int bins);
+cudaError_t launch_mi_tc (const BspGeom& g, const TcPlan& p, bool hist_pass,
+    const TcMiArgs& mi, const float* coeff, const void* qimg, float* part,
+    double* score_part, int* count_part, int* err, cudaStream_t st);
 // Moving gradient xyz-interleaved -> float4 (w = 0), for 16-byte loads.
 cudaError_t launch_pad_grad4 (const float* grad3, float4* grad4, long long n,
     cudaStream_t st);

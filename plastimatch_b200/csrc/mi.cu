@@ -464,6 +464,46 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
 }
 
+// The same two passes on the tensor-core kernel (field and adjoint as
+// GEMMs; the histograms in the same integer units, so pass 1 agrees with
+// mi_run's up to the field's rounding); the caller has checked
+// tc_mi_supported.
+int
+mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
+    const PartLayout& lay, const void* qlut, float* part, double* score_part,
+    int* count_part, int* err, const float* d_coeff, DevResult* d_res,
+    float* grad_out, double* grad64_out, cudaStream_t st, int* launches)
+{
+    if (!s->ready) return B200BSP_E_STATE;
+    const int B = s->bins;
+    const int nh = 2 * B + B * B;
+    if (cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
+            st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    TcMiArgs mi;
+    mi.fbin = s->d_fbin;
+    mi.mbin = s->d_mbin;
+    mi.bins = B;
+    mi.lut = s->d_lut;
+    mi.nvf = s->d_nvf;
+    mi.hist = s->d_hist;
+    if (launch_mi_tc (g, plan, true, mi, d_coeff, qlut, part, score_part,
+            count_part, err, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd, s->d_lut,
+        s->d_nvf, d_res);
+    if (launch_mi_tc (g, plan, false, mi, d_coeff, qlut, part, score_part,
+            count_part, err, st) != cudaSuccess
+        || launch_gather_grad (g, lay, part, d_res, 1, grad_out, grad64_out,
+            nullptr, nullptr, nullptr, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    if (launches) *launches += 4;
+    return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+}
+
 int
 mi_fetch (MiState* s, const DevResult* d_res, double* f_hist, double* m_hist,
     double* j_hist, cudaStream_t st)

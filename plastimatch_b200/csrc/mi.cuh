@@ -42,6 +42,10 @@ int mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
 int mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     const float* d_luts, DevResult* d_res, float* grad_out,
     double* grad64_out, cudaStream_t st, int* launches);
+int mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
+    const PartLayout& lay, const void* qlut, float* part, double* score_part,
+    int* count_part, int* err, const float* d_coeff, DevResult* d_res,
+    float* grad_out, double* grad64_out, cudaStream_t st, int* launches);
 int mi_fetch (MiState* s, const DevResult* d_res, double* f_hist,
     double* m_hist, double* j_hist, cudaStream_t st);
 void mi_finish (MiState* s, MiResult* r);

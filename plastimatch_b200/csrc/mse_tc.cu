@@ -56,6 +56,18 @@ constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;
 #define TC_SPT 2
 #endif
 
+// What the kernel computes (template argument MODE):
+//   TC_MSE_NEAREST  MSE score + gradient, moving gradient at the nearest voxel
+//   TC_MSE_LINEAR   MSE score + gradient, trilinear moving gradient
+//   TC_MI_GRAD      Mattes MI pass 2: dc/dv from the PVI-8 factor table
+//   TC_MI_HIST      Mattes MI pass 1: PVI-8 histograms (no adjoint)
+// The MI modes run the axis-aligned voxel phase only.
+constexpr int TC_MSE_NEAREST = 0;
+constexpr int TC_MSE_LINEAR = 1;
+constexpr int TC_MI_GRAD = 2;
+constexpr int TC_MI_HIST = 3;
+constexpr float TC_MI_WUNIT = 16777216.0f;   // histogram weights in 2^-24
+
 // Adjoint-operand rows: (c, t) -> r = 8 (3 (t >> 3) + c) + (t & 7), so the
 // three components of one tile sit at the same place in consecutive 8-row
 // groups.  T <= 26 needs 12 groups = 96 rows; the MMA reads 128 rows per
@@ -95,6 +107,15 @@ struct TcArgs {
     double* score_part;   // [CTA]: sum of diff^2 over the CTA's batches
     int* count_part;      // [CTA]: voxels counted
     int* err;
+    // Mattes MI modes (TC_MI_GRAD, TC_MI_HIST): bin images, bins, the pass-2
+    // factor table [fixed bin][moving bin] and the voxel count (float), the
+    // global histogram f[B], m[B], j[B*B], count
+    const uint8_t* fbin;
+    const uint8_t* mbin;
+    int bins;
+    const float* mi_lut;
+    const float* mi_nvf;
+    unsigned long long* hist;
 };
 
 __device__ __forceinline__ void
@@ -117,6 +138,64 @@ split_bf16x2 (float a, float b, uint32_t& hi, uint32_t& lo)
     __nv_bfloat162 l = __floats2bfloat162_rn (a - ha, b - hb);
     hi = *(uint32_t*) &h;
     lo = *(uint32_t*) &l;
+}
+
+// dc/dv of one sample into the adjoint operand at p (hi at p, lo at
+// p + DC_HALF; components 1024 bytes apart).
+__device__ __forceinline__ void
+store_dc (uint8_t* p, float dc0, float dc1, float dc2)
+{
+    uint32_t h01, l01, h2, l2;
+    split_bf16x2 (dc0, dc1, h01, l01);
+    split_bf16x2 (dc2, 0.f, h2, l2);
+    *(unsigned short*) (p) = (unsigned short) h01;
+    *(unsigned short*) (p + DC_HALF) = (unsigned short) l01;
+    *(unsigned short*) (p + 1024) = (unsigned short) (h01 >> 16);
+    *(unsigned short*) (p + DC_HALF + 1024) = (unsigned short) (l01 >> 16);
+    *(unsigned short*) (p + 2048) = (unsigned short) h2;
+    *(unsigned short*) (p + DC_HALF + 2048) = (unsigned short) l2;
+}
+
+// Mattes MI pass 2 at one sample (the reference's bspline_mi_pvi_8_dc_dv,
+// src/register/bspline_mi.cxx): the derivative of each PVI-8 corner weight
+// along x, y, z times that corner's factor f[fixed bin][corner bin],
+// negated, divided by the voxel count, then projected by the moving
+// image's projection matrix in place (each row sees the rows above already
+// updated, as the reference does).  w2: the upper-corner fractions.
+__device__ __forceinline__ void
+mi_dc_dv (const TcArgs& a, const float w2[3], int fb, const int mb[8],
+    float nv, float dc[3])
+{
+    const float* l2 = w2;
+    const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
+    const float dw[24] = {
+        (-1) * l1[1] * l1[2], l1[0] * (-1) * l1[2], l1[0] * l1[1] * (-1),
+        (+1) * l1[1] * l1[2], l2[0] * (-1) * l1[2], l2[0] * l1[1] * (-1),
+        (-1) * l2[1] * l1[2], l1[0] * (+1) * l1[2], l1[0] * l2[1] * (-1),
+        (+1) * l2[1] * l1[2], l2[0] * (+1) * l1[2], l2[0] * l2[1] * (-1),
+        (-1) * l1[1] * l2[2], l1[0] * (-1) * l2[2], l1[0] * l1[1] * (+1),
+        (+1) * l1[1] * l2[2], l2[0] * (-1) * l2[2], l2[0] * l1[1] * (+1),
+        (-1) * l2[1] * l2[2], l1[0] * (+1) * l2[2], l1[0] * l2[1] * (+1),
+        (+1) * l2[1] * l2[2], l2[0] * (+1) * l2[2], l2[0] * l2[1] * (+1)};
+    const float* lut = a.mi_lut + fb * a.bins;
+    float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const float f = __ldg (lut + mb[k]);
+        d0 -= dw[3 * k + 0] * f;
+        d1 -= dw[3 * k + 1] * f;
+        d2 -= dw[3 * k + 2] * f;
+    }
+    d0 = d0 / nv;
+    d1 = d1 / nv;
+    d2 = d2 / nv;
+    const float* p = a.g.mproj;
+    d0 = d0 * p[0] + d1 * p[1] + d2 * p[2];
+    d1 = d0 * p[3] + d1 * p[4] + d2 * p[5];
+    d2 = d0 * p[6] + d1 * p[7] + d2 * p[8];
+    dc[0] = d0;
+    dc[1] = d1;
+    dc[2] = d2;
 }
 
 struct TcCtx {
@@ -568,7 +647,76 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
 // is guarded, and the moving gradient is one 16-byte load.  Both rounds use
 // W = vx * T0 voxels per row so one sample -> (row, x) mapping serves every
 // batch; a round-1 tile slot past the batch's last tile is dead.
-template <int GRAD_MODE>
+// Mattes MI pass 1 at one sample: the PVI-8 corner weights (products of
+// the per-axis fractions, in the reference's order) as integers in 2^-24
+// units, so the sums do not depend on their order; corners with equal
+// moving bins are merged first, and lanes whose corners all share one bin
+// combine across the warp (match + reduce) so that one lane per distinct
+// (fixed, moving) bin pair updates the shared histograms.  Every lane of
+// the warp calls this (warp collectives).
+__device__ __forceinline__ void
+mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
+    int fb, const int mb_in[8], int& cnt)
+{
+    const int B = a.bins;
+    unsigned long long* hf = (unsigned long long*) (x.sm + SM_DC);
+    unsigned long long* hm = hf + B;
+    unsigned long long* hj = hf + 2 * B;
+    const float* l2 = w2;
+    const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
+    const float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
+        l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
+        l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
+    int mb[8];
+    unsigned int q[8];
+    bool first[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        mb[k] = mb_in[k];
+        q[k] = __float2uint_rn (w[k] * TC_MI_WUNIT);
+        first[k] = live;
+    }
+    bool single = true;
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+#pragma unroll
+        for (int k2 = 0; k2 < k; k2++) {
+            if (first[k] && first[k2] && mb[k2] == mb[k]) {
+                q[k2] += q[k];
+                first[k] = false;
+            }
+        }
+        single = single && !first[k];
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        const unsigned peers = __match_any_sync (live_mask, fb);
+        if (x.lane == __ffs (peers) - 1) {
+            atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
+        }
+        cnt++;
+    }
+    const unsigned single_mask = __ballot_sync (0xffffffffu, live && single);
+    if (live && single) {
+        const int key = fb * B + mb[0];
+        const unsigned peers = __match_any_sync (single_mask, key);
+        const unsigned sum = __reduce_add_sync (peers, q[0]);
+        if (x.lane == __ffs (peers) - 1) {
+            atomicAdd (&hm[mb[0]], (unsigned long long) sum);
+            atomicAdd (&hj[key], (unsigned long long) sum);
+        }
+    } else if (live) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if (first[k]) {
+                atomicAdd (&hm[mb[k]], (unsigned long long) q[k]);
+                atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
+            }
+        }
+    }
+}
+
+template <int MODE>
 __device__ __forceinline__ void
 voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
     int tx0, int ty, int tz, double& sc, int& cnt)
@@ -592,8 +740,9 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
     float scf = 0.f;
 
     // Padding voxels (V..127) carry no samples; zero their adjoint columns
-    // in the rows of live tiles (see voxel_phase_xline).
-    const int npad = 128 - a.V;
+    // in the rows of live tiles (see voxel_phase_xline).  The histogram
+    // pass has no adjoint (its histograms live in that area).
+    const int npad = MODE == TC_MI_HIST ? 0 : 128 - a.V;
     for (int o = x.tid; o < npad * T; o += TC_THREADS) {
         const int tb = o / npad, v = a.V + (o - tb * npad);
         uint8_t* p = dch + (v >> 6) * DC_CHUNK + (3 * (tb >> 3)) * 1024
@@ -651,9 +800,12 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
             }
         }
         cbar ();
-        // 2. samples s + 256 u (u < TC_SPT), s = tid + 256 TC_SPT k
+        // 2. samples s + 256 u (u < TC_SPT), s = tid + 256 TC_SPT k; the MI
+        //    histogram pass keeps every lane of a warp in the loop (warp
+        //    collectives), the other modes let a lane leave at the plane end
         const int X0 = r * W;
-        for (int s0 = x.tid; s0 < plane; s0 += TC_SPT * TC_THREADS) {
+        const int s_end = MODE == TC_MI_HIST ? plane + x.lane : plane;
+        for (int s0 = x.tid; s0 < s_end; s0 += TC_SPT * TC_THREADS) {
             bool ok[TC_SPT];
             int mvf[TC_SPT], mvr[TC_SPT], fidx[TC_SPT];
             uint32_t doff[TC_SPT];
@@ -704,47 +856,70 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                         + (v & 7) * 2)
                     : 0xffffffffu;
             }
-            float cr[TC_SPT][8], fv[TC_SPT];
-            float4 gr[TC_SPT];
+            if constexpr (MODE == TC_MSE_NEAREST || MODE == TC_MSE_LINEAR) {
+                float cr[TC_SPT][8], fv[TC_SPT];
+                float4 gr[TC_SPT];
 #pragma unroll
-            for (int u = 0; u < TC_SPT; u++) {
-                const float* mp = a.mimg + mvf[u];
-                cr[u][0] = __ldg (mp);
-                cr[u][1] = __ldg (mp + 1);
-                cr[u][2] = __ldg (mp + dxm);
-                cr[u][3] = __ldg (mp + dxm + 1);
-                cr[u][4] = __ldg (mp + dxym);
-                cr[u][5] = __ldg (mp + dxym + 1);
-                cr[u][6] = __ldg (mp + dxym + dxm);
-                cr[u][7] = __ldg (mp + dxym + dxm + 1);
-                fv[u] = __ldg (a.fimg + fidx[u]);
-                if (GRAD_MODE == 0) gr[u] = __ldg (a.mgrad4 + mvr[u]);
-            }
-#pragma unroll
-            for (int u = 0; u < TC_SPT; u++) {
-                float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
-                diff = ok[u] ? diff : 0.f;
-                scf = fmaf (diff, diff, scf);
-                cnt += ok[u] ? 1 : 0;
-                float dc0, dc1, dc2;
-                if (GRAD_MODE == 0) {
-                    dc0 = diff * gr[u].x; dc1 = diff * gr[u].y; dc2 = diff * gr[u].z;
-                } else {
-                    float grd[3];
-                    trilinear_lerp_grad (g, w2[u], cr[u], grd);
-                    dc0 = diff * grd[0]; dc1 = diff * grd[1]; dc2 = diff * grd[2];
+                for (int u = 0; u < TC_SPT; u++) {
+                    const float* mp = a.mimg + mvf[u];
+                    cr[u][0] = __ldg (mp);
+                    cr[u][1] = __ldg (mp + 1);
+                    cr[u][2] = __ldg (mp + dxm);
+                    cr[u][3] = __ldg (mp + dxm + 1);
+                    cr[u][4] = __ldg (mp + dxym);
+                    cr[u][5] = __ldg (mp + dxym + 1);
+                    cr[u][6] = __ldg (mp + dxym + dxm);
+                    cr[u][7] = __ldg (mp + dxym + dxm + 1);
+                    fv[u] = __ldg (a.fimg + fidx[u]);
+                    if (MODE == TC_MSE_NEAREST) gr[u] = __ldg (a.mgrad4 + mvr[u]);
                 }
-                if (doff[u] != 0xffffffffu) {
-                    uint8_t* p = dch + doff[u];
-                    uint32_t h01, l01, h2, l2;
-                    split_bf16x2 (dc0, dc1, h01, l01);
-                    split_bf16x2 (dc2, 0.f, h2, l2);
-                    *(unsigned short*) (p) = (unsigned short) h01;
-                    *(unsigned short*) (p + DC_HALF) = (unsigned short) l01;
-                    *(unsigned short*) (p + 1024) = (unsigned short) (h01 >> 16);
-                    *(unsigned short*) (p + DC_HALF + 1024) = (unsigned short) (l01 >> 16);
-                    *(unsigned short*) (p + 2048) = (unsigned short) h2;
-                    *(unsigned short*) (p + DC_HALF + 2048) = (unsigned short) l2;
+#pragma unroll
+                for (int u = 0; u < TC_SPT; u++) {
+                    float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
+                    diff = ok[u] ? diff : 0.f;
+                    scf = fmaf (diff, diff, scf);
+                    cnt += ok[u] ? 1 : 0;
+                    float dc0, dc1, dc2;
+                    if (MODE == TC_MSE_NEAREST) {
+                        dc0 = diff * gr[u].x; dc1 = diff * gr[u].y; dc2 = diff * gr[u].z;
+                    } else {
+                        float grd[3];
+                        trilinear_lerp_grad (g, w2[u], cr[u], grd);
+                        dc0 = diff * grd[0]; dc1 = diff * grd[1]; dc2 = diff * grd[2];
+                    }
+                    if (doff[u] != 0xffffffffu) store_dc (dch + doff[u], dc0, dc1, dc2);
+                }
+            } else {
+                // PVI-8: the fixed voxel's bin and the bins of the eight
+                // corners (the trilinear corners, in the same order)
+                int fb[TC_SPT], mb[TC_SPT][8];
+#pragma unroll
+                for (int u = 0; u < TC_SPT; u++) {
+                    const uint8_t* mp = a.mbin + mvf[u];
+                    mb[u][0] = __ldg (mp);
+                    mb[u][1] = __ldg (mp + 1);
+                    mb[u][2] = __ldg (mp + dxm);
+                    mb[u][3] = __ldg (mp + dxm + 1);
+                    mb[u][4] = __ldg (mp + dxym);
+                    mb[u][5] = __ldg (mp + dxym + 1);
+                    mb[u][6] = __ldg (mp + dxym + dxm);
+                    mb[u][7] = __ldg (mp + dxym + dxm + 1);
+                    fb[u] = __ldg (a.fbin + fidx[u]);
+                }
+                if constexpr (MODE == TC_MI_GRAD) {
+                    const float nv = __ldg (a.mi_nvf);
+#pragma unroll
+                    for (int u = 0; u < TC_SPT; u++) {
+                        float dc[3];
+                        mi_dc_dv (a, w2[u], fb[u], mb[u], nv, dc);
+                        if (!ok[u]) dc[0] = dc[1] = dc[2] = 0.f;
+                        if (doff[u] != 0xffffffffu) store_dc (dch + doff[u], dc[0], dc[1], dc[2]);
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < TC_SPT; u++) {
+                        mi_hist_add (a, x, ok[u], w2[u], fb[u], mb[u], cnt);
+                    }
                 }
             }
         }
@@ -861,10 +1036,11 @@ cblock_sum (double& v, int& n, double* sh_v, int* sh_n, const TcCtx& x)
 
 // Tensor-core warp: for every batch and 128-voxel block, wait for the
 // forward operands, issue the forward GEMM, wait for dc/dv, issue the
-// adjoint.  Bounded waits; gives up when a compute wait failed.
+// adjoint (the MI histogram pass has no adjoint).  Bounded waits; gives up
+// when a compute wait failed.
 __device__ __forceinline__ void
-mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, uint64_t* bars,
-    volatile int* s_abort)
+mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, bool adjoint,
+    uint64_t* bars, volatile int* s_abort)
 {
     uint32_t ph_c = 0, ph_dc = 0;
     for (int i = 0; i < nb_local && !*s_abort; i++) {
@@ -876,6 +1052,7 @@ mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, uint64_t* bars,
             if (!ok) { *s_abort = 1; atomicExch (a.err, 3); return; }
             ph_c ^= 1;
             issue_forward (a, x, &bars[2]);
+            if (!adjoint) continue;
             ok = false;
             for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
                 if (mbar_try_wait (&bars[1], ph_dc)) { ok = true; break; }
@@ -887,7 +1064,7 @@ mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, uint64_t* bars,
     }
 }
 
-template <int GRAD_MODE>
+template <int MODE>
 __global__ void __launch_bounds__ (TC_BLOCK, 2)
 mse_tc_kernel (TcArgs a)
 {
@@ -947,7 +1124,9 @@ mse_tc_kernel (TcArgs a)
     volatile int* abort_flag = &s_abort;
 
     if (mma_warp) {
-        if (x.lane == 0) mma_loop (a, x, nb_local, s_bar, abort_flag);
+        if (x.lane == 0) {
+            mma_loop (a, x, nb_local, MODE != TC_MI_HIST, s_bar, abort_flag);
+        }
         __syncwarp ();
     } else {
         uint32_t ph_d = 0, ph_g = 0;
@@ -981,12 +1160,14 @@ mse_tc_kernel (TcArgs a)
                 const int b = blockIdx.x + i * gridDim.x;
                 coords (b, tx0, ty, tz);
                 if (!cwait (a, x, &s_bar[2], ph_d, abort_flag, 1)) break;
-                if (a.axis) {
-                    voxel_phase_axis<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                if constexpr (MODE >= TC_MI_GRAD) {
+                    voxel_phase_axis<MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                } else if (a.axis) {
+                    voxel_phase_axis<MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
                 } else {
-                    voxel_phase_xline<GRAD_MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
+                    voxel_phase_xline<MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
                 }
-                warp_arrive (x, &s_bar[1]);
+                if (MODE != TC_MI_HIST) warp_arrive (x, &s_bar[1]);
                 if (i + 1 < nb_local) {
                     int nx0, ny, nz;
                     coords (b + gridDim.x, nx0, ny, nz);
@@ -995,10 +1176,11 @@ mse_tc_kernel (TcArgs a)
                     build_c (a, x);
                     warp_arrive (x, &s_bar[0]);
                 }
+                if (MODE == TC_MI_HIST) continue;
                 if (!cwait (a, x, &s_bar[3], ph_g, abort_flag, 2)) break;
                 finish_batch (b);
             }
-        } else {
+        } else if constexpr (MODE < TC_MI_GRAD) {
             // Tiles of more than 128 voxels: Q is reloaded per 128-voxel
             // block, so batches run one after another.
             for (int i = 0; i < nb_local; i++) {
@@ -1017,7 +1199,7 @@ mse_tc_kernel (TcArgs a)
                     warp_arrive (x, &s_bar[0]);
                     ok = cwait (a, x, &s_bar[2], ph_d, abort_flag, 1);
                     if (!ok) break;
-                    voxel_phase<GRAD_MODE> (a, x, voxel_slot (a, x, mb), tx0,
+                    voxel_phase<MODE> (a, x, voxel_slot (a, x, mb), tx0,
                         ty, tz, sc, cnt);
                     warp_arrive (x, &s_bar[1]);
                     ok = cwait (a, x, &s_bar[3], ph_g, abort_flag, 2);
@@ -1026,12 +1208,30 @@ mse_tc_kernel (TcArgs a)
                 finish_batch (b);
             }
         }
-        // the CTA's score and voxel count (its batches in order; every
-        // compute warp gets here, also after a failed wait)
-        cblock_sum (sc, cnt, sh_v, sh_n, x);
-        if (x.tid == 0) {
-            a.score_part[blockIdx.x] = sc;
-            a.count_part[blockIdx.x] = cnt;
+        if constexpr (MODE == TC_MI_HIST) {
+            // the CTA's histograms and count into the global ones (integer
+            // sums: the order does not matter)
+            cbar ();
+            const int nh = 2 * a.bins + a.bins * a.bins;
+            const unsigned long long* h = (const unsigned long long*) (x.sm + SM_DC);
+            for (int i = x.tid; i < nh; i += TC_THREADS) {
+                if (h[i]) atomicAdd (&a.hist[i], h[i]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cnt += __shfl_down_sync (0xffffffffu, cnt, o);
+            }
+            if (x.lane == 0 && cnt) {
+                atomicAdd (&a.hist[nh], (unsigned long long) cnt);
+            }
+        } else {
+            // the CTA's score and voxel count (its batches in order; every
+            // compute warp gets here, also after a failed wait)
+            cblock_sum (sc, cnt, sh_v, sh_n, x);
+            if (x.tid == 0) {
+                a.score_part[blockIdx.x] = sc;
+                a.count_part[blockIdx.x] = cnt;
+            }
         }
     }
 
@@ -1116,22 +1316,19 @@ tc_build_tables (const BspGeom& g, const TcPlan& p, void** d_qlut)
     return B200BSP_OK;
 }
 
-cudaError_t
-launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
-    const float* fimg, const float* mimg, const float* mgrad,
-    const float4* mgrad4, const float* coeff, const void* qimg, float* part,
-    double* score_part, int* count_part, int* err, cudaStream_t st)
+// Kernel arguments common to every mode; returns whether the axis-aligned
+// voxel phase applies: diagonal step and projection, one 128-voxel block
+// per tile, rounds whose field copy and position tables fit the C and
+// knot-block areas, and divisors >= 2 for the multiply-high reciprocals.
+static bool
+tc_args (const BspGeom& g, const TcPlan& p, TcArgs& a)
 {
-    TcArgs a;
+    a = TcArgs ();
     a.g = g;
     a.T = p.bx;
     a.N = p.n_mma;
     a.mblk = p.mblk;
     a.V = g.vpr[0] * g.vpr[1] * g.vpr[2];
-    // The axis-aligned voxel phase: diagonal step and projection, one
-    // 128-voxel block per tile, rounds whose field copy and position tables
-    // fit the C and knot-block areas, and divisors >= 2 for the
-    // multiply-high reciprocals.
     a.T0 = (a.T + 1) / 2;
     a.W = g.vpr[0] * a.T0;
     a.plane = a.W * g.vpr[1] * g.vpr[2];
@@ -1143,31 +1340,67 @@ launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
             }
         }
     }
-    a.axis = diag && p.mblk == 1 && g.vpr[0] >= 2 && a.W >= 2
-        && 12 * a.plane <= SM_C_BYTES
-        && 2 * a.W + 4 * g.vpr[1] * g.vpr[2] <= SM_S_FLOATS
-        && (grad_mode == 1 || mgrad4 != nullptr);
     a.mW = a.W >= 2 ? 0xFFFFFFFFu / (unsigned) a.W + 1u : 0u;
     a.mvx = g.vpr[0] >= 2 ? 0xFFFFFFFFu / (unsigned) g.vpr[0] + 1u : 0u;
-    a.mgrad4 = mgrad4;
     a.nbx = (g.rdims[0] + p.bx - 1) / p.bx;
     a.nbatches = p.nbatches;
+    return diag && p.mblk == 1 && g.vpr[0] >= 2 && a.W >= 2
+        && 12 * a.plane <= SM_C_BYTES
+        && 2 * a.W + 4 * g.vpr[1] * g.vpr[2] <= SM_S_FLOATS;
+}
+
+template <int MODE>
+static cudaError_t
+launch_mode (const TcPlan& p, const TcArgs& a, cudaStream_t st)
+{
+    auto k = mse_tc_kernel<MODE>;
+    cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int) p.smem);
+    k<<<p.grid, TC_BLOCK, p.smem, st>>> (a);
+    return cudaGetLastError ();
+}
+
+cudaError_t
+launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
+    const float* fimg, const float* mimg, const float* mgrad,
+    const float4* mgrad4, const float* coeff, const void* qimg, float* part,
+    double* score_part, int* count_part, int* err, cudaStream_t st)
+{
+    TcArgs a;
+    a.axis = tc_args (g, p, a) && (grad_mode == 1 || mgrad4 != nullptr);
+    a.mgrad4 = mgrad4;
     a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;
     a.qimg = (const uint4*) qimg;
     a.part = part; a.score_part = score_part; a.count_part = count_part;
     a.err = err;
-    if (grad_mode == 0) {
-        auto k = mse_tc_kernel<0>;
-        cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int) p.smem);
-        k<<<p.grid, TC_BLOCK, p.smem, st>>> (a);
-    } else {
-        auto k = mse_tc_kernel<1>;
-        cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int) p.smem);
-        k<<<p.grid, TC_BLOCK, p.smem, st>>> (a);
-    }
-    return cudaGetLastError ();
+    return grad_mode == 0 ? launch_mode<TC_MSE_NEAREST> (p, a, st)
+                          : launch_mode<TC_MSE_LINEAR> (p, a, st);
+}
+
+bool
+tc_mi_supported (const BspGeom& g, const TcPlan& p, int bins)
+{
+    TcArgs a;
+    return tc_args (g, p, a)
+        && (2 * bins + bins * bins) * 8 <= 2 * DC_HALF + DC_TAIL;
+}
+
+cudaError_t
+launch_mi_tc (const BspGeom& g, const TcPlan& p, bool hist_pass,
+    const TcMiArgs& mi, const float* coeff, const void* qimg, float* part,
+    double* score_part, int* count_part, int* err, cudaStream_t st)
+{
+    TcArgs a;
+    if (!tc_args (g, p, a)) return cudaErrorInvalidValue;
+    a.axis = 1;
+    a.coeff = coeff;
+    a.qimg = (const uint4*) qimg;
+    a.part = part; a.score_part = score_part; a.count_part = count_part;
+    a.err = err;
+    a.fbin = mi.fbin; a.mbin = mi.mbin; a.bins = mi.bins;
+    a.mi_lut = mi.lut; a.mi_nvf = mi.nvf; a.hist = mi.hist;
+    return hist_pass ? launch_mode<TC_MI_HIST> (p, a, st)
+                     : launch_mode<TC_MI_GRAD> (p, a, st);
 }
 
 } // namespace b200

@@ -770,8 +770,15 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     int rc = begin_eval (c, coeff, &dcoeff);
     if (rc) return rc;
     float* g_dev = is_device_ptr (grad) ? grad : c->d_grad;
-    rc = mi_run (&c->mi, c->geom, dcoeff, c->d_luts, c->d_res, g_dev, nullptr,
-        c->stream, &c->last_launches);
+    if (c->opts.form == B200BSP_FORM_TC
+        && tc_mi_supported (c->geom, c->plan, c->mi.bins)) {
+        rc = mi_run_tc (&c->mi, c->geom, c->plan, c->lay, c->d_qlut,
+            c->d_part, c->d_score_part, c->d_count_part, c->d_err, dcoeff,
+            c->d_res, g_dev, nullptr, c->stream, &c->last_launches);
+    } else {
+        rc = mi_run (&c->mi, c->geom, dcoeff, c->d_luts, c->d_res, g_dev,
+            nullptr, c->stream, &c->last_launches);
+    }
     if (rc) return fail (c, rc, "MI evaluation failed: %s",
         cudaGetErrorString (cudaGetLastError ()));
     mark_main_done (c);
