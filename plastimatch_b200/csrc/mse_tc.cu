@@ -650,17 +650,18 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
 // Mattes MI pass 1 at one sample: the PVI-8 corner weights (products of
 // the per-axis fractions, in the reference's order) as integers in 2^-24
 // units, so the sums do not depend on their order; corners with equal
-// moving bins are merged first, and lanes whose corners all share one bin
-// combine across the warp (match + reduce) so that one lane per distinct
-// (fixed, moving) bin pair updates the shared histograms.  Every lane of
-// the warp calls this (warp collectives).
+// moving bins are merged first, then equal (fixed, moving) bin pairs
+// combine across the warp (match + reduce), lanes whose corners all share
+// one bin in one step, the others corner by corner, so that one lane per
+// distinct pair updates the shared joint histogram.  The moving histogram
+// is the joint one's column sums, taken when the CTA flushes.  Every lane
+// of the warp calls this (warp collectives).
 __device__ __forceinline__ void
 mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
     int fb, const int mb_in[8], int& cnt)
 {
     const int B = a.bins;
     unsigned long long* hf = (unsigned long long*) (x.sm + SM_DC);
-    unsigned long long* hm = hf + B;
     unsigned long long* hj = hf + 2 * B;
     const float* l2 = w2;
     const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
@@ -696,21 +697,27 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
         }
         cnt++;
     }
+    // (a warp's sum stays below 32 * (2^24 + 8) < 2^32)
     const unsigned single_mask = __ballot_sync (0xffffffffu, live && single);
     if (live && single) {
         const int key = fb * B + mb[0];
         const unsigned peers = __match_any_sync (single_mask, key);
         const unsigned sum = __reduce_add_sync (peers, q[0]);
         if (x.lane == __ffs (peers) - 1) {
-            atomicAdd (&hm[mb[0]], (unsigned long long) sum);
             atomicAdd (&hj[key], (unsigned long long) sum);
         }
-    } else if (live) {
+    }
+    if (__ballot_sync (0xffffffffu, live && !single) == 0u) return;
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            if (first[k]) {
-                atomicAdd (&hm[mb[k]], (unsigned long long) q[k]);
-                atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
+    for (int k = 0; k < 8; k++) {
+        const bool act = live && !single && first[k];
+        const unsigned am = __ballot_sync (0xffffffffu, act);
+        if (act) {
+            const int key = fb * B + mb[k];
+            const unsigned peers = __match_any_sync (am, key);
+            const unsigned sum = __reduce_add_sync (peers, q[k]);
+            if (x.lane == __ffs (peers) - 1) {
+                atomicAdd (&hj[key], (unsigned long long) sum);
             }
         }
     }
@@ -1212,10 +1219,15 @@ mse_tc_kernel (TcArgs a)
             // the CTA's histograms and count into the global ones (integer
             // sums: the order does not matter)
             cbar ();
-            const int nh = 2 * a.bins + a.bins * a.bins;
+            const int B = a.bins, nh = 2 * B + B * B;
             const unsigned long long* h = (const unsigned long long*) (x.sm + SM_DC);
             for (int i = x.tid; i < nh; i += TC_THREADS) {
-                if (h[i]) atomicAdd (&a.hist[i], h[i]);
+                unsigned long long v = h[i];
+                if (i >= B && i < 2 * B) {          // moving: joint column sum
+                    v = 0;
+                    for (int fb = 0; fb < B; fb++) v += h[2 * B + fb * B + (i - B)];
+                }
+                if (v) atomicAdd (&a.hist[i], v);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
