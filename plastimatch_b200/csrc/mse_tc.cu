@@ -649,16 +649,17 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
 // batch; a round-1 tile slot past the batch's last tile is dead.
 // Mattes MI pass 1 at one sample: the PVI-8 corner weights (products of
 // the per-axis fractions, in the reference's order) as integers in 2^-24
-// units, so the sums do not depend on their order; corners with equal
-// moving bins are merged first, then equal (fixed, moving) bin pairs
-// combine across the warp (match + reduce), lanes whose corners all share
-// one bin in one step, the others corner by corner, so that one lane per
-// distinct pair updates the shared joint histogram.  The moving histogram
-// is the joint one's column sums, taken when the CTA flushes.  Every lane
-// of the warp calls this (warp collectives).
+// units, so the sums do not depend on their order.  Corners with equal
+// moving bins are merged first; a sample then has one, two or (rarely)
+// more (fixed, moving) bin pairs.  The first two pairs of every lane
+// combine across the warp (match + reduce, one round each) so that one lane
+// per distinct pair updates the shared joint histogram; further pairs go
+// straight to the shared atomics.  The moving histogram is the joint one's
+// column sums, taken when the CTA flushes.  Every lane of the warp calls
+// this (warp collectives).
 __device__ __forceinline__ void
 mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
-    int fb, const int mb_in[8], int& cnt)
+    int fb, const int mb[8], int& cnt)
 {
     const int B = a.bins;
     unsigned long long* hf = (unsigned long long*) (x.sm + SM_DC);
@@ -668,16 +669,13 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
     const float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
         l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
         l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
-    int mb[8];
     unsigned int q[8];
     bool first[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        mb[k] = mb_in[k];
         q[k] = __float2uint_rn (w[k] * TC_MI_WUNIT);
         first[k] = live;
     }
-    bool single = true;
 #pragma unroll
     for (int k = 1; k < 8; k++) {
 #pragma unroll
@@ -687,38 +685,51 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
                 first[k] = false;
             }
         }
-        single = single && !first[k];
+    }
+    // second pair: the first remaining corner after corner 0
+    bool two = false, many = false;
+    int mb2 = 0;
+    unsigned int q2 = 0;
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+        many = many || (first[k] && two);
+        mb2 = (first[k] && !two) ? mb[k] : mb2;
+        q2 = (first[k] && !two) ? q[k] : q2;
+        two = two || first[k];
     }
     const unsigned live_mask = __ballot_sync (0xffffffffu, live);
     if (live) {
-        const unsigned peers = __match_any_sync (live_mask, fb);
+        cnt++;
+        // fixed histogram: one count per voxel
+        unsigned peers = __match_any_sync (live_mask, fb);
         if (x.lane == __ffs (peers) - 1) {
             atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
         }
-        cnt++;
-    }
-    // (a warp's sum stays below 32 * (2^24 + 8) < 2^32)
-    const unsigned single_mask = __ballot_sync (0xffffffffu, live && single);
-    if (live && single) {
+        // first pair (a warp's sum stays below 32 * (2^24 + 8) < 2^32)
         const int key = fb * B + mb[0];
-        const unsigned peers = __match_any_sync (single_mask, key);
+        peers = __match_any_sync (live_mask, key);
         const unsigned sum = __reduce_add_sync (peers, q[0]);
         if (x.lane == __ffs (peers) - 1) {
             atomicAdd (&hj[key], (unsigned long long) sum);
         }
     }
-    if (__ballot_sync (0xffffffffu, live && !single) == 0u) return;
+    const unsigned two_mask = __ballot_sync (0xffffffffu, two);
+    if (two) {
+        const int key = fb * B + mb2;
+        const unsigned peers = __match_any_sync (two_mask, key);
+        const unsigned sum = __reduce_add_sync (peers, q2);
+        if (x.lane == __ffs (peers) - 1) {
+            atomicAdd (&hj[key], (unsigned long long) sum);
+        }
+    }
+    if (many) {
+        bool seen = false;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const bool act = live && !single && first[k];
-        const unsigned am = __ballot_sync (0xffffffffu, act);
-        if (act) {
-            const int key = fb * B + mb[k];
-            const unsigned peers = __match_any_sync (am, key);
-            const unsigned sum = __reduce_add_sync (peers, q[k]);
-            if (x.lane == __ffs (peers) - 1) {
-                atomicAdd (&hj[key], (unsigned long long) sum);
+        for (int k = 1; k < 8; k++) {
+            if (first[k] && seen) {
+                atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
             }
+            seen = seen || first[k];
         }
     }
 }
