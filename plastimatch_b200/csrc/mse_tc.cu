@@ -654,9 +654,10 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
 // more (fixed, moving) bin pairs.  The first two pairs of every lane
 // combine across the warp (match + reduce, one round each) so that one lane
 // per distinct pair updates the shared joint histogram; further pairs go
-// straight to the shared atomics.  The moving histogram is the joint one's
-// column sums, taken when the CTA flushes.  Every lane of the warp calls
-// this (warp collectives).
+// straight to the shared atomics.  The fixed histogram counts each first-
+// pair group's voxels; the moving histogram is the joint one's column sums,
+// taken when the CTA flushes.  Every lane of the warp calls this (warp
+// collectives).
 __device__ __forceinline__ void
 mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
     int fb, const int mb[8], int& cnt)
@@ -700,17 +701,14 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
     const unsigned live_mask = __ballot_sync (0xffffffffu, live);
     if (live) {
         cnt++;
-        // fixed histogram: one count per voxel
-        unsigned peers = __match_any_sync (live_mask, fb);
-        if (x.lane == __ffs (peers) - 1) {
-            atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
-        }
-        // first pair (a warp's sum stays below 32 * (2^24 + 8) < 2^32)
+        // first pair (a warp's sum stays below 32 * (2^24 + 8) < 2^32); its
+        // leader also counts the group's voxels into the fixed histogram
         const int key = fb * B + mb[0];
-        peers = __match_any_sync (live_mask, key);
+        const unsigned peers = __match_any_sync (live_mask, key);
         const unsigned sum = __reduce_add_sync (peers, q[0]);
         if (x.lane == __ffs (peers) - 1) {
             atomicAdd (&hj[key], (unsigned long long) sum);
+            atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
         }
     }
     const unsigned two_mask = __ballot_sync (0xffffffffu, two);
