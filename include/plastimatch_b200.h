@@ -165,6 +165,13 @@ int b200bsp_score_mi (b200bsp_ctx* ctx, const float* coeff, float* score,
 int b200bsp_regularize (b200bsp_ctx* ctx, const float* coeff,
     const b200bsp_reg_parms* parms, float* rmetric, float* grad);
 
+/* As b200bsp_regularize with the score returned in double (the device sums
+ * it in double; the reference stores it in a float).  No reference
+ * counterpart: for gradient checks by finite differences, where the float
+ * rounding of the score would swamp a 1e-3 mm step. */
+int b200bsp_regularize_f64 (b200bsp_ctx* ctx, const float* coeff,
+    const b200bsp_reg_parms* parms, double* rmetric, float* grad);
+
 /* The whole cost function bspline_score() (src/register/bspline.cxx:
  * 558-632) for one similarity metric: metric_type 0 = MSE, 1 = MI;
  * total_score = lambda * smetric (+ rmetric when reg != NULL), total_grad

@@ -137,6 +137,7 @@ _SIGS = {
     "b200bsp_score_mse_f64": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "b200bsp_score_mi": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "b200bsp_regularize": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_regularize_f64": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "b200bsp_score": (C.c_int, [_VP, _VP, C.c_int, C.c_float, _VP, _VP, _VP,
                                 _VP, _VP]),
     "b200bsp_interpolate_vf": (C.c_int, [_VP, _VP, _VP]),
@@ -443,6 +444,15 @@ class Context:
         s = C.c_float()
         _check(lib().b200bsp_regularize(self._h, _ptr(coeff), C.byref(parms),
                                         C.addressof(s), _ptr(g)), self._h)
+        return s.value, g
+
+    def regularize_f64(self, coeff, parms: RegParms, grad=None):
+        """(rmetric as a double, grad): for finite-difference checks."""
+        g = np.zeros(self.num_coeff, np.float32) if grad is None else grad
+        s = C.c_double()
+        _check(lib().b200bsp_regularize_f64(self._h, _ptr(coeff),
+                                            C.byref(parms), C.addressof(s),
+                                            _ptr(g)), self._h)
         return s.value, g
 
     def score(self, coeff, metric="mse", lam=1.0, reg: RegParms | None = None):

@@ -797,9 +797,9 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     return check_device_error (c);
 }
 
-extern "C" int
-b200bsp_regularize (b200bsp_ctx* c, const float* coeff,
-    const b200bsp_reg_parms* parms, float* rmetric, float* grad)
+static int
+regularize (b200bsp_ctx* c, const float* coeff,
+    const b200bsp_reg_parms* parms, double* rmetric, float* grad)
 {
     if (!parms) return fail (c, B200BSP_E_BADARG, "null parms");
     const float* dcoeff = nullptr;
@@ -829,8 +829,25 @@ b200bsp_regularize (b200bsp_ctx* c, const float* coeff,
     double S = 0;
     rc = reg_fetch (&c->reg, &S, c->stream);
     if (rc) return fail (c, rc, "regulariser fetch failed");
-    if (rmetric) *rmetric = (float) S;
+    if (rmetric) *rmetric = S;
     return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_regularize (b200bsp_ctx* c, const float* coeff,
+    const b200bsp_reg_parms* parms, float* rmetric, float* grad)
+{
+    double S = 0.0;
+    const int rc = regularize (c, coeff, parms, &S, grad);
+    if (!rc && rmetric) *rmetric = (float) S;
+    return rc;
+}
+
+extern "C" int
+b200bsp_regularize_f64 (b200bsp_ctx* c, const float* coeff,
+    const b200bsp_reg_parms* parms, double* rmetric, float* grad)
+{
+    return regularize (c, coeff, parms, rmetric, grad);
 }
 
 extern "C" int
