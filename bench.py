@@ -245,6 +245,73 @@ def registration_c1(P, with_cpu):
     return out
 
 
+def batched_c5(P, n_regs=16, its=40):
+    """Batched multi-atlas registration: n_regs MSE registrations of seeded
+    uneven sizes (U{128..320} x U{128..320} x U{64..160} voxels, in-plane and
+    slice spacing U[1, 2.5] mm, Gaussian-blob content, moving = fixed under
+    a seeded B-spline warp with 10 mm spacing and N(0, 2 mm) coefficients),
+    a 10 mm control grid (vox_per_rgn = round(10 mm / spacing), at least
+    4), zero initial coefficients, `its` L-BFGS iterations each (max_feval
+    100).  Wall time with all registrations advancing together (one graph
+    launch per round of evaluations), for the tensor-core and the FP32
+    forms, and of the same registrations run one after another."""
+    from plastimatch_b200 import synth
+    from plastimatch_b200.geometry import BsplineGrid, Volume
+    g = synth.rng(20261207)
+    cases = []
+    for k in range(n_regs):
+        dim = (int(g.integers(128, 321)), int(g.integers(128, 321)),
+               int(g.integers(64, 161)))
+        sxy, sz = float(g.uniform(1.0, 2.5)), float(g.uniform(1.0, 2.5))
+        fixed = synth.gaussian_blobs(dim, spacing=(sxy, sxy, sz),
+                                     seed=20261207 + 100 * k)
+        vpr = tuple(max(4, int(round(10.0 / s))) for s in (sxy, sxy, sz))
+        g0 = BsplineGrid.for_volume(fixed, vpr)
+        with P.Context(fixed, fixed, g0) as wctx:       # the moving image
+            wctx.set_images()
+            mimg = wctx.warp(synth.random_coeff(g0, 2.0,
+                                                20261207 + 100 * k + 1))
+        moving = Volume(mimg.reshape(fixed.img.shape), origin=fixed.origin,
+                        spacing=fixed.spacing)
+        cases.append((fixed, moving, BsplineGrid.for_volume(fixed, vpr)))
+    nvox = [c[2].num_roi_voxels for c in cases]
+    out = {"registrations": n_regs, "iterations": its,
+           "voxels_total": int(sum(nvox))}
+
+    def run(form, batched):
+        ctxs = [P.Context(f, m, gr, form=form).set_images()
+                for f, m, gr in cases]
+        try:
+            x = [np.zeros(gr.num_coeff, np.float32) for _, _, gr in cases]
+            if batched:
+                with P.Batch(ctxs) as b:
+                    b.optimize_lbfgs([xi.copy() for xi in x], max_its=2,
+                                     max_feval=4)                # warm-up
+                    t0 = time.perf_counter()
+                    res = b.optimize_lbfgs(x, max_its=its, max_feval=100)
+                    dt = time.perf_counter() - t0
+            else:
+                for c, xi in zip(ctxs, x):
+                    c.optimize_lbfgs(xi.copy(), max_its=2, max_feval=4)
+                t0 = time.perf_counter()
+                res = [c.optimize_lbfgs(xi, max_its=its, max_feval=100)[1]
+                       for c, xi in zip(ctxs, x)]
+                dt = time.perf_counter() - t0
+        finally:
+            for c in ctxs:
+                c.close()
+        fe = [r["fevals"] for r in res]
+        return {"wall_s": dt, "fevals": int(sum(fe)),
+                "gvox_per_s": float(sum(f * n for f, n in zip(fe, nvox))
+                                    / dt / 1e9),
+                "final_scores": [round(float(r["score"]), 4) for r in res]}
+
+    out["tc_batched"] = run("tc", True)
+    out["tc_one_after_another"] = run("tc", False)
+    out["fp32_batched"] = run("fp32", True)
+    return out
+
+
 def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
                   evals=50):
     """The same workload with the curvature regulariser added (lambda 0.005)
@@ -382,6 +449,7 @@ def main():
     if rank == 0:
         extra["registration_64cubed_vpr8_30_lbfgs_its"] = registration_c1(
             P, not args.no_cpu_baseline and world == 1)
+        extra["batched_16_registrations_40_lbfgs_its"] = batched_c5(P)
 
     # end to end through the C ABI with pinned host buffers
     h_coeff = torch.from_numpy(coeff).pin_memory()

@@ -349,6 +349,42 @@ int b200bsp_score_mse_static (const b200bsp_volume* fixed,
  * ctx is NULL). */
 const char* b200bsp_last_error (const b200bsp_ctx* ctx);
 
+/* ---- batched registrations (no reference counterpart) ----------------
+ *
+ * A batch groups contexts on one device (uneven volume sizes and grids) so
+ * that one CUDA graph launch evaluates all of them: each context's tile
+ * pass and finish kernel run on a branch of the graph, and a tensor-core
+ * context's persistent kernel takes its share of the SM slots in
+ * proportion to its work (kept until the batch is destroyed), so every
+ * registration's kernel is resident at once.  The Plastimatch counterpart
+ * is one registration per process, run one after another. */
+typedef struct b200bsp_batch b200bsp_batch;
+
+/* The contexts must be distinct, on one device, with images set; the batch
+ * does not own them (destroy it before them). */
+int b200bsp_batch_create (b200bsp_ctx* const* ctxs, int n,
+    b200bsp_batch** out);
+void b200bsp_batch_destroy (b200bsp_batch* batch);
+const char* b200bsp_batch_last_error (const b200bsp_batch* batch);
+
+/* MSE score + gradient of every context in one graph launch; coeffs[i],
+ * grads[i] (num_coeff floats of context i), scores (n floats) and num_vox
+ * (n int64, may be NULL) are device memory.  Blocks until done.  The graph
+ * is captured on the first call with a given set of buffers and replayed
+ * after that. */
+int b200bsp_batch_score_mse (b200bsp_batch* batch, const float* const* coeffs,
+    float* const* grads, float* scores, int64_t* num_vox);
+
+/* One L-BFGS registration per context (MSE, similarity weight lambda, no
+ * regulariser), all advancing together: every round of function
+ * evaluations is one batch graph launch over the registrations still
+ * running.  Each registration follows b200bsp_optimize_lbfgs's trial
+ * sequence; coeffs[i] (host or device) holds its start and receives its
+ * result, results[i] its status. */
+int b200bsp_batch_optimize_lbfgs (b200bsp_batch* batch, float lambda,
+    const b200bsp_lbfgs_parms* parms, float* const* coeffs,
+    b200bsp_lbfgs_result* results);
+
 #ifdef __cplusplus
 }
 #endif

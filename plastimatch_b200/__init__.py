@@ -161,6 +161,12 @@ _SIGS = {
                                          C.c_int]),
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_batch_create": (C.c_int, [_VP, C.c_int, _VP]),
+    "b200bsp_batch_destroy": (None, [_VP]),
+    "b200bsp_batch_last_error": (C.c_char_p, [_VP]),
+    "b200bsp_batch_score_mse": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_batch_optimize_lbfgs": (C.c_int, [_VP, C.c_float, _VP, _VP,
+                                               _VP]),
 }
 
 
@@ -495,3 +501,63 @@ class Context:
                                   _ptr(out)), self._h)
         return out.reshape(nz, ny, nx)
 
+
+
+class Batch:
+    """Registrations on one device evaluated together (b200bsp_batch): one
+    CUDA graph launch per round of evaluations over all contexts."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(
+            *[c._h.value for c in self.contexts])
+        h = C.c_void_p()
+        _check(lib().b200bsp_batch_create(arr, len(self.contexts),
+                                          C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().b200bsp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _fail(self, rc):
+        if rc:
+            msg = lib().b200bsp_batch_last_error(self._h)
+            raise B200Error(rc, msg.decode() if msg else "")
+
+    def score_mse(self, coeffs, grads, scores, num_vox=None):
+        """All buffers torch CUDA tensors: coeffs[i], grads[i] (float32,
+        num_coeff of context i), scores (n float32), num_vox (n int64)."""
+        n = len(self.contexts)
+        cp = (C.c_void_p * n)(*[_ptr(c) for c in coeffs])
+        gp = (C.c_void_p * n)(*[_ptr(g) for g in grads])
+        self._fail(lib().b200bsp_batch_score_mse(
+            self._h, cp, gp, _ptr(scores), _ptr(num_vox, np.int64)))
+
+    def optimize_lbfgs(self, coeffs, lam=1.0, **parms):
+        """One L-BFGS registration per context from coeffs[i] (numpy float32
+        arrays, updated in place): a list of result dicts."""
+        n = len(self.contexts)
+        arrs = [np.ascontiguousarray(c, np.float32) for c in coeffs]
+        cp = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+        res = (LbfgsResult * n)()
+        p = lbfgs_parms(**parms)
+        self._fail(lib().b200bsp_batch_optimize_lbfgs(self._h, lam,
+                                                      C.byref(p), cp, res))
+        for a, c in zip(arrs, coeffs):
+            if a is not c:
+                c[...] = a
+        return [r.as_dict() for r in res]

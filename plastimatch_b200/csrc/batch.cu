@@ -1,0 +1,413 @@
+// Batched registrations: many contexts (uneven volume sizes, one device)
+// evaluated together.
+//
+// One batch evaluation is one CUDA graph launch: the graph forks from the
+// batch's stream into every context's stream, runs that context's tile pass
+// and finish kernel there, gathers the contexts' device error flags and
+// joins.  A persistent tensor-core tile kernel normally takes two CTAs per
+// SM; in a batch each context's kernel takes its share of those slots in
+// proportion to its voxels, so the kernels of all registrations are
+// resident side by side and the launch fills the GPU once, like one
+// persistent kernel over the union of the work.  Graphs are captured once
+// per set of participating contexts and replayed.
+//
+// The batched L-BFGS runs one host thread per registration with the
+// device-side L-BFGS of optimize.cu; their function evaluations meet at a
+// barrier, and the last thread to arrive launches the batch evaluation of
+// everyone waiting (registrations that have finished drop out of the set).
+// Each registration's trial sequence is that of b200bsp_optimize_lbfgs.
+#include <algorithm>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "kernels.cuh"
+#include "../../include/plastimatch_b200.h"
+
+namespace b200 {
+cudaStream_t ctx_stream (const b200bsp_ctx* c);                 // runtime.cu
+int ctx_device (const b200bsp_ctx* c);
+long long ctx_work (const b200bsp_ctx* c, bool* persistent);
+void ctx_set_tc_grid (b200bsp_ctx* c, int ctas);
+int* ctx_err_flag (b200bsp_ctx* c);
+int ctx_report_device_error (b200bsp_ctx* c, int e);
+int lbfgs_optimize_batched (b200bsp_ctx* ctx, float lambda,
+    const b200bsp_lbfgs_parms* parms, float* coeff, b200bsp_lbfgs_result* res,
+    void* member, int (*eval) (void*, int, const float*, float*, float*)); // optimize.cu
+
+// Largest error flag over the participating contexts.
+__global__ void
+batch_err_kernel (int* const* flags, int n, int* out)
+{
+    int e = 0;
+    for (int i = threadIdx.x; i < n; i += 32) {
+        if (flags[i]) e = max (e, *flags[i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e = max (e, __shfl_down_sync (0xffffffffu, e, o));
+    if (threadIdx.x == 0) *out = e;
+}
+} // namespace b200
+
+using namespace b200;
+
+struct b200bsp_batch {
+    std::vector<b200bsp_ctx*> ctx;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    int** d_flags = nullptr;            // per context: its error flag
+    int* d_err = nullptr;
+    int* h_err = nullptr;
+    struct Graph {
+        std::vector<const void*> key;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    std::string err;
+
+    // batched L-BFGS state
+    std::mutex mu;
+    std::condition_variable cv;
+    int active = 0, waiting = 0;
+    long long generation = 0;
+    std::vector<char> want;
+    std::vector<const float*> lb_coeff;
+    std::vector<float*> lb_grad;
+    float* d_scores = nullptr;
+    float* h_scores = nullptr;
+    int lb_status = 0;
+};
+
+static int
+bfail (b200bsp_batch* b, int code, const char* msg)
+{
+    if (b) b->err = msg;
+    return code;
+}
+
+#define BCK(b, x)                                                           \
+    do {                                                                    \
+        cudaError_t e_ = (x);                                               \
+        if (e_ != cudaSuccess) {                                            \
+            cudaGetLastError ();                                            \
+            return bfail (b, B200BSP_E_CUDA, cudaGetErrorString (e_));      \
+        }                                                                   \
+    } while (0)
+
+// Capture (or find) the graph evaluating contexts `sel` with the given
+// device buffers, and launch it on the batch stream.  The graph ends with
+// the copy of the error flag (and, for the batch's own score buffer, of the
+// scores) into page-locked host memory, so one synchronisation ends it.
+static int
+launch_eval (b200bsp_batch* b, const std::vector<int>& sel,
+    const float* const* coeffs, float* const* grads, float* scores,
+    int64_t* nvox)
+{
+    const bool own_scores = scores == b->d_scores;
+    std::vector<const void*> key;
+    for (int i : sel) {
+        key.push_back ((const void*) (intptr_t) i);
+        key.push_back (coeffs[i]);
+        key.push_back (grads[i]);
+    }
+    key.push_back (scores);
+    key.push_back (nvox);
+    cudaGraphExec_t exec = nullptr;
+    for (auto& gph : b->graphs) {
+        if (gph.key == key) exec = gph.exec;
+    }
+    if (!exec) {
+        cudaGraph_t graph = nullptr;
+        BCK (b, cudaStreamBeginCapture (b->st, cudaStreamCaptureModeRelaxed));
+        int rc = 0;
+        if (cudaEventRecord (b->fork, b->st) != cudaSuccess) rc = B200BSP_E_CUDA;
+        for (size_t k = 0; k < sel.size () && !rc; k++) {
+            const int i = sel[k];
+            cudaStream_t s = ctx_stream (b->ctx[i]);
+            if (cudaStreamWaitEvent (s, b->fork, 0) != cudaSuccess) {
+                rc = B200BSP_E_CUDA;
+                break;
+            }
+            rc = b200bsp_score_mse (b->ctx[i], coeffs[i], scores + i, grads[i],
+                nvox ? nvox + i : nullptr);
+            if (!rc && (cudaEventRecord (b->join[i], s) != cudaSuccess
+                    || cudaStreamWaitEvent (b->st, b->join[i], 0) != cudaSuccess)) {
+                rc = B200BSP_E_CUDA;
+            }
+        }
+        if (!rc) {
+            batch_err_kernel<<<1, 32, 0, b->st>>> (b->d_flags, (int) b->ctx.size (),
+                b->d_err);
+            if (cudaMemcpyAsync (b->h_err, b->d_err, sizeof (int),
+                    cudaMemcpyDeviceToHost, b->st) != cudaSuccess
+                || (own_scores && cudaMemcpyAsync (b->h_scores, b->d_scores,
+                    b->ctx.size () * sizeof (float), cudaMemcpyDeviceToHost,
+                    b->st) != cudaSuccess)) {
+                rc = B200BSP_E_CUDA;
+            }
+        }
+        cudaError_t ce = cudaStreamEndCapture (b->st, &graph);
+        if (rc || ce != cudaSuccess) {
+            cudaGetLastError ();
+            if (graph) cudaGraphDestroy (graph);
+            return bfail (b, rc ? rc : B200BSP_E_CUDA,
+                "capturing the batch evaluation failed");
+        }
+        ce = cudaGraphInstantiate (&exec, graph, 0);
+        cudaGraphDestroy (graph);
+        if (ce != cudaSuccess) {
+            cudaGetLastError ();
+            return bfail (b, B200BSP_E_CUDA, "graph instantiation failed");
+        }
+        b->graphs.push_back ({key, exec});
+    }
+    BCK (b, cudaGraphLaunch (exec, b->st));
+    BCK (b, cudaStreamSynchronize (b->st));
+    if (*b->h_err) {
+        for (int i : sel) ctx_report_device_error (b->ctx[i], *b->h_err);
+        return bfail (b, B200BSP_E_TIMEOUT,
+            "a bounded device-side wait gave up in a batch evaluation");
+    }
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_batch_create (b200bsp_ctx* const* ctxs, int n, b200bsp_batch** out)
+{
+    if (!ctxs || n < 1 || !out) return B200BSP_E_BADARG;
+    *out = nullptr;
+    const int dev = ctx_device (ctxs[0]);
+    for (int i = 0; i < n; i++) {
+        if (!ctxs[i] || ctx_device (ctxs[i]) != dev) return B200BSP_E_BADARG;
+        for (int j = 0; j < i; j++) {
+            if (ctxs[j] == ctxs[i]) return B200BSP_E_BADARG;
+        }
+    }
+    auto* b = new b200bsp_batch ();
+    b->ctx.assign (ctxs, ctxs + n);
+    b->device = dev;
+    b->join.assign (n, nullptr);
+    b->want.assign (n, 0);
+    b->lb_coeff.assign (n, nullptr);
+    b->lb_grad.assign (n, nullptr);
+    int rc = B200BSP_OK;
+    if (cudaSetDevice (dev) != cudaSuccess
+        || cudaStreamCreateWithFlags (&b->st, cudaStreamNonBlocking) != cudaSuccess
+        || cudaEventCreateWithFlags (&b->fork, cudaEventDisableTiming) != cudaSuccess
+        || cudaMalloc (&b->d_flags, n * sizeof (int*)) != cudaSuccess
+        || cudaMalloc (&b->d_err, sizeof (int)) != cudaSuccess
+        || cudaMallocHost (&b->h_err, sizeof (int)) != cudaSuccess
+        || cudaMalloc (&b->d_scores, n * sizeof (float)) != cudaSuccess
+        || cudaMallocHost (&b->h_scores, n * sizeof (float)) != cudaSuccess) {
+        rc = B200BSP_E_OOM;
+    }
+    for (int i = 0; i < n && !rc; i++) {
+        if (cudaEventCreateWithFlags (&b->join[i], cudaEventDisableTiming)
+            != cudaSuccess) {
+            rc = B200BSP_E_CUDA;
+        }
+    }
+    if (!rc) {
+        std::vector<int*> flags (n);
+        for (int i = 0; i < n; i++) flags[i] = ctx_err_flag (ctxs[i]);
+        if (cudaMemcpy (b->d_flags, flags.data (), n * sizeof (int*),
+                cudaMemcpyHostToDevice) != cudaSuccess) {
+            rc = B200BSP_E_CUDA;
+        }
+    }
+    if (rc) {
+        cudaGetLastError ();
+        b200bsp_batch_destroy (b);
+        return rc;
+    }
+    // Split the persistent kernels' CTA slots (two per SM) by voxels.
+    int sms = 148;
+    cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long total = 0;
+    std::vector<long long> work (n);
+    std::vector<bool> pers (n);
+    for (int i = 0; i < n; i++) {
+        bool p = false;
+        work[i] = ctx_work (ctxs[i], &p);
+        pers[i] = p;
+        if (p) total += work[i];
+    }
+    for (int i = 0; i < n; i++) {
+        if (!pers[i] || total == 0) continue;
+        const long long share = (2LL * sms * work[i] + total / 2) / total;
+        ctx_set_tc_grid (ctxs[i], (int) std::max (1LL, share));
+    }
+    *out = b;
+    return B200BSP_OK;
+}
+
+extern "C" void
+b200bsp_batch_destroy (b200bsp_batch* b)
+{
+    if (!b) return;
+    cudaSetDevice (b->device);
+    if (b->st) cudaStreamSynchronize (b->st);
+    for (auto& g : b->graphs) cudaGraphExecDestroy (g.exec);
+    for (auto* c : b->ctx) ctx_set_tc_grid (c, 0);
+    for (auto e : b->join) if (e) cudaEventDestroy (e);
+    if (b->fork) cudaEventDestroy (b->fork);
+    if (b->st) cudaStreamDestroy (b->st);
+    cudaFree (b->d_flags);
+    cudaFree (b->d_err);
+    cudaFreeHost (b->h_err);
+    cudaFree (b->d_scores);
+    cudaFreeHost (b->h_scores);
+    delete b;
+}
+
+extern "C" const char*
+b200bsp_batch_last_error (const b200bsp_batch* b)
+{
+    return b ? b->err.c_str () : "null batch";
+}
+
+extern "C" int
+b200bsp_batch_score_mse (b200bsp_batch* b, const float* const* coeffs,
+    float* const* grads, float* scores, int64_t* num_vox)
+{
+    if (!b || !coeffs || !grads || !scores) {
+        return bfail (b, B200BSP_E_BADARG, "null argument");
+    }
+    const int n = (int) b->ctx.size ();
+    for (int i = 0; i < n; i++) {
+        if (!coeffs[i] || !grads[i]) return bfail (b, B200BSP_E_BADARG, "null buffer");
+        cudaPointerAttributes a1, a2;
+        if (cudaPointerGetAttributes (&a1, coeffs[i]) != cudaSuccess
+            || cudaPointerGetAttributes (&a2, grads[i]) != cudaSuccess
+            || a1.type != cudaMemoryTypeDevice || a2.type != cudaMemoryTypeDevice) {
+            cudaGetLastError ();
+            return bfail (b, B200BSP_E_BADARG,
+                "batch buffers must be device memory");
+        }
+    }
+    BCK (b, cudaSetDevice (b->device));
+    std::vector<int> sel (n);
+    for (int i = 0; i < n; i++) sel[i] = i;
+    std::lock_guard<std::mutex> lk (b->mu);
+    return launch_eval (b, sel, coeffs, grads, scores, num_vox);
+}
+
+// ---- batched L-BFGS ---------------------------------------------------------
+
+// Called by a registration's thread with its trial coefficients (device,
+// float) ready: waits until the batch evaluation that includes it is done;
+// the score comes back in *score and the gradient in its device buffer.
+static int
+batch_member_eval (void* user, int i, const float* coeff, float* grad,
+    float* score)
+{
+    auto* b = (b200bsp_batch*) user;
+    std::unique_lock<std::mutex> lk (b->mu);
+    b->want[i] = 1;
+    b->lb_coeff[i] = coeff;
+    b->lb_grad[i] = grad;
+    b->waiting++;
+    const long long gen = b->generation;
+    if (b->waiting == b->active) {
+        std::vector<int> sel;
+        std::vector<const float*> cs (b->ctx.size (), nullptr);
+        std::vector<float*> gs (b->ctx.size (), nullptr);
+        for (int k = 0; k < (int) b->ctx.size (); k++) {
+            if (b->want[k]) {
+                sel.push_back (k);
+                cs[k] = b->lb_coeff[k];
+                gs[k] = b->lb_grad[k];
+            }
+        }
+        b->lb_status = launch_eval (b, sel, cs.data (), gs.data (),
+            b->d_scores, nullptr);
+        std::fill (b->want.begin (), b->want.end (), 0);
+        b->waiting = 0;
+        b->generation++;
+        b->cv.notify_all ();
+    } else {
+        b->cv.wait (lk, [&] { return b->generation != gen; });
+    }
+    *score = b->h_scores[i];
+    return b->lb_status;
+}
+
+// A registration's thread is done: the others no longer wait for it.
+static void
+batch_member_leave (b200bsp_batch* b)
+{
+    std::unique_lock<std::mutex> lk (b->mu);
+    b->active--;
+    if (b->active > 0 && b->waiting == b->active) {
+        // everyone left is waiting: evaluate them
+        std::vector<int> sel;
+        std::vector<const float*> cs (b->ctx.size (), nullptr);
+        std::vector<float*> gs (b->ctx.size (), nullptr);
+        for (int k = 0; k < (int) b->ctx.size (); k++) {
+            if (b->want[k]) {
+                sel.push_back (k);
+                cs[k] = b->lb_coeff[k];
+                gs[k] = b->lb_grad[k];
+            }
+        }
+        b->lb_status = launch_eval (b, sel, cs.data (), gs.data (),
+            b->d_scores, nullptr);
+        std::fill (b->want.begin (), b->want.end (), 0);
+        b->waiting = 0;
+        b->generation++;
+        b->cv.notify_all ();
+    }
+}
+
+extern "C" int
+b200bsp_batch_optimize_lbfgs (b200bsp_batch* b, float lambda,
+    const b200bsp_lbfgs_parms* parms, float* const* coeffs,
+    b200bsp_lbfgs_result* results)
+{
+    if (!b || !coeffs || !results) return bfail (b, B200BSP_E_BADARG, "null argument");
+    const int n = (int) b->ctx.size ();
+    for (int i = 0; i < n; i++) {
+        if (!coeffs[i]) return bfail (b, B200BSP_E_BADARG, "null coefficients");
+    }
+    {
+        std::lock_guard<std::mutex> lk (b->mu);
+        b->active = n;
+        b->waiting = 0;
+        std::fill (b->want.begin (), b->want.end (), 0);
+    }
+    std::vector<int> rcs (n, B200BSP_OK);
+    std::vector<std::thread> th;
+    th.reserve (n);
+    for (int i = 0; i < n; i++) {
+        th.emplace_back ([&, i] {
+            cudaSetDevice (b->device);
+            struct Member {
+                b200bsp_batch* b;
+                int i;
+            } m{b, i};
+            rcs[i] = lbfgs_optimize_batched (b->ctx[i], lambda, parms,
+                coeffs[i], &results[i], &m,
+                [] (void* u, int, const float* c, float* g, float* s) {
+                    auto* mm = (Member*) u;
+                    return batch_member_eval (mm->b, mm->i, c, g, s);
+                });
+            batch_member_leave (b);
+        });
+    }
+    for (auto& t : th) t.join ();
+    for (int i = 0; i < n; i++) {
+        if (rcs[i]) {
+            char msg[96];
+            snprintf (msg, sizeof msg, "registration %d failed (status %d)", i,
+                rcs[i]);
+            return bfail (b, rcs[i], msg);
+        }
+    }
+    return B200BSP_OK;
+}

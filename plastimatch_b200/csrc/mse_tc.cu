@@ -46,6 +46,8 @@ constexpr int TC_WARPS = TC_THREADS / 32;
 constexpr int TC_BLOCK = TC_THREADS + 32;      // + one tensor-core issuing warp
 constexpr int GS_STRIDE = 65;                  // odd: conflict-free G copy
 constexpr int TC_TMAX = 26;          // tiles per batch at most
+constexpr int TC_MAX_MBLK = 8;       // 128-voxel blocks per tile at most
+                                     // (vox_per_rgn up to 10 x 10 x 10)
 constexpr int TC_TMEM_COLS = 256;
 constexpr int TC_D_COL = 0;          // forward accumulator [0, N)
 constexpr int TC_G_COL = 128;        // adjoint accumulator [128, 192)
@@ -104,8 +106,8 @@ struct TcArgs {
     const float* coeff;
     const uint4* qimg;
     float* part;          // [batch][c][knot of the (T+3) x 4 x 4 footprint]
-    double* score_part;   // [CTA]: sum of diff^2 over the CTA's batches
-    int* count_part;      // [CTA]: voxels counted
+    double* score_part;   // [batch]: sum of diff^2
+    int* count_part;      // [batch]: voxels counted
     int* err;
     // Mattes MI modes (TC_MI_GRAD, TC_MI_HIST): bin images, bins, the pass-2
     // factor table [fixed bin][moving bin] and the voxel count (float), the
@@ -1028,28 +1030,6 @@ warp_arrive (const TcCtx& x, uint64_t* bar)
     if (x.lane == 0) mbar_arrive (bar);
 }
 
-// Deterministic sum over the compute warps (fixed tree order).
-__device__ __forceinline__ void
-cblock_sum (double& v, int& n, double* sh_v, int* sh_n, const TcCtx& x)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v += __shfl_down_sync (0xffffffffu, v, o);
-        n += __shfl_down_sync (0xffffffffu, n, o);
-    }
-    if (x.lane == 0) { sh_v[x.warp] = v; sh_n[x.warp] = n; }
-    cbar ();
-    if (x.warp == 0) {
-        v = (x.lane < TC_WARPS) ? sh_v[x.lane] : 0.0;
-        n = (x.lane < TC_WARPS) ? sh_n[x.lane] : 0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            v += __shfl_down_sync (0xffffffffu, v, o);
-            n += __shfl_down_sync (0xffffffffu, n, o);
-        }
-    }
-}
-
 // Tensor-core warp: for every batch and 128-voxel block, wait for the
 // forward operands, issue the forward GEMM, wait for dc/dv, issue the
 // adjoint (the MI histogram pass has no adjoint).  Bounded waits; gives up
@@ -1155,11 +1135,35 @@ mse_tc_kernel (TcArgs a)
         };
         // G -> shared -> the batch's partial gradient (the next writer of
         // the G copy's area, the voxel phase, starts after a compute
-        // barrier)
+        // barrier).  The batch's score and count: each warp's tree sum into
+        // shared memory before the barrier that follows the G copy, then
+        // thread 0 adds the eight in warp order (no barrier of its own;
+        // the slots are rewritten only a batch later).
         auto finish_batch = [&](int b) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sc += __shfl_down_sync (0xffffffffu, sc, o);
+                cnt += __shfl_down_sync (0xffffffffu, cnt, o);
+            }
+            if (x.lane == 0) {
+                sh_v[x.warp] = sc;
+                sh_n[x.warp] = cnt;
+            }
+            sc = 0.0;
+            cnt = 0;
             dump_g (a, x);
             tc_fence_before ();
             cbar ();
+            if (x.tid == 0) {
+                double v = 0.0;
+                int n = 0;
+                for (int w = 0; w < TC_WARPS; w++) {
+                    v += sh_v[w];
+                    n += sh_n[w];
+                }
+                a.score_part[b] = v;
+                a.count_part[b] = n;
+            }
             gather_knots (a, x, b);
         };
         if (a.mblk == 1 && nb_local > 0) {
@@ -1245,14 +1249,6 @@ mse_tc_kernel (TcArgs a)
             if (x.lane == 0 && cnt) {
                 atomicAdd (&a.hist[nh], (unsigned long long) cnt);
             }
-        } else {
-            // the CTA's score and voxel count (its batches in order; every
-            // compute warp gets here, also after a failed wait)
-            cblock_sum (sc, cnt, sh_v, sh_n, x);
-            if (x.tid == 0) {
-                a.score_part[blockIdx.x] = sc;
-                a.count_part[blockIdx.x] = cnt;
-            }
         }
     }
 
@@ -1268,7 +1264,7 @@ tc_plan (const BspGeom& g, TcPlan* p, int ctas_per_sm, int sm_count)
 {
     int V = g.vpr[0] * g.vpr[1] * g.vpr[2];
     int mblk = (V + 127) / 128;
-    if (mblk > 4) return false;
+    if (mblk > TC_MAX_MBLK) return false;
     int nb_row = (g.rdims[0] + TC_TMAX - 1) / TC_TMAX;
     int T = (g.rdims[0] + nb_row - 1) / nb_row;      // balanced batches
     p->bx = T;

@@ -494,6 +494,10 @@ struct ContextObjective : Objective {
     float* grad_f;
     long long n;
     cudaStream_t st;
+    // batched evaluation (a registration of a batch): the score and the
+    // gradient come from the batch's graph launch instead
+    void* member = nullptr;
+    int (*batch_eval) (void*, int, const float*, float*, float*) = nullptr;
     int eval (const double* x, double* g, double* f) override
     {
         const unsigned grid = (unsigned) std::min<long long> ((n + 255) / 256,
@@ -501,10 +505,16 @@ struct ContextObjective : Objective {
         to_float_kernel<<<grid, 256, 0, st>>> (x, coeff_f, n);
         float s = 0.f;
         int64_t nv = 0;
-        int rc = metric == 0
-            ? b200bsp_score_mse (ctx, coeff_f, &s, grad_f, &nv)
-            : b200bsp_score_mi (ctx, coeff_f, &s, grad_f, &nv, nullptr,
-                nullptr, nullptr);
+        int rc;
+        if (batch_eval) {
+            rc = cudaStreamSynchronize (st) == cudaSuccess
+                ? batch_eval (member, 0, coeff_f, grad_f, &s) : B200BSP_E_CUDA;
+        } else {
+            rc = metric == 0
+                ? b200bsp_score_mse (ctx, coeff_f, &s, grad_f, &nv)
+                : b200bsp_score_mi (ctx, coeff_f, &s, grad_f, &nv, nullptr,
+                    nullptr, nullptr);
+        }
         if (rc) return rc;
         // Bspline_score::accumulate: total = lambda * smetric, total_grad =
         // lambda * smetric_grad (src/register/bspline_score.cxx:63-74)
@@ -588,38 +598,14 @@ f2d_kernel (const float* __restrict__ a, double* __restrict__ out, long long n)
     }
 }
 
-} // namespace b200
-
-using namespace b200;
-
-extern "C" void
-b200bsp_lbfgs_default_parms (b200bsp_lbfgs_parms* p)
+// L-BFGS over a context's coefficients (host or device floats, updated in
+// place with the last evaluated point), evaluations by `obj`.
+static int
+optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
+    int64_t nc, float* coeff, b200bsp_lbfgs_result* res,
+    ContextObjective& obj)
 {
-    p->m = 6;
-    p->epsilon = 1e-5;
-    p->max_its = 10;            // Bspline_parms defaults (bspline_parms.cxx:16-17)
-    p->max_feval = 10;
-    p->max_linesearch = 40;
-    p->min_step = 1e-20;
-    p->max_step = 1e20;
-    p->ftol = 1e-4;
-    p->gtol = 0.9;
-    p->xtol = 1e-16;
-}
-
-extern "C" int
-b200bsp_optimize_lbfgs (b200bsp_ctx* ctx, int metric_type, float lambda,
-    const b200bsp_reg_parms* reg, const b200bsp_lbfgs_parms* parms,
-    float* coeff, b200bsp_lbfgs_result* res)
-{
-    if (!ctx || !coeff || !res) return static_fail (B200BSP_E_BADARG, "null argument");
-    b200bsp_lbfgs_parms p;
-    if (parms) p = *parms; else b200bsp_lbfgs_default_parms (&p);
-    int rc = check_parms (&p);
-    if (rc) return rc;
-    int64_t nc = 0;
-    rc = b200bsp_grid_info (ctx, nullptr, nullptr, &nc);
-    if (rc) return rc;
+    int rc = B200BSP_OK;
     Lbfgs w;
     if (w.alloc (nc, p.m)) return static_fail (B200BSP_E_OOM, "optimiser buffers");
     float* buf = nullptr;
@@ -627,8 +613,6 @@ b200bsp_optimize_lbfgs (b200bsp_ctx* ctx, int metric_type, float lambda,
         cudaGetLastError ();
         return static_fail (B200BSP_E_OOM, "optimiser buffers");
     }
-    ContextObjective obj;
-    obj.ctx = ctx; obj.metric = metric_type; obj.lambda = lambda; obj.reg = reg;
     obj.coeff_f = buf; obj.grad_f = buf + nc; obj.n = nc;
     // the context's stream orders every kernel of the run
     cudaStream_t st = ctx_stream (ctx);
@@ -663,6 +647,64 @@ b200bsp_optimize_lbfgs (b200bsp_ctx* ctx, int metric_type, float lambda,
     }
     cudaFree (buf);
     return rc;
+}
+
+// One registration of a batch (batch.cu): MSE, no regulariser, each
+// evaluation through `eval` (the batch's barrier and graph launch).
+int
+lbfgs_optimize_batched (b200bsp_ctx* ctx, float lambda,
+    const b200bsp_lbfgs_parms* parms, float* coeff, b200bsp_lbfgs_result* res,
+    void* member, int (*eval) (void*, int, const float*, float*, float*))
+{
+    b200bsp_lbfgs_parms p;
+    if (parms) p = *parms; else b200bsp_lbfgs_default_parms (&p);
+    int rc = check_parms (&p);
+    if (rc) return rc;
+    int64_t nc = 0;
+    rc = b200bsp_grid_info (ctx, nullptr, nullptr, &nc);
+    if (rc) return rc;
+    ContextObjective obj;
+    obj.ctx = ctx; obj.metric = 0; obj.lambda = lambda; obj.reg = nullptr;
+    obj.member = member;
+    obj.batch_eval = eval;
+    return optimize_on_context (ctx, p, nc, coeff, res, obj);
+}
+
+} // namespace b200
+
+using namespace b200;
+
+extern "C" void
+b200bsp_lbfgs_default_parms (b200bsp_lbfgs_parms* p)
+{
+    p->m = 6;
+    p->epsilon = 1e-5;
+    p->max_its = 10;            // Bspline_parms defaults (bspline_parms.cxx:16-17)
+    p->max_feval = 10;
+    p->max_linesearch = 40;
+    p->min_step = 1e-20;
+    p->max_step = 1e20;
+    p->ftol = 1e-4;
+    p->gtol = 0.9;
+    p->xtol = 1e-16;
+}
+
+extern "C" int
+b200bsp_optimize_lbfgs (b200bsp_ctx* ctx, int metric_type, float lambda,
+    const b200bsp_reg_parms* reg, const b200bsp_lbfgs_parms* parms,
+    float* coeff, b200bsp_lbfgs_result* res)
+{
+    if (!ctx || !coeff || !res) return static_fail (B200BSP_E_BADARG, "null argument");
+    b200bsp_lbfgs_parms p;
+    if (parms) p = *parms; else b200bsp_lbfgs_default_parms (&p);
+    int rc = check_parms (&p);
+    if (rc) return rc;
+    int64_t nc = 0;
+    rc = b200bsp_grid_info (ctx, nullptr, nullptr, &nc);
+    if (rc) return rc;
+    ContextObjective obj;
+    obj.ctx = ctx; obj.metric = metric_type; obj.lambda = lambda; obj.reg = reg;
+    return optimize_on_context (ctx, p, nc, coeff, res, obj);
 }
 
 extern "C" int

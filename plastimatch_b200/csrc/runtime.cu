@@ -60,6 +60,7 @@ struct b200bsp_ctx {
 
     PartLayout lay;
     TcPlan plan;
+    int tc_grid = 0;          // CTAs of the tile kernel; 0: plan.grid
     int nscore_parts = 0;
     bool images_set = false;
 
@@ -295,6 +296,47 @@ ctx_stream (const b200bsp_ctx* c)
     return c->stream;
 }
 
+int
+ctx_device (const b200bsp_ctx* c)
+{
+    return c->device;
+}
+
+// Work of one evaluation's tile pass (voxels of the ROI's tiles) and
+// whether that pass is the persistent tensor-core kernel.
+long long
+ctx_work (const b200bsp_ctx* c, bool* persistent)
+{
+    *persistent = c->opts.form == B200BSP_FORM_TC;
+    return (long long) c->geom.ntiles * c->geom.vpr[0] * c->geom.vpr[1]
+        * c->geom.vpr[2];
+}
+
+// CTAs the persistent tile kernel runs on (0: one pair per SM).
+void
+ctx_set_tc_grid (b200bsp_ctx* c, int ctas)
+{
+    c->tc_grid = ctas;
+}
+
+// The device-side error flag of the tile kernel (nullptr for the FP32
+// form, which has no bounded waits).
+int*
+ctx_err_flag (b200bsp_ctx* c)
+{
+    return c->opts.form == B200BSP_FORM_TC ? c->d_err : nullptr;
+}
+
+// Record a device error flag read by a caller that checked it (clears it).
+int
+ctx_report_device_error (b200bsp_ctx* c, int e)
+{
+    if (!e) return B200BSP_OK;
+    cudaMemsetAsync (c->d_err, 0, sizeof (int), c->stream);
+    return fail (c, B200BSP_E_TIMEOUT,
+        "a bounded device-side wait gave up (code %d)", e);
+}
+
 } // namespace b200
 
 extern "C" int
@@ -440,7 +482,7 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
             L.kx = L.bx + 3; L.ky = 4; L.kz = 4;
             L.slots = 1;
             part_elems = (size_t) c->plan.nbatches * L.kx * L.ky * L.kz * 3;
-            c->nscore_parts = c->plan.grid;      // one score part per CTA
+            c->nscore_parts = c->plan.nbatches;
         }
     } else if (!rc2) {
         if (mse_fp32_smem_bytes (g) > 200 * 1024) {
@@ -652,7 +694,9 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
             c->d_mgrad, dcoeff, c->d_luts, c->d_part, c->d_score_part,
             c->d_count_part, c->stream));
     } else {
-        CK (launch_mse_tc (g, c->plan, c->opts.mse_grad, c->d_fixed,
+        TcPlan plan = c->plan;
+        if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
+        CK (launch_mse_tc (g, plan, c->opts.mse_grad, c->d_fixed,
             c->d_moving, c->d_mgrad, c->d_mgrad4, dcoeff, c->d_qlut,
             c->d_part, c->d_score_part, c->d_count_part, c->d_err,
             c->stream));

@@ -27,17 +27,22 @@ def gaussian_blobs(dim, spacing=(1.0, 1.0, 1.0), n_blobs=20, seed=SEED_BASE,
     amplitude U[100,1000], sigma U[3,10] voxels) plus N(0, noise_sigma)."""
     g = rng(seed)
     nx, ny, nz = (int(d) for d in dim)
-    img = np.zeros((nz, ny, nx), np.float64)
-    z = np.arange(nz)[:, None, None]
-    y = np.arange(ny)[None, :, None]
-    x = np.arange(nx)[None, None, :]
-    for _ in range(n_blobs):
+    z = np.arange(nz, dtype=np.float64)
+    y = np.arange(ny, dtype=np.float64)
+    x = np.arange(nx, dtype=np.float64)
+    ez = np.empty((n_blobs, nz))
+    ey = np.empty((n_blobs, ny))
+    ex = np.empty((n_blobs, nx))
+    for b in range(n_blobs):
         cx, cy, cz = g.uniform(0, nx), g.uniform(0, ny), g.uniform(0, nz)
         amp = g.uniform(100.0, 1000.0)
         sig = g.uniform(3.0, 10.0)
-        img += amp * (np.exp(-((x - cx) ** 2) / (2 * sig * sig))
-                      * np.exp(-((y - cy) ** 2) / (2 * sig * sig))
-                      * np.exp(-((z - cz) ** 2) / (2 * sig * sig)))
+        ez[b] = amp * np.exp(-((z - cz) ** 2) / (2 * sig * sig))
+        ey[b] = np.exp(-((y - cy) ** 2) / (2 * sig * sig))
+        ex[b] = np.exp(-((x - cx) ** 2) / (2 * sig * sig))
+    # each blob is separable: the sum is one (z*y) x blobs x (x) product
+    zy = (ez[:, :, None] * ey[:, None, :]).reshape(n_blobs, nz * ny)
+    img = (zy.T @ ex).reshape(nz, ny, nx)
     img += g.normal(0.0, noise_sigma, img.shape)
     return Volume(img.astype(np.float32), origin=origin, spacing=spacing)
 

@@ -84,6 +84,22 @@ def test_mse_64cubed_vpr8(form):
     np.testing.assert_array_equal(g, g2)
 
 
+@pytest.mark.parametrize("vpr", [(9, 9, 7), (10, 10, 10)])
+def test_mse_large_tiles_tensor_core_form(vpr):
+    # 567 and 1000 voxels per tile: five and eight 128-voxel blocks, the
+    # tensor-core kernel's non-pipelined path (a 10 mm grid at 1 mm spacing)
+    fixed, moving, _, _ = _c1_case(seed=23)
+    grid = BsplineGrid.for_volume(fixed, vpr)
+    coeff = synth.random_coeff(grid, 1.0, 24)
+    with P.Context(fixed, moving, grid, form="tc") as ctx:
+        ctx.set_images()
+        s, g, n = ctx.score_mse(coeff)
+    mg = O.port_volume_grad(moving)
+    f64 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg, precision="f64")
+    r32 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg)
+    check(s, g, n, f64, r32.grad, r32.num_vox)
+
+
 @pytest.mark.parametrize("form", FORMS)
 def test_mse_zero_coefficients_and_no_overlap(form):
     fixed, moving, grid, _ = _c1_case(seed=7)
