@@ -75,8 +75,17 @@ typedef struct {
     int mse_grad;       /* B200BSP_MSE_GRAD_* */
     int mi_bins;        /* fixed and moving histogram bins (reference default 32) */
     int device;         /* CUDA device ordinal */
-    int reserved[4];    /* zero */
+    int mi_window;      /* B200BSP_MI_* (0: the reference's PVI-8) */
+    int reserved[3];    /* zero */
 } b200bsp_opts;
+
+/* Mattes MI histogram windows: PVI-8 partial-volume binning (the
+ * reference's, bspline_mi.cxx) or cubic B-spline Parzen windows on the
+ * moving intensity and a box window on the fixed one (Mattes et al., IEEE
+ * TMI 22(1) 2003; no reference counterpart).  Parzen needs mi_bins >= 5;
+ * each image's value range maps onto bins 2 .. mi_bins - 2. */
+#define B200BSP_MI_PVI8    0
+#define B200BSP_MI_PARZEN  1
 
 /* Regularisation weights of Regularization_parms
  * (src/register/regularization_parms.h:16-43). */

@@ -600,6 +600,7 @@ typedef struct {
     int ok;
     int64_t mvf, mvr;
     double w1[3], w2[3];
+    int clamped[3];          /* li_clamp held the position at an end */
 } tri64;
 
 /* One voxel's correspondence + clamp in double: the same decisions as
@@ -624,6 +625,7 @@ locate64 (const double fxyz[3], const double dxyz[3], const vol64* mv)
     for (int d = 0; d < 3; d++) {
         double ma = mijk[d];
         int64_t dmax = mv->dim[d] - 1;
+        r.clamped[d] = ma < 0. || ma >= dmax;
         if (ma < 0.) { f[d] = 0; rr[d] = 0; r.w2[d] = 0.; }
         else if (ma >= dmax) { f[d] = dmax - 1; rr[d] = dmax; r.w2[d] = 1.; }
         else {
@@ -1127,6 +1129,191 @@ orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     tile_loop64 (g, &fx, coeff, mi64_visit, &c, grad);
     *score = c.smetric;
     *num_vox = c.num_vox;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Mattes MI with cubic B-spline Parzen windows                          */
+/* ------------------------------------------------------------------ */
+
+/* Plastimatch implements Mattes MI only with partial-volume (PVI-8)
+ * binning; this is the Parzen-window form of the published method: Mattes,
+ * Haynor, Vesselle, Lewellen, Eubank, "PET-CT image registration in the
+ * chest using free-form deformations", IEEE Trans. Med. Imaging 22(1),
+ * 120-128 (2003), section II.B-C.  The joint histogram takes a zero-order
+ * B-spline window on the fixed intensity and a cubic B-spline window on
+ * the moving intensity at the warped position; the marginals are its sums;
+ * the cost is S = -sum p log(p / (p_f p_m)); and since the fixed marginal
+ * does not depend on the transform,
+ *   dS/dmu = 1/(N delta_m) sum_x [sum_k beta3'(k - u(x)) log(p(i(x), k) /
+ *            p_m(k))] grad m(T(x)) . dT(x)/dmu,
+ * with u(x) the moving value's continuous bin index.  The spatial gradient
+ * is that of the trilinear interpolant, rotated to world coordinates
+ * (proj^T times the index-space gradient), and zero along an axis where
+ * li_clamp holds the position at the image's end (the value is constant
+ * there). */
+
+void
+orc_parzen_init (orc_parzen* p, int64_t bins, const float* f_img, int64_t nf,
+    const float* m_img, int64_t nm)
+{
+    float fmin = f_img[0], fmax = f_img[0], mmin = m_img[0], mmax = m_img[0];
+    for (int64_t i = 1; i < nf; i++) {
+        if (f_img[i] < fmin) fmin = f_img[i];
+        if (f_img[i] > fmax) fmax = f_img[i];
+    }
+    for (int64_t i = 1; i < nm; i++) {
+        if (m_img[i] < mmin) mmin = m_img[i];
+        if (m_img[i] > mmax) mmax = m_img[i];
+    }
+    p->bins = bins;
+    p->f_min = fmin;
+    p->m_min = mmin;
+    p->f_delta = fmax > fmin ? (fmax - fmin) / (float) (bins - 4) : 1.0f;
+    p->m_delta = mmax > mmin ? (mmax - mmin) / (float) (bins - 4) : 1.0f;
+}
+
+/* centred cubic B-spline and its derivative */
+static double
+bspline3 (double t)
+{
+    double a = fabs (t);
+    if (a < 1.0) return 2.0 / 3.0 - a * a + 0.5 * a * a * a;
+    if (a < 2.0) return (2.0 - a) * (2.0 - a) * (2.0 - a) / 6.0;
+    return 0.0;
+}
+
+static double
+bspline3_d (double t)
+{
+    double a = fabs (t), sg = t < 0 ? -1.0 : 1.0;
+    if (a < 1.0) return -2.0 * t + 1.5 * t * a;
+    if (a < 2.0) return -sg * 0.5 * (2.0 - a) * (2.0 - a);
+    return 0.0;
+}
+
+/* fixed bin in float arithmetic, as the device computes it */
+static int64_t
+parzen_fbin (const orc_parzen* p, float v)
+{
+    int64_t b = (int64_t) floorf ((v - p->f_min) / p->f_delta) + 2;
+    if (b < 2) b = 2;
+    if (b > p->bins - 3) b = p->bins - 3;
+    return b;
+}
+
+typedef struct {
+    const vol64* mv;
+    const float* f_img;
+    const float* m_img;
+    const orc_parzen* p;
+    double* jh;
+    const double* lut;       /* pass 2: log(p / p_m) per joint bin */
+    double scale;            /* pass 2: 1 / (N delta_m) */
+    int pass;
+    int64_t num_vox;
+} parzen64_ctx;
+
+static void
+parzen64_visit (void* vctx, int64_t fidx, const double fxyz[3],
+    const double dxyz[3], double* dc_dv, int* has_grad)
+{
+    parzen64_ctx* c = (parzen64_ctx*) vctx;
+    tri64 t = locate64 (fxyz, dxyz, c->mv);
+    if (!t.ok) return;
+    const int64_t B = c->p->bins;
+    double w[8], mval = 0, mk[8];
+    corner_weights64 (w, &t);
+    for (int k = 0; k < 8; k++) {
+        mk[k] = c->m_img[corner_index (t.mvf, k, c->mv->dim)];
+        mval += w[k] * mk[k];
+    }
+    const int64_t fb = parzen_fbin (c->p, c->f_img[fidx]);
+    const double u = (mval - (double) c->p->m_min) / (double) c->p->m_delta + 2.0;
+    int64_t k0 = (int64_t) floor (u);
+    if (k0 > B - 3) k0 = B - 3;
+    if (k0 < 1) k0 = 1;
+    if (c->pass == 1) {
+        for (int j = 0; j < 4; j++) {
+            const int64_t kb = k0 - 1 + j;
+            c->jh[fb * B + kb] += bspline3 ((double) kb - u);
+        }
+        c->num_vox++;
+        return;
+    }
+    double s = 0;
+    for (int j = 0; j < 4; j++) {
+        const int64_t kb = k0 - 1 + j;
+        s += bspline3_d ((double) kb - u) * c->lut[fb * B + kb];
+    }
+    /* index-space gradient of the trilinear interpolant, then proj^T */
+    double gi[3] = {0, 0, 0};
+    for (int k = 0; k < 8; k++) {
+        double sx = (k & 1) ? 1. : -1., sy = (k & 2) ? 1. : -1.;
+        double sz = (k & 4) ? 1. : -1.;
+        double wx = (k & 1) ? t.w2[0] : t.w1[0];
+        double wy = (k & 2) ? t.w2[1] : t.w1[1];
+        double wz = (k & 4) ? t.w2[2] : t.w1[2];
+        gi[0] += sx * wy * wz * mk[k];
+        gi[1] += wx * sy * wz * mk[k];
+        gi[2] += wx * wy * sz * mk[k];
+    }
+    /* where li_clamp holds the position, the value does not move with it */
+    for (int d = 0; d < 3; d++) if (t.clamped[d]) gi[d] = 0;
+    for (int j = 0; j < 3; j++) {
+        double gw = 0;
+        for (int d = 0; d < 3; d++) gw += c->mv->proj[3*d+j] * gi[d];
+        dc_dv[j] = c->scale * s * gw;
+    }
+    *has_grad = 1;
+}
+
+int
+orc_mi_parzen_f64 (const orc_grid* g, const orc_vol* fixed,
+    const float* f_img, const orc_vol* moving, const float* m_img,
+    const float* coeff, const orc_parzen* p, double* score, double* grad,
+    int64_t* num_vox, double* jh)
+{
+    vol64 fx, mv;
+    if (p->bins < 5 || vol64_init (&fx, fixed) || vol64_init (&mv, moving)) {
+        return -1;
+    }
+    const int64_t B = p->bins;
+    memset (jh, 0, sizeof(double) * B * B);
+    parzen64_ctx c = { &mv, f_img, m_img, p, jh, 0, 0., 1, 0 };
+    tile_loop64 (g, &fx, coeff, parzen64_visit, &c, 0);
+    *num_vox = c.num_vox;
+    if (c.num_vox < 1) {
+        *score = FLT_MAX;
+        memset (grad, 0, sizeof(double) * g->num_coeff);
+        return 0;
+    }
+    const double N = (double) c.num_vox;
+    double* pf = (double*) calloc (B, sizeof(double));
+    double* pm = (double*) calloc (B, sizeof(double));
+    double* lut = (double*) calloc (B * B, sizeof(double));
+    for (int64_t i = 0; i < B; i++)
+        for (int64_t k = 0; k < B; k++) {
+            pf[i] += jh[i * B + k] / N;
+            pm[k] += jh[i * B + k] / N;
+        }
+    double s = 0;
+    for (int64_t i = 0; i < B; i++)
+        for (int64_t k = 0; k < B; k++) {
+            double pj = jh[i * B + k] / N;
+            if (pj > 0) {
+                s -= pj * log (pj / (pf[i] * pm[k]));
+                lut[i * B + k] = log (pj / pm[k]);
+            }
+        }
+    *score = s;
+    c.pass = 2;
+    c.lut = lut;
+    c.scale = 1.0 / (N * (double) p->m_delta);
+    tile_loop64 (g, &fx, coeff, parzen64_visit, &c, grad);
+    free (pf);
+    free (pm);
+    free (lut);
     return 0;
 }
 

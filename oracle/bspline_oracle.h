@@ -82,6 +82,22 @@ int orc_mi_f32 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     const orc_vol* moving, const float* m_img, const float* coeff,
     const orc_hist* fh, const orc_hist* mh, float* score, float* grad,
     int64_t* num_vox, double* f_hist, double* m_hist, double* j_hist);
+/* Mattes MI with cubic B-spline Parzen windows (no reference
+ * implementation; restated from the published method, see the definition).
+ * bins >= 5; the value range of each image is mapped with two padding bins
+ * at either end. */
+typedef struct {
+    int64_t bins;
+    float f_min, f_delta;    /* fixed: bin = floor((v - f_min) / f_delta) + 2 */
+    float m_min, m_delta;    /* moving: window centre (v - m_min) / m_delta + 2 */
+} orc_parzen;
+void orc_parzen_init (orc_parzen* p, int64_t bins, const float* f_img,
+    int64_t nf, const float* m_img, int64_t nm);
+int orc_mi_parzen_f64 (const orc_grid* g, const orc_vol* fixed,
+    const float* f_img, const orc_vol* moving, const float* m_img,
+    const float* coeff, const orc_parzen* p, double* score, double* grad,
+    int64_t* num_vox, double* jh);
+
 int orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     const orc_vol* moving, const float* m_img, const float* coeff,
     const orc_hist* fh, const orc_hist* mh, double* score, double* grad,

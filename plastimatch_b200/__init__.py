@@ -51,7 +51,11 @@ class GridDesc(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("form", C.c_int), ("mse_grad", C.c_int), ("mi_bins", C.c_int),
-                ("device", C.c_int), ("reserved", C.c_int * 4)]
+                ("device", C.c_int), ("mi_window", C.c_int),
+                ("reserved", C.c_int * 3)]
+
+
+MI_WINDOW = {"pvi8": 0, "parzen": 1}
 
 
 class RegParms(C.Structure):
@@ -336,7 +340,7 @@ class Context:
 
     def __init__(self, fixed: Volume, moving: Volume, grid: BsplineGrid,
                  form: str = "tc", mse_grad: str = "nearest",
-                 mi_bins: int = 32, device: int = 0):
+                 mi_bins: int = 32, device: int = 0, mi_window: str = "pvi8"):
         L = lib()
         self.fixed, self.moving, self.grid = fixed, moving, grid
         self.form = form
@@ -346,6 +350,7 @@ class Context:
         o.form = FORMS[form]
         o.mse_grad = MSE_GRAD[mse_grad]
         o.mi_bins = mi_bins
+        o.mi_window = MI_WINDOW[mi_window]
         o.device = device
         self._fd, self._md = _vol_desc(fixed), _vol_desc(moving)
         self._gd = GridDesc((C.c_int64 * 3)(*grid.roi_offset),

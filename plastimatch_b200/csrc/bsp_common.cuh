@@ -45,6 +45,7 @@ struct Sample {
     int mvr;        // linear index of the nearest ("round") voxel
     float w1[3];    // fraction for the lower corner, per axis
     float w2[3];    // fraction for the upper corner, per axis
+    int clamp;      // bit d: li_clamp held the position at an end of axis d
 };
 
 // World position of fixed voxel (i, j, k): origin + step * ijk.
@@ -68,6 +69,7 @@ locate (const BspGeom& g, const float fxyz[3], const float dxyz[3], Sample& s)
     float t1 = (fxyz[1] + dxyz[1]) - g.morigin[1];
     float t2 = (fxyz[2] + dxyz[2]) - g.morigin[2];
     int f[3], r[3];
+    s.clamp = 0;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         float ma = t0 * g.mproj[3*d+0] + t1 * g.mproj[3*d+1]
@@ -75,6 +77,7 @@ locate (const BspGeom& g, const float fxyz[3], const float dxyz[3], Sample& s)
         if (!(ma > -0.5f && ma < (float) g.mdim[d] - 0.5f)) return false;
         int dmax = g.mdim[d] - 1;
         float w2;
+        if (ma < 0.f || ma >= (float) dmax) s.clamp |= 1 << d;
         if (ma < 0.f) {
             f[d] = 0; r[d] = 0; w2 = 0.f;
         } else if (ma >= (float) dmax) {
@@ -201,6 +204,60 @@ trilinear_lerp_grad (const BspGeom& g, const float w2[3], const float m[8],
     float x0 = fmaf (w2[2], a1 - a0, a0);
     float x1 = fmaf (w2[2], b1 - b0, b0);
     out[0] = g.minv_spacing[0] * (x1 - x0);
+}
+
+// Centred cubic B-spline and its derivative (the Parzen window of the
+// Mattes MI variant).
+__device__ __forceinline__ float
+bspline3f (float t)
+{
+    const float a = fabsf (t);
+    if (a < 1.f) return 2.f / 3.f - a * a + 0.5f * a * a * a;
+    if (a < 2.f) return (2.f - a) * (2.f - a) * (2.f - a) * (1.f / 6.f);
+    return 0.f;
+}
+
+__device__ __forceinline__ float
+bspline3f_d (float t)
+{
+    const float a = fabsf (t);
+    if (a < 1.f) return -2.f * t + 1.5f * t * a;
+    if (a < 2.f) return (t < 0.f ? 0.5f : -0.5f) * (2.f - a) * (2.f - a);
+    return 0.f;
+}
+
+// Index-space gradient of the trilinear interpolant (w2: upper-corner
+// fractions, m: corners in li_value's order); an axis in `clamp` (bit d)
+// gets 0, since li_clamp holds the value constant there.
+__device__ __forceinline__ void
+trilinear_igrad (const float w2[3], const float m[8], int clamp, float out[3])
+{
+    const float w1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
+    out[0] = w1[1] * w1[2] * (m[1] - m[0]) + w2[1] * w1[2] * (m[3] - m[2])
+        + w1[1] * w2[2] * (m[5] - m[4]) + w2[1] * w2[2] * (m[7] - m[6]);
+    out[1] = w1[0] * w1[2] * (m[2] - m[0]) + w2[0] * w1[2] * (m[3] - m[1])
+        + w1[0] * w2[2] * (m[6] - m[4]) + w2[0] * w2[2] * (m[7] - m[5]);
+    out[2] = w1[0] * w1[1] * (m[4] - m[0]) + w2[0] * w1[1] * (m[5] - m[1])
+        + w1[0] * w2[1] * (m[6] - m[2]) + w2[0] * w2[1] * (m[7] - m[3]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (clamp & (1 << d)) out[d] = 0.f;
+    }
+}
+
+// Mattes MI with cubic B-spline Parzen windows: the fixed voxel's bin is
+// precomputed; the moving value's window centre in bins, the first of its
+// four bins (clamped so the four stay inside [1, bins - 1]).
+__device__ __forceinline__ float
+parzen_centre (float v, float m_min, float m_delta)
+{
+    return __fdiv_rn (v - m_min, m_delta) + 2.f;
+}
+
+__device__ __forceinline__ int
+parzen_first_bin (float u, int bins)
+{
+    return min (max ((int) floorf (u), 1), bins - 3) - 1;
 }
 
 // The eight corner values of a trilinear cell, in li_value's order.

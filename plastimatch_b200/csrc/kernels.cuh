@@ -54,15 +54,20 @@ cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
 
 // Mattes MI on the tensor-core kernel (axis-aligned geometry, tiles of at
 // most 128 voxels, histograms that fit the adjoint operand's area): pass 1
-// (hist_pass: PVI-8 histograms into mi.hist, integer 2^-24 units, count
-// last) or pass 2 (dc/dv from the factor table -> per-batch partials).
+// (hist_pass: PVI-8 or Parzen histograms into mi.hist, integer 2^-24 units,
+// count last) or pass 2 (dc/dv from the factor table -> per-batch
+// partials).
 struct TcMiArgs {
     const uint8_t* fbin;
     const uint8_t* mbin;
     int bins;
     const float* lut;            // [fixed bin][moving bin] pass-2 factors
-    const float* nvf;            // voxel count as float
+    const float* nvf;            // voxel count as float (Parzen: [1] the
+                                 // pass-2 scale 1 / (N delta_m))
     unsigned long long* hist;    // f[B], m[B], j[B*B], count
+    bool parzen;                 // cubic B-spline Parzen windows
+    const float* mimg;           // Parzen: the moving image
+    float m_min, m_delta;        // Parzen: moving value -> window centre
 };
 bool tc_mi_supported (const BspGeom& g, const TcPlan& p, int bins);
 cudaError_t launch_mi_tc (const BspGeom& g, const TcPlan& p, bool hist_pass,

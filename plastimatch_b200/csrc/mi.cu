@@ -74,8 +74,8 @@ bin_image_kernel (const float* __restrict__ img, long long n, float offset,
 }
 
 static int
-eqsp_range (const float* d_img, size_t n, int bins, float* d_scratch,
-    float* offset, float* delta, cudaStream_t st)
+image_range (const float* d_img, size_t n, float* d_scratch, float* mn_out,
+    float* mx_out, cudaStream_t st)
 {
     const int blocks = 296;
     minmax_kernel<<<blocks, 256, 0, st>>> (d_img, (long long) n, d_scratch);
@@ -90,6 +90,30 @@ eqsp_range (const float* d_img, size_t n, int bins, float* d_scratch,
         mn = std::fmin (mn, mm[2 * b]);
         mx = std::fmax (mx, mm[2 * b + 1]);
     }
+    *mn_out = mn;
+    *mx_out = mx;
+    return B200BSP_OK;
+}
+
+// Parzen fixed bins: floor((v - min) / delta) + 2 in [2, bins - 3].
+__global__ void
+parzen_bin_kernel (const float* __restrict__ img, long long n, float vmin,
+    float delta, int bins, uint8_t* __restrict__ out)
+{
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        const int b = (int) floorf (__fdiv_rn (img[i] - vmin, delta)) + 2;
+        out[i] = (uint8_t) min (max (b, 2), bins - 3);
+    }
+}
+
+static int
+eqsp_range (const float* d_img, size_t n, int bins, float* d_scratch,
+    float* offset, float* delta, cudaStream_t st)
+{
+    float mn, mx;
+    int rc = image_range (d_img, n, d_scratch, &mn, &mx, st);
+    if (rc) return rc;
     // delta = (max - min) / (bins - 1); offset = min - 0.5 * delta
     *delta = (mx - mn) / (float) (bins - 1);
     *offset = (float) (mn - 0.5 * (double) *delta);
@@ -100,9 +124,10 @@ eqsp_range (const float* d_img, size_t n, int bins, float* d_scratch,
 }
 
 int
-mi_alloc (MiState* s, const BspGeom& g, int bins)
+mi_alloc (MiState* s, const BspGeom& g, int bins, int window)
 {
     s->bins = bins;
+    s->window = window;
     size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
     size_t nm = (size_t) g.mdim[0] * g.mdim[1] * g.mdim[2];
     size_t nh = 2 * bins + bins * bins + 1;
@@ -111,7 +136,7 @@ mi_alloc (MiState* s, const BspGeom& g, int bins)
         || cudaMalloc (&s->d_hist, nh * sizeof (unsigned long long)) != cudaSuccess
         || cudaMalloc (&s->d_histd, nh * sizeof (double)) != cudaSuccess
         || cudaMalloc (&s->d_lut, bins * bins * sizeof (float)) != cudaSuccess
-        || cudaMalloc (&s->d_nvf, sizeof (float)) != cudaSuccess
+        || cudaMalloc (&s->d_nvf, 2 * sizeof (float)) != cudaSuccess
         || cudaMalloc (&s->d_minmax, 2 * 296 * sizeof (float)) != cudaSuccess
         || cudaMalloc (&s->d_part, (size_t) 64 * 3 * g.ntiles * sizeof (float))
             != cudaSuccess
@@ -140,6 +165,23 @@ int
 mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
     const float* d_moving, size_t nf, size_t nm, cudaStream_t st)
 {
+    if (s->window == B200BSP_MI_PARZEN) {
+        // value ranges mapped onto bins 2 .. bins - 2 (two padding bins at
+        // either end hold the cubic window's tails)
+        float fmn, fmx, mmn, mmx;
+        int rc = image_range (d_fixed, nf, s->d_minmax, &fmn, &fmx, st);
+        if (!rc) rc = image_range (d_moving, nm, s->d_minmax, &mmn, &mmx, st);
+        if (rc) return rc;
+        s->pz_fmin = fmn;
+        s->pz_mmin = mmn;
+        s->pz_fdelta = fmx > fmn ? (fmx - fmn) / (float) (s->bins - 4) : 1.f;
+        s->pz_mdelta = mmx > mmn ? (mmx - mmn) / (float) (s->bins - 4) : 1.f;
+        parzen_bin_kernel<<<1184, 256, 0, st>>> (d_fixed, (long long) nf,
+            s->pz_fmin, s->pz_fdelta, s->bins, s->d_fbin);
+        if (cudaGetLastError () != cudaSuccess) return B200BSP_E_CUDA;
+        s->ready = true;
+        return B200BSP_OK;
+    }
     int rc = eqsp_range (d_fixed, nf, s->bins, s->d_minmax, &s->f_offset,
         &s->f_delta, st);
     if (rc) return rc;
@@ -313,6 +355,218 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
     if (lane == 0 && cnt) atomicAdd (&ghist[nh], (unsigned long long) cnt);
 }
 
+// ---- Parzen windows: pass 1 ----------------------------------------------------
+//
+// Mattes MI with cubic B-spline Parzen windows (Mattes et al., IEEE TMI
+// 22(1) 2003): each inside voxel adds the cubic window's four weights at
+// its moving value to the joint histogram row of its fixed bin (integers in
+// 2^-24 units, order-independent sums); lanes whose (fixed bin, first
+// window bin) agree combine across the warp first.  Marginals are the joint
+// histogram's sums (taken by the score kernel).
+
+__device__ __forceinline__ void
+parzen_hist_add (unsigned long long* hj, int B, bool live, int fb, float u,
+    int lane, int& cnt)
+{
+    const int k0 = parzen_first_bin (u, B);
+    unsigned int q[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        q[j] = __float2uint_rn (bspline3f ((float) (k0 + j) - u) * MI_WUNIT);
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        cnt++;
+        const int key = fb * B + k0;
+        const unsigned peers = __match_any_sync (live_mask, key);
+        unsigned sum[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) sum[j] = __reduce_add_sync (peers, q[j]);
+        if (lane == __ffs (peers) - 1) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (sum[j]) atomicAdd (&hj[key + j], (unsigned long long) sum[j]);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__ (MIH_THREADS)
+parzen_hist_kernel (BspGeom g, const float* __restrict__ coeff,
+    const float* __restrict__ luts, const uint8_t* __restrict__ fbin,
+    const float* __restrict__ mimg, int B, float m_min, float m_delta,
+    unsigned long long* __restrict__ ghist)
+{
+    extern __shared__ unsigned long long hsm[];   // j[B*B]
+    __shared__ float sC[192];
+    __shared__ float slut[4 * 3 * 64];
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    const int V = vx * vy * vz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < B * B; i += MIH_THREADS) hsm[i] = 0ull;
+    for (int o = threadIdx.x; o < 4 * (vx + vy + vz); o += MIH_THREADS) {
+        slut[o] = luts[o];
+    }
+    const float* sbx = slut;
+    const float* sby = slut + 4 * vx;
+    const float* sbz = sby + 4 * vy;
+    const int dx = g.mdim[0], dxy = g.mdim[0] * g.mdim[1];
+    int cnt = 0;
+    __syncthreads ();
+    for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+        const int tx = t % g.rdims[0];
+        const int ty = (t / g.rdims[0]) % g.rdims[1];
+        const int tz = t / (g.rdims[0] * g.rdims[1]);
+        for (int o = threadIdx.x; o < 192; o += MIH_THREADS) {
+            int m = o / 3, c = o - 3 * m;
+            int i = m & 3, j = (m >> 2) & 3, k = m >> 4;
+            sC[o] = coeff[3 * ((tz + k) * g.cdims[1] * g.cdims[0]
+                + (ty + j) * g.cdims[0] + (tx + i)) + c];
+        }
+        __syncthreads ();
+        // warp-uniform trip count: every lane reaches the warp collectives
+        for (int v0 = 32 * warp; v0 < V; v0 += MIH_THREADS) {
+            const int v = v0 + lane;
+            const int vv = v < V ? v : 0;
+            int lx = vv % vx, ly = (vv / vx) % vy, lz = vv / (vx * vy);
+            int fi = g.roi_off[0] + vx * tx + lx;
+            int fj = g.roi_off[1] + vy * ty + ly;
+            int fk = g.roi_off[2] + vz * tz + lz;
+            bool live = v < V && fi < g.roi_off[0] + g.roi_dim[0]
+                && fj < g.roi_off[1] + g.roi_dim[1]
+                && fk < g.roi_off[2] + g.roi_dim[2];
+            int fb = 0;
+            float u = 2.f;
+            if (live) {
+                float fxyz[3], d[3] = {0.f, 0.f, 0.f};
+                fixed_position (g, fi, fj, fk, fxyz);
+                int m = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    float C = sbz[lz * 4 + k];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        float Bv = sby[ly * 4 + j] * C;
+#pragma unroll
+                        for (int i = 0; i < 4; i++, m++) {
+                            float A = sbx[lx * 4 + i] * Bv;
+                            d[0] += A * sC[3 * m + 0];
+                            d[1] += A * sC[3 * m + 1];
+                            d[2] += A * sC[3 * m + 2];
+                        }
+                    }
+                }
+                Sample s;
+                live = locate (g, fxyz, d, s);
+                if (live) {
+                    const Corners cr = load_corners (mimg, s.mvf, dx, dxy);
+                    u = parzen_centre (trilinear (s, cr), m_min, m_delta);
+                    fb = fbin[fi + g.fdim[0] * (fj + g.fdim[1] * fk)];
+                }
+            }
+            parzen_hist_add (hsm, B, live, fb, u, lane, cnt);
+        }
+        __syncthreads ();
+    }
+    const int nh = 2 * B + B * B;
+    for (int i = threadIdx.x; i < B * B; i += MIH_THREADS) {
+        if (hsm[i]) atomicAdd (&ghist[2 * B + i], hsm[i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync (0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd (&ghist[nh], (unsigned long long) cnt);
+}
+
+// Score and pass-2 table: p = joint / N (weights in 2^-24 units), p_f and
+// p_m its row and column sums, S = -sum p log(p / (p_f p_m)) (terms with
+// p = 0 drop out), the factor log(p / p_m) per joint bin, and
+// 1 / (N delta_m) for pass 2.  Marginals and joint go to histd as weights.
+__global__ void __launch_bounds__ (1024)
+parzen_score_kernel (const unsigned long long* __restrict__ ghist, int B,
+    float m_delta, double* __restrict__ histd, float* __restrict__ lut,
+    float* __restrict__ nvf, DevResult* __restrict__ res)
+{
+    __shared__ double sh_v[32];
+    __shared__ int sh_n[32];
+    __shared__ double s_pf[MI_MAX_BINS], s_pm[MI_MAX_BINS];
+    const int nh = 2 * B + B * B;
+    const long long N = (long long) ghist[nh];
+    const double* j = histd + 2 * B;
+    for (int i = threadIdx.x; i < B * B; i += blockDim.x) {
+        histd[2 * B + i] = (double) ghist[2 * B + i] * MI_WUNIT_INV;
+    }
+    __syncthreads ();
+    for (int i = threadIdx.x; i < 2 * B; i += blockDim.x) {
+        double v = 0.0;
+        if (i < B) {
+            for (int k = 0; k < B; k++) v += j[i * B + k];
+            s_pf[i] = v;
+        } else {
+            for (int r = 0; r < B; r++) v += j[r * B + (i - B)];
+            s_pm[i - B] = v;
+        }
+        histd[i] = v;
+    }
+    __syncthreads ();
+    const double fnv = (double) N;
+    double acc = 0.0;
+    for (int jb = threadIdx.x; jb < B * B; jb += blockDim.x) {
+        const int fb = jb / B, mb = jb - fb * B;
+        const double pj = j[jb] / fnv;
+        float f = 0.f;
+        if (N > 0 && pj > 0.0) {
+            const double pm = s_pm[mb] / fnv, pf = s_pf[fb] / fnv;
+            acc -= pj * log (pj / (pf * pm));
+            f = (float) log (pj / pm);
+        }
+        lut[jb] = f;
+    }
+    int dummy = 0;
+    block_sum<1024> (acc, dummy, sh_v, sh_n);
+    if (threadIdx.x == 0) {
+        res->raw = acc;
+        res->score = N > 0 ? acc : (double) FLT_MAX;
+        res->score_f = N > 0 ? (float) acc : FLT_MAX;
+        res->num_vox = N;
+        res->error = 0;
+        nvf[0] = (float) N;
+        nvf[1] = N > 0 ? (float) (1.0 / (fnv * (double) m_delta)) : 0.f;
+    }
+}
+
+// Pass 2 on the FP32 tile kernel: dc/dv = 1/(N delta_m) * sum over the
+// window's bins of beta3'(k - u) log(p(f, k) / p_m(k)) times the world
+// gradient of the trilinear interpolant (proj^T times the index gradient).
+struct ParzenGradVoxel {
+    static constexpr bool kNeedCorners = true;
+    const uint8_t* fbin;
+    const float* lut;
+    const float* nvf;
+    int B;
+    float m_min, m_delta;
+    __device__ __forceinline__ bool
+    voxel (const BspGeom& g, int fidx, const Sample& s, const Corners& cr,
+        float dc[3], double&) const
+    {
+        const float u = parzen_centre (trilinear (s, cr), m_min, m_delta);
+        const int k0 = parzen_first_bin (u, B);
+        const float* row = lut + (int) __ldg (fbin + fidx) * B;
+        float sum = 0.f;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            sum += bspline3f_d ((float) (k0 + j) - u) * __ldg (row + k0 + j);
+        }
+        float gi[3];
+        trilinear_igrad (s.w2, cr.m, s.clamp, gi);
+        const float sc = __ldg (nvf + 1) * sum;
+        const float* p = g.mproj;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dc[c] = sc * (p[c] * gi[0] + p[3 + c] * gi[1] + p[6 + c] * gi[2]);
+        }
+        return true;
+    }
+};
+
 // ---- score and pass-2 factor table -----------------------------------------
 
 __global__ void __launch_bounds__ (1024)
@@ -423,8 +677,8 @@ struct MiGradVoxel {
 
 int
 mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
-    const float* d_luts, DevResult* d_res, float* grad_out,
-    double* grad64_out, cudaStream_t st, int* launches)
+    const float* d_moving, const float* d_luts, DevResult* d_res,
+    float* grad_out, double* grad64_out, cudaStream_t st, int* launches)
 {
     if (!s->ready) return B200BSP_E_STATE;
     const int B = s->bins;
@@ -433,14 +687,38 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
             st) != cudaSuccess) {
         return B200BSP_E_CUDA;
     }
+    int sms = 148;
+    cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, 0);
+    PartLayout lay;
+    lay.bx = lay.by = lay.bz = 1;
+    lay.nbx = g.rdims[0]; lay.nby = g.rdims[1]; lay.nbz = g.rdims[2];
+    lay.kx = lay.ky = lay.kz = 4;
+    lay.slots = 64;
+    if (s->window == B200BSP_MI_PARZEN) {
+        const int grid = std::min (g.ntiles, 8 * sms);
+        parzen_hist_kernel<<<grid, MIH_THREADS,
+            (size_t) B * B * sizeof (unsigned long long), st>>> (g, d_coeff,
+            d_luts, s->d_fbin, d_moving, B, s->pz_mmin, s->pz_mdelta,
+            s->d_hist);
+        parzen_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->pz_mdelta,
+            s->d_histd, s->d_lut, s->d_nvf, d_res);
+        ParzenGradVoxel f{s->d_fbin, s->d_lut, s->d_nvf, B, s->pz_mmin,
+            s->pz_mdelta};
+        if (launch_fp32_tile (g, f, d_moving, d_coeff, d_luts, s->d_part,
+                s->d_score_part, s->d_count_part, st) != cudaSuccess
+            || launch_gather_grad (g, lay, s->d_part, d_res, 1, grad_out,
+                grad64_out, nullptr, nullptr, nullptr, st) != cudaSuccess) {
+            return B200BSP_E_CUDA;
+        }
+        if (launches) *launches += 4;
+        return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+    }
     size_t hsmem = (size_t) nh * sizeof (unsigned long long);
     auto hk = mi_hist_kernel;
     if (hsmem > 48 * 1024) {
         cudaFuncSetAttribute (hk, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int) hsmem);
     }
-    int sms = 148;
-    cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, 0);
     int grid = std::min (g.ntiles, 8 * sms);
     hk<<<grid, MIH_THREADS, hsmem, st>>> (g, d_coeff, d_luts, s->d_fbin,
         s->d_mbin, B, s->d_hist);
@@ -451,11 +729,6 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
             s->d_score_part, s->d_count_part, st) != cudaSuccess) {
         return B200BSP_E_CUDA;
     }
-    PartLayout lay;
-    lay.bx = lay.by = lay.bz = 1;
-    lay.nbx = g.rdims[0]; lay.nby = g.rdims[1]; lay.nbz = g.rdims[2];
-    lay.kx = lay.ky = lay.kz = 4;
-    lay.slots = 64;
     if (launch_gather_grad (g, lay, s->d_part, d_res, 1, grad_out, grad64_out,
             nullptr, nullptr, nullptr, st) != cudaSuccess) {
         return B200BSP_E_CUDA;
@@ -471,8 +744,9 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
 int
 mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     const PartLayout& lay, const void* qlut, float* part, double* score_part,
-    int* count_part, int* err, const float* d_coeff, DevResult* d_res,
-    float* grad_out, double* grad64_out, cudaStream_t st, int* launches)
+    int* count_part, int* err, const float* d_coeff, const float* d_moving,
+    DevResult* d_res, float* grad_out, double* grad64_out, cudaStream_t st,
+    int* launches)
 {
     if (!s->ready) return B200BSP_E_STATE;
     const int B = s->bins;
@@ -488,12 +762,21 @@ mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     mi.lut = s->d_lut;
     mi.nvf = s->d_nvf;
     mi.hist = s->d_hist;
+    mi.parzen = s->window == B200BSP_MI_PARZEN;
+    mi.mimg = d_moving;
+    mi.m_min = s->pz_mmin;
+    mi.m_delta = s->pz_mdelta;
     if (launch_mi_tc (g, plan, true, mi, d_coeff, qlut, part, score_part,
             count_part, err, st) != cudaSuccess) {
         return B200BSP_E_CUDA;
     }
-    mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd, s->d_lut,
-        s->d_nvf, d_res);
+    if (mi.parzen) {
+        parzen_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->pz_mdelta,
+            s->d_histd, s->d_lut, s->d_nvf, d_res);
+    } else {
+        mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd,
+            s->d_lut, s->d_nvf, d_res);
+    }
     if (launch_mi_tc (g, plan, false, mi, d_coeff, qlut, part, score_part,
             count_part, err, st) != cudaSuccess
         || launch_gather_grad (g, lay, part, d_res, 1, grad_out, grad64_out,

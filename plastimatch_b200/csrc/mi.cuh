@@ -1,4 +1,5 @@
-// Mattes mutual information (PVI-8) on the device: state and entry points.
+// Mattes mutual information on the device (PVI-8, the reference's binning,
+// or cubic B-spline Parzen windows): state and entry points.
 #pragma once
 
 #include <cstddef>
@@ -19,14 +20,19 @@ struct MiResult {
 
 struct MiState {
     int bins = 0;
+    int window = 0;                           // B200BSP_MI_PVI8 / _PARZEN
     bool ready = false;
+    // Parzen: fixed bin = floor((v - pz_fmin) / pz_fdelta) + 2; moving
+    // window centre (v - pz_mmin) / pz_mdelta + 2
+    float pz_fmin = 0.f, pz_fdelta = 1.f, pz_mmin = 0.f, pz_mdelta = 1.f;
     float f_offset = 0.f, f_delta = 1.f, m_offset = 0.f, m_delta = 1.f;
     uint8_t* d_fbin = nullptr;                // fixed-image bin per voxel
     uint8_t* d_mbin = nullptr;                // moving-image bin per voxel
     unsigned long long* d_hist = nullptr;     // f[B], m[B], j[B*B], N (fixed point)
     double* d_histd = nullptr;                // f, m, j as doubles
     float* d_lut = nullptr;                   // dS/dP per joint bin (0 = skip)
-    float* d_nvf = nullptr;                   // num_vox as float
+    float* d_nvf = nullptr;                   // num_vox as float; Parzen:
+                                              // [1] = 1 / (num_vox delta_m)
     float* d_minmax = nullptr;                // per-block min/max scratch
     float* d_part = nullptr;                  // pass-2 tile partials, 64 slots
     double* d_score_part = nullptr;
@@ -35,17 +41,18 @@ struct MiState {
     DevResult* h_res = nullptr;
 };
 
-int mi_alloc (MiState* s, const BspGeom& g, int bins);
+int mi_alloc (MiState* s, const BspGeom& g, int bins, int window);
 void mi_free (MiState* s);
 int mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
     const float* d_moving, size_t nf, size_t nm, cudaStream_t st);
 int mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
-    const float* d_luts, DevResult* d_res, float* grad_out,
-    double* grad64_out, cudaStream_t st, int* launches);
+    const float* d_moving, const float* d_luts, DevResult* d_res,
+    float* grad_out, double* grad64_out, cudaStream_t st, int* launches);
 int mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     const PartLayout& lay, const void* qlut, float* part, double* score_part,
-    int* count_part, int* err, const float* d_coeff, DevResult* d_res,
-    float* grad_out, double* grad64_out, cudaStream_t st, int* launches);
+    int* count_part, int* err, const float* d_coeff, const float* d_moving,
+    DevResult* d_res, float* grad_out, double* grad64_out, cudaStream_t st,
+    int* launches);
 int mi_fetch (MiState* s, const DevResult* d_res, double* f_hist,
     double* m_hist, double* j_hist, cudaStream_t st);
 void mi_finish (MiState* s, MiResult* r);

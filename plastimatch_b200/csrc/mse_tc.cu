@@ -63,11 +63,21 @@ constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;
 //   TC_MSE_LINEAR   MSE score + gradient, trilinear moving gradient
 //   TC_MI_GRAD      Mattes MI pass 2: dc/dv from the PVI-8 factor table
 //   TC_MI_HIST      Mattes MI pass 1: PVI-8 histograms (no adjoint)
+//   TC_PZ_GRAD      Mattes MI with cubic B-spline Parzen windows, pass 2
+//   TC_PZ_HIST      the same, pass 1 (joint histogram, no adjoint)
 // The MI modes run the axis-aligned voxel phase only.
 constexpr int TC_MSE_NEAREST = 0;
 constexpr int TC_MSE_LINEAR = 1;
 constexpr int TC_MI_GRAD = 2;
 constexpr int TC_MI_HIST = 3;
+constexpr int TC_PZ_GRAD = 4;
+constexpr int TC_PZ_HIST = 5;
+
+__host__ __device__ constexpr bool
+tc_hist_mode (int mode)
+{
+    return mode == TC_MI_HIST || mode == TC_PZ_HIST;
+}
 constexpr float TC_MI_WUNIT = 16777216.0f;   // histogram weights in 2^-24
 
 // Adjoint-operand rows: (c, t) -> r = 8 (3 (t >> 3) + c) + (t & 7), so the
@@ -118,6 +128,7 @@ struct TcArgs {
     const float* mi_lut;
     const float* mi_nvf;
     unsigned long long* hist;
+    float pz_mmin, pz_mdelta;    // Parzen: moving value -> window centre
 };
 
 __device__ __forceinline__ void
@@ -734,6 +745,64 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
     }
 }
 
+// Mattes MI with cubic B-spline Parzen windows, pass 1 at one sample: the
+// window's four weights at the moving value u (integers in 2^-24 units)
+// into the fixed bin's row of the shared joint histogram; lanes with the
+// same (fixed bin, first window bin) combine across the warp first.  Every
+// lane of the warp calls this.
+__device__ __forceinline__ void
+pz_hist_add (const TcArgs& a, const TcCtx& x, bool live, int fb, float u,
+    int& cnt)
+{
+    const int B = a.bins;
+    unsigned long long* hj = (unsigned long long*) (x.sm + SM_DC) + 2 * B;
+    const int k0 = parzen_first_bin (u, B);
+    unsigned int q[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        q[j] = __float2uint_rn (bspline3f ((float) (k0 + j) - u) * TC_MI_WUNIT);
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        cnt++;
+        const int key = fb * B + k0;
+        const unsigned peers = __match_any_sync (live_mask, key);
+        unsigned sum[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) sum[j] = __reduce_add_sync (peers, q[j]);
+        if (x.lane == __ffs (peers) - 1) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (sum[j]) atomicAdd (&hj[key + j], (unsigned long long) sum[j]);
+            }
+        }
+    }
+}
+
+// Pass 2 at one sample: 1/(N delta_m) * sum over the window's bins of
+// beta3'(k - u) log(p(f, k) / p_m(k)), times the world gradient of the
+// trilinear interpolant (axis-aligned here: the diagonal of proj times the
+// index gradient; 0 along an axis the clamp holds).
+__device__ __forceinline__ void
+pz_dc_dv (const TcArgs& a, float u, int fb, const float w2[3],
+    const float m[8], int clamp, float dc[3])
+{
+    const int B = a.bins;
+    const int k0 = parzen_first_bin (u, B);
+    const float* row = a.mi_lut + fb * B;
+    float sum = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        sum += bspline3f_d ((float) (k0 + j) - u) * __ldg (row + k0 + j);
+    }
+    float gi[3];
+    trilinear_igrad (w2, m, clamp, gi);
+    const float sc = __ldg (a.mi_nvf + 1) * sum;
+    dc[0] = sc * (a.g.mproj[0] * gi[0]);
+    dc[1] = sc * (a.g.mproj[4] * gi[1]);
+    dc[2] = sc * (a.g.mproj[8] * gi[2]);
+}
+
 template <int MODE>
 __device__ __forceinline__ void
 voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
@@ -760,7 +829,7 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
     // Padding voxels (V..127) carry no samples; zero their adjoint columns
     // in the rows of live tiles (see voxel_phase_xline).  The histogram
     // pass has no adjoint (its histograms live in that area).
-    const int npad = MODE == TC_MI_HIST ? 0 : 128 - a.V;
+    const int npad = tc_hist_mode (MODE) ? 0 : 128 - a.V;
     for (int o = x.tid; o < npad * T; o += TC_THREADS) {
         const int tb = o / npad, v = a.V + (o - tb * npad);
         uint8_t* p = dch + (v >> 6) * DC_CHUNK + (3 * (tb >> 3)) * 1024
@@ -822,12 +891,13 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
         //    histogram pass keeps every lane of a warp in the loop (warp
         //    collectives), the other modes let a lane leave at the plane end
         const int X0 = r * W;
-        const int s_end = MODE == TC_MI_HIST ? plane + x.lane : plane;
+        const int s_end = tc_hist_mode (MODE) ? plane + x.lane : plane;
         for (int s0 = x.tid; s0 < s_end; s0 += TC_SPT * TC_THREADS) {
             bool ok[TC_SPT];
             int mvf[TC_SPT], mvr[TC_SPT], fidx[TC_SPT];
             uint32_t doff[TC_SPT];
             float w2[TC_SPT][3];
+            int clampb[TC_SPT];
 #pragma unroll
             for (int u = 0; u < TC_SPT; u++) {
                 const int sv = s0 + u * TC_THREADS;
@@ -848,9 +918,13 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                 bool in = in_plane && rw.w != 0u && X < xlim;
                 int f[3];
                 bool up[3];
+                clampb[u] = 0;
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     in = in && ma[d] > -0.5f && ma[d] < g.m_hi[d];
+                    if (MODE == TC_PZ_GRAD && (ma[d] < 0.f || ma[d] >= g.m_fmax[d] + 1.f)) {
+                        clampb[u] |= 1 << d;
+                    }
                     // floor(max(ma, 0)) in the low mantissa bits of
                     // max(ma, 0) + 2^23 rounded down; corner clamped to
                     // dim - 2, fraction saturated to [0, 1] (li_clamp)
@@ -874,7 +948,36 @@ voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
                         + (v & 7) * 2)
                     : 0xffffffffu;
             }
-            if constexpr (MODE == TC_MSE_NEAREST || MODE == TC_MSE_LINEAR) {
+            if constexpr (MODE == TC_PZ_GRAD || MODE == TC_PZ_HIST) {
+                float cr[TC_SPT][8];
+                int fb[TC_SPT];
+#pragma unroll
+                for (int u = 0; u < TC_SPT; u++) {
+                    const float* mp = a.mimg + mvf[u];
+                    cr[u][0] = __ldg (mp);
+                    cr[u][1] = __ldg (mp + 1);
+                    cr[u][2] = __ldg (mp + dxm);
+                    cr[u][3] = __ldg (mp + dxm + 1);
+                    cr[u][4] = __ldg (mp + dxym);
+                    cr[u][5] = __ldg (mp + dxym + 1);
+                    cr[u][6] = __ldg (mp + dxym + dxm);
+                    cr[u][7] = __ldg (mp + dxym + dxm + 1);
+                    fb[u] = __ldg (a.fbin + fidx[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < TC_SPT; u++) {
+                    const float uc = parzen_centre (trilinear_lerp (w2[u], cr[u]),
+                        a.pz_mmin, a.pz_mdelta);
+                    if constexpr (MODE == TC_PZ_HIST) {
+                        pz_hist_add (a, x, ok[u], fb[u], uc, cnt);
+                    } else {
+                        float dc[3];
+                        pz_dc_dv (a, uc, fb[u], w2[u], cr[u], clampb[u], dc);
+                        if (!ok[u]) dc[0] = dc[1] = dc[2] = 0.f;
+                        if (doff[u] != 0xffffffffu) store_dc (dch + doff[u], dc[0], dc[1], dc[2]);
+                    }
+                }
+            } else if constexpr (MODE == TC_MSE_NEAREST || MODE == TC_MSE_LINEAR) {
                 float cr[TC_SPT][8], fv[TC_SPT];
                 float4 gr[TC_SPT];
 #pragma unroll
@@ -1121,7 +1224,7 @@ mse_tc_kernel (TcArgs a)
 
     if (mma_warp) {
         if (x.lane == 0) {
-            mma_loop (a, x, nb_local, MODE != TC_MI_HIST, s_bar, abort_flag);
+            mma_loop (a, x, nb_local, !tc_hist_mode (MODE), s_bar, abort_flag);
         }
         __syncwarp ();
     } else {
@@ -1187,7 +1290,7 @@ mse_tc_kernel (TcArgs a)
                 } else {
                     voxel_phase_xline<MODE> (a, x, vs0, tx0, ty, tz, sc, cnt);
                 }
-                if (MODE != TC_MI_HIST) warp_arrive (x, &s_bar[1]);
+                if (!tc_hist_mode (MODE)) warp_arrive (x, &s_bar[1]);
                 if (i + 1 < nb_local) {
                     int nx0, ny, nz;
                     coords (b + gridDim.x, nx0, ny, nz);
@@ -1196,7 +1299,7 @@ mse_tc_kernel (TcArgs a)
                     build_c (a, x);
                     warp_arrive (x, &s_bar[0]);
                 }
-                if (MODE == TC_MI_HIST) continue;
+                if (tc_hist_mode (MODE)) continue;
                 if (!cwait (a, x, &s_bar[3], ph_g, abort_flag, 2)) break;
                 finish_batch (b);
             }
@@ -1228,7 +1331,7 @@ mse_tc_kernel (TcArgs a)
                 finish_batch (b);
             }
         }
-        if constexpr (MODE == TC_MI_HIST) {
+        if constexpr (tc_hist_mode (MODE)) {
             // the CTA's histograms and count into the global ones (integer
             // sums: the order does not matter)
             cbar ();
@@ -1236,7 +1339,9 @@ mse_tc_kernel (TcArgs a)
             const unsigned long long* h = (const unsigned long long*) (x.sm + SM_DC);
             for (int i = x.tid; i < nh; i += TC_THREADS) {
                 unsigned long long v = h[i];
-                if (i >= B && i < 2 * B) {          // moving: joint column sum
+                if (MODE == TC_PZ_HIST && i < 2 * B) {
+                    v = 0;                          // marginals: score kernel
+                } else if (i >= B && i < 2 * B) {   // moving: joint column sum
                     v = 0;
                     for (int fb = 0; fb < B; fb++) v += h[2 * B + fb * B + (i - B)];
                 }
@@ -1416,6 +1521,13 @@ launch_mi_tc (const BspGeom& g, const TcPlan& p, bool hist_pass,
     a.err = err;
     a.fbin = mi.fbin; a.mbin = mi.mbin; a.bins = mi.bins;
     a.mi_lut = mi.lut; a.mi_nvf = mi.nvf; a.hist = mi.hist;
+    if (mi.parzen) {
+        a.mimg = mi.mimg;
+        a.pz_mmin = mi.m_min;
+        a.pz_mdelta = mi.m_delta;
+        return hist_pass ? launch_mode<TC_PZ_HIST> (p, a, st)
+                         : launch_mode<TC_PZ_GRAD> (p, a, st);
+    }
     return hist_pass ? launch_mode<TC_MI_HIST> (p, a, st)
                      : launch_mode<TC_MI_GRAD> (p, a, st);
 }

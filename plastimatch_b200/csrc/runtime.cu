@@ -360,6 +360,14 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     if (o.mse_grad != 0 && o.mse_grad != 1) {
         return fail (nullptr, B200BSP_E_BADARG, "unknown mse_grad %d", o.mse_grad);
     }
+    if (o.mi_window != B200BSP_MI_PVI8 && o.mi_window != B200BSP_MI_PARZEN) {
+        return fail (nullptr, B200BSP_E_BADARG, "unknown mi_window %d",
+            o.mi_window);
+    }
+    if (o.mi_window == B200BSP_MI_PARZEN && o.mi_bins < 5) {
+        return fail (nullptr, B200BSP_E_BADARG,
+            "Parzen-window MI needs at least 5 bins");
+    }
     if (o.mi_bins < 2 || o.mi_bins > MI_MAX_BINS) {
         return fail (nullptr, B200BSP_E_BADARG, "mi_bins must be in [2, %d]",
             MI_MAX_BINS);
@@ -503,7 +511,7 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
         if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
     }
-    if (!rc2 && mi_alloc (&c->mi, c->geom, o.mi_bins)) {
+    if (!rc2 && mi_alloc (&c->mi, c->geom, o.mi_bins, o.mi_window)) {
         rc2 = fail (c, B200BSP_E_OOM, "MI buffers: out of device memory");
     }
     if (!rc2) {
@@ -801,11 +809,12 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     double* j_hist)
 {
     if (!c) return B200BSP_E_BADARG;
-    for (int d = 0; d < 3; d++) {
+    for (int d = 0; d < 3 && c->opts.mi_window == B200BSP_MI_PVI8; d++) {
         if (c->geom.roi_off[d] != 0 || c->geom.roi_dim[d] != c->geom.fdim[d]) {
             // The reference's histogram pass scans the whole fixed image
             // while its gradient pass scans the ROI; the two agree only
-            // when the ROI is the whole image.
+            // when the ROI is the whole image.  (The Parzen variant scans
+            // the ROI in both passes.)
             return fail (c, B200BSP_E_UNSUPPORTED,
                 "MI needs the ROI to cover the whole fixed image");
         }
@@ -818,10 +827,11 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
         && tc_mi_supported (c->geom, c->plan, c->mi.bins)) {
         rc = mi_run_tc (&c->mi, c->geom, c->plan, c->lay, c->d_qlut,
             c->d_part, c->d_score_part, c->d_count_part, c->d_err, dcoeff,
-            c->d_res, g_dev, nullptr, c->stream, &c->last_launches);
+            c->d_moving, c->d_res, g_dev, nullptr, c->stream,
+            &c->last_launches);
     } else {
-        rc = mi_run (&c->mi, c->geom, dcoeff, c->d_luts, c->d_res, g_dev,
-            nullptr, c->stream, &c->last_launches);
+        rc = mi_run (&c->mi, c->geom, dcoeff, c->d_moving, c->d_luts,
+            c->d_res, g_dev, nullptr, c->stream, &c->last_launches);
     }
     if (rc) return fail (c, rc, "MI evaluation failed: %s",
         cudaGetErrorString (cudaGetLastError ()));
