@@ -318,8 +318,10 @@ void b200bsp_lbfgs_default_parms (b200bsp_lbfgs_parms* parms);
  * or device) holds x0 on entry; on return it holds what Plastimatch's
  * transform holds after its optimiser: the last evaluated coefficients
  * (a stop inside a line search leaves the last trial point there), and
- * res->score the last evaluated total score.  Allocates the optimiser's
- * device vectors ((2m + 5) doubles per coefficient) for the call. */
+ * res->score the last evaluated total score.  The first run on a context
+ * allocates the optimiser's device vectors ((2m + 5) doubles and 2 floats
+ * per coefficient); the context keeps them for later runs with the same m
+ * and frees them with itself. */
 int b200bsp_optimize_lbfgs (b200bsp_ctx* ctx, int metric_type, float lambda,
     const b200bsp_reg_parms* reg, const b200bsp_lbfgs_parms* parms,
     float* coeff, b200bsp_lbfgs_result* res);

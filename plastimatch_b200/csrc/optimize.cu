@@ -30,6 +30,8 @@ namespace b200 {
 
 int static_fail (int code, const char* msg);   // runtime.cu
 cudaStream_t ctx_stream (const b200bsp_ctx* c); // runtime.cu
+void* ctx_opt_ws (const b200bsp_ctx* c);
+void ctx_set_opt_ws (b200bsp_ctx* c, void* ws, void (*release) (void*));
 
 constexpr int OPT_THREADS = 256;
 constexpr int OPT_BLOCKS = 296;
@@ -60,6 +62,55 @@ dot_final_kernel (const double* __restrict__ part, int n, double* out)
         double s = 0.0;
         for (int i = 0; i < n; i++) s += part[i];
         *out = s;
+    }
+}
+
+// *out = sum of part (dot_final_kernel's order), divided by *den if given
+__global__ void
+dot_final_div_kernel (const double* __restrict__ part, int n,
+    const double* __restrict__ den, double* out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++) s += part[i];
+        *out = den ? s / *den : s;
+    }
+}
+
+// y = (sign * *a) * x + b * y, the coefficient read on the device
+__global__ void
+axpby_dev_kernel (const double* __restrict__ a, double sign,
+    const double* __restrict__ x, double b, double* __restrict__ y,
+    long long n)
+{
+    const double av = sign * *a;
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        y[i] = av * x[i] + b * y[i];
+    }
+}
+
+// y = (*a - *c) * x + 1 * y
+__global__ void
+axpy_diff_kernel (const double* __restrict__ a, const double* __restrict__ c,
+    const double* __restrict__ x, double* __restrict__ y, long long n)
+{
+    const double av = *a - *c;
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        y[i] = av * x[i] + 1.0 * y[i];
+    }
+}
+
+// y = 0 * y + (*num / *den) * y
+__global__ void
+scale_ratio_kernel (const double* __restrict__ num,
+    const double* __restrict__ den, double* __restrict__ y, long long n)
+{
+    const double bv = *num / *den;
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        y[i] = 0.0 * y[i] + bv * y[i];
     }
 }
 
@@ -131,6 +182,8 @@ struct Lbfgs {
     double *x = nullptr, *g = nullptr, *d = nullptr, *xp = nullptr,
         *gp = nullptr, *s = nullptr, *y = nullptr, *part = nullptr,
         *scalar = nullptr;
+    // device scalars of the two-loop recursion: ys[m], alpha[m], beta, yy
+    double* dsc = nullptr;
     double* h_scalar = nullptr;
     cudaStream_t st = nullptr;
     int err = 0;
@@ -147,8 +200,8 @@ struct Lbfgs {
         };
         a (&x, n); a (&g, n); a (&d, n); a (&xp, n); a (&gp, n);
         a (&s, (size_t) m * n); a (&y, (size_t) m * n);
-        a (&part, OPT_BLOCKS); a (&scalar, 1);
-        if (!err && cudaMallocHost (&h_scalar, sizeof (double)) != cudaSuccess) {
+        a (&part, OPT_BLOCKS); a (&scalar, 2); a (&dsc, 2 * (size_t) m + 2);
+        if (!err && cudaMallocHost (&h_scalar, 2 * sizeof (double)) != cudaSuccess) {
             cudaGetLastError ();
             err = B200BSP_E_OOM;
         }
@@ -158,11 +211,36 @@ struct Lbfgs {
     {
         cudaFree (x); cudaFree (g); cudaFree (d); cudaFree (xp); cudaFree (gp);
         cudaFree (s); cudaFree (y); cudaFree (part); cudaFree (scalar);
+        cudaFree (dsc);
         cudaFreeHost (h_scalar);
     }
     unsigned grid () const
     {
         return (unsigned) std::min<long long> ((n + 255) / 256, 148 * 8);
+    }
+    // dot product into a device scalar (*den divides it when given); no
+    // synchronisation
+    void dot_dev (const double* a, const double* b, double* out,
+        const double* den = nullptr)
+    {
+        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (a, b, n, part);
+        dot_final_div_kernel<<<1, 32, 0, st>>> (part, OPT_BLOCKS, den, out);
+    }
+    // |a|^2 and |b|^2 with one synchronisation
+    void norms2 (const double* a, const double* b, double* na, double* nb)
+    {
+        dot_dev (a, a, scalar);
+        dot_dev (b, b, scalar + 1);
+        if (cudaMemcpyAsync (h_scalar, scalar, 2 * sizeof (double),
+                cudaMemcpyDeviceToHost, st) != cudaSuccess
+            || cudaStreamSynchronize (st) != cudaSuccess) {
+            cudaGetLastError ();
+            err = B200BSP_E_CUDA;
+            *na = *nb = 0.0;
+            return;
+        }
+        *na = h_scalar[0];
+        *nb = h_scalar[1];
     }
     double dot (const double* a, const double* b)
     {
@@ -407,14 +485,15 @@ lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
     b200bsp_lbfgs_result* res)
 {
     const int m = p.m;
-    std::vector<double> alpha (m), ys_hist (m);
     double f = 0.0;
     int rc = obj.eval (w.x, w.g, &f);
     if (rc) return rc;
     res->score = f;
     res->iterations = 0;
-    double xnorm = std::sqrt (w.dot (w.x, w.x));
-    double gnorm = std::sqrt (w.dot (w.g, w.g));
+    double xnorm, gnorm;
+    w.norms2 (w.x, w.g, &xnorm, &gnorm);
+    xnorm = std::sqrt (xnorm);
+    gnorm = std::sqrt (gnorm);
     if (w.err) return w.err;
     if (xnorm < 1.0) xnorm = 1.0;
     if (gnorm / xnorm <= p.epsilon) {
@@ -440,8 +519,9 @@ lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
         }
         res->score = f;
         res->iterations = k;
-        xnorm = std::sqrt (w.dot (w.x, w.x));
-        gnorm = std::sqrt (w.dot (w.g, w.g));
+        w.norms2 (w.x, w.g, &xnorm, &gnorm);
+        xnorm = std::sqrt (xnorm);
+        gnorm = std::sqrt (gnorm);
         if (w.err) return w.err;
         if (stop_rule (p, k, obj.fevals)) {
             res->status = B200BSP_LBFGS_STOPPED;
@@ -452,30 +532,38 @@ lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
             res->status = B200BSP_LBFGS_CONVERGED;
             return B200BSP_OK;
         }
-        // new correction pair
+        // new correction pair; the two-loop recursion runs on the device
+        // with its scalars in device memory (no synchronisation until the
+        // next line search)
+        double* ys_d = w.dsc;                 // [m]
+        double* alpha_d = w.dsc + m;          // [m]
+        double* beta_d = w.dsc + 2 * m;
+        double* yy_d = w.dsc + 2 * m + 1;
         sub_kernel<<<w.grid (), 256, 0, w.st>>> (w.x, w.xp, w.sv (end), w.n);
         sub_kernel<<<w.grid (), 256, 0, w.st>>> (w.g, w.gp, w.yv (end), w.n);
-        const double ys = w.dot (w.yv (end), w.sv (end));
-        const double yy = w.dot (w.yv (end), w.yv (end));
-        if (w.err) return w.err;
-        ys_hist[end] = ys;
+        w.dot_dev (w.yv (end), w.sv (end), ys_d + end);
+        w.dot_dev (w.yv (end), w.yv (end), yy_d);
+        const int newest = end;
         const int bound = std::min (m, k);
         ++k;
         end = (end + 1) % m;
-        // two-loop recursion
         w.axpby (-1.0, w.g, 0.0, w.d);
         int j = end;
         for (int i = 0; i < bound; i++) {
             j = (j + m - 1) % m;
-            alpha[j] = w.dot (w.sv (j), w.d) / ys_hist[j];
-            w.axpby (-alpha[j], w.yv (j), 1.0, w.d);
+            w.dot_dev (w.sv (j), w.d, alpha_d + j, ys_d + j);
+            axpby_dev_kernel<<<w.grid (), 256, 0, w.st>>> (alpha_d + j, -1.0,
+                w.yv (j), 1.0, w.d, w.n);
         }
-        w.axpby (0.0, w.d, ys / yy, w.d);
+        scale_ratio_kernel<<<w.grid (), 256, 0, w.st>>> (ys_d + newest, yy_d,
+            w.d, w.n);
         for (int i = 0; i < bound; i++) {
-            const double beta = w.dot (w.yv (j), w.d) / ys_hist[j];
-            w.axpby (alpha[j] - beta, w.sv (j), 1.0, w.d);
+            w.dot_dev (w.yv (j), w.d, beta_d, ys_d + j);
+            axpy_diff_kernel<<<w.grid (), 256, 0, w.st>>> (alpha_d + j, beta_d,
+                w.sv (j), w.d, w.n);
             j = (j + 1) % m;
         }
+        if (cudaGetLastError () != cudaSuccess) return B200BSP_E_CUDA;
         if (w.err) return w.err;
         step = 1.0;
     }
@@ -598,6 +686,38 @@ f2d_kernel (const float* __restrict__ a, double* __restrict__ out, long long n)
     }
 }
 
+// A context's optimiser workspace: the L-BFGS vectors and the float
+// coefficient / gradient buffers, allocated on the first run and kept by
+// the context (reallocated only when the history length changes), so a
+// registration allocates nothing after its first run.
+struct OptWorkspace {
+    Lbfgs w;
+    float* buf = nullptr;
+    ~OptWorkspace () { cudaFree (buf); }
+};
+
+static void
+release_ws (void* p)
+{
+    delete (OptWorkspace*) p;
+}
+
+static OptWorkspace*
+context_workspace (b200bsp_ctx* ctx, int64_t nc, int m)
+{
+    auto* ws = (OptWorkspace*) ctx_opt_ws (ctx);
+    if (ws && ws->w.n == nc && ws->w.m == m) return ws;
+    ws = new OptWorkspace ();
+    if (ws->w.alloc (nc, m)
+        || cudaMalloc (&ws->buf, 2 * nc * sizeof (float)) != cudaSuccess) {
+        cudaGetLastError ();
+        delete ws;
+        return nullptr;
+    }
+    ctx_set_opt_ws (ctx, ws, release_ws);
+    return ws;
+}
+
 // L-BFGS over a context's coefficients (host or device floats, updated in
 // place with the last evaluated point), evaluations by `obj`.
 static int
@@ -606,13 +726,11 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
     ContextObjective& obj)
 {
     int rc = B200BSP_OK;
-    Lbfgs w;
-    if (w.alloc (nc, p.m)) return static_fail (B200BSP_E_OOM, "optimiser buffers");
-    float* buf = nullptr;
-    if (cudaMalloc (&buf, 2 * nc * sizeof (float)) != cudaSuccess) {
-        cudaGetLastError ();
-        return static_fail (B200BSP_E_OOM, "optimiser buffers");
-    }
+    OptWorkspace* ws = context_workspace (ctx, nc, p.m);
+    if (!ws) return static_fail (B200BSP_E_OOM, "optimiser buffers");
+    Lbfgs& w = ws->w;
+    w.err = 0;
+    float* buf = ws->buf;
     obj.coeff_f = buf; obj.grad_f = buf + nc; obj.n = nc;
     // the context's stream orders every kernel of the run
     cudaStream_t st = ctx_stream (ctx);
@@ -623,7 +741,6 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
             dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st)
         != cudaSuccess) {
         cudaGetLastError ();
-        cudaFree (buf);
         return static_fail (B200BSP_E_CUDA, "coefficient upload");
     }
     f2d_kernel<<<w.grid (), 256, 0, st>>> (buf, w.x, nc);
@@ -645,7 +762,6 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
             rc = static_fail (B200BSP_E_CUDA, "coefficient download");
         }
     }
-    cudaFree (buf);
     return rc;
 }
 

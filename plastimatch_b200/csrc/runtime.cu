@@ -61,6 +61,9 @@ struct b200bsp_ctx {
     PartLayout lay;
     TcPlan plan;
     int tc_grid = 0;          // CTAs of the tile kernel; 0: plan.grid
+    // the optimiser's device workspace, kept between runs (optimize.cu)
+    void* opt_ws = nullptr;
+    void (*opt_ws_free) (void*) = nullptr;
     int nscore_parts = 0;
     bool images_set = false;
 
@@ -218,6 +221,8 @@ free_all (b200bsp_ctx* c)
     cudaFreeHost (c->h_res); cudaFreeHost (c->h_scalar);
     mi_free (&c->mi);
     reg_free (&c->reg);
+    if (c->opt_ws_free) c->opt_ws_free (c->opt_ws);
+    c->opt_ws = nullptr;
     for (auto& e : c->ev) if (e) cudaEventDestroy (e);
     if (c->own_stream) cudaStreamDestroy (c->own_stream);
 }
@@ -300,6 +305,23 @@ int
 ctx_device (const b200bsp_ctx* c)
 {
     return c->device;
+}
+
+// The optimiser's workspace slot: kept by the context, freed with it.
+void*
+ctx_opt_ws (const b200bsp_ctx* c)
+{
+    return c->opt_ws;
+}
+
+void
+ctx_set_opt_ws (b200bsp_ctx* c, void* ws, void (*release) (void*))
+{
+    if (c->opt_ws_free && c->opt_ws && c->opt_ws != ws) {
+        c->opt_ws_free (c->opt_ws);
+    }
+    c->opt_ws = ws;
+    c->opt_ws_free = release;
 }
 
 // Work of one evaluation's tile pass (voxels of the ROI's tiles) and
