@@ -283,6 +283,7 @@ def batched_c5(P, n_regs=16, its=40):
                 for f, m, gr in cases]
         try:
             x = [np.zeros(gr.num_coeff, np.float32) for _, _, gr in cases]
+            tiles = [c.autotune(xi, evals=2) for c, xi in zip(ctxs, x)]
             if batched:
                 with P.Batch(ctxs) as b:
                     b.optimize_lbfgs([xi.copy() for xi in x], max_its=2,
@@ -302,6 +303,7 @@ def batched_c5(P, n_regs=16, its=40):
                 c.close()
         fe = [r["fevals"] for r in res]
         return {"wall_s": dt, "fevals": int(sum(fe)),
+                "autotuned_tiles_per_batch": tiles,
                 "gvox_per_s": float(sum(f * n for f, n in zip(fe, nvox))
                                     / dt / 1e9),
                 "final_scores": [round(float(r["score"]), 4) for r in res]}

@@ -189,6 +189,16 @@ int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
     float* total_grad, float* smetric, int64_t* num_vox);
 
+/* Autotuner (no reference counterpart): times `evals` MSE evaluations at
+ * `coeff` for each way the tensor-core kernel may split a row of tiles
+ * into batches (the fewest batches of at most 26 tiles, and up to two
+ * more) and keeps the fastest for the context's later calls; *tiles
+ * receives its tiles per batch (1 for the FP32 form, which has nothing to
+ * tune).  Results stay within the parity bars whatever the split, and are
+ * deterministic for a given split. */
+int b200bsp_autotune (b200bsp_ctx* ctx, const float* coeff, int evals,
+    int* tiles);
+
 /* Dense displacement field over the ROI (bspline_interpolate_vf,
  * src/base/bspline_interpolate.cxx:112-142): vf is dim[0]*dim[1]*dim[2]*3
  * floats of the fixed image, xyz interleaved; voxels outside the ROI are

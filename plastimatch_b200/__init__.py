@@ -165,6 +165,7 @@ _SIGS = {
                                          C.c_int]),
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_autotune": (C.c_int, [_VP, _VP, C.c_int, _VP]),
     "b200bsp_batch_create": (C.c_int, [_VP, C.c_int, _VP]),
     "b200bsp_batch_destroy": (None, [_VP]),
     "b200bsp_batch_last_error": (C.c_char_p, [_VP]),
@@ -422,6 +423,14 @@ class Context:
         _check(lib().b200bsp_score_mse(self._h, _ptr(coeff), C.addressof(s),
                                        _ptr(g), C.addressof(n)), self._h)
         return s.value, g, n.value
+
+    def autotune(self, coeff, evals=3) -> int:
+        """b200bsp_autotune: pick the tensor-core kernel's batch split by
+        timing; returns its tiles per batch."""
+        t = C.c_int()
+        _check(lib().b200bsp_autotune(self._h, _ptr(coeff), evals,
+                                      C.byref(t)), self._h)
+        return t.value
 
     def score_mse_f64(self, coeff):
         g = np.zeros(self.num_coeff, np.float64)

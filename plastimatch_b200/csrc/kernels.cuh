@@ -44,7 +44,11 @@ struct TcPlan {
     int threads;
     int grid;
 };
-bool tc_plan (const BspGeom& g, TcPlan* plan, int ctas_per_sm, int sm_count);
+// extra_row_batches: split each row of tiles into that many more batches
+// than the fewest (the autotuner's knob); false when unsupported.
+bool tc_plan (const BspGeom& g, TcPlan* plan, int ctas_per_sm, int sm_count,
+    int extra_row_batches = 0);
+constexpr int TC_TUNE_MAX_EXTRA = 2;      // autotuner candidates: 0 .. this
 int tc_build_tables (const BspGeom& g, const TcPlan& plan, void** d_qlut);
 cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
     int grad_mode, const float* fimg, const float* mimg, const float* mgrad,

@@ -1365,12 +1365,19 @@ mse_tc_kernel (TcArgs a)
 }
 
 bool
-tc_plan (const BspGeom& g, TcPlan* p, int ctas_per_sm, int sm_count)
+tc_plan (const BspGeom& g, TcPlan* p, int ctas_per_sm, int sm_count,
+    int extra_row_batches)
 {
     int V = g.vpr[0] * g.vpr[1] * g.vpr[2];
     int mblk = (V + 127) / 128;
     if (mblk > TC_MAX_MBLK) return false;
-    int nb_row = (g.rdims[0] + TC_TMAX - 1) / TC_TMAX;
+    // batches per row of tiles: the fewest that keep T <= TC_TMAX, plus the
+    // autotuner's extra; a row split into several batches needs T >= 3
+    // (the finish kernel's gather assumes a knot meets at most two)
+    int nb_row = (g.rdims[0] + TC_TMAX - 1) / TC_TMAX + extra_row_batches;
+    if (nb_row > g.rdims[0] || (nb_row > 1 && (g.rdims[0] + nb_row - 1) / nb_row < 3)) {
+        return false;
+    }
     int T = (g.rdims[0] + nb_row - 1) / nb_row;      // balanced batches
     p->bx = T;
     p->mblk = mblk;

@@ -128,6 +128,23 @@ mapped_alias (void* p)
     return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
+// Make `p` the context's tensor-core plan: the partial-gradient layout of
+// its batches and the number of score parts follow it.
+static void
+use_tc_plan (b200bsp_ctx* c, const TcPlan& p)
+{
+    const BspGeom& g = c->geom;
+    c->plan = p;
+    PartLayout& L = c->lay;
+    L.bx = p.bx; L.by = 1; L.bz = 1;
+    L.nbx = (g.rdims[0] + L.bx - 1) / L.bx;
+    L.nby = g.rdims[1];
+    L.nbz = g.rdims[2];
+    L.kx = L.bx + 3; L.ky = 4; L.kz = 4;
+    L.slots = 1;
+    c->nscore_parts = p.nbatches;
+}
+
 // Cofactor inverse in float (Plastimatch src/base/direction_cosines.cxx:
 // 135-158); the caller rejects |det| < 1e-8 as the reference does.
 static bool
@@ -498,21 +515,22 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     int sm_count = 148;
     cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount, o.device);
     size_t part_elems = 0;
+    size_t score_parts = 0;
     if (!rc2 && o.form == B200BSP_FORM_TC) {
         if (!tc_plan (g, &c->plan, 2, sm_count)) {
             rc2 = fail (c, B200BSP_E_UNSUPPORTED,
                 "tensor-core form: grid with vox_per_rgn (%d,%d,%d) not "
                 "supported; use B200BSP_FORM_FP32", g.vpr[0], g.vpr[1], g.vpr[2]);
         } else {
-            PartLayout& L = c->lay;
-            L.bx = c->plan.bx; L.by = 1; L.bz = 1;
-            L.nbx = (g.rdims[0] + L.bx - 1) / L.bx;
-            L.nby = g.rdims[1];
-            L.nbz = g.rdims[2];
-            L.kx = L.bx + 3; L.ky = 4; L.kz = 4;
-            L.slots = 1;
-            part_elems = (size_t) c->plan.nbatches * L.kx * L.ky * L.kz * 3;
-            c->nscore_parts = c->plan.nbatches;
+            // buffers for every batch split the autotuner may choose
+            for (int e = 0; e <= TC_TUNE_MAX_EXTRA; e++) {
+                TcPlan p;
+                if (!tc_plan (g, &p, 2, sm_count, e)) continue;
+                part_elems = std::max (part_elems,
+                    (size_t) p.nbatches * (p.bx + 3) * 16 * 3);
+                score_parts = std::max (score_parts, (size_t) p.nbatches);
+            }
+            use_tc_plan (c, c->plan);
         }
     } else if (!rc2) {
         if (mse_fp32_smem_bytes (g) > 200 * 1024) {
@@ -527,8 +545,9 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         c->nscore_parts = g.ntiles;
     }
     alloc ((void**) &c->d_part, part_elems * sizeof (float));
-    alloc ((void**) &c->d_score_part, (size_t) std::max (c->nscore_parts, 1) * sizeof (double));
-    alloc ((void**) &c->d_count_part, (size_t) std::max (c->nscore_parts, 1) * sizeof (int));
+    score_parts = std::max (score_parts, (size_t) std::max (c->nscore_parts, 1));
+    alloc ((void**) &c->d_score_part, score_parts * sizeof (double));
+    alloc ((void**) &c->d_count_part, score_parts * sizeof (int));
     if (!rc2 && o.form == B200BSP_FORM_TC) {
         rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
         if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
@@ -823,6 +842,60 @@ b200bsp_score_mse_f64 (b200bsp_ctx* c, const float* coeff, double* score,
     if (score) *score = c->h_res->score;
     if (num_vox) *num_vox = c->h_res->num_vox;
     return check_device_error (c, c->h_res->error);
+}
+
+extern "C" int
+b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (evals < 1) return fail (c, B200BSP_E_BADARG, "evals must be >= 1");
+    if (c->opts.form != B200BSP_FORM_TC) {
+        if (tiles) *tiles = 1;
+        return B200BSP_OK;
+    }
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    int sm_count = 148;
+    cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount,
+        c->device);
+    cudaEvent_t e0, e1;
+    CK (cudaEventCreate (&e0));
+    CK (cudaEventCreate (&e1));
+    const TcPlan start = c->plan;
+    TcPlan best = start;
+    float best_ms = 0.f;
+    for (int e = 0; e <= TC_TUNE_MAX_EXTRA && !rc; e++) {
+        TcPlan p;
+        if (!tc_plan (c->geom, &p, 2, sm_count, e)) continue;
+        use_tc_plan (c, p);
+        rc = run_mse (c, dcoeff, c->d_grad, nullptr, nullptr, nullptr,
+            nullptr);                                    // warm-up
+        if (!rc && cudaEventRecord (e0, c->stream) != cudaSuccess) rc = B200BSP_E_CUDA;
+        for (int i = 0; i < evals && !rc; i++) {
+            rc = run_mse (c, dcoeff, c->d_grad, nullptr, nullptr, nullptr,
+                nullptr);
+        }
+        float ms = 0.f;
+        if (!rc && (cudaEventRecord (e1, c->stream) != cudaSuccess
+                || cudaEventSynchronize (e1) != cudaSuccess
+                || cudaEventElapsedTime (&ms, e0, e1) != cudaSuccess)) {
+            rc = B200BSP_E_CUDA;
+        }
+        if (!rc && (best_ms == 0.f || ms < best_ms)) {
+            best_ms = ms;
+            best = p;
+        }
+    }
+    cudaEventDestroy (e0);
+    cudaEventDestroy (e1);
+    use_tc_plan (c, rc ? start : best);
+    if (rc) {
+        cudaGetLastError ();
+        return fail (c, rc, "autotuning failed");
+    }
+    if (tiles) *tiles = best.bx;
+    return check_device_error (c);
 }
 
 extern "C" int

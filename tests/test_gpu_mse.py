@@ -160,3 +160,29 @@ def test_mse_page_locked_host_outputs(form):
                 s64, g64, n64 = ctx.score_mse_f64(coeff)
                 assert sc.value == s64
                 np.testing.assert_array_equal(hg.numpy(), g64)
+
+
+@pytest.mark.parametrize("shape,vpr", [((96, 80, 48), (5, 5, 5)),
+                                       ((200, 64, 40), (4, 4, 4))])
+def test_autotune_keeps_parity(shape, vpr):
+    """The autotuner's batch split changes only how tiles are grouped: the
+    results stay within the bars, repeat exactly, and the chosen split is
+    one the kernel supports (at least 3 tiles per batch)."""
+    fixed = synth.gaussian_blobs(shape, spacing=(1.0, 1.0, 2.0), seed=41)
+    g0 = BsplineGrid.for_volume(fixed, 8)
+    moving = synth.warp_trilinear(fixed, fixed, g0,
+                                  synth.random_coeff(g0, 1.5, 42))
+    grid = BsplineGrid.for_volume(fixed, vpr)
+    coeff = synth.random_coeff(grid, 1.0, 43)
+    with P.Context(fixed, moving, grid, form="tc") as ctx:
+        ctx.set_images()
+        t = ctx.autotune(coeff, evals=2)
+        s, g, n = ctx.score_mse(coeff)
+        s2, g2, n2 = ctx.score_mse(coeff)
+    assert 3 <= t <= 26
+    mg = O.port_volume_grad(moving)
+    f64 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg, precision="f64")
+    r32 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg)
+    check(s, g, n, f64, r32.grad, r32.num_vox)
+    assert s == s2 and n == n2
+    np.testing.assert_array_equal(g, g2)
