@@ -126,6 +126,35 @@ locate_fast (const BspGeom& g, const float fxyz[3], const float dxyz[3],
     return in;
 }
 
+// locate_fast with the clamp flags: bit d set where li_clamp holds the
+// position at an end of axis d (ma < 0 or ma >= dim - 1).
+__device__ __forceinline__ bool
+locate_fast_c (const BspGeom& g, const float fxyz[3], const float dxyz[3],
+    int& mvf, int& mvr, float w2[3], int& clamp)
+{
+    float t0 = (fxyz[0] + dxyz[0]) - g.morigin[0];
+    float t1 = (fxyz[1] + dxyz[1]) - g.morigin[1];
+    float t2 = (fxyz[2] + dxyz[2]) - g.morigin[2];
+    bool in = true;
+    int f[3], r[3];
+    clamp = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        float ma = t0 * g.mproj[3*d+0] + t1 * g.mproj[3*d+1]
+            + t2 * g.mproj[3*d+2];
+        in = in && (ma > -0.5f) && (ma < g.m_hi[d]);
+        if (ma < 0.f || ma >= g.m_fmax[d] + 1.f) clamp |= 1 << d;
+        float fc = fminf (fmaxf (floorf (ma), 0.f), g.m_fmax[d]);
+        float w = __saturatef (ma - fc);
+        w2[d] = w;
+        f[d] = (int) fc;
+        r[d] = f[d] + (w >= 0.5f ? 1 : 0);
+    }
+    mvf = f[0] + g.mdim[0] * (f[1] + g.mdim[1] * f[2]);
+    mvr = r[0] + g.mdim[0] * (r[1] + g.mdim[1] * r[2]);
+    return in;
+}
+
 // Conversion-free variants for the hot loops: the XU pipe (int <-> float,
 // floor, float -> bf16) is narrow, so the per-sample path uses integer and
 // FMA-pipe arithmetic instead.  The magic constant 2^23 = 8388608 puts an

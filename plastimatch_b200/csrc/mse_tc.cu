@@ -365,13 +365,158 @@ voxel_slot (const TcArgs& a, const TcCtx& x, int mb)
     return s;
 }
 
+// Mattes MI pass 1 at one sample: the PVI-8 corner weights (products of
+// the per-axis fractions, in the reference's order) as integers in 2^-24
+// units, so the sums do not depend on their order.  Corners with equal
+// moving bins are merged first; a sample then has one, two or (rarely)
+// more (fixed, moving) bin pairs.  The first two pairs of every lane
+// combine across the warp (match + reduce, one round each) so that one lane
+// per distinct pair updates the shared joint histogram; further pairs go
+// straight to the shared atomics.  The fixed histogram counts each first-
+// pair group's voxels; the moving histogram is the joint one's column sums,
+// taken when the CTA flushes.  Every lane of the warp calls this (warp
+// collectives).
+__device__ __forceinline__ void
+mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
+    int fb, const int mb[8], int& cnt)
+{
+    const int B = a.bins;
+    unsigned long long* hf = (unsigned long long*) (x.sm + SM_DC);
+    unsigned long long* hj = hf + 2 * B;
+    const float* l2 = w2;
+    const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
+    const float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
+        l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
+        l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
+    unsigned int q[8];
+    bool first[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        q[k] = __float2uint_rn (w[k] * TC_MI_WUNIT);
+        first[k] = live;
+    }
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+#pragma unroll
+        for (int k2 = 0; k2 < k; k2++) {
+            if (first[k] && first[k2] && mb[k2] == mb[k]) {
+                q[k2] += q[k];
+                first[k] = false;
+            }
+        }
+    }
+    // second pair: the first remaining corner after corner 0
+    bool two = false, many = false;
+    int mb2 = 0;
+    unsigned int q2 = 0;
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+        many = many || (first[k] && two);
+        mb2 = (first[k] && !two) ? mb[k] : mb2;
+        q2 = (first[k] && !two) ? q[k] : q2;
+        two = two || first[k];
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        cnt++;
+        // first pair (a warp's sum stays below 32 * (2^24 + 8) < 2^32); its
+        // leader also counts the group's voxels into the fixed histogram
+        const int key = fb * B + mb[0];
+        const unsigned peers = __match_any_sync (live_mask, key);
+        const unsigned sum = __reduce_add_sync (peers, q[0]);
+        if (x.lane == __ffs (peers) - 1) {
+            atomicAdd (&hj[key], (unsigned long long) sum);
+            atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
+        }
+    }
+    const unsigned two_mask = __ballot_sync (0xffffffffu, two);
+    if (two) {
+        const int key = fb * B + mb2;
+        const unsigned peers = __match_any_sync (two_mask, key);
+        const unsigned sum = __reduce_add_sync (peers, q2);
+        if (x.lane == __ffs (peers) - 1) {
+            atomicAdd (&hj[key], (unsigned long long) sum);
+        }
+    }
+    if (many) {
+        bool seen = false;
+#pragma unroll
+        for (int k = 1; k < 8; k++) {
+            if (first[k] && seen) {
+                atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
+            }
+            seen = seen || first[k];
+        }
+    }
+}
+
+// Mattes MI with cubic B-spline Parzen windows, pass 1 at one sample: the
+// window's four weights at the moving value u (integers in 2^-24 units)
+// into the fixed bin's row of the shared joint histogram; lanes with the
+// same (fixed bin, first window bin) combine across the warp first.  Every
+// lane of the warp calls this.
+__device__ __forceinline__ void
+pz_hist_add (const TcArgs& a, const TcCtx& x, bool live, int fb, float u,
+    int& cnt)
+{
+    const int B = a.bins;
+    unsigned long long* hj = (unsigned long long*) (x.sm + SM_DC) + 2 * B;
+    const int k0 = parzen_first_bin (u, B);
+    unsigned int q[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        q[j] = __float2uint_rn (bspline3f ((float) (k0 + j) - u) * TC_MI_WUNIT);
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        cnt++;
+        const int key = fb * B + k0;
+        const unsigned peers = __match_any_sync (live_mask, key);
+        unsigned sum[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) sum[j] = __reduce_add_sync (peers, q[j]);
+        if (x.lane == __ffs (peers) - 1) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (sum[j]) atomicAdd (&hj[key + j], (unsigned long long) sum[j]);
+            }
+        }
+    }
+}
+
+// Pass 2 at one sample: 1/(N delta_m) * sum over the window's bins of
+// beta3'(k - u) log(p(f, k) / p_m(k)), times the world gradient of the
+// trilinear interpolant (proj^T times the index gradient; 0 along an axis
+// the clamp holds).
+__device__ __forceinline__ void
+pz_dc_dv (const TcArgs& a, float u, int fb, const float w2[3],
+    const float m[8], int clamp, float dc[3])
+{
+    const int B = a.bins;
+    const int k0 = parzen_first_bin (u, B);
+    const float* row = a.mi_lut + fb * B;
+    float sum = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        sum += bspline3f_d ((float) (k0 + j) - u) * __ldg (row + k0 + j);
+    }
+    float gi[3];
+    trilinear_igrad (w2, m, clamp, gi);
+    const float sc = __ldg (a.mi_nvf + 1) * sum;
+    const float* p = a.g.mproj;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        dc[c] = sc * (p[c] * gi[0] + p[3 + c] * gi[1] + p[6 + c] * gi[2]);
+    }
+}
+
 // Voxel phase for one M block: thread (quarter q, lane) owns one voxel of
 // every tile in [t_lo, t_hi).  Tiles go four at a time: the field values
 // come from TMEM, then all four correspondences, then all gathers (8
 // corners, fixed value, moving gradient), then the arithmetic.  Sample
 // indices are clamped inside the moving image even when the sample is
 // rejected, so only the fixed-image load needs a guard.
-template <int GRAD_MODE>
+template <int MODE>
 __device__ __forceinline__ void
 voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
     int ty, int tz, double& sc, int& cnt)
@@ -403,7 +548,7 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
         tmem_ld4x3_wait (lb + x.t_lo + t4, lb + T + x.t_lo + t4,
             lb + 2 * T + x.t_lo + t4, dv);
         bool ok[4];
-        int mvf[4], mvr[4];
+        int mvf[4], mvr[4], clampb[4];
         float w2[4][3];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
@@ -412,8 +557,65 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
             float fxyz[3] = {fmaf (ft, xstep[0], pj[0]), fmaf (ft, xstep[1], pj[1]),
                 fmaf (ft, xstep[2], pj[2])};
             float d[3] = {dv[u], dv[4 + u], dv[8 + u]};
-            bool in = locate_fast (g, fxyz, d, mvf[u], mvr[u], w2[u]);
+            bool in = locate_fast_c (g, fxyz, d, mvf[u], mvr[u], w2[u],
+                clampb[u]);
             ok[u] = in && yz_ok && tt < t_cnt && g.vpr[0] * tt < fi_room;
+        }
+        if constexpr (MODE >= TC_MI_GRAD) {
+            // Mattes MI: the fixed voxel's bin (guarded: a dead slot may lie
+            // past the image) and the corners' bins (PVI-8) or values
+            // (Parzen), then the histogram or the dc/dv of each sample
+            constexpr bool pz = MODE == TC_PZ_GRAD || MODE == TC_PZ_HIST;
+            int fb[4];
+            float crm[4][8];
+            int mb[4][8];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                fb[u] = ok[u] ? (int) __ldg (a.fbin + frow + g.vpr[0] * (t4 + u)) : 0;
+                const int o[8] = {0, 1, dxm, dxm + 1, dxym, dxym + 1,
+                    dxym + dxm, dxym + dxm + 1};
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    if (pz) crm[u][k] = __ldg (a.mimg + mvf[u] + o[k]);
+                    else mb[u][k] = __ldg (a.mbin + mvf[u] + o[k]);
+                }
+            }
+            const float nv = MODE == TC_MI_GRAD ? __ldg (a.mi_nvf) : 0.f;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int t = x.t_lo + t4 + u;
+                float dc[3] = {0.f, 0.f, 0.f};
+                if constexpr (MODE == TC_MI_HIST) {
+                    mi_hist_add (a, x, ok[u], w2[u], fb[u], mb[u], cnt);
+                } else if constexpr (MODE == TC_PZ_HIST) {
+                    pz_hist_add (a, x, ok[u], fb[u],
+                        parzen_centre (trilinear_lerp (w2[u], crm[u]),
+                            a.pz_mmin, a.pz_mdelta), cnt);
+                } else if (ok[u]) {
+                    if constexpr (MODE == TC_MI_GRAD) {
+                        mi_dc_dv (a, w2[u], fb[u], mb[u], nv, dc);
+                    } else {
+                        pz_dc_dv (a, parzen_centre (trilinear_lerp (w2[u],
+                            crm[u]), a.pz_mmin, a.pz_mdelta), fb[u], w2[u],
+                            crm[u], clampb[u], dc);
+                    }
+                }
+                if (!tc_hist_mode (MODE) && t < x.t_hi) {
+                    const uint32_t o = (3 * (t >> 3)) * 1024u + (t & 7) * 128u
+                        + ((vs.vunit ^ (uint32_t) (t & 7)) << 4);
+                    unsigned short hh, ll;
+                    split_bf16 (dc[0], hh, ll);
+                    *(unsigned short*) (dch + o) = hh;
+                    *(unsigned short*) (dch + DC_HALF + o) = ll;
+                    split_bf16 (dc[1], hh, ll);
+                    *(unsigned short*) (dch + 1024 + o) = hh;
+                    *(unsigned short*) (dch + DC_HALF + 1024 + o) = ll;
+                    split_bf16 (dc[2], hh, ll);
+                    *(unsigned short*) (dch + 2048 + o) = hh;
+                    *(unsigned short*) (dch + DC_HALF + 2048 + o) = ll;
+                }
+            }
+            continue;
         }
         float cr[4][8], fv[4], gx[4], gy[4], gz[4];
 #pragma unroll
@@ -428,7 +630,7 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
             cr[u][6] = __ldg (mp + dxym + dxm);
             cr[u][7] = __ldg (mp + dxym + dxm + 1);
             fv[u] = ok[u] ? __ldg (a.fimg + frow + g.vpr[0] * (t4 + u)) : 0.f;
-            if (GRAD_MODE == 0) {
+            if (MODE == TC_MSE_NEAREST) {
                 const float* gp = a.mgrad + 3 * mvr[u];
                 gx[u] = __ldg (gp + 0);
                 gy[u] = __ldg (gp + 1);
@@ -443,7 +645,7 @@ voxel_phase (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs, int tx0,
                 const float diff = trilinear_lerp (w2[u], cr[u]) - fv[u];
                 scf = fmaf (diff, diff, scf);
                 cnt++;
-                if (GRAD_MODE == 0) {
+                if (MODE == TC_MSE_NEAREST) {
                     dc0 = diff * gx[u]; dc1 = diff * gy[u]; dc2 = diff * gz[u];
                 } else {
                     float gr[3];
@@ -660,149 +862,6 @@ voxel_phase_xline (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
 // is guarded, and the moving gradient is one 16-byte load.  Both rounds use
 // W = vx * T0 voxels per row so one sample -> (row, x) mapping serves every
 // batch; a round-1 tile slot past the batch's last tile is dead.
-// Mattes MI pass 1 at one sample: the PVI-8 corner weights (products of
-// the per-axis fractions, in the reference's order) as integers in 2^-24
-// units, so the sums do not depend on their order.  Corners with equal
-// moving bins are merged first; a sample then has one, two or (rarely)
-// more (fixed, moving) bin pairs.  The first two pairs of every lane
-// combine across the warp (match + reduce, one round each) so that one lane
-// per distinct pair updates the shared joint histogram; further pairs go
-// straight to the shared atomics.  The fixed histogram counts each first-
-// pair group's voxels; the moving histogram is the joint one's column sums,
-// taken when the CTA flushes.  Every lane of the warp calls this (warp
-// collectives).
-__device__ __forceinline__ void
-mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
-    int fb, const int mb[8], int& cnt)
-{
-    const int B = a.bins;
-    unsigned long long* hf = (unsigned long long*) (x.sm + SM_DC);
-    unsigned long long* hj = hf + 2 * B;
-    const float* l2 = w2;
-    const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
-    const float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
-        l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
-        l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
-    unsigned int q[8];
-    bool first[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        q[k] = __float2uint_rn (w[k] * TC_MI_WUNIT);
-        first[k] = live;
-    }
-#pragma unroll
-    for (int k = 1; k < 8; k++) {
-#pragma unroll
-        for (int k2 = 0; k2 < k; k2++) {
-            if (first[k] && first[k2] && mb[k2] == mb[k]) {
-                q[k2] += q[k];
-                first[k] = false;
-            }
-        }
-    }
-    // second pair: the first remaining corner after corner 0
-    bool two = false, many = false;
-    int mb2 = 0;
-    unsigned int q2 = 0;
-#pragma unroll
-    for (int k = 1; k < 8; k++) {
-        many = many || (first[k] && two);
-        mb2 = (first[k] && !two) ? mb[k] : mb2;
-        q2 = (first[k] && !two) ? q[k] : q2;
-        two = two || first[k];
-    }
-    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
-    if (live) {
-        cnt++;
-        // first pair (a warp's sum stays below 32 * (2^24 + 8) < 2^32); its
-        // leader also counts the group's voxels into the fixed histogram
-        const int key = fb * B + mb[0];
-        const unsigned peers = __match_any_sync (live_mask, key);
-        const unsigned sum = __reduce_add_sync (peers, q[0]);
-        if (x.lane == __ffs (peers) - 1) {
-            atomicAdd (&hj[key], (unsigned long long) sum);
-            atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
-        }
-    }
-    const unsigned two_mask = __ballot_sync (0xffffffffu, two);
-    if (two) {
-        const int key = fb * B + mb2;
-        const unsigned peers = __match_any_sync (two_mask, key);
-        const unsigned sum = __reduce_add_sync (peers, q2);
-        if (x.lane == __ffs (peers) - 1) {
-            atomicAdd (&hj[key], (unsigned long long) sum);
-        }
-    }
-    if (many) {
-        bool seen = false;
-#pragma unroll
-        for (int k = 1; k < 8; k++) {
-            if (first[k] && seen) {
-                atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
-            }
-            seen = seen || first[k];
-        }
-    }
-}
-
-// Mattes MI with cubic B-spline Parzen windows, pass 1 at one sample: the
-// window's four weights at the moving value u (integers in 2^-24 units)
-// into the fixed bin's row of the shared joint histogram; lanes with the
-// same (fixed bin, first window bin) combine across the warp first.  Every
-// lane of the warp calls this.
-__device__ __forceinline__ void
-pz_hist_add (const TcArgs& a, const TcCtx& x, bool live, int fb, float u,
-    int& cnt)
-{
-    const int B = a.bins;
-    unsigned long long* hj = (unsigned long long*) (x.sm + SM_DC) + 2 * B;
-    const int k0 = parzen_first_bin (u, B);
-    unsigned int q[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        q[j] = __float2uint_rn (bspline3f ((float) (k0 + j) - u) * TC_MI_WUNIT);
-    }
-    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
-    if (live) {
-        cnt++;
-        const int key = fb * B + k0;
-        const unsigned peers = __match_any_sync (live_mask, key);
-        unsigned sum[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) sum[j] = __reduce_add_sync (peers, q[j]);
-        if (x.lane == __ffs (peers) - 1) {
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (sum[j]) atomicAdd (&hj[key + j], (unsigned long long) sum[j]);
-            }
-        }
-    }
-}
-
-// Pass 2 at one sample: 1/(N delta_m) * sum over the window's bins of
-// beta3'(k - u) log(p(f, k) / p_m(k)), times the world gradient of the
-// trilinear interpolant (axis-aligned here: the diagonal of proj times the
-// index gradient; 0 along an axis the clamp holds).
-__device__ __forceinline__ void
-pz_dc_dv (const TcArgs& a, float u, int fb, const float w2[3],
-    const float m[8], int clamp, float dc[3])
-{
-    const int B = a.bins;
-    const int k0 = parzen_first_bin (u, B);
-    const float* row = a.mi_lut + fb * B;
-    float sum = 0.f;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        sum += bspline3f_d ((float) (k0 + j) - u) * __ldg (row + k0 + j);
-    }
-    float gi[3];
-    trilinear_igrad (w2, m, clamp, gi);
-    const float sc = __ldg (a.mi_nvf + 1) * sum;
-    dc[0] = sc * (a.g.mproj[0] * gi[0]);
-    dc[1] = sc * (a.g.mproj[4] * gi[1]);
-    dc[2] = sc * (a.g.mproj[8] * gi[2]);
-}
-
 template <int MODE>
 __device__ __forceinline__ void
 voxel_phase_axis (const TcArgs& a, const TcCtx& x, const VoxelSlot& vs,
@@ -1303,7 +1362,7 @@ mse_tc_kernel (TcArgs a)
                 if (!cwait (a, x, &s_bar[3], ph_g, abort_flag, 2)) break;
                 finish_batch (b);
             }
-        } else if constexpr (MODE < TC_MI_GRAD) {
+        } else {
             // Tiles of more than 128 voxels: Q is reloaded per 128-voxel
             // block, so batches run one after another.
             for (int i = 0; i < nb_local; i++) {
@@ -1324,11 +1383,12 @@ mse_tc_kernel (TcArgs a)
                     if (!ok) break;
                     voxel_phase<MODE> (a, x, voxel_slot (a, x, mb), tx0,
                         ty, tz, sc, cnt);
+                    if (tc_hist_mode (MODE)) continue;
                     warp_arrive (x, &s_bar[1]);
                     ok = cwait (a, x, &s_bar[3], ph_g, abort_flag, 2);
                 }
                 if (!ok) break;
-                finish_batch (b);
+                if (!tc_hist_mode (MODE)) finish_batch (b);
             }
         }
         if constexpr (tc_hist_mode (MODE)) {
@@ -1506,11 +1566,15 @@ launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
                           : launch_mode<TC_MSE_LINEAR> (p, a, st);
 }
 
+// MI on the tensor-core kernel: the axis-aligned voxel phase (one block per
+// tile) or the general one (several 128-voxel blocks per tile); tiles of
+// one block in rotated geometry take the FP32 passes.
 bool
 tc_mi_supported (const BspGeom& g, const TcPlan& p, int bins)
 {
     TcArgs a;
-    return tc_args (g, p, a)
+    const bool axis = tc_args (g, p, a);
+    return (axis || p.mblk > 1)
         && (2 * bins + bins * bins) * 8 <= 2 * DC_HALF + DC_TAIL;
 }
 
@@ -1520,8 +1584,8 @@ launch_mi_tc (const BspGeom& g, const TcPlan& p, bool hist_pass,
     double* score_part, int* count_part, int* err, cudaStream_t st)
 {
     TcArgs a;
-    if (!tc_args (g, p, a)) return cudaErrorInvalidValue;
-    a.axis = 1;
+    a.axis = tc_args (g, p, a);
+    if (!a.axis && p.mblk == 1) return cudaErrorInvalidValue;
     a.coeff = coeff;
     a.qimg = (const uint4*) qimg;
     a.part = part; a.score_part = score_part; a.count_part = count_part;

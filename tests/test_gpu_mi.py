@@ -73,7 +73,7 @@ def test_mi_64cubed_bins(form, bins):
     np.testing.assert_array_equal(g, g2)
 
 
-@pytest.mark.parametrize("vpr", [(6, 5, 4), (5, 5, 5), (8, 8, 8)])
+@pytest.mark.parametrize("vpr", [(6, 5, 4), (5, 5, 5), (8, 8, 8), (9, 7, 6)])
 def test_mi_tensor_core_form_matches_fp32_form(vpr):
     """The tensor-core MI passes (field and adjoint as GEMMs) against the
     FP32 tile passes: histograms within 1e-5 (L2), score 1e-5, gradient

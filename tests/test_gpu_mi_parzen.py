@@ -55,6 +55,8 @@ CASES = {
     "tiles_of_512": dict(vpr=(8, 8, 8)),
     "rotated": dict(dcos=(0.0, 1.0, 0.0, -1.0, 0.0, 0.0, 0.0, 0.0, 1.0)),
     "roi": dict(roi=((4, 3, 2), (36, 30, 28))),
+    "rotated_tiles_of_512": dict(vpr=(8, 8, 8), dcos=(
+        0.0, 1.0, 0.0, -1.0, 0.0, 0.0, 0.0, 0.0, 1.0)),
 }
 
 
