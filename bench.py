@@ -162,6 +162,32 @@ def cpu_reference_time(fixed, moving, grid, coeff, evals, threads,
     return float(np.median(ts)), kind, threads
 
 
+def cpu_reference_others(fixed, moving, grid, coeff, threads):
+    """One evaluation each, on the same workload, of the reference's other
+    paths: MSE flavour h on one thread (the serial form), Mattes MI flavour
+    g (PVI-8, 32 bins) and the analytic regulariser 'c' (curvature 0.005)
+    on all host threads; seconds, with the device's Gvox/s beside them in
+    also_measured."""
+    import oracle as O
+    if not O.ref_available():
+        return None
+    out = {"threads": threads}
+    for name, fn in (
+            ("mse_flavour_h_1_thread_s",
+             lambda: O.ref_metric(grid, fixed, moving, coeff, flavor="h",
+                                  threads=1)),
+            ("mi_flavour_g_s",
+             lambda: O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                                  metric="mi", threads=threads)),
+            ("regularizer_analytic_c_s",
+             lambda: O.ref_regularize(grid, fixed, coeff, 0.005, impl="c",
+                                      threads=threads))):
+        t0 = time.perf_counter()
+        fn()
+        out[name] = time.perf_counter() - t0
+    return out
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -539,6 +565,8 @@ def main():
                    "kind": kind,
                    "sample": f"{args.cpu_evals} full evaluations of the same "
                              "256x256x128 workload (median)"}
+            extra["cpu_reference_other_paths"] = cpu_reference_others(
+                fixed, moving, grid, coeff, host_threads())
         traffic = profile_traffic(args.form)
         out = {
             "metric": METRIC, "value": value, "unit": "Gvox/s",
