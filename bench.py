@@ -541,10 +541,12 @@ def main():
 
     extra = extra_metrics(P, ctx, stream, flush, d_coeff, d_grad,
                           grid.num_roi_voxels, args.warmup)
-    if rank == 0:
-        # the device-only workloads first: the reference's OpenMP threads
-        # (registration_c1's CPU leg) keep host cores busy for a while
-        # after they finish, which would slow the host-side line searches
+    if rank == 0 and world == 1:
+        # one-GPU workloads, measured at N = 1 only (the other ranks would
+        # idle meanwhile); the device-only ones first: the reference's
+        # OpenMP threads (registration_c1's CPU leg) keep host cores busy
+        # for a while after they finish, which would slow the host-side
+        # line searches
         extra["batched_16_registrations_40_lbfgs_its"] = batched_c5(P)
         extra["mi_parzen_registration_512x512x160_pyramid_4_2_1"] = \
             mi_registration_c4(P)
