@@ -189,6 +189,21 @@ int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
     float* total_grad, float* smetric, int64_t* num_vox);
 
+/* Mattes MI split into its two passes, for one volume split into slabs
+ * across GPUs (no reference counterpart): each slab's context has the whole
+ * images and the slab as its ROI.  b200bsp_mi_hist runs pass 1 over the
+ * ROI and returns the histograms as exact integers -- hist[0..B) fixed,
+ * [B..2B) moving, [2B..2B+B*B) joint (PVI-8 weights in 2^-24 units; the
+ * Parzen form fills the joint part only), hist[2B+B*B] the voxel count -- so
+ * the slabs' histograms add up exactly to the whole ROI's.
+ * b200bsp_mi_grad takes such summed histograms, returns the score they give
+ * and this ROI's part of the gradient in double (the slabs' parts add up to
+ * the whole gradient).  Neither call checks that the ROI is the whole image:
+ * the caller's slabs must tile it. */
+int b200bsp_mi_hist (b200bsp_ctx* ctx, const float* coeff, int64_t* hist);
+int b200bsp_mi_grad (b200bsp_ctx* ctx, const float* coeff,
+    const int64_t* hist, float* score, double* grad, int64_t* num_vox);
+
 /* Autotuner (no reference counterpart): times `evals` MSE evaluations at
  * `coeff` for each way the tensor-core kernel may split a row of tiles
  * into batches (the fewest batches of at most 26 tiles, and up to two

@@ -216,6 +216,41 @@ def port_mi(grid, fixed, moving, coeff, bins=32, precision="f32") -> Result:
                   j_hist.reshape(bins, bins))
 
 
+def port_mi_pass1(grid, fixed, moving, coeff, bins=32):
+    """PVI-8 pass 1 over the grid's ROI in double: (f, m, j, num_vox)."""
+    g = orc_grid(grid, fixed)
+    fh, mh = port_hist_eqsp(fixed.img, bins), port_hist_eqsp(moving.img, bins)
+    nv = C.c_int64(0)
+    f, m, j = np.zeros(bins), np.zeros(bins), np.zeros(bins * bins)
+    rc = port().orc_mi_f64_pass1(
+        C.byref(g), C.byref(orc_vol(fixed)), _p(fixed.img),
+        C.byref(orc_vol(moving)), _p(moving.img),
+        _p(np.ascontiguousarray(coeff, np.float32)), C.byref(fh), C.byref(mh),
+        C.byref(nv), _p(f, f64p), _p(m, f64p), _p(j, f64p))
+    if rc:
+        raise RuntimeError(f"oracle mi pass 1 failed rc={rc}")
+    return f, m, j, nv.value
+
+
+def port_mi_pass2(grid, fixed, moving, coeff, f, m, j, num_vox, bins=32):
+    """PVI-8 pass 2 over the grid's ROI with given histograms: (score,
+    gradient of this ROI, double)."""
+    g = orc_grid(grid, fixed)
+    fh, mh = port_hist_eqsp(fixed.img, bins), port_hist_eqsp(moving.img, bins)
+    s = C.c_double(0)
+    gr = np.zeros(grid.num_coeff, np.float64)
+    f, m, j = (np.ascontiguousarray(a, np.float64) for a in (f, m, j))
+    rc = port().orc_mi_f64_pass2(
+        C.byref(g), C.byref(orc_vol(fixed)), _p(fixed.img),
+        C.byref(orc_vol(moving)), _p(moving.img),
+        _p(np.ascontiguousarray(coeff, np.float32)), C.byref(fh), C.byref(mh),
+        C.c_int64(num_vox), _p(f, f64p), _p(m, f64p), _p(j, f64p),
+        C.byref(s), _p(gr, f64p))
+    if rc:
+        raise RuntimeError(f"oracle mi pass 2 failed rc={rc}")
+    return s.value, gr
+
+
 def port_parzen_params(fixed, moving, bins=32) -> OrcParzen:
     p = OrcParzen()
     f = np.ascontiguousarray(fixed.img, np.float32)

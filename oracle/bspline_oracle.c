@@ -1104,11 +1104,14 @@ mi64_visit (void* vctx, int64_t fidx, const double fxyz[3],
     *has_grad = 1;
 }
 
+/* Pass 1 alone over the grid's ROI: histograms (cleared first) and the
+ * voxel count.  Summed over slabs that tile an ROI they give that ROI's
+ * pass 1 (up to the order of the double additions). */
 int
-orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+orc_mi_f64_pass1 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     const orc_vol* moving, const float* m_img, const float* coeff,
-    const orc_hist* fhp, const orc_hist* mhp, double* score, double* grad,
-    int64_t* num_vox, double* fh, double* mh, double* jh)
+    const orc_hist* fhp, const orc_hist* mhp, int64_t* num_vox, double* fh,
+    double* mh, double* jh)
 {
     vol64 fx, mv;
     if (vol64_init (&fx, fixed) || vol64_init (&mv, moving)) return -1;
@@ -1117,7 +1120,24 @@ orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     memset (jh, 0, sizeof(double) * fhp->bins * mhp->bins);
     mi64_ctx c = { &mv, f_img, m_img, fhp, mhp, fh, mh, jh, 1, 0., 0., 0 };
     tile_loop64 (g, &fx, coeff, mi64_visit, &c, 0);
-    double fnv = (double) c.num_vox, s = 0;
+    *num_vox = c.num_vox;
+    return 0;
+}
+
+/* Pass 2 over the grid's ROI with given histograms and voxel count (e.g.
+ * summed over slabs): the score from them and this ROI's gradient. */
+int
+orc_mi_f64_pass2 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+    const orc_vol* moving, const float* m_img, const float* coeff,
+    const orc_hist* fhp, const orc_hist* mhp, int64_t num_vox,
+    const double* fh, const double* mh, const double* jh, double* score,
+    double* grad)
+{
+    vol64 fx, mv;
+    if (vol64_init (&fx, fixed) || vol64_init (&mv, moving)) return -1;
+    mi64_ctx c = { &mv, f_img, m_img, fhp, mhp, (double*) fh, (double*) mh,
+        (double*) jh, 2, 0., 0., num_vox };
+    double fnv = (double) num_vox, s = 0;
     double thresh = 0.001 / (mhp->bins * fhp->bins);
     for (int64_t jb = 0; jb < fhp->bins * mhp->bins; jb++) {
         int64_t mb = jb % mhp->bins, fb = jb / mhp->bins;
@@ -1125,11 +1145,22 @@ orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     }
     c.smetric = s / fnv;
     c.num_vox_f = fnv;
-    c.pass = 2;
     tile_loop64 (g, &fx, coeff, mi64_visit, &c, grad);
     *score = c.smetric;
-    *num_vox = c.num_vox;
     return 0;
+}
+
+int
+orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
+    const orc_vol* moving, const float* m_img, const float* coeff,
+    const orc_hist* fhp, const orc_hist* mhp, double* score, double* grad,
+    int64_t* num_vox, double* fh, double* mh, double* jh)
+{
+    int rc = orc_mi_f64_pass1 (g, fixed, f_img, moving, m_img, coeff, fhp,
+        mhp, num_vox, fh, mh, jh);
+    if (rc) return rc;
+    return orc_mi_f64_pass2 (g, fixed, f_img, moving, m_img, coeff, fhp, mhp,
+        *num_vox, fh, mh, jh, score, grad);
 }
 
 /* ------------------------------------------------------------------ */

@@ -98,6 +98,15 @@ int orc_mi_parzen_f64 (const orc_grid* g, const orc_vol* fixed,
     const float* coeff, const orc_parzen* p, double* score, double* grad,
     int64_t* num_vox, double* jh);
 
+int orc_mi_f64_pass1 (const orc_grid* g, const orc_vol* fixed,
+    const float* f_img, const orc_vol* moving, const float* m_img,
+    const float* coeff, const orc_hist* fhp, const orc_hist* mhp,
+    int64_t* num_vox, double* fh, double* mh, double* jh);
+int orc_mi_f64_pass2 (const orc_grid* g, const orc_vol* fixed,
+    const float* f_img, const orc_vol* moving, const float* m_img,
+    const float* coeff, const orc_hist* fhp, const orc_hist* mhp,
+    int64_t num_vox, const double* fh, const double* mh, const double* jh,
+    double* score, double* grad);
 int orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     const orc_vol* moving, const float* m_img, const float* coeff,
     const orc_hist* fh, const orc_hist* mh, double* score, double* grad,

@@ -166,6 +166,8 @@ _SIGS = {
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
     "b200bsp_autotune": (C.c_int, [_VP, _VP, C.c_int, _VP]),
+    "b200bsp_mi_hist": (C.c_int, [_VP, _VP, _VP]),
+    "b200bsp_mi_grad": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "b200bsp_batch_create": (C.c_int, [_VP, C.c_int, _VP]),
     "b200bsp_batch_destroy": (None, [_VP]),
     "b200bsp_batch_last_error": (C.c_char_p, [_VP]),
@@ -456,6 +458,27 @@ class Context:
                                       _ptr(jh, np.float64)), self._h)
         if with_hist:
             return s.value, g, n.value, (fh, mh, jh.reshape(b, b))
+        return s.value, g, n.value
+
+    def mi_hist(self, coeff) -> np.ndarray:
+        """MI pass 1 over the ROI: exact integer histograms (f, m, joint,
+        count) as int64 (b200bsp_mi_hist)."""
+        b = self.mi_bins
+        h = np.zeros(2 * b + b * b + 1, np.int64)
+        _check(lib().b200bsp_mi_hist(self._h, _ptr(coeff), _ptr(h, np.int64)),
+               self._h)
+        return h
+
+    def mi_grad(self, coeff, hist):
+        """MI pass 2 with given (summed) histograms: (score, this ROI's
+        gradient in double, num_vox) (b200bsp_mi_grad)."""
+        h = np.ascontiguousarray(hist, np.int64)
+        g = np.zeros(self.num_coeff, np.float64)
+        s = C.c_float()
+        n = C.c_int64()
+        _check(lib().b200bsp_mi_grad(self._h, _ptr(coeff), _ptr(h, np.int64),
+                                     C.addressof(s), _ptr(g, np.float64),
+                                     C.addressof(n)), self._h)
         return s.value, g, n.value
 
     def regularize(self, coeff, parms: RegParms, grad=None):

@@ -678,12 +678,14 @@ struct MiGradVoxel {
 int
 mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     const float* d_moving, const float* d_luts, DevResult* d_res,
-    float* grad_out, double* grad64_out, cudaStream_t st, int* launches)
+    float* grad_out, double* grad64_out, cudaStream_t st, int* launches,
+    int passes)
 {
     if (!s->ready) return B200BSP_E_STATE;
     const int B = s->bins;
     const int nh = 2 * B + B * B;
-    if (cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
+    if ((passes & MI_PASS_HIST)
+        && cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
             st) != cudaSuccess) {
         return B200BSP_E_CUDA;
     }
@@ -696,10 +698,15 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     lay.slots = 64;
     if (s->window == B200BSP_MI_PARZEN) {
         const int grid = std::min (g.ntiles, 8 * sms);
-        parzen_hist_kernel<<<grid, MIH_THREADS,
-            (size_t) B * B * sizeof (unsigned long long), st>>> (g, d_coeff,
-            d_luts, s->d_fbin, d_moving, B, s->pz_mmin, s->pz_mdelta,
-            s->d_hist);
+        if (passes & MI_PASS_HIST) {
+            parzen_hist_kernel<<<grid, MIH_THREADS,
+                (size_t) B * B * sizeof (unsigned long long), st>>> (g,
+                d_coeff, d_luts, s->d_fbin, d_moving, B, s->pz_mmin,
+                s->pz_mdelta, s->d_hist);
+        }
+        if (!(passes & MI_PASS_GRAD)) {
+            return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+        }
         parzen_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->pz_mdelta,
             s->d_histd, s->d_lut, s->d_nvf, d_res);
         ParzenGradVoxel f{s->d_fbin, s->d_lut, s->d_nvf, B, s->pz_mmin,
@@ -720,8 +727,13 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
             (int) hsmem);
     }
     int grid = std::min (g.ntiles, 8 * sms);
-    hk<<<grid, MIH_THREADS, hsmem, st>>> (g, d_coeff, d_luts, s->d_fbin,
-        s->d_mbin, B, s->d_hist);
+    if (passes & MI_PASS_HIST) {
+        hk<<<grid, MIH_THREADS, hsmem, st>>> (g, d_coeff, d_luts, s->d_fbin,
+            s->d_mbin, B, s->d_hist);
+    }
+    if (!(passes & MI_PASS_GRAD)) {
+        return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+    }
     mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd, s->d_lut,
         s->d_nvf, d_res);
     MiGradVoxel f{s->d_fbin, s->d_mbin, s->d_lut, s->d_nvf, B};
@@ -746,12 +758,13 @@ mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     const PartLayout& lay, const void* qlut, float* part, double* score_part,
     int* count_part, int* err, const float* d_coeff, const float* d_moving,
     DevResult* d_res, float* grad_out, double* grad64_out, cudaStream_t st,
-    int* launches)
+    int* launches, int passes)
 {
     if (!s->ready) return B200BSP_E_STATE;
     const int B = s->bins;
     const int nh = 2 * B + B * B;
-    if (cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
+    if ((passes & MI_PASS_HIST)
+        && cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
             st) != cudaSuccess) {
         return B200BSP_E_CUDA;
     }
@@ -766,9 +779,13 @@ mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     mi.mimg = d_moving;
     mi.m_min = s->pz_mmin;
     mi.m_delta = s->pz_mdelta;
-    if (launch_mi_tc (g, plan, true, mi, d_coeff, qlut, part, score_part,
+    if ((passes & MI_PASS_HIST)
+        && launch_mi_tc (g, plan, true, mi, d_coeff, qlut, part, score_part,
             count_part, err, st) != cudaSuccess) {
         return B200BSP_E_CUDA;
+    }
+    if (!(passes & MI_PASS_GRAD)) {
+        return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
     }
     if (mi.parzen) {
         parzen_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->pz_mdelta,

@@ -45,14 +45,19 @@ int mi_alloc (MiState* s, const BspGeom& g, int bins, int window);
 void mi_free (MiState* s);
 int mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
     const float* d_moving, size_t nf, size_t nm, cudaStream_t st);
+// passes: MI_PASS_HIST (histograms into d_hist), MI_PASS_GRAD (score and
+// gradient from the histograms in d_hist), or both
+constexpr int MI_PASS_HIST = 1;
+constexpr int MI_PASS_GRAD = 2;
 int mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     const float* d_moving, const float* d_luts, DevResult* d_res,
-    float* grad_out, double* grad64_out, cudaStream_t st, int* launches);
+    float* grad_out, double* grad64_out, cudaStream_t st, int* launches,
+    int passes = MI_PASS_HIST | MI_PASS_GRAD);
 int mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     const PartLayout& lay, const void* qlut, float* part, double* score_part,
     int* count_part, int* err, const float* d_coeff, const float* d_moving,
     DevResult* d_res, float* grad_out, double* grad64_out, cudaStream_t st,
-    int* launches);
+    int* launches, int passes = MI_PASS_HIST | MI_PASS_GRAD);
 int mi_fetch (MiState* s, const DevResult* d_res, double* f_hist,
     double* m_hist, double* j_hist, cudaStream_t st);
 void mi_finish (MiState* s, MiResult* r);

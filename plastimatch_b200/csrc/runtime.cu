@@ -898,6 +898,25 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     return check_device_error (c);
 }
 
+// One or both MI passes on the context's form (tensor-core modes where they
+// apply); gradients to grad (float) or grad64 (double), device pointers.
+static int
+mi_passes (b200bsp_ctx* c, const float* dcoeff, float* grad, double* grad64,
+    int passes)
+{
+    if (c->opts.form == B200BSP_FORM_TC
+        && tc_mi_supported (c->geom, c->plan, c->mi.bins)) {
+        TcPlan plan = c->plan;
+        if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
+        return mi_run_tc (&c->mi, c->geom, plan, c->lay, c->d_qlut,
+            c->d_part, c->d_score_part, c->d_count_part, c->d_err, dcoeff,
+            c->d_moving, c->d_res, grad, grad64, c->stream,
+            &c->last_launches, passes);
+    }
+    return mi_run (&c->mi, c->geom, dcoeff, c->d_moving, c->d_luts, c->d_res,
+        grad, grad64, c->stream, &c->last_launches, passes);
+}
+
 extern "C" int
 b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     float* grad, int64_t* num_vox, double* f_hist, double* m_hist,
@@ -918,16 +937,7 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     int rc = begin_eval (c, coeff, &dcoeff);
     if (rc) return rc;
     float* g_dev = is_device_ptr (grad) ? grad : c->d_grad;
-    if (c->opts.form == B200BSP_FORM_TC
-        && tc_mi_supported (c->geom, c->plan, c->mi.bins)) {
-        rc = mi_run_tc (&c->mi, c->geom, c->plan, c->lay, c->d_qlut,
-            c->d_part, c->d_score_part, c->d_count_part, c->d_err, dcoeff,
-            c->d_moving, c->d_res, g_dev, nullptr, c->stream,
-            &c->last_launches);
-    } else {
-        rc = mi_run (&c->mi, c->geom, dcoeff, c->d_moving, c->d_luts,
-            c->d_res, g_dev, nullptr, c->stream, &c->last_launches);
-    }
+    rc = mi_passes (c, dcoeff, g_dev, nullptr, MI_PASS_HIST | MI_PASS_GRAD);
     if (rc) return fail (c, rc, "MI evaluation failed: %s",
         cudaGetErrorString (cudaGetLastError ()));
     mark_main_done (c);
@@ -943,6 +953,59 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     mi_finish (&c->mi, &mr);
     if (score) *score = mr.score_f;
     if (num_vox) *num_vox = mr.num_vox;
+    return check_device_error (c);
+}
+
+extern "C" int
+b200bsp_mi_hist (b200bsp_ctx* c, const float* coeff, int64_t* hist)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (!hist) return fail (c, B200BSP_E_BADARG, "null histogram buffer");
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    rc = mi_passes (c, dcoeff, nullptr, nullptr, MI_PASS_HIST);
+    if (rc) return fail (c, rc, "MI pass 1 failed: %s",
+        cudaGetErrorString (cudaGetLastError ()));
+    const int B = c->mi.bins;
+    const size_t nh = (size_t) 2 * B + (size_t) B * B + 1;
+    CK (cudaMemcpyAsync (hist, c->mi.d_hist, nh * sizeof (int64_t),
+        is_device_ptr (hist) ? cudaMemcpyDeviceToDevice
+                             : cudaMemcpyDeviceToHost, c->stream));
+    rc = end_eval (c, true);
+    if (rc) return rc;
+    return check_device_error (c);
+}
+
+extern "C" int
+b200bsp_mi_grad (b200bsp_ctx* c, const float* coeff, const int64_t* hist,
+    float* score, double* grad, int64_t* num_vox)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (!hist || !grad) return fail (c, B200BSP_E_BADARG, "null argument");
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    const int B = c->mi.bins;
+    const size_t nh = (size_t) 2 * B + (size_t) B * B + 1;
+    CK (cudaMemcpyAsync (c->mi.d_hist, hist, nh * sizeof (int64_t),
+        is_device_ptr (hist) ? cudaMemcpyDeviceToDevice
+                             : cudaMemcpyHostToDevice, c->stream));
+    const bool dev_grad = is_device_ptr (grad);
+    rc = mi_passes (c, dcoeff, nullptr, dev_grad ? grad : c->d_grad64,
+        MI_PASS_GRAD);
+    if (rc) return fail (c, rc, "MI pass 2 failed: %s",
+        cudaGetErrorString (cudaGetLastError ()));
+    CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
+        cudaMemcpyDeviceToHost, c->stream));
+    if (!dev_grad) {
+        CK (cudaMemcpyAsync (grad, c->d_grad64, c->num_coeff * sizeof (double),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    rc = end_eval (c, true);
+    if (rc) return rc;
+    if (score) *score = c->h_res->score_f;
+    if (num_vox) *num_vox = c->h_res->num_vox;
     return check_device_error (c);
 }
 

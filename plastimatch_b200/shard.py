@@ -1,4 +1,4 @@
-"""Multi-GPU forms of the MSE cost function.
+"""Multi-GPU forms of the MSE and Mattes MI cost functions.
 
 Replicas (independent registrations, one per GPU) need nothing from this
 module: each process creates its own Context.
@@ -14,8 +14,15 @@ context, and one all-reduce of the raw sums -- sum of diff^2, the voxel
 count and the unnormalised gradient, in double precision -- gives the global
 result, normalised afterwards as bspline_score_normalize (:43-72) does.
 
+Mattes MI needs the whole volume's histograms before its gradient pass, so
+a slab evaluation is two calls around two all-reduces: pass 1 on every slab
+(b200bsp_mi_hist: exact integer histograms), one all-reduce of the
+histograms (the sum is the whole ROI's, bit for bit), pass 2 on every slab
+with the summed histograms (b200bsp_mi_grad: the score and the slab's part
+of the gradient), one all-reduce of the gradient.
+
 No tensor-core work crosses GPUs and no GPU reads another's memory; the only
-exchange is the all-reduce (NCCL over NVLink on GPUs, gloo on CPU).
+exchanges are the all-reduces (NCCL over NVLink on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
@@ -117,6 +124,38 @@ def context_evaluator(fixed: Volume, moving: Volume, form: str = "tc",
     return run
 
 
+class ContextMiEvaluator:
+    """MI passes of slabs on the GPU through a Context per slab grid: hist()
+    returns the slab's integer histograms, grad() the score of the given
+    (summed) histograms and the slab's gradient part in double."""
+
+    def __init__(self, fixed: Volume, moving: Volume, form: str = "tc",
+                 mi_bins: int = 32, mi_window: str = "pvi8", device: int = 0):
+        self.fixed, self.moving = fixed, moving
+        self.kw = dict(form=form, mi_bins=mi_bins, mi_window=mi_window,
+                       device=device)
+        self.contexts = {}
+
+    def _ctx(self, g: BsplineGrid):
+        from . import Context
+        key = (g.roi_offset, g.roi_dim)
+        if key not in self.contexts:
+            ctx = Context(self.fixed, self.moving, g, **self.kw)
+            ctx.set_images()
+            self.contexts[key] = ctx
+        return self.contexts[key]
+
+    def hist(self, g: BsplineGrid, coeff: np.ndarray) -> np.ndarray:
+        return self._ctx(g).mi_hist(coeff)
+
+    def grad(self, g: BsplineGrid, coeff: np.ndarray, hist: np.ndarray):
+        return self._ctx(g).mi_grad(coeff, hist)
+
+    def hist_len(self) -> int:
+        b = self.kw["mi_bins"]
+        return 2 * b + b * b + 1
+
+
 class SlabScorer:
     """MSE score + gradient of one volume sharded by z-slab over a
     torch.distributed process group (every rank calls score_mse with the
@@ -157,3 +196,37 @@ class SlabScorer:
         score = buf[n] / nv
         grad = (2.0 * buf[:n] / nv).astype(np.float32)
         return float(np.float32(score)), grad, nv
+
+    def score_mi(self, coeff: np.ndarray, mi_eval):
+        """(score, gradient float32, num_vox), as b200bsp_score_mi over the
+        whole ROI.  mi_eval: hist(grid, coeff) -> histograms (any numeric
+        dtype; the count last), grad(grid, coeff, hist) -> (score, slab
+        gradient, num_vox), hist_len()."""
+        import torch
+        n = self.grid.num_coeff
+        c_local = None
+        if self.slab.empty:
+            h = np.zeros(mi_eval.hist_len())
+        else:
+            c_local = slab_coeff(self.grid, self.slab, coeff)
+            h = np.asarray(mi_eval.hist(self.local_grid, c_local))
+        t = torch.from_numpy(np.ascontiguousarray(h))
+        if self.device is not None:
+            t = t.to(self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+        h = t.cpu().numpy()
+        buf = np.zeros(n + 1, np.float64)
+        if not self.slab.empty:
+            s, g, _ = mi_eval.grad(self.local_grid, c_local, h)
+            scatter_grad(self.grid, self.slab, g, buf[:n])
+            if self.rank == 0:
+                buf[n] = s
+        t = torch.from_numpy(buf)
+        if self.device is not None:
+            t = t.to(self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+        buf = t.cpu().numpy()
+        nv = int(round(float(h[-1])))
+        if nv < 1:
+            return FLT_MAX, np.zeros(n, np.float32), 0
+        return float(np.float32(buf[n])), buf[:n].astype(np.float32), nv
