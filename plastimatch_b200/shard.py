@@ -151,6 +151,8 @@ class ContextMiEvaluator:
     def grad(self, g: BsplineGrid, coeff: np.ndarray, hist: np.ndarray):
         return self._ctx(g).mi_grad(coeff, hist)
 
+    hist_dtype = np.int64
+
     def hist_len(self) -> int:
         b = self.kw["mi_bins"]
         return 2 * b + b * b + 1
@@ -199,14 +201,18 @@ class SlabScorer:
 
     def score_mi(self, coeff: np.ndarray, mi_eval):
         """(score, gradient float32, num_vox), as b200bsp_score_mi over the
-        whole ROI.  mi_eval: hist(grid, coeff) -> histograms (any numeric
-        dtype; the count last), grad(grid, coeff, hist) -> (score, slab
-        gradient, num_vox), hist_len()."""
+        whole ROI.  mi_eval: hist(grid, coeff) -> histograms (the count
+        last; of type mi_eval.hist_dtype, float64 when absent),
+        grad(grid, coeff, hist) -> (score, slab gradient, num_vox),
+        hist_len()."""
         import torch
         n = self.grid.num_coeff
         c_local = None
         if self.slab.empty:
-            h = np.zeros(mi_eval.hist_len())
+            # zeros of the evaluator's histogram type: every rank must pass
+            # the same dtype to the all-reduce
+            h = np.zeros(mi_eval.hist_len(),
+                         getattr(mi_eval, "hist_dtype", np.float64))
         else:
             c_local = slab_coeff(self.grid, self.slab, coeff)
             h = np.asarray(mi_eval.hist(self.local_grid, c_local))

@@ -165,13 +165,25 @@ def _mi_case():
     return fixed, moving, grid, coeff
 
 
-def _mi_rank_main(rank, world, port, q):
+def _mi_thin_case():
+    """Two tiles along z: a third rank gets an empty slab."""
+    fixed = synth.gaussian_blobs((20, 18, 7), spacing=(1.0, 1.0, 1.2),
+                                 seed=54)
+    g0 = BsplineGrid.for_volume(fixed, 5)
+    moving = synth.warp_trilinear(fixed, fixed, g0,
+                                  synth.random_coeff(g0, 1.0, 55))
+    grid = BsplineGrid.for_volume(fixed, (5, 4, 4))
+    coeff = synth.random_coeff(grid, 0.8, 56)
+    return fixed, moving, grid, coeff
+
+
+def _mi_rank_main(rank, world, port, q, thin=False):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        fixed, moving, grid, coeff = _mi_case()
+        fixed, moving, grid, coeff = _mi_thin_case() if thin else _mi_case()
         sc = shard.SlabScorer(grid, None)
         s, g, n = sc.score_mi(coeff, OracleMiEvaluator(fixed, moving, 16))
         q.put((rank, s, g, n))
@@ -179,15 +191,16 @@ def _mi_rank_main(rank, world, port, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_slab_mi_matches_whole_volume(world):
+@pytest.mark.parametrize("world,thin", [(2, False), (3, False), (3, True)])
+def test_slab_mi_matches_whole_volume(world, thin):
     """MI over z-slabs: histograms all-reduced between the passes, slab
     gradients all-reduced after; equal to the whole-volume oracle (score
-    within 1e-6 relative, returned in float32; gradient 1e-6 L2)."""
+    within 1e-6 relative, returned in float32; gradient 1e-6 L2).  The thin
+    case leaves one rank an empty slab."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_mi_rank_main, args=(r, world, port, q))
+    procs = [ctx.Process(target=_mi_rank_main, args=(r, world, port, q, thin))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -195,7 +208,9 @@ def test_slab_mi_matches_whole_volume(world):
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    fixed, moving, grid, coeff = _mi_case()
+    fixed, moving, grid, coeff = _mi_thin_case() if thin else _mi_case()
+    if thin:
+        assert sum(s.empty for s in shard.plan_slabs(grid, world)) == 1
     ref = O.port_mi(grid, fixed, moving, coeff, bins=16, precision="f64")
     for _, s, g, n in res:
         assert n == ref.num_vox
