@@ -183,11 +183,34 @@ int b200bsp_regularize_f64 (b200bsp_ctx* ctx, const float* coeff,
 
 /* The whole cost function bspline_score() (src/register/bspline.cxx:
  * 558-632) for one similarity metric: metric_type 0 = MSE, 1 = MI;
- * total_score = lambda * smetric (+ rmetric when reg != NULL), total_grad
- * likewise. */
+ * total_score = lambda * smetric (+ rmetric when reg != NULL, + stiffness *
+ * lmetric when landmarks are set), total_grad likewise, in that order. */
 int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
     float* total_grad, float* smetric, int64_t* num_vox);
+
+/* Landmark pairs for the cost function: Bspline_landmarks::set_landmarks
+ * and ::initialize (src/register/bspline_landmarks.cxx:145-215), with the
+ * stiffness of Bspline_landmarks::landmark_stiffness.  fixed_xyz and
+ * moving_xyz are host arrays of points in mm (xyz per point); the first
+ * min(n_fixed, n_moving) pairs are used, and a count of 0 removes the
+ * landmarks.  Each fixed landmark must lie inside the fixed image
+ * (B200BSP_E_BADARG; the reference exits) and its tile, taken from the
+ * absolute voxel index as the reference takes it, inside the grid
+ * (B200BSP_E_UNSUPPORTED). */
+int b200bsp_set_landmarks (b200bsp_ctx* ctx, const float* fixed_xyz,
+    int64_t n_fixed, const float* moving_xyz, int64_t n_moving,
+    float stiffness);
+
+/* The landmark term alone, bspline_landmarks_score_a
+ * (src/register/bspline_landmarks.cxx:25-134): lmetric = the mean squared
+ * distance between the moving landmarks and the fixed landmarks carried by
+ * the field; ADDS its gradient (stiffness / n times the residual, spread
+ * over the landmark's 64 knots) into grad, as the reference adds into
+ * total_grad (grad may be NULL).  Float arithmetic in the reference's
+ * order: results equal the reference's bit for bit. */
+int b200bsp_landmarks_score (b200bsp_ctx* ctx, const float* coeff,
+    float* lmetric, float* grad);
 
 /* Mattes MI split into its two passes, for one volume split into slabs
  * across GPUs (no reference counterpart): each slab's context has the whole

@@ -306,6 +306,45 @@ def port_reg(grid, fixed, coeff, pen, precision="f32") -> Result:
     return Result(s.value, gr)
 
 
+def port_landmarks_init(grid, fixed, fixed_pts):
+    """Bspline_landmarks::initialize restated: (p, q) int64 arrays (n, 3),
+    the tile and in-tile offset of each fixed landmark; raises ValueError
+    when one lies outside the fixed image."""
+    f = np.ascontiguousarray(np.asarray(fixed_pts, np.float32).reshape(-1, 3))
+    n = len(f)
+    p = np.zeros((n, 3), np.int64)
+    q = np.zeros((n, 3), np.int64)
+    port().orc_landmarks_init.restype = C.c_int64
+    bad = port().orc_landmarks_init(C.byref(orc_grid(grid, fixed)),
+                                    C.byref(orc_vol(fixed)), _p(f),
+                                    C.c_int64(n), _p(p, i64p), _p(q, i64p))
+    if bad:
+        raise ValueError(f"fixed landmark {bad - 1} outside the fixed image")
+    return p, q
+
+
+def port_landmarks(grid, fixed, coeff, fixed_pts, moving_pts,
+                   stiffness=1.0, grad=None) -> Result:
+    """bspline_landmarks_score_a restated in the reference's float
+    arithmetic: Result(lmetric, gradient), the landmark gradient added in
+    place to a copy of `grad` (zeros when None), as the reference adds it to
+    total_grad."""
+    f = np.ascontiguousarray(np.asarray(fixed_pts, np.float32).reshape(-1, 3))
+    m = np.ascontiguousarray(np.asarray(moving_pts, np.float32).reshape(-1, 3))
+    n = min(len(f), len(m))
+    f, m = np.ascontiguousarray(f[:n]), np.ascontiguousarray(m[:n])
+    p, q = port_landmarks_init(grid, fixed, f)
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    gr = (np.zeros(grid.num_coeff, np.float32) if grad is None
+          else np.array(grad, np.float32))
+    s = C.c_float(0)
+    port().orc_landmarks_f32(C.byref(orc_grid(grid, fixed)), _p(coeff),
+                             C.c_int64(n), _p(f), _p(m), _p(p, i64p),
+                             _p(q, i64p), C.c_float(stiffness), C.byref(s),
+                             _p(gr))
+    return Result(s.value, gr)
+
+
 def port_interpolate_vf(grid, fixed, coeff) -> np.ndarray:
     """bspline_interpolate_vf restated: field over the ROI, zero elsewhere;
     shape (nz, ny, nx, 3)."""
@@ -431,6 +470,45 @@ def ref_score(grid, fixed, moving, coeff, flavor="g", metric="mse", bins=32,
         C.c_char(flavor.encode()), C.c_int(1 if metric == "mi" else 0),
         C.c_int(bins), C.c_char(reg_impl.encode() if reg_impl else b"\0"),
         C.c_float(curvature), C.c_int(threads), _p(gr), C.byref(res))
+    if rc:
+        raise RuntimeError("reference score failed")
+    return Result(res.total_score, gr, res.num_vox)
+
+
+def ref_landmarks(grid, fixed, coeff, fixed_pts, moving_pts,
+                  stiffness=1.0) -> Result:
+    """The reference's own landmark term: Result(lmetric, gradient)."""
+    f = np.ascontiguousarray(np.asarray(fixed_pts, np.float32).reshape(-1, 3))
+    m = np.ascontiguousarray(np.asarray(moving_pts, np.float32).reshape(-1, 3))
+    gr = np.zeros(grid.num_coeff, np.float32)
+    res = RefResult()
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = ref().ref_landmarks(C.byref(_ref_geom(fixed)),
+                             C.byref(_ref_grid(grid)), _p(coeff), _p(f),
+                             _p(m), C.c_int64(min(len(f), len(m))),
+                             C.c_float(stiffness), _p(gr), C.byref(res))
+    if rc:
+        raise RuntimeError("reference landmarks failed")
+    return Result(res.score, gr)
+
+
+def ref_score_landmarks(grid, fixed, moving, coeff, fixed_pts, moving_pts,
+                        stiffness=1.0, flavor="g", metric="mse", bins=32,
+                        reg_impl="", curvature=0.0, threads=0) -> Result:
+    """bspline_score() with one metric, the optional analytic regulariser
+    and landmark pairs: Result(total_score, total_grad, num_vox)."""
+    f = np.ascontiguousarray(np.asarray(fixed_pts, np.float32).reshape(-1, 3))
+    m = np.ascontiguousarray(np.asarray(moving_pts, np.float32).reshape(-1, 3))
+    gr = np.zeros(grid.num_coeff, np.float32)
+    res = RefResult()
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    rc = ref().ref_score_landmarks(
+        C.byref(_ref_geom(fixed)), _p(fixed.img), C.byref(_ref_geom(moving)),
+        _p(moving.img), C.byref(_ref_grid(grid)), _p(coeff),
+        C.c_char(flavor.encode()), C.c_int(1 if metric == "mi" else 0),
+        C.c_int(bins), C.c_char(reg_impl.encode() if reg_impl else b"\0"),
+        C.c_float(curvature), _p(f), _p(m), C.c_int64(min(len(f), len(m))),
+        C.c_float(stiffness), C.c_int(threads), _p(gr), C.byref(res))
     if rc:
         raise RuntimeError("reference score failed")
     return Result(res.total_score, gr, res.num_vox)

@@ -1839,3 +1839,92 @@ orc_resample_li (const int64_t idim[3], const float iorigin[3],
         }
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Landmarks                                                          */
+
+/* Bspline_landmarks::initialize (src/register/bspline_landmarks.cxx:
+ * 150-204): landmark position relative to the image origin, projected to
+ * voxel coordinates by the fixed image's proj matrix (PROJECT_X/Y/Z,
+ * src/base/volume_macros.h:76-81), truncated toward zero, split into tile
+ * and offset by vox_per_rgn.  The tile comes from the absolute voxel
+ * index, not from the ROI. */
+int64_t
+orc_landmarks_init (const orc_grid* g, const orc_vol* fixed,
+    const float* fixed_xyz, int64_t n, int64_t* p, int64_t* q)
+{
+    for (int64_t l = 0; l < n; l++) {
+        float xyz[3];
+        for (int d = 0; d < 3; d++) {
+            xyz[d] = fixed_xyz[3*l+d] - g->img_origin[d];
+        }
+        for (int d = 0; d < 3; d++) {
+            const float* pr = fixed->proj + 3 * d;
+            float ijk = xyz[0] * pr[0] + xyz[1] * pr[1] + xyz[2] * pr[2];
+            if (!(ijk > -1.f && ijk < (float) g->img_dim[d])) return l + 1;
+            int64_t v = (int64_t) ijk;
+            if (v < 0 || v >= g->img_dim[d]) return l + 1;
+            p[3*l+d] = v / g->vox_per_rgn[d];
+            q[3*l+d] = v % g->vox_per_rgn[d];
+        }
+    }
+    return 0;
+}
+
+/* bspline_landmarks_score_a (src/register/bspline_landmarks.cxx:25-134):
+ * field at the landmark (bspline_interp_pix over q_lut,
+ * src/base/bspline_interpolate.cxx:21-48), residual moving - (fixed +
+ * field), squared distance summed in float, dc/dv = -(stiffness / n) *
+ * residual added to the 64 knots (Bspline_score::update_grad,
+ * src/register/bspline_score.cxx:117-143); lmetric = sum / n. */
+void
+orc_landmarks_f32 (const orc_grid* g, const float* coeff, int64_t n,
+    const float* fixed_xyz, const float* moving_xyz, const int64_t* p,
+    const int64_t* q, float stiffness, float* lmetric, float* grad)
+{
+    const int64_t* vpr = g->vox_per_rgn;
+    const int64_t* cd = g->cdims;
+    float* q_lut = (float*) malloc (sizeof(float) * 64
+        * vpr[0] * vpr[1] * vpr[2]);
+    orc_q_lut (q_lut, vpr);
+    float land_score = 0.f;
+    const float land_grad_coeff = stiffness / (float) n;
+    for (int64_t l = 0; l < n; l++) {
+        const int64_t* pl = p + 3 * l;
+        const int64_t qidx = q[3*l+0] + vpr[0] * (q[3*l+1] + vpr[1] * q[3*l+2]);
+        const float* ql = q_lut + 64 * qidx;
+        float dxyz[3] = {0.f, 0.f, 0.f};
+        int m = 0;
+        for (int k = 0; k < 4; k++)
+            for (int j = 0; j < 4; j++)
+                for (int i = 0; i < 4; i++) {
+                    int64_t cidx = 3 * ((pl[2] + k) * cd[1] * cd[0]
+                        + (pl[1] + j) * cd[0] + (pl[0] + i));
+                    dxyz[0] += ql[m] * coeff[cidx+0];
+                    dxyz[1] += ql[m] * coeff[cidx+1];
+                    dxyz[2] += ql[m] * coeff[cidx+2];
+                    m++;
+                }
+        float diff[3], dc_dv[3];
+        for (int d = 0; d < 3; d++) {
+            float mxyz = fixed_xyz[3*l+d] + dxyz[d];
+            diff[d] = moving_xyz[3*l+d] - mxyz;
+        }
+        float l_dist = diff[0]*diff[0] + diff[1]*diff[1] + diff[2]*diff[2];
+        land_score += l_dist;
+        for (int d = 0; d < 3; d++) dc_dv[d] = - land_grad_coeff * diff[d];
+        m = 0;
+        for (int k = 0; k < 4; k++)
+            for (int j = 0; j < 4; j++)
+                for (int i = 0; i < 4; i++) {
+                    int64_t cidx = 3 * ((pl[2] + k) * cd[1] * cd[0]
+                        + (pl[1] + j) * cd[0] + (pl[0] + i));
+                    grad[cidx+0] += dc_dv[0] * ql[m];
+                    grad[cidx+1] += dc_dv[1] * ql[m];
+                    grad[cidx+2] += dc_dv[2] * ql[m];
+                    m++;
+                }
+    }
+    free (q_lut);
+    *lmetric = land_score / (float) n;
+}

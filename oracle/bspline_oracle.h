@@ -120,6 +120,17 @@ int orc_reg_f32 (const orc_grid* g, const float* coeff,
 int orc_reg_f64 (const orc_grid* g, const float* coeff,
     const float penalties[8], double* rmetric, double* grad);
 
+/* Landmarks.  orc_landmarks_init: the tile p[3n] and in-tile offset q[3n]
+ * of each fixed landmark (Bspline_landmarks::initialize); returns the
+ * index + 1 of the first landmark outside the fixed image, 0 when all lie
+ * inside.  orc_landmarks_f32: bspline_landmarks_score_a in the reference's
+ * float arithmetic, lmetric and the gradient ADDED into grad. */
+int64_t orc_landmarks_init (const orc_grid* g, const orc_vol* fixed,
+    const float* fixed_xyz, int64_t n, int64_t* p, int64_t* q);
+void orc_landmarks_f32 (const orc_grid* g, const float* coeff, int64_t n,
+    const float* fixed_xyz, const float* moving_xyz, const int64_t* p,
+    const int64_t* q, float stiffness, float* lmetric, float* grad);
+
 /* Dense vector field over the ROI (bspline_interpolate_vf) and the warped
  * moving image (bspline_warp, linear interpolation; ROI must be the whole
  * image, returns -2 otherwise). */

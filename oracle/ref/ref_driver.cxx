@@ -19,6 +19,7 @@
 
 #include "bspline.h"
 #include "bspline_interpolate.h"
+#include "bspline_landmarks.h"
 #include "bspline_mi.h"
 #include "bspline_mse.h"
 #include "bspline_optimize.h"
@@ -30,6 +31,7 @@
 #include "joint_histogram.h"
 #include "mha_io.h"
 #include "metric_state.h"
+#include "pointset.h"
 #include "regularization_parms.h"
 #include "volume.h"
 #include "volume_grad.h"
@@ -97,7 +99,16 @@ make_volume (const ref_geom* g, const float* img, int planes)
     return v;
 }
 
+/* Landmark pairs (points in mm) and their stiffness. */
+struct Ref_landmarks {
+    const float* fixed_xyz;
+    const float* moving_xyz;
+    int64_t n;
+    float stiffness;
+};
+
 struct Ref_setup {
+    Labeled_pointset lm_fixed, lm_moving;
     Bspline_xform bxf;
     Bspline_parms parms;
     Regularization_parms rparms;
@@ -110,7 +121,7 @@ setup (Ref_setup* s, const ref_geom* fg, const float* fimg,
     const ref_geom* mg, const float* mimg, const float* mgrad,
     const ref_grid* grid, const float* coeff, char flavor,
     int metric_mi, int bins, char reg_impl, float reg_lambda,
-    int threads)
+    int threads, const Ref_landmarks* lm = 0)
 {
     if (threads > 0) omp_set_num_threads (threads);
     float origin[3], spacing[3];
@@ -137,6 +148,19 @@ setup (Ref_setup* s, const ref_geom* fg, const float* fimg,
     s->rparms.implementation = reg_impl;
     s->rparms.curvature_penalty = reg_lambda;
     s->parms.regularization_parms = &s->rparms;
+
+    if (lm && lm->n > 0) {
+        /* as bspline_stage.cxx:318-329 sets them up before the state's
+           initialize() computes their grid coordinates */
+        for (int64_t l = 0; l < lm->n; l++) {
+            s->lm_fixed.insert_lps ("", lm->fixed_xyz[3*l],
+                lm->fixed_xyz[3*l+1], lm->fixed_xyz[3*l+2]);
+            s->lm_moving.insert_lps ("", lm->moving_xyz[3*l],
+                lm->moving_xyz[3*l+1], lm->moving_xyz[3*l+2]);
+        }
+        s->parms.blm->set_landmarks (&s->lm_fixed, &s->lm_moving);
+        s->parms.blm->landmark_stiffness = lm->stiffness;
+    }
 
     s->bod.set_bspline_parms (&s->parms);
     s->bod.set_bspline_xform (&s->bxf);
@@ -244,6 +268,52 @@ ref_score (const ref_geom* fg, const float* fimg,
     Ref_setup s;
     setup (&s, fg, fimg, mg, mimg, mgrad, grid, coeff, flavor, metric_mi,
         bins, reg_impl, curvature_penalty, threads);
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    bspline_score (&s.bod);
+    res->total_score = bst->ssd.total_score;
+    res->rmetric = bst->ssd.rmetric;
+    res->num_coeff = s.bxf.num_coeff;
+    res->score = bst->ssd.metric_record.empty ()
+        ? 0.f : bst->ssd.metric_record[0].score;
+    memcpy (grad, bst->ssd.total_grad, sizeof(float) * s.bxf.num_coeff);
+    return 0;
+}
+
+/* The landmark term alone: Bspline_landmarks::initialize through the
+ * state's initialize(), then bspline_landmarks_score
+ * (src/register/bspline_landmarks.cxx:25-145) into a freshly reset
+ * Bspline_score.  Writes lmetric (in res->score) and total_grad. */
+int
+ref_landmarks (const ref_geom* fg, const ref_grid* grid, const float* coeff,
+    const float* fixed_xyz, const float* moving_xyz, int64_t n,
+    float stiffness, float* grad, ref_result* res)
+{
+    Quiet q;
+    Ref_setup s;
+    Ref_landmarks lm = {fixed_xyz, moving_xyz, n, stiffness};
+    setup (&s, fg, 0, 0, 0, 0, grid, coeff, 'g', 0, 32, '\0', 0.f, 0, &lm);
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    bst->ssd.reset_score ();
+    bspline_landmarks_score (&s.parms, bst, &s.bxf);
+    res->score = bst->ssd.lmetric;
+    res->num_coeff = s.bxf.num_coeff;
+    memcpy (grad, bst->ssd.total_grad, sizeof(float) * s.bxf.num_coeff);
+    return 0;
+}
+
+/* bspline_score() as ref_score, with landmark pairs as well. */
+int
+ref_score_landmarks (const ref_geom* fg, const float* fimg,
+    const ref_geom* mg, const float* mimg, const ref_grid* grid,
+    const float* coeff, char flavor, int metric_mi, int bins, char reg_impl,
+    float curvature_penalty, const float* fixed_xyz, const float* moving_xyz,
+    int64_t n, float stiffness, int threads, float* grad, ref_result* res)
+{
+    Quiet q;
+    Ref_setup s;
+    Ref_landmarks lm = {fixed_xyz, moving_xyz, n, stiffness};
+    setup (&s, fg, fimg, mg, mimg, 0, grid, coeff, flavor, metric_mi, bins,
+        reg_impl, curvature_penalty, threads, &lm);
     Bspline_state* bst = s.bod.get_bspline_state ();
     bspline_score (&s.bod);
     res->total_score = bst->ssd.total_score;

@@ -142,6 +142,9 @@ _SIGS = {
     "b200bsp_score_mi": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "b200bsp_regularize": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "b200bsp_regularize_f64": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "b200bsp_set_landmarks": (C.c_int, [_VP, _VP, C.c_int64, _VP, C.c_int64,
+                                        C.c_float]),
+    "b200bsp_landmarks_score": (C.c_int, [_VP, _VP, _VP, _VP]),
     "b200bsp_score": (C.c_int, [_VP, _VP, C.c_int, C.c_float, _VP, _VP, _VP,
                                 _VP, _VP]),
     "b200bsp_interpolate_vf": (C.c_int, [_VP, _VP, _VP]),
@@ -496,6 +499,25 @@ class Context:
         _check(lib().b200bsp_regularize_f64(self._h, _ptr(coeff),
                                             C.byref(parms), C.addressof(s),
                                             _ptr(g)), self._h)
+        return s.value, g
+
+    def set_landmarks(self, fixed_pts, moving_pts, stiffness=1.0):
+        """Landmark pairs (points in mm, one xyz row each) that score()
+        adds as stiffness * mean squared distance (b200bsp_set_landmarks);
+        empty lists remove them."""
+        f = np.ascontiguousarray(np.asarray(fixed_pts, np.float32).reshape(-1, 3))
+        m = np.ascontiguousarray(np.asarray(moving_pts, np.float32).reshape(-1, 3))
+        _check(lib().b200bsp_set_landmarks(self._h, _ptr(f), len(f), _ptr(m),
+                                           len(m), stiffness), self._h)
+        return self
+
+    def landmarks_score(self, coeff, grad=None):
+        """(lmetric, grad): grad accumulates the landmark gradient
+        (b200bsp_landmarks_score)."""
+        g = np.zeros(self.num_coeff, np.float32) if grad is None else grad
+        s = C.c_float()
+        _check(lib().b200bsp_landmarks_score(self._h, _ptr(coeff),
+                                             C.addressof(s), _ptr(g)), self._h)
         return s.value, g
 
     def score(self, coeff, metric="mse", lam=1.0, reg: RegParms | None = None):

@@ -107,4 +107,11 @@ cudaError_t launch_gather_grad (const BspGeom& g, const PartLayout& lay,
 cudaError_t launch_volume_grad (const int dim[3], const float spacing[3],
     const float inv_dc[9], const float* img, float* grad, cudaStream_t st);
 
+// Landmark term (landmarks.cu): n landmarks with tiles p[3n], q_lut rows
+// w[64n], fixed/moving xyz fm[6n]; scratch dc[4n]; ADDS the gradient into
+// grad and writes lmetric (device float).
+cudaError_t launch_landmarks (const BspGeom& g, int n, const int* p,
+    const float* w, const float* fm, const float* coeff, float grad_coeff,
+    float* dc, float* grad, float* lmetric, cudaStream_t st);
+
 } // namespace b200

@@ -31,6 +31,7 @@ namespace b200 {
 int static_fail (int code, const char* msg);   // runtime.cu
 cudaStream_t ctx_stream (const b200bsp_ctx* c); // runtime.cu
 void* ctx_opt_ws (const b200bsp_ctx* c);
+int ctx_landmarks (const b200bsp_ctx* c, float* stiffness);
 void ctx_set_opt_ws (b200bsp_ctx* c, void* ws, void (*release) (void*));
 
 constexpr int OPT_THREADS = 256;
@@ -571,8 +572,9 @@ lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
 
 // ---- objectives -----------------------------------------------------------
 
-// bspline_score() on the context: lambda * metric (+ regulariser), values
-// and gradients in float as the reference's Bspline_score holds them.
+// bspline_score() on the context: lambda * metric (+ regulariser, +
+// landmarks when the context has them), values and gradients in float as
+// the reference's Bspline_score holds them.
 struct ContextObjective : Objective {
     b200bsp_ctx* ctx;
     int metric;
@@ -614,6 +616,14 @@ struct ContextObjective : Objective {
             rc = b200bsp_regularize (ctx, coeff_f, reg, &r, grad_f);
             if (rc) return rc;
             total += r;
+        }
+        float stiffness = 0.f;
+        if (ctx_landmarks (ctx, &stiffness) > 0) {
+            // src/register/bspline.cxx:624-628
+            float lm = 0.f;
+            rc = b200bsp_landmarks_score (ctx, coeff_f, &lm, grad_f);
+            if (rc) return rc;
+            total += stiffness * lm;
         }
         to_double_kernel<<<grid, 256, 0, st>>> (grad_f, g, n);
         if (cudaGetLastError () != cudaSuccess) return B200BSP_E_CUDA;

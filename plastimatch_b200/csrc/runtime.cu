@@ -70,6 +70,14 @@ struct b200bsp_ctx {
     MiState mi;
     RegState reg;
 
+    // landmark pairs (b200bsp_set_landmarks)
+    int lm_n = 0;
+    float lm_stiffness = 1.f;
+    int* d_lm_p = nullptr;            // tile of each fixed landmark [3n]
+    float* d_lm_w = nullptr;          // its q_lut row [64n]
+    float* d_lm_fm = nullptr;         // fixed xyz, moving xyz [6n]
+    float* d_lm_dc = nullptr;         // dc/dv + squared distance [4n], lmetric
+
     bool timing = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     float last_total_ms = 0.f, last_main_ms = 0.f;
@@ -235,6 +243,8 @@ free_all (b200bsp_ctx* c)
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
     cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
     cudaFree (c->d_qlut); cudaFree (c->d_inv_dc);
+    cudaFree (c->d_lm_p); cudaFree (c->d_lm_w); cudaFree (c->d_lm_fm);
+    cudaFree (c->d_lm_dc);
     cudaFreeHost (c->h_res); cudaFreeHost (c->h_scalar);
     mi_free (&c->mi);
     reg_free (&c->reg);
@@ -322,6 +332,15 @@ int
 ctx_device (const b200bsp_ctx* c)
 {
     return c->device;
+}
+
+// Landmark count (0: none set) and stiffness, for the optimiser's
+// objective.
+int
+ctx_landmarks (const b200bsp_ctx* c, float* stiffness)
+{
+    if (stiffness) *stiffness = c->lm_stiffness;
+    return c->lm_n;
 }
 
 // The optimiser's workspace slot: kept by the context, freed with it.
@@ -1062,6 +1081,167 @@ b200bsp_regularize_f64 (b200bsp_ctx* c, const float* coeff,
     return regularize (c, coeff, parms, rmetric, grad);
 }
 
+// One axis of a q_lut row as Bspline_xform::allocate builds it
+// (src/base/bspline_xform.cxx:378-430): float offset, double polynomial,
+// rounded to float.
+static void
+qlut_axis (float out[4], int64_t i, int64_t vpr)
+{
+    const float ii = ((float) i) / vpr;
+    const float t3 = ii * ii * ii, t2 = ii * ii, t1 = ii;
+    out[0] = (float) ((1.0/6.0) * (- 1.0 * t3 + 3.0 * t2 - 3.0 * t1 + 1.0));
+    out[1] = (float) ((1.0/6.0) * (+ 3.0 * t3 - 6.0 * t2 + 4.0));
+    out[2] = (float) ((1.0/6.0) * (- 3.0 * t3 + 3.0 * t2 + 3.0 * t1 + 1.0));
+    out[3] = (float) ((1.0/6.0) * (+ 1.0 * t3));
+}
+
+static void
+free_landmarks (b200bsp_ctx* c)
+{
+    cudaFree (c->d_lm_p); cudaFree (c->d_lm_w); cudaFree (c->d_lm_fm);
+    cudaFree (c->d_lm_dc);
+    c->d_lm_p = nullptr; c->d_lm_w = nullptr; c->d_lm_fm = nullptr;
+    c->d_lm_dc = nullptr;
+    c->lm_n = 0;
+}
+
+extern "C" int
+b200bsp_set_landmarks (b200bsp_ctx* c, const float* fixed_xyz,
+    int64_t n_fixed, const float* moving_xyz, int64_t n_moving,
+    float stiffness)
+{
+    if (!c) return B200BSP_E_BADARG;
+    CK (cudaSetDevice (c->device));
+    // Bspline_landmarks::set_landmarks: the shorter list sets the count
+    const int64_t n = n_fixed < n_moving ? n_fixed : n_moving;
+    if (n <= 0) {
+        CK (cudaStreamSynchronize (c->stream));
+        free_landmarks (c);
+        return B200BSP_OK;
+    }
+    if (!fixed_xyz || !moving_xyz) {
+        return fail (c, B200BSP_E_BADARG, "null landmark list");
+    }
+    if (n > (1 << 24)) {
+        return fail (c, B200BSP_E_BADARG, "at most 2^24 landmarks");
+    }
+    // Bspline_landmarks::initialize (src/register/bspline_landmarks.cxx:
+    // 150-204): grid coordinates of each fixed landmark, in float, through
+    // the fixed image's projection matrix; the voxel index truncates
+    // toward zero and must lie inside the image.
+    float inv[9], proj[9];
+    if (!inv3f (inv, c->fixed.dcos)) {
+        return fail (c, B200BSP_E_BADARG, "singular direction cosines");
+    }
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            proj[3*i+j] = inv[3*i+j] / c->fixed.spacing[i];
+        }
+    }
+    const BspGeom& g = c->geom;
+    std::vector<int> hp ((size_t) 3 * n);
+    std::vector<float> hw ((size_t) 64 * n), hfm ((size_t) 6 * n);
+    for (int64_t l = 0; l < n; l++) {
+        float xyz[3];
+        for (int d = 0; d < 3; d++) {
+            xyz[d] = fixed_xyz[3*l+d] - c->fixed.origin[d];
+        }
+        int64_t q[3];
+        for (int d = 0; d < 3; d++) {
+            const float ijk = xyz[0] * proj[3*d+0] + xyz[1] * proj[3*d+1]
+                + xyz[2] * proj[3*d+2];
+            // (the range test first: the cast is defined only in range)
+            const bool in = ijk > -1.f && ijk < (float) c->fixed.dim[d];
+            const int64_t v = in ? (int64_t) ijk : -1;
+            if (v < 0 || v >= c->fixed.dim[d]) {
+                free_landmarks (c);
+                return fail (c, B200BSP_E_BADARG,
+                    "fixed landmark %lld outside of the fixed image",
+                    (long long) l);
+            }
+            hp[3*l+d] = (int) (v / g.vpr[d]);
+            q[d] = v % g.vpr[d];
+            // The reference takes the tile from the absolute voxel index;
+            // it must be one of the grid's tiles.
+            if (hp[3*l+d] >= g.rdims[d]) {
+                free_landmarks (c);
+                return fail (c, B200BSP_E_UNSUPPORTED,
+                    "fixed landmark %lld lies beyond the grid's tiles",
+                    (long long) l);
+            }
+        }
+        float A[4], B[4], C[4];
+        qlut_axis (A, q[0], g.vpr[0]);
+        qlut_axis (B, q[1], g.vpr[1]);
+        qlut_axis (C, q[2], g.vpr[2]);
+        for (int tz = 0; tz < 4; tz++)
+            for (int ty = 0; ty < 4; ty++)
+                for (int tx = 0; tx < 4; tx++)
+                    hw[64*l + 16*tz + 4*ty + tx] = A[tx] * B[ty] * C[tz];
+        for (int d = 0; d < 3; d++) {
+            hfm[6*l+d] = fixed_xyz[3*l+d];
+            hfm[6*l+3+d] = moving_xyz[3*l+d];
+        }
+    }
+    CK (cudaStreamSynchronize (c->stream));
+    free_landmarks (c);
+    CK (cudaMalloc ((void**) &c->d_lm_p, hp.size () * sizeof (int)));
+    CK (cudaMalloc ((void**) &c->d_lm_w, hw.size () * sizeof (float)));
+    CK (cudaMalloc ((void**) &c->d_lm_fm, hfm.size () * sizeof (float)));
+    CK (cudaMalloc ((void**) &c->d_lm_dc, (4 * n + 1) * sizeof (float)));
+    CK (cudaMemcpy (c->d_lm_p, hp.data (), hp.size () * sizeof (int),
+        cudaMemcpyHostToDevice));
+    CK (cudaMemcpy (c->d_lm_w, hw.data (), hw.size () * sizeof (float),
+        cudaMemcpyHostToDevice));
+    CK (cudaMemcpy (c->d_lm_fm, hfm.data (), hfm.size () * sizeof (float),
+        cudaMemcpyHostToDevice));
+    c->lm_n = (int) n;
+    c->lm_stiffness = stiffness;
+    return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_landmarks_score (b200bsp_ctx* c, const float* coeff, float* lmetric,
+    float* grad)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (c->lm_n < 1) return fail (c, B200BSP_E_STATE, "no landmarks set");
+    if (!coeff) return fail (c, B200BSP_E_BADARG, "null coefficients");
+    CK (cudaSetDevice (c->device));
+    const float* dcoeff = coeff;
+    if (!is_device_ptr (coeff)) {
+        CK (cudaMemcpyAsync (c->d_coeff, coeff, c->num_coeff * sizeof (float),
+            cudaMemcpyHostToDevice, c->stream));
+        dcoeff = c->d_coeff;
+    }
+    const bool dev_grad = is_device_ptr (grad);
+    float* g_dev = dev_grad ? grad : c->d_grad;
+    if (grad && !dev_grad) {
+        CK (cudaMemcpyAsync (c->d_grad, grad, c->num_coeff * sizeof (float),
+            cudaMemcpyHostToDevice, c->stream));
+    } else if (!grad) {
+        CK (cudaMemsetAsync (c->d_grad, 0, c->num_coeff * sizeof (float),
+            c->stream));
+    }
+    // land_grad_coeff = landmark_stiffness / num_landmarks, in float
+    const float grad_coeff = c->lm_stiffness / (float) c->lm_n;
+    float* d_lmetric = c->d_lm_dc + 4 * (size_t) c->lm_n;
+    CK (launch_landmarks (c->geom, c->lm_n, c->d_lm_p, c->d_lm_w,
+        c->d_lm_fm, dcoeff, grad_coeff, c->d_lm_dc, g_dev, d_lmetric,
+        c->stream));
+    if (grad && !dev_grad) {
+        CK (cudaMemcpyAsync (grad, c->d_grad, c->num_coeff * sizeof (float),
+            cudaMemcpyDeviceToHost, c->stream));
+    }
+    float lm = 0.f;
+    CK (cudaMemcpyAsync (c->h_scalar, d_lmetric, sizeof (float),
+        cudaMemcpyDeviceToHost, c->stream));
+    CK (cudaStreamSynchronize (c->stream));
+    lm = *c->h_scalar;
+    if (lmetric) *lmetric = lm;
+    return B200BSP_OK;
+}
+
 extern "C" int
 b200bsp_score (b200bsp_ctx* c, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
@@ -1085,6 +1265,13 @@ b200bsp_score (b200bsp_ctx* c, const float* coeff, int metric_type,
         rc = b200bsp_regularize (c, coeff, reg, &r, g.data ());
         if (rc) return rc;
         total += r;
+    }
+    if (c->lm_n > 0) {
+        // landmark score and gradient (src/register/bspline.cxx:624-628)
+        float lm = 0.f;
+        rc = b200bsp_landmarks_score (c, coeff, &lm, g.data ());
+        if (rc) return rc;
+        total += c->lm_stiffness * lm;
     }
     if (is_device_ptr (total_grad)) {
         CK (cudaMemcpy (total_grad, g.data (), c->num_coeff * sizeof (float),

@@ -75,6 +75,27 @@ RESAMPLE_CASES = {
 }
 
 
+# Landmark fixtures: the inputs of an MSE case, landmark pairs (spread,
+# clustered so that landmarks share knots, and inside the first half voxel,
+# which truncates to index 0) and the reference's landmark term alone and
+# its whole bspline_score (MSE flavour g + curvature 0.005 + landmarks).
+LANDMARK_CASES = {"landmarks_small": ("mse_small", 0.8, 17),
+                  "landmarks_dcos": ("mse_dcos", 2.5, 23)}
+
+
+def landmark_points(fixed, n, seed):
+    rng = np.random.default_rng(seed)
+    dim = np.array(fixed.dim, np.float64)
+    ijk = rng.uniform(0.0, 1.0, (n, 3)) * (dim - 1.0)
+    ijk[: n // 4] = dim / 2 + rng.uniform(-1.5, 1.5, (n // 4, 3))
+    ijk[n // 4] = (-0.4, -0.3, -0.2)
+    dc = np.array(fixed.dcos, np.float64).reshape(3, 3)
+    step = dc * np.array(fixed.spacing, np.float64)[None, :]
+    f = (np.array(fixed.origin, np.float64) + ijk @ step.T).astype(np.float32)
+    m = (f + rng.normal(0.0, 1.5, f.shape)).astype(np.float32)
+    return f, m
+
+
 def resample_input():
     v = synth.gaussian_blobs((37, 30, 23), spacing=(0.9, 1.1, 2.5), seed=71)
     return Volume(v.img, origin=(-11.3, 4.2, 7.7), spacing=v.spacing)
@@ -150,6 +171,37 @@ def main(force=False):
             rec["warped"], rec["warp_vf"] = O.ref_warp(grid, fixed, moving,
                                                        coeff, WARP_DEFAULT)
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **rec)
+        print("wrote", name)
+
+    for name, (base, stiffness, n) in LANDMARK_CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
+        dim, sp, vpr, roff, rdim, seed, dcos, remap, csig = CASES[base]
+        fixed, moving = make_pair(dim, sp, seed, dcos, remap)
+        grid = BsplineGrid.for_volume(fixed, vpr, roi_offset=roff,
+                                      roi_dim=rdim)
+        coeff = synth.random_coeff(grid, csig, seed=seed + 3)
+        fpts, mpts = landmark_points(fixed, n, seed + 4)
+        rl = O.ref_landmarks(grid, fixed, coeff, fpts, mpts, stiffness)
+        rt = O.ref_score(grid, fixed, moving, coeff, flavor="g",
+                         reg_impl="c", curvature=0.005)
+        rs = O.ref_score_landmarks(grid, fixed, moving, coeff, fpts, mpts,
+                                   stiffness, flavor="g", reg_impl="c",
+                                   curvature=0.005)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            fixed=fixed.img, moving=moving.img,
+            f_origin=np.array(fixed.origin, np.float32),
+            f_spacing=np.array(fixed.spacing, np.float32),
+            m_origin=np.array(moving.origin, np.float32),
+            m_spacing=np.array(moving.spacing, np.float32),
+            dcos=np.array(fixed.dcos, np.float32),
+            roi_offset=np.array(grid.roi_offset), roi_dim=np.array(grid.roi_dim),
+            vpr=np.array(grid.vox_per_rgn), coeff=coeff,
+            fixed_pts=fpts, moving_pts=mpts, stiffness=np.float32(stiffness),
+            lm_score=np.float32(rl.score), lm_grad=rl.grad,
+            total_score=np.float32(rt.score), total_grad=rt.grad,
+            total_lm_score=np.float32(rs.score), total_lm_grad=rs.grad)
         print("wrote", name)
 
     for name, (mode, rate) in RESAMPLE_CASES.items():
