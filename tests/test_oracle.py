@@ -30,6 +30,22 @@ def test_port_mse_o_bit_exact(name):
     np.testing.assert_array_equal(r.grad, rec["o_grad"])
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built")
+@pytest.mark.parametrize("flavor", ["p", "q", "r"])
+@pytest.mark.parametrize("name", [n for n in golden_names("mse") if n != "mse_roi"])
+def test_reference_flavours_pqr_equal_o(name, flavor):
+    """The reference's flavours p, q and r compute flavour o's MSE (the
+    exact trilinear-derivative gradient) and differ from it only in the
+    order of float sums: same voxel count, score within 1e-6 relative,
+    gradient within 1e-5 relative (L2).  The restatement of o therefore
+    checks all four."""
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.ref_metric(grid, fixed, moving, coeff, flavor=flavor)
+    assert r.num_vox == rec["o_num_vox"]
+    assert abs(r.score - rec["o_score"]) <= 1e-6 * abs(rec["o_score"])
+    assert rel_err(r.grad, rec["o_grad"]) < 1e-5
+
+
 @pytest.mark.parametrize("name", golden_names("mse"))
 def test_port_mse_f64_close(name):
     fixed, moving, grid, coeff, rec = load_golden(name)
