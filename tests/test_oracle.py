@@ -46,6 +46,25 @@ def test_reference_flavours_pqr_equal_o(name, flavor):
     assert rel_err(r.grad, rec["o_grad"]) < 1e-5
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built")
+@pytest.mark.parametrize("name", golden_names("mi"))
+def test_reference_mi_flavours_equal_g(name):
+    """The reference's MI flavours compute flavour g's PVI-8 MI: same score
+    and voxel count, gradient within 1e-5 relative (L2), so the device's
+    g semantics stand for them.  Exception: d, e, f and i ignore the
+    direction cosines and differ from g (and from the others) on rotated
+    grids."""
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    rotated = not np.allclose(np.asarray(fixed.dcos).reshape(3, 3), np.eye(3))
+    for flavor in "cdefhikl":
+        r = O.ref_metric(grid, fixed, moving, coeff, flavor=flavor,
+                         metric="mi", bins=32)
+        same = np.float32(r.score) == rec["mi_score"] \
+            and r.num_vox == rec["mi_num_vox"] \
+            and rel_err(r.grad, rec["mi_grad"]) < 1e-5
+        assert same != (rotated and flavor in "defi"), flavor
+
+
 @pytest.mark.parametrize("name", golden_names("mse"))
 def test_port_mse_f64_close(name):
     fixed, moving, grid, coeff, rec = load_golden(name)
