@@ -47,6 +47,17 @@ def test_reference_flavours_pqr_equal_o(name, flavor):
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference not built")
+@pytest.mark.parametrize("name", [n for n in golden_names("mse") if n != "mse_roi"])
+def test_reference_flavour_k_equals_c(name):
+    """MSE flavour k is flavour c bit for bit (same voxel-serial sums)."""
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    r = O.ref_metric(grid, fixed, moving, coeff, flavor="k")
+    assert np.float32(r.score) == rec["c_score"]
+    assert r.num_vox == rec["c_num_vox"]
+    np.testing.assert_array_equal(r.grad, rec["c_grad"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built")
 @pytest.mark.parametrize("name", golden_names("mi"))
 def test_reference_mi_flavours_equal_g(name):
     """The reference's MI flavours compute flavour g's PVI-8 MI: same score
