@@ -17,6 +17,14 @@ e2e     the same evaluation through the public C ABI with host (pinned)
         buffers: coefficient upload, kernels, gradient + score download.
 N > 1   independent replicas, one per GPU (weak scaling, no collective on
         the data path); max device time over ranks.
+fp32_form / tc_over_fp32
+        the other device form (plain FP32 SIMT) timed the same way in the
+        same run, its fraction of the FP32 FMA peak, and the tensor-core
+        form's speed-up over it (device and end to end).
+accuracy
+        score and gradient relative error of the timed form's evaluation
+        against the double-precision oracle and the reference's own float
+        flavour g on the same inputs (after the timed region).
 """
 from __future__ import annotations
 
@@ -40,6 +48,8 @@ WORKLOAD = {"workload": "mse_score_grad_256x256x128_vpr5",
             "content": "CT-like int16 phantom (body/lung/bone ellipsoids + N(0,20))",
             "gradient": "nearest-voxel moving gradient (reference flavour g)"}
 ALGO_BYTES_PER_VOXEL = 20   # fixed f32 + moving f32 + moving gradient 3xf32
+# forward field 2*64*3 + adjoint 2*64*3 + trilinear, difference and dc/dv
+ALGO_FLOP_PER_VOXEL = 808
 
 
 def make_workload(seed=20261205):
@@ -425,6 +435,139 @@ def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
     return out
 
 
+def measure_form(P, form, args, workload, local_rank, dist, flush):
+    """Device and end-to-end throughput of one form on the workload.
+
+    Returns a dict: device ms per evaluation (CUDA events on the context's
+    stream, L2 flushed before every step and excluded, max over ranks),
+    end-to-end ms through the C ABI with pinned host buffers, the tile
+    kernel's own ms (the library's events, median of three probes), the
+    launches per evaluation, the autotuned tiles per batch, and the last
+    evaluation's score, gradient and voxel count (host copies)."""
+    import ctypes as C
+    import torch
+    fixed, moving, grid, coeff = workload
+    dev = f"cuda:{local_rank}"
+    ctx = P.Context(fixed, moving, grid, form=form, device=local_rank)
+    stream = torch.cuda.Stream(device=local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_images()
+    # the library's batch-split autotuner (setup, like a GEMM heuristic),
+    # before any timing
+    tiles = ctx.autotune(coeff, evals=3) if form == "tc" else None
+    d_coeff = torch.from_numpy(coeff).to(dev)
+    d_grad = torch.zeros(grid.num_coeff, device=dev)
+    d_score = torch.zeros(1, device=dev)
+    d_nvox = torch.zeros(1, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        ctx.score_mse(d_coeff, grad_out=d_grad, score_out=d_score,
+                      nvox_out=d_nvox)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.fill_(1)
+                ev[i][0].record(stream)
+                step()
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    t = torch.tensor([dev_ms], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms = float(t.item())
+
+    # per-evaluation main-kernel time (library events on the same stream;
+    # the instrumentation is on for these probes only)
+    main_ms = []
+    ctx.enable_timing(True)
+    for _ in range(3):
+        flush.fill_(1)
+        stream.synchronize()
+        s_h, g_h, n_h = ctx.score_mse(d_coeff)
+        _, m_ms, launches = ctx.last_timing()
+        main_ms.append(m_ms)
+    ctx.enable_timing(False)
+
+    # end to end through the C ABI with pinned host buffers
+    h_coeff = torch.from_numpy(coeff).pin_memory()
+    h_grad = torch.zeros(grid.num_coeff).pin_memory()
+    lib = P.lib()
+    s_c = C.c_float()
+    n_c = C.c_int64()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rc = lib.b200bsp_score_mse(ctx._h, h_coeff.data_ptr(),
+                                   C.addressof(s_c), h_grad.data_ptr(),
+                                   C.addressof(n_c))
+        b.record(stream)
+        b.synchronize()
+        if rc:
+            raise RuntimeError(lib.b200bsp_last_error(ctx._h))
+        if i >= args.warmup:
+            e2e.append(a.elapsed_time(b))
+    e2e_ms = float(np.mean(e2e))
+    t = torch.tensor([e2e_ms], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    return {"ctx": ctx, "stream": stream, "d_coeff": d_coeff,
+            "d_grad": d_grad, "dev_ms": dev_ms, "e2e_ms": e2e_ms,
+            "kernel_ms": float(np.median(main_ms)), "launches": launches,
+            "tiles": tiles, "score": s_h, "grad": g_h, "num_vox": n_h,
+            "clocks": clk.summary()}
+
+
+def accuracy_block(workload, score, grad, num_vox, threads):
+    """Score and gradient relative error of a device evaluation against the
+    double-precision oracle and against the reference's own float flavour
+    g on the same inputs (computed after the timed region)."""
+    import oracle as O
+    fixed, moving, grid, coeff = workload
+    mg = O.port_volume_grad(moving)
+    f64 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg,
+                     precision="f64")
+
+    def rel(a, b):
+        a = np.asarray(a, np.float64)
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    out = {"vs_fp64_oracle": {
+               "score_rel": abs(score - f64.score) / abs(f64.score),
+               "grad_rel_l2": rel(grad, f64.grad),
+               "num_vox": int(f64.num_vox)},
+           "bars": {"score_rel": 1e-5, "grad_rel_l2": 1e-3}}
+    if O.ref_available():
+        r = O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                         threads=threads)
+        out["vs_reference_flavour_g"] = {
+            "score_rel": abs(score - r.score) / abs(r.score),
+            "grad_rel_l2": rel(grad, r.grad),
+            "num_vox": int(r.num_vox)}
+    out["device_num_vox"] = int(num_vox)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -434,6 +577,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-evals", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip also_measured (regulariser, MI, the "
+                         "registration workloads)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -456,95 +602,24 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    fixed, moving, grid, coeff = make_workload()
-    ctx = P.Context(fixed, moving, grid, form=args.form, device=local_rank)
-    stream = torch.cuda.Stream(device=local_rank)
-    ctx.set_stream(stream.cuda_stream)
-    ctx.set_images()
-    # the library's batch-split autotuner (setup, like a GEMM heuristic),
-    # before any timing
-    tiles = ctx.autotune(coeff, evals=3) if args.form == "tc" else None
-
-    d_coeff = torch.from_numpy(coeff).to(f"cuda:{local_rank}")
-    d_grad = torch.zeros(grid.num_coeff, device=f"cuda:{local_rank}")
-    d_score = torch.zeros(1, device=f"cuda:{local_rank}")
-    d_nvox = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local_rank}")
+    workload = make_workload()
+    fixed, moving, grid, coeff = workload
     flush = torch.empty(256 << 20, dtype=torch.uint8,
                         device=f"cuda:{local_rank}")
-    torch.cuda.synchronize()
+    m = measure_form(P, args.form, args, workload, local_rank, dist, flush)
+    ctx, stream = m["ctx"], m["stream"]
+    # the other form, timed the same way in the same run (the metric's
+    # comparison); replicas time it too so every rank takes the same
+    # collective steps
+    other = "fp32" if args.form == "tc" else "tc"
+    mo = measure_form(P, other, args, workload, local_rank, dist, flush)
+    mo["ctx"].close()
 
-    def step():
-        ctx.score_mse(d_coeff, grad_out=d_grad, score_out=d_score,
-                      nvox_out=d_nvox)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            flush.fill_(1)
-            step()
-    torch.cuda.synchronize()
-
-    ev = [(torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    main_ms = []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        with torch.cuda.stream(stream):
-            for i in range(args.steps):
-                flush.fill_(1)
-                ev[i][0].record(stream)
-                step()
-                ev[i][1].record(stream)
-        torch.cuda.synchronize()
-        # per-evaluation main-kernel time (library events on the same
-        # stream; the instrumentation is on for these probes only)
-        ctx.enable_timing(True)
-        for _ in range(3):
-            flush.fill_(1)
-            stream.synchronize()
-            s_h, g_h, n_h = ctx.score_mse(d_coeff)
-            _, m_ms, launches = ctx.last_timing()
-            main_ms.append(m_ms)
-        ctx.enable_timing(False)
-    if dist:
-        dist.barrier()
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
-    t = torch.tensor([dev_ms], device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_ms = float(t.item())
-
-    # end to end through the C ABI with pinned host buffers
-    h_coeff = torch.from_numpy(coeff).pin_memory()
-    h_grad = torch.zeros(grid.num_coeff).pin_memory()
-    import ctypes as C
-    lib = P.lib()
-    s_c = C.c_float()
-    n_c = C.c_int64()
-    e2e = []
-    for i in range(args.warmup + args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        rc = lib.b200bsp_score_mse(ctx._h, h_coeff.data_ptr(), C.addressof(s_c),
-                                   h_grad.data_ptr(), C.addressof(n_c))
-        b.record(stream)
-        b.synchronize()
-        if rc:
-            raise RuntimeError(P.lib().b200bsp_last_error(ctx._h))
-        if i >= args.warmup:
-            e2e.append(a.elapsed_time(b))
-    e2e_ms = float(np.mean(e2e))
-    t = torch.tensor([e2e_ms], device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item())
-
-    extra = extra_metrics(P, ctx, stream, flush, d_coeff, d_grad,
-                          grid.num_roi_voxels, args.warmup)
-    if rank == 0 and world == 1:
+    extra = {}
+    if not args.no_extra:
+        extra = extra_metrics(P, ctx, stream, flush, m["d_coeff"],
+                              m["d_grad"], grid.num_roi_voxels, args.warmup)
+    if rank == 0 and world == 1 and not args.no_extra:
         # one-GPU workloads, measured at N = 1 only (the other ranks would
         # idle meanwhile); the device-only ones first: the reference's
         # OpenMP threads (registration_c1's CPU leg) keep host cores busy
@@ -557,11 +632,41 @@ def main():
             P, not args.no_cpu_baseline and world == 1)
 
     nvox = grid.num_roi_voxels
-    value = world * nvox / (dev_ms * 1e-3) / 1e9
-    e2e_value = world * nvox / (e2e_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    main = float(np.median(main_ms))
-    achieved = ALGO_BYTES_PER_VOXEL * nvox / (main * 1e-3) / 1e9
+
+    def summary(r, form):
+        value = world * nvox / (r["dev_ms"] * 1e-3) / 1e9
+        e2e_value = world * nvox / (r["e2e_ms"] * 1e-3) / 1e9
+        achieved = ALGO_BYTES_PER_VOXEL * nvox / (r["kernel_ms"] * 1e-3) / 1e9
+        return value, e2e_value, {
+            "bound": "hbm", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak,
+            "traffic": profile_traffic(form), "peak_source": peak_kind,
+            "kernel_ms": r["kernel_ms"],
+            "algorithmic_bytes_per_launch": ALGO_BYTES_PER_VOXEL * nvox}
+
+    value, e2e_value, roofline = summary(m, args.form)
+    o_value, o_e2e, o_roof = summary(mo, other)
+    props = torch.cuda.get_device_properties(local_rank)
+    clk = m["clocks"]
+    sm_mhz = clk.get("sm_max_mhz") or 1965.0
+    # FP32 FMA peak at the sampled maximum SM clock: SMs x 128 lanes x 2
+    fp32_peak = props.multi_processor_count * 128 * 2 * sm_mhz * 1e6 / 1e12
+    fp32_r = m if args.form == "fp32" else mo
+    fp32_tflops = ALGO_FLOP_PER_VOXEL * nvox / (fp32_r["kernel_ms"] * 1e-3) / 1e12
+    other_block = {"form": other, "value": o_value, "unit": "Gvox/s",
+                   "ms_per_step": mo["dev_ms"],
+                   "e2e": {"value": o_e2e, "unit": "Gvox/s"},
+                   "kernel_ms": mo["kernel_ms"], "roofline": o_roof}
+    if other == "fp32":
+        other_block["fma"] = {
+            "achieved_tflops": fp32_tflops, "peak_tflops": fp32_peak,
+            "frac": fp32_tflops / fp32_peak,
+            "flop_per_voxel": ALGO_FLOP_PER_VOXEL,
+            "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock"}
+    tc_v, fp_v = (value, o_value) if args.form == "tc" else (o_value, value)
+    tc_e, fp_e = ((e2e_value, o_e2e) if args.form == "tc"
+                  else (o_e2e, e2e_value))
     out = None
     if rank == 0:
         cpu = None
@@ -572,13 +677,15 @@ def main():
                    "kind": kind,
                    "sample": f"{args.cpu_evals} full evaluations of the same "
                              "256x256x128 workload (median)"}
-            extra["cpu_reference_other_paths"] = cpu_reference_others(
-                fixed, moving, grid, coeff, host_threads())
-        traffic = profile_traffic(args.form)
+            if not args.no_extra:
+                extra["cpu_reference_other_paths"] = cpu_reference_others(
+                    fixed, moving, grid, coeff, host_threads())
+        acc = accuracy_block(workload, m["score"], m["grad"], m["num_vox"],
+                             host_threads())
         out = {
             "metric": METRIC, "value": value, "unit": "Gvox/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_ms, "higher_is_better": True,
+            "ms_per_step": m["dev_ms"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": dict(WORKLOAD, form=args.form,
@@ -589,21 +696,20 @@ def main():
                            l2="inputs 167 MB > L2 and 256 MiB flush write "
                               "before every timed step (excluded)",
                            parallelism=f"replicas x{world}",
-                           tiles_per_batch=tiles),
+                           tiles_per_batch=m["tiles"]),
             "e2e": {"value": e2e_value, "unit": "Gvox/s",
                     "h2d_bytes_per_step": 4 * grid.num_coeff,
                     "d2h_bytes_per_step": 4 * grid.num_coeff + 32},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": peak_kind,
-                         "kernel_ms": main,
-                         "algorithmic_bytes_per_launch":
-                             ALGO_BYTES_PER_VOXEL * nvox},
+            "roofline": roofline,
+            "accuracy": acc,
+            ("fp32_form" if other == "fp32" else "tc_form"): other_block,
+            "tc_over_fp32": {"value": tc_v / fp_v, "e2e": tc_e / fp_e,
+                             "target": 5.0},
             "cpu_baseline": cpu,
             "also_measured": extra,
-            "gpu_launches": launches * args.steps,
-            "clocks": clk.summary(),
-            "score": s_h, "num_vox": n_h,
+            "gpu_launches": m["launches"] * args.steps,
+            "clocks": clk,
+            "score": m["score"], "num_vox": m["num_vox"],
         }
         print(json.dumps(out), flush=True)
     ctx.close()

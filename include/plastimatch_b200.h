@@ -76,7 +76,11 @@ typedef struct {
     int mi_bins;        /* fixed and moving histogram bins (reference default 32) */
     int device;         /* CUDA device ordinal */
     int mi_window;      /* B200BSP_MI_* (0: the reference's PVI-8) */
-    int reserved[3];    /* zero */
+    int wait_limit;     /* polls before a device-side wait of the tensor-core
+                           MSE kernel gives up with B200BSP_E_TIMEOUT
+                           (0: the default, 1 << 22) */
+    int mi_hist;        /* B200BSP_MI_HIST_* (0: equal spacing) */
+    int reserved;       /* zero */
 } b200bsp_opts;
 
 /* Mattes MI histogram windows: PVI-8 partial-volume binning (the
@@ -86,6 +90,16 @@ typedef struct {
  * each image's value range maps onto bins 2 .. mi_bins - 2. */
 #define B200BSP_MI_PVI8    0
 #define B200BSP_MI_PARZEN  1
+
+/* PVI-8 histogram bins (Bspline_parms::mi_hist_type,
+ * src/register/histogram.h:14-17): equal spacing over each image's value
+ * range (bspline_initialize_mi_hist_eqsp, joint_histogram.cxx:115-139) or
+ * V-optimal bins (bspline_initialize_mi_hist_vopt, :195-324; the image is
+ * read back to the host once in b200bsp_set_images for its dynamic
+ * programme).  V-optimal needs mi_bins <= 1000; the reference falls back
+ * to equal spacing above that (B200BSP_E_BADARG here). */
+#define B200BSP_MI_HIST_EQSP  0
+#define B200BSP_MI_HIST_VOPT  1
 
 /* Regularisation weights of Regularization_parms
  * (src/register/regularization_parms.h:16-43). */
@@ -201,6 +215,22 @@ int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
 int b200bsp_set_landmarks (b200bsp_ctx* ctx, const float* fixed_xyz,
     int64_t n_fixed, const float* moving_xyz, int64_t n_moving,
     float stiffness);
+
+/* Image ROIs of the cost function: Bspline_state::fixed_roi and
+ * ::moving_roi (src/register/bspline_state.h:44-45), uchar mask volumes
+ * (x fastest, nonzero = inside) with their own geometry.  A fixed voxel
+ * counts only where the fixed ROI holds at its position, and a moving
+ * position only where the moving ROI holds there (inside_roi and
+ * bspline_find_correspondence_dcos_roi, src/util/bspline_correspond.cxx:
+ * 52-145) -- the reference's ROI flavours (MSE i, bspline_mse.cxx:82-288;
+ * MI h, bspline_mi.cxx:1232-1504).  Either pair (geometry, mask) may be
+ * NULL for none; masks are host or device memory.  Replaces the previous
+ * ROIs; all four NULL removes them.  Allocates device memory for the masks
+ * (kept until the next call or b200bsp_destroy).  MI with ROIs runs on the
+ * FP32 tile passes in either form. */
+int b200bsp_set_roi (b200bsp_ctx* ctx, const b200bsp_volume* fixed_roi,
+    const uint8_t* fixed_mask, const b200bsp_volume* moving_roi,
+    const uint8_t* moving_mask);
 
 /* The landmark term alone, bspline_landmarks_score_a
  * (src/register/bspline_landmarks.cxx:25-134): lmetric = the mean squared

@@ -54,7 +54,8 @@ class OrcGrid(C.Structure):
 
 class OrcHist(C.Structure):
     _fields_ = [("bins", C.c_int64), ("offset", C.c_float),
-                ("delta", C.c_float)]
+                ("delta", C.c_float), ("keys", C.c_int64),
+                ("key_lut", C.POINTER(C.c_int32))]
 
 
 class OrcParzen(C.Structure):
@@ -121,6 +122,37 @@ def ref():
 
 # ---------------------------------------------------------------- port ---
 
+class OrcRoi(C.Structure):
+    _fields_ = [("vol", OrcVol), ("mask", C.POINTER(C.c_uint8))]
+
+
+class _RoiScope:
+    """orc_set_roi for the duration of one oracle call (ROIs are
+    plastimatch_b200.geometry.Roi or None)."""
+
+    def __init__(self, fixed_roi, moving_roi):
+        self.keep = []
+        self.f = self._mk(fixed_roi)
+        self.m = self._mk(moving_roi)
+
+    def _mk(self, roi):
+        if roi is None:
+            return None
+        r = OrcRoi()
+        r.vol = orc_vol(roi)
+        r.mask = roi.mask.ctypes.data_as(C.POINTER(C.c_uint8))
+        self.keep.append(roi.mask)
+        return r
+
+    def __enter__(self):
+        port().orc_set_roi(C.byref(self.f) if self.f else None,
+                           C.byref(self.m) if self.m else None)
+        return self
+
+    def __exit__(self, *a):
+        port().orc_set_roi(None, None)
+
+
 def orc_vol(v) -> OrcVol:
     o = OrcVol()
     d = (C.c_int64 * 3)(*v.dim)
@@ -156,7 +188,14 @@ def port_basis_lut(vpr: int) -> np.ndarray:
 
 
 def port_mse(grid, fixed, moving, coeff, moving_grad=None, grad_mode=0,
-             precision="f32") -> Result:
+             precision="f32", fixed_roi=None, moving_roi=None) -> Result:
+    """MSE flavour g (nearest-voxel gradient, grad_mode 0) or o (trilinear
+    derivative, 1) in float, or both in double; with image ROIs, flavour
+    i's ROI tests."""
+    if fixed_roi is not None or moving_roi is not None:
+        with _RoiScope(fixed_roi, moving_roi):
+            return port_mse(grid, fixed, moving, coeff, moving_grad,
+                            grad_mode, precision)
     if moving_grad is None and grad_mode == 0:
         moving_grad = port_volume_grad(moving)
     g = orc_grid(grid, fixed)
@@ -190,9 +229,34 @@ def port_hist_eqsp(img: np.ndarray, bins: int) -> OrcHist:
     return h
 
 
-def port_mi(grid, fixed, moving, coeff, bins=32, precision="f32") -> Result:
+def port_hist_vopt(img: np.ndarray, bins: int) -> OrcHist:
+    """V-optimal histogram parameters; the key table lives on the returned
+    object (h._lut) for as long as it does."""
+    h = OrcHist(bins, 0.0, 0.0)
+    lut = np.zeros(1000, np.int32)
+    a = np.ascontiguousarray(img, np.float32).ravel()
+    port().orc_hist_vopt(C.byref(h), lut.ctypes.data_as(C.POINTER(C.c_int32)),
+                         _p(a), C.c_int64(a.size))
+    h._lut = lut
+    return h
+
+
+def port_hist(img, bins, hist="eqsp"):
+    return port_hist_vopt(img, bins) if hist == "vopt" else \
+        port_hist_eqsp(img, bins)
+
+
+def port_mi(grid, fixed, moving, coeff, bins=32, precision="f32",
+            fixed_roi=None, moving_roi=None, hist="eqsp") -> Result:
+    """Mattes MI flavour g (PVI-8) in float or double; with image ROIs,
+    flavour h's ROI tests in both passes; hist "eqsp" (equal-spacing bins)
+    or "vopt" (V-optimal bins)."""
+    if fixed_roi is not None or moving_roi is not None:
+        with _RoiScope(fixed_roi, moving_roi):
+            return port_mi(grid, fixed, moving, coeff, bins, precision,
+                           hist=hist)
     g = orc_grid(grid, fixed)
-    fh, mh = port_hist_eqsp(fixed.img, bins), port_hist_eqsp(moving.img, bins)
+    fh, mh = port_hist(fixed.img, bins, hist), port_hist(moving.img, bins, hist)
     nv = C.c_int64(0)
     f_hist = np.zeros(bins)
     m_hist = np.zeros(bins)
@@ -422,20 +486,35 @@ def _ref_grid(grid) -> RefGrid:
 
 
 def ref_metric(grid, fixed, moving, coeff, flavor="g", metric="mse",
-               bins=32, threads=0, moving_grad=None) -> Result:
-    """One reference flavour evaluation (bspline_score_mse / _mi)."""
+               bins=32, threads=0, moving_grad=None, fixed_roi=None,
+               moving_roi=None, hist="eqsp") -> Result:
+    """One reference flavour evaluation (bspline_score_mse / _mi); with
+    image ROIs (geometry.Roi) the reference's ROI flavours (i / h); MI
+    histogram type "eqsp" or "vopt" (Bspline_parms::mi_hist_type)."""
+    ref().ref_set_mi_hist_type(C.c_int(1 if hist == "vopt" else 0))
     gr = np.zeros(grid.num_coeff, np.float32)
     res = RefResult()
     fh = np.zeros(bins)
     mh = np.zeros(bins)
     jh = np.zeros(bins * bins)
     coeff = np.ascontiguousarray(coeff, np.float32)
-    rc = ref().ref_metric(
-        C.byref(_ref_geom(fixed)), _p(fixed.img), C.byref(_ref_geom(moving)),
-        _p(moving.img), _p(moving_grad), C.byref(_ref_grid(grid)), _p(coeff),
-        C.c_char(flavor.encode()), C.c_int(1 if metric == "mi" else 0),
-        C.c_int(bins), C.c_int(threads), _p(gr), C.byref(res),
-        _p(fh, f64p), _p(mh, f64p), _p(jh, f64p))
+    head = (C.byref(_ref_geom(fixed)), _p(fixed.img),
+            C.byref(_ref_geom(moving)), _p(moving.img), _p(moving_grad),
+            C.byref(_ref_grid(grid)), _p(coeff), C.c_char(flavor.encode()),
+            C.c_int(1 if metric == "mi" else 0), C.c_int(bins),
+            C.c_int(threads))
+    tail = (_p(gr), C.byref(res), _p(fh, f64p), _p(mh, f64p), _p(jh, f64p))
+    if fixed_roi is None and moving_roi is None:
+        rc = ref().ref_metric(*head, *tail)
+    else:
+        u8 = C.POINTER(C.c_uint8)
+        rois = []
+        for r in (fixed_roi, moving_roi):
+            if r is None:
+                rois += [None, None]
+            else:
+                rois += [C.byref(_ref_geom(r)), r.mask.ctypes.data_as(u8)]
+        rc = ref().ref_metric_roi(*head, *rois, *tail)
     if rc:
         raise RuntimeError("reference metric failed")
     r = Result(res.score, gr, res.num_vox)

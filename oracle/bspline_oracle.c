@@ -226,6 +226,56 @@ correspond_f (float mijk[3], const float fxyz[3], const float dxyz[3],
     return inside_f (mijk, mv->dim);
 }
 
+/* Image ROIs (uchar mask volumes with their own geometry), as
+ * Bspline_state::fixed_roi / moving_roi hold them.  Set for the duration of
+ * one oracle call by orc_set_roi (NULL: none). */
+static const orc_roi* g_froi = 0;
+static const orc_roi* g_mroi = 0;
+/* set while the double-precision MI histogram pass runs: its fixed ROI
+ * test takes LOOP_X's accumulated positions, as the reference's does */
+static int g_roi_pass1 = 0;
+
+void
+orc_set_roi (const orc_roi* fixed_roi, const orc_roi* moving_roi)
+{
+    g_froi = fixed_roi;
+    g_mroi = moving_roi;
+}
+
+/* inside_roi (src/util/bspline_correspond.cxx:52-74): project the world
+ * position into the ROI volume, clamp each index to [0, dim - 1]
+ * (float_to_plm_long_clamp, :11-50; floor inside), read the mask. */
+static inline int
+inside_roi_f (const float xyz[3], const orc_roi* r)
+{
+    float tmp[3], pf[3];
+    int64_t p[3];
+    const orc_vol* v = &r->vol;
+    for (int d = 0; d < 3; d++) tmp[d] = xyz[d] - v->origin[d];
+    for (int d = 0; d < 3; d++)
+        pf[d] = tmp[0] * v->proj[3*d+0] + tmp[1] * v->proj[3*d+1]
+            + tmp[2] * v->proj[3*d+2];
+    for (int d = 0; d < 3; d++) {
+        if (pf[d] < 0.f) p[d] = 0;
+        else if (pf[d] >= v->dim[d]) p[d] = v->dim[d] - 1;
+        else p[d] = (int64_t) floor (pf[d]);
+    }
+    return (int) r->mask[vidx (v->dim, p[0], p[1], p[2])];
+}
+
+/* bspline_find_correspondence_dcos_roi (src/util/bspline_correspond.cxx:
+ * 112-145): the inside test, then the moving ROI at the moving position. */
+static inline int
+correspond_roi_f (float mijk[3], const float fxyz[3], const float dxyz[3],
+    const orc_vol* mv)
+{
+    if (!correspond_f (mijk, fxyz, dxyz, mv)) return 0;
+    if (!g_mroi) return 1;
+    float mxyz[3];
+    for (int d = 0; d < 3; d++) mxyz[d] = fxyz[d] + dxyz[d];
+    return inside_roi_f (mxyz, g_mroi);
+}
+
 /* li_value (src/base/interpolate.cxx:135-158). */
 static inline float
 li_value_f (const float f1[3], const float f2[3], int64_t mvf,
@@ -413,9 +463,12 @@ mse_g_f32 (const orc_grid* g, const orc_vol* fx, const float* f_img,
             for (int d = 0; d < 3; d++)
                 fxyz[d] = g->img_origin[d] + fijk[0] * fx->step[3*d+0]
                     + fijk[1] * fx->step[3*d+1] + fijk[2] * fx->step[3*d+2];
+            /* flavour i (bspline_mse.cxx:82-288): the fixed ROI at the
+               fixed position, the moving ROI at the moving position */
+            if (g_froi && !inside_roi_f (fxyz, g_froi)) continue;
             int64_t fidx = vidx (fx->dim, fijk[0], fijk[1], fijk[2]);
             interp_pix_c (dxyz, g, coeff, tile, q, bx, by, bz);
-            if (!correspond_f (mijk, fxyz, dxyz, mv)) continue;
+            if (!correspond_roi_f (mijk, fxyz, dxyz, mv)) continue;
             for (int d = 0; d < 3; d++)
                 li_clamp_f (mijk[d], mv->dim[d] - 1, &mf[d], &mr[d],
                     &li1[d], &li2[d]);
@@ -640,6 +693,17 @@ locate64 (const double fxyz[3], const double dxyz[3], const vol64* mv)
     return r;
 }
 
+/* The moving ROI at the moving position, decided in float as the
+ * reference does. */
+static inline int
+moving_roi64 (const double fxyz[3], const double dxyz[3])
+{
+    if (!g_mroi) return 1;
+    float mxyz[3];
+    for (int d = 0; d < 3; d++) mxyz[d] = (float) fxyz[d] + (float) dxyz[d];
+    return inside_roi_f (mxyz, g_mroi);
+}
+
 static inline void
 corner_weights64 (double w[8], const tri64* t)
 {
@@ -698,6 +762,32 @@ tile_loop64 (const orc_grid* g, const vol64* fx, const float* coeff,
                 fxyz[d] = (double) g->img_origin[d]
                     + fijk[0] * fx->step[3*d+0] + fijk[1] * fx->step[3*d+1]
                     + fijk[2] * fx->step[3*d+2];
+            if (g_froi) {
+                /* the ROI decision in the reference's float positions:
+                   POSITION_FROM_COORDS, or in the whole-image histogram
+                   scan the position LOOP_Z/Y/X accumulate along x
+                   (src/base/volume_macros.h:38-97) */
+                float fxyz_f[3];
+                if (g_roi_pass1) {
+                    float s[9];
+                    for (int i = 0; i < 9; i++) s[i] = (float) fx->step[i];
+                    fxyz_f[0] = g->img_origin[0] + fijk[2] * s[2] + fijk[1] * s[1];
+                    fxyz_f[1] = g->img_origin[1] + fijk[2] * s[5] + fijk[1] * s[4];
+                    fxyz_f[2] = g->img_origin[2] + fijk[2] * s[8] + fijk[1] * s[7];
+                    for (int64_t i = 0; i < fijk[0]; i++) {
+                        fxyz_f[0] += s[0];
+                        fxyz_f[1] += s[3];
+                        fxyz_f[2] += s[6];
+                    }
+                } else {
+                    for (int d = 0; d < 3; d++)
+                        fxyz_f[d] = g->img_origin[d]
+                            + fijk[0] * (float) fx->step[3*d+0]
+                            + fijk[1] * (float) fx->step[3*d+1]
+                            + fijk[2] * (float) fx->step[3*d+2];
+                }
+                if (!inside_roi_f (fxyz_f, g_froi)) continue;
+            }
             double w[64];
             int m = 0;
             for (int k = 0; k < 4; k++)
@@ -754,7 +844,7 @@ mse64_visit (void* vctx, int64_t fidx, const double fxyz[3],
 {
     mse64_ctx* c = (mse64_ctx*) vctx;
     tri64 t = locate64 (fxyz, dxyz, c->mv);
-    if (!t.ok) return;
+    if (!t.ok || !moving_roi64 (fxyz, dxyz)) return;
     double w[8], mval = 0;
     corner_weights64 (w, &t);
     for (int k = 0; k < 8; k++)
@@ -823,12 +913,94 @@ orc_hist_eqsp (orc_hist* h, const float* img, int64_t n)
     }
     h->delta = (mx - mn) / (h->bins - 1);
     h->offset = mn - 0.5 * h->delta;
+    h->keys = 0;
+    h->key_lut = 0;
 }
 
 static inline int
 bin_of (float v, const orc_hist* h)
 {
-    return (int) floor ((v - h->offset) / h->delta);
+    int b = (int) floor ((v - h->offset) / h->delta);
+    return h->key_lut ? h->key_lut[b] : b;
+}
+
+/* vopt_bin_error (src/register/joint_histogram.cxx:61-79): the squared
+ * error of one bin spanning keys [start, end] from the prefix tables;
+ * DBL_MAX for a bin holding less than one voxel. */
+static double
+vopt_err (int64_t start, int64_t end, const double* s, const double* ssq,
+    const double* cnt)
+{
+    double sq = ssq[end] - ssq[start];
+    double d = s[end] - s[start];
+    double w = (double) end - (double) start + 1.0;
+    double n = cnt[end] - cnt[start];
+    double v = sq - (d * d) / w;
+    if (n < 1.0) return DBL_MAX;
+    return v;
+}
+
+void
+orc_hist_vopt (orc_hist* h, int32_t* key_lut, const float* img, int64_t n)
+{
+    const int64_t K = 1000, B = h->bins;
+    double* hist = (double*) calloc (K, sizeof(double));
+    double* avg = (double*) calloc (K, sizeof(double));
+    double* s = (double*) malloc (K * sizeof(double));
+    double* ssq = (double*) malloc (K * sizeof(double));
+    double* cnt = (double*) malloc (K * sizeof(double));
+    double* err = (double*) calloc (B * K, sizeof(double));
+    int64_t* trk = (int64_t*) calloc (B * K, sizeof(int64_t));
+    float mn = img[0], mx = img[0];
+    for (int64_t i = 1; i < n; i++) {
+        if (img[i] < mn) mn = img[i];
+        else if (img[i] > mx) mx = img[i];
+    }
+    h->keys = K;
+    h->delta = (mx - mn) / (K - 1);
+    h->offset = mn - 0.5 * h->delta;
+    for (int64_t i = 0; i < n; i++) {
+        int b = (int) floor ((img[i] - h->offset) / h->delta);
+        hist[b]++;
+        avg[b] += img[i] - h->offset;
+    }
+    for (int64_t i = 0; i < K; i++) {
+        if (hist[i] > 0) avg[i] = avg[i] / hist[i];
+        else if (i > 0) avg[i] = avg[i-1];
+    }
+    s[0] = avg[0];
+    ssq[0] = avg[0] * avg[0];
+    cnt[0] = hist[0];
+    for (int64_t i = 1; i < K; i++) {
+        s[i] = s[i-1] + avg[i];
+        ssq[i] = ssq[i-1] + avg[i] * avg[i];
+        cnt[i] = cnt[i-1] + hist[i];
+    }
+    for (int64_t i = 0; i < K; i++) err[i] = vopt_err (0, i, s, ssq, cnt);
+    for (int64_t j = 1; j < B; j++) {
+        for (int64_t i = 0; i < K; i++) {
+            err[K*j+i] = DBL_MAX;
+            trk[K*j+i] = 0;
+            for (int64_t k = 0; k < i; k++) {
+                double c = err[K*(j-1)+k] + vopt_err (k + 1, i, s, ssq, cnt);
+                if (c <= err[K*j+i]) {
+                    err[K*j+i] = c;
+                    trk[K*j+i] = k;
+                }
+            }
+        }
+    }
+    for (int64_t i = 0; i < K; i++) key_lut[i] = 0;
+    int64_t curr = K - 1;
+    for (int64_t j = B - 1; j >= 0; j--) {
+        int64_t next = trk[K*j+curr];
+        int64_t bottom = j == 0 ? 0 : next + 1;
+        for (int64_t i = bottom; i <= curr; i++) key_lut[i] = (int32_t) j;
+        curr = next;
+    }
+    h->key_lut = key_lut;
+    free (hist); free (avg); free (s); free (ssq); free (cnt); free (err);
+    free (trk);
 }
 
 /* Joint_histogram::add_pvi_8 (src/register/joint_histogram.cxx:423-486). */
@@ -928,10 +1100,14 @@ mi_dc_dv (float dc_dv[3], const double* fh, const double* mh,
     dc_dv[2] = dc_dv[0] * pr[6] + dc_dv[1] * pr[7] + dc_dv[2] * pr[8];
 }
 
-/* bspline_score_g_mi (src/register/bspline_mi.cxx:1505-1750).  Pass 1 is
- * the voxel scan with incremental world positions; pass 2 is the tile loop.
- * The reference's pass 1 covers the whole fixed image, so this requires the
- * ROI to be the whole image (as in every configuration the reference tests). */
+/* bspline_score_g_mi (src/register/bspline_mi.cxx:1505-1750); with image
+ * ROIs set, bspline_score_h_mi (:1232-1504), which adds the fixed ROI test
+ * at the fixed position and the moving ROI test at the moving position to
+ * both passes.  Pass 1 is the voxel scan over the whole fixed image with
+ * incremental world positions and tile index fijk / vox_per_rgn; pass 2 is
+ * the tile loop over the grid's ROI.  Pass 1's tile index is in range only
+ * when the grid starts at voxel 0 and its tiles cover the image (returns -2
+ * otherwise; the reference reads past its tables there). */
 int
 orc_mi_f32 (const orc_grid* g, const orc_vol* fx, const float* f_img,
     const orc_vol* mv, const float* m_img, const float* coeff,
@@ -940,7 +1116,8 @@ orc_mi_f32 (const orc_grid* g, const orc_vol* fx, const float* f_img,
 {
     const int64_t* vpr = g->vox_per_rgn;
     for (int d = 0; d < 3; d++)
-        if (g->roi_offset[d] != 0 || g->roi_dim[d] != fx->dim[d]) return -2;
+        if (g->roi_offset[d] != 0 || g->rdims[d] * vpr[d] < fx->dim[d])
+            return -2;
     float* bx = (float*) malloc (sizeof(float) * 4 * vpr[0]);
     float* by = (float*) malloc (sizeof(float) * 4 * vpr[1]);
     float* bz = (float*) malloc (sizeof(float) * 4 * vpr[2]);
@@ -974,8 +1151,9 @@ orc_mi_f32 (const orc_grid* g, const orc_vol* fx, const float* f_img,
                 p[0] = fijk[0] / vpr[0]; q[0] = fijk[0] % vpr[0];
                 float dxyz[3], mijk[3], li1[3], li2[3];
                 int64_t mf[3], mr[3];
+                if (g_froi && !inside_roi_f (fxyz, g_froi)) continue;
                 interp_pix_c (dxyz, g, coeff, p, q, bx, by, bz);
-                if (!correspond_f (mijk, fxyz, dxyz, mv)) continue;
+                if (!correspond_roi_f (mijk, fxyz, dxyz, mv)) continue;
                 for (int d = 0; d < 3; d++)
                     li_clamp_f (mijk[d], mv->dim[d] - 1, &mf[d], &mr[d],
                         &li1[d], &li2[d]);
@@ -1020,8 +1198,9 @@ orc_mi_f32 (const orc_grid* g, const orc_vol* fx, const float* f_img,
             for (int d = 0; d < 3; d++)
                 fx3[d] = g->img_origin[d] + fijk[0] * st[3*d+0]
                     + fijk[1] * st[3*d+1] + fijk[2] * st[3*d+2];
+            if (g_froi && !inside_roi_f (fx3, g_froi)) continue;
             interp_pix_c (dxyz, g, coeff, tile, q, bx, by, bz);
-            if (!correspond_f (mijk, fx3, dxyz, mv)) continue;
+            if (!correspond_roi_f (mijk, fx3, dxyz, mv)) continue;
             for (int d = 0; d < 3; d++)
                 li_clamp_f (mijk[d], mv->dim[d] - 1, &mf[d], &mr[d],
                     &li1[d], &li2[d]);
@@ -1060,7 +1239,7 @@ mi64_visit (void* vctx, int64_t fidx, const double fxyz[3],
 {
     mi64_ctx* c = (mi64_ctx*) vctx;
     tri64 t = locate64 (fxyz, dxyz, c->mv);
-    if (!t.ok) return;
+    if (!t.ok || !moving_roi64 (fxyz, dxyz)) return;
     double w[8];
     corner_weights64 (w, &t);
     int fb = bin_of (c->f_img[fidx], c->fhp);
@@ -1119,7 +1298,9 @@ orc_mi_f64_pass1 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     memset (mh, 0, sizeof(double) * mhp->bins);
     memset (jh, 0, sizeof(double) * fhp->bins * mhp->bins);
     mi64_ctx c = { &mv, f_img, m_img, fhp, mhp, fh, mh, jh, 1, 0., 0., 0 };
+    g_roi_pass1 = 1;
     tile_loop64 (g, &fx, coeff, mi64_visit, &c, 0);
+    g_roi_pass1 = 0;
     *num_vox = c.num_vox;
     return 0;
 }
@@ -1156,7 +1337,14 @@ orc_mi_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     const orc_hist* fhp, const orc_hist* mhp, double* score, double* grad,
     int64_t* num_vox, double* fh, double* mh, double* jh)
 {
-    int rc = orc_mi_f64_pass1 (g, fixed, f_img, moving, m_img, coeff, fhp,
+    /* pass 1 scans the whole fixed image (see orc_mi_f32) */
+    orc_grid g1 = *g;
+    for (int d = 0; d < 3; d++) {
+        if (g->roi_offset[d] != 0 || g->rdims[d] * g->vox_per_rgn[d]
+            < fixed->dim[d]) return -2;
+        g1.roi_dim[d] = fixed->dim[d];
+    }
+    int rc = orc_mi_f64_pass1 (&g1, fixed, f_img, moving, m_img, coeff, fhp,
         mhp, num_vox, fh, mh, jh);
     if (rc) return rc;
     return orc_mi_f64_pass2 (g, fixed, f_img, moving, m_img, coeff, fhp, mhp,

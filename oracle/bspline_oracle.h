@@ -51,7 +51,21 @@ typedef struct {
     int64_t bins;
     float offset;
     float delta;
+    /* V-optimal histograms (HIST_VOPT): offset/delta span `keys` fine
+       keys and key_lut[key] gives the bin; NULL for equal spacing */
+    int64_t keys;
+    const int32_t* key_lut;
 } orc_hist;
+
+/* An image ROI: a uchar mask volume (x fastest) and its geometry
+ * (Bspline_state::fixed_roi / moving_roi).  orc_set_roi makes the MSE and
+ * MI routines test them (flavours i and h) until cleared with NULLs; the
+ * pointers must stay valid meanwhile. */
+typedef struct {
+    orc_vol vol;
+    const uint8_t* mask;
+} orc_roi;
+void orc_set_roi (const orc_roi* fixed_roi, const orc_roi* moving_roi);
 
 int orc_vol_init (orc_vol* v, const int64_t dim[3], const float origin[3],
     const float spacing[3], const float dcos[9]);
@@ -78,6 +92,12 @@ int orc_mse_f64 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
 
 /* Mattes MI with PVI-8 histograms (flavour g). */
 void orc_hist_eqsp (orc_hist* h, const float* img, int64_t n);
+/* bspline_initialize_mi_hist_vopt (src/register/joint_histogram.cxx:
+ * 195-324): 1000 fine keys over the value range and the bin of each key
+ * (key_lut[1000], caller's buffer) chosen by the V-optimal dynamic
+ * programme.  h->bins set by the caller (<= 1000). */
+void orc_hist_vopt (orc_hist* h, int32_t* key_lut, const float* img,
+    int64_t n);
 int orc_mi_f32 (const orc_grid* g, const orc_vol* fixed, const float* f_img,
     const orc_vol* moving, const float* m_img, const float* coeff,
     const orc_hist* fh, const orc_hist* mh, float* score, float* grad,

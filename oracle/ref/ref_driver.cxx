@@ -107,6 +107,15 @@ struct Ref_landmarks {
     float stiffness;
 };
 
+/* Histogram type of the next MI setups (Bspline_parms::mi_hist_type). */
+static Mi_hist_type g_hist_type = HIST_EQSP;
+
+extern "C" void
+ref_set_mi_hist_type (int vopt)
+{
+    g_hist_type = vopt ? HIST_VOPT : HIST_EQSP;
+}
+
 struct Ref_setup {
     Labeled_pointset lm_fixed, lm_moving;
     Bspline_xform bxf;
@@ -145,6 +154,7 @@ setup (Ref_setup* s, const ref_geom* fg, const float* fimg,
     s->parms.implementation = flavor;
     s->parms.mi_hist_fixed_bins = bins;
     s->parms.mi_hist_moving_bins = bins;
+    s->parms.mi_hist_type = g_hist_type;
     s->rparms.implementation = reg_impl;
     s->rparms.curvature_penalty = reg_lambda;
     s->parms.regularization_parms = &s->rparms;
@@ -206,6 +216,61 @@ ref_metric (const ref_geom* fg, const float* fimg,
     setup (&s, fg, fimg, mg, mimg, mgrad, grid, coeff, flavor, metric_mi,
         bins, '\0', 0.f, threads);
     Bspline_state* bst = s.bod.get_bspline_state ();
+    bst->ssd.reset_score ();
+    if (metric_mi) {
+        bspline_score_mi (&s.bod);
+    } else {
+        bspline_score_mse (&s.bod);
+    }
+    res->score = bst->ssd.curr_smetric;
+    res->num_vox = bst->ssd.curr_num_vox;
+    res->num_coeff = s.bxf.num_coeff;
+    memcpy (grad, bst->ssd.curr_smetric_grad, sizeof(float) * s.bxf.num_coeff);
+    if (metric_mi) {
+        Joint_histogram* jh = bst->get_mi_hist ();
+        res->fixed_bins = jh->fixed.bins;
+        res->moving_bins = jh->moving.bins;
+        res->f_offset = jh->fixed.offset;
+        res->f_delta = jh->fixed.delta;
+        res->m_offset = jh->moving.offset;
+        res->m_delta = jh->moving.delta;
+        if (f_hist) memcpy (f_hist, jh->f_hist, sizeof(double) * jh->fixed.bins);
+        if (m_hist) memcpy (m_hist, jh->m_hist, sizeof(double) * jh->moving.bins);
+        if (j_hist) memcpy (j_hist, jh->j_hist,
+            sizeof(double) * jh->fixed.bins * jh->moving.bins);
+    }
+    return 0;
+}
+
+/* ref_metric with image ROIs: uchar mask volumes (x fastest, any
+ * geometry; NULL: none) set on the metric state as a registration stage
+ * does (src/register/bspline_stage.cxx:152-205), so the dispatchers route
+ * MSE to flavour i (or k for 'c'/'k') and MI to flavour h
+ * (bspline_mse.cxx:1879-1887, bspline_mi.cxx:3036-3055). */
+int
+ref_metric_roi (const ref_geom* fg, const float* fimg,
+    const ref_geom* mg, const float* mimg, const float* mgrad,
+    const ref_grid* grid, const float* coeff, char flavor, int metric_mi,
+    int bins, int threads, const ref_geom* frg, const unsigned char* froi,
+    const ref_geom* mrg, const unsigned char* mroi, float* grad,
+    ref_result* res, double* f_hist, double* m_hist, double* j_hist)
+{
+    Quiet q;
+    Ref_setup s;
+    setup (&s, fg, fimg, mg, mimg, mgrad, grid, coeff, flavor, metric_mi,
+        bins, '\0', 0.f, threads);
+    Bspline_state* bst = s.bod.get_bspline_state ();
+    if (froi) {
+        s.ms->fixed_roi = Volume::New (frg->dim, frg->origin, frg->spacing,
+            frg->dcos, PT_UCHAR, 1);
+        memcpy (s.ms->fixed_roi->img, froi, s.ms->fixed_roi->npix);
+    }
+    if (mroi) {
+        s.ms->moving_roi = Volume::New (mrg->dim, mrg->origin, mrg->spacing,
+            mrg->dcos, PT_UCHAR, 1);
+        memcpy (s.ms->moving_roi->img, mroi, s.ms->moving_roi->npix);
+    }
+    bst->set_metric_state (s.ms);
     bst->ssd.reset_score ();
     if (metric_mi) {
         bspline_score_mi (&s.bod);

@@ -52,10 +52,12 @@ class GridDesc(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("form", C.c_int), ("mse_grad", C.c_int), ("mi_bins", C.c_int),
                 ("device", C.c_int), ("mi_window", C.c_int),
-                ("reserved", C.c_int * 3)]
+                ("wait_limit", C.c_int), ("mi_hist", C.c_int),
+                ("reserved", C.c_int)]
 
 
 MI_WINDOW = {"pvi8": 0, "parzen": 1}
+MI_HIST = {"eqsp": 0, "vopt": 1}
 
 
 class RegParms(C.Structure):
@@ -145,6 +147,7 @@ _SIGS = {
     "b200bsp_set_landmarks": (C.c_int, [_VP, _VP, C.c_int64, _VP, C.c_int64,
                                         C.c_float]),
     "b200bsp_landmarks_score": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "b200bsp_set_roi": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "b200bsp_score": (C.c_int, [_VP, _VP, C.c_int, C.c_float, _VP, _VP, _VP,
                                 _VP, _VP]),
     "b200bsp_interpolate_vf": (C.c_int, [_VP, _VP, _VP]),
@@ -346,7 +349,8 @@ class Context:
 
     def __init__(self, fixed: Volume, moving: Volume, grid: BsplineGrid,
                  form: str = "tc", mse_grad: str = "nearest",
-                 mi_bins: int = 32, device: int = 0, mi_window: str = "pvi8"):
+                 mi_bins: int = 32, device: int = 0, mi_window: str = "pvi8",
+                 mi_hist: str = "eqsp", wait_limit: int = 0):
         L = lib()
         self.fixed, self.moving, self.grid = fixed, moving, grid
         self.form = form
@@ -357,6 +361,8 @@ class Context:
         o.mse_grad = MSE_GRAD[mse_grad]
         o.mi_bins = mi_bins
         o.mi_window = MI_WINDOW[mi_window]
+        o.mi_hist = MI_HIST[mi_hist]
+        o.wait_limit = wait_limit
         o.device = device
         self._fd, self._md = _vol_desc(fixed), _vol_desc(moving)
         self._gd = GridDesc((C.c_int64 * 3)(*grid.roi_offset),
@@ -509,6 +515,23 @@ class Context:
         m = np.ascontiguousarray(np.asarray(moving_pts, np.float32).reshape(-1, 3))
         _check(lib().b200bsp_set_landmarks(self._h, _ptr(f), len(f), _ptr(m),
                                            len(m), stiffness), self._h)
+        return self
+
+    def set_roi(self, fixed_roi=None, moving_roi=None):
+        """Image ROIs (geometry.Roi or None) that every later evaluation
+        respects: fixed voxels outside the fixed ROI and moving positions
+        outside the moving ROI do not count (b200bsp_set_roi); no
+        arguments remove them."""
+        args = []
+        self._roi_keep = []
+        for r in (fixed_roi, moving_roi):
+            if r is None:
+                args += [None, None]
+            else:
+                d = _vol_desc(r)
+                self._roi_keep += [d, r.mask]
+                args += [C.byref(d), r.mask.ctypes.data]
+        _check(lib().b200bsp_set_roi(self._h, *args), self._h)
         return self
 
     def landmarks_score(self, coeff, grad=None):

@@ -37,7 +37,61 @@ struct BspGeom {
     int nknots;
     float m_hi[3];        // dim - 0.5: strict upper bound of the inside test
     float m_fmax[3];      // dim - 2: largest floor corner after clamping
+    // Image ROIs (Bspline_state::fixed_roi / moving_roi; null: none).  The
+    // fixed one as a byte per fixed voxel: bit 0 its ROI test at the
+    // voxel's position (origin + step * ijk), bit 1 at the position the
+    // reference's whole-image MI scan accumulates (LOOP_X).  The moving one
+    // as its mask volume and geometry, tested at each moving position.
+    const uint8_t* fmask;
+    const uint8_t* mroi;
+    int mroi_dim[3];
+    float mroi_origin[3];
+    float mroi_proj[9];
 };
+
+// The fixed ROI test of voxel fidx (bit 0, or bit 1 for the whole-image
+// histogram scan).
+__device__ __forceinline__ bool
+roi_fixed_ok (const BspGeom& g, int fidx, int bit = 1)
+{
+    return !g.fmask || (__ldg (g.fmask + fidx) & bit);
+}
+
+// inside_roi (src/util/bspline_correspond.cxx:52-74): project the world
+// position into the ROI volume in the reference's float order (PROJECT_X/
+// Y/Z, no contraction), clamp each index to [0, dim - 1] (floor inside,
+// float_to_plm_long_clamp :11-50), read the mask (nonzero: inside).
+__device__ __forceinline__ bool
+inside_roi_dev (const uint8_t* mask, const int dim[3], const float origin[3],
+    const float proj[9], const float xyz[3])
+{
+    float tmp[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) tmp[d] = __fsub_rn (xyz[d], origin[d]);
+    int p[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const float pf = __fadd_rn (__fadd_rn (__fmul_rn (tmp[0], proj[3 * d]),
+            __fmul_rn (tmp[1], proj[3 * d + 1])), __fmul_rn (tmp[2], proj[3 * d + 2]));
+        // pf >= dim (as float) -> dim - 1; pf < 0 (or NaN) -> 0
+        p[d] = pf >= (float) dim[d] ? dim[d] - 1
+            : (pf > 0.f ? (int) floorf (pf) : 0);
+    }
+    return __ldg (mask + p[0] + dim[0] * (p[1] + dim[1] * p[2])) != 0;
+}
+
+// The moving ROI test at the moving position mxyz = fxyz + dxyz
+// (bspline_find_correspondence_dcos_roi, src/util/bspline_correspond.cxx:
+// 112-145).
+__device__ __forceinline__ bool
+roi_moving_ok (const BspGeom& g, const float fxyz[3], const float dxyz[3])
+{
+    if (!g.mroi) return true;
+    const float mxyz[3] = {__fadd_rn (fxyz[0], dxyz[0]),
+        __fadd_rn (fxyz[1], dxyz[1]), __fadd_rn (fxyz[2], dxyz[2])};
+    return inside_roi_dev (g.mroi, g.mroi_dim, g.mroi_origin, g.mroi_proj,
+        mxyz);
+}
 
 // Where one fixed voxel lands in the moving image.
 struct Sample {

@@ -402,3 +402,58 @@ launch_pad_grad4 (const float* grad3, float4* grad4, long long n,
 }
 
 } // namespace b200
+
+namespace b200 {
+
+// The fixed ROI test of every fixed voxel as a byte (bit 0: at origin +
+// step * ijk, POSITION_FROM_COORDS, src/base/volume_macros.h:82-97; bit 1:
+// at the position LOOP_Z/Y/X accumulate, :38-76, which the reference's
+// whole-image MI histogram scan uses).  One thread per image row walks x,
+// accumulating as LOOP_X does.
+__global__ void
+fixed_roi_mask_kernel (int nx, int ny, int nz, RoiGeom fg, RoiGeom rg,
+    const uint8_t* __restrict__ roi, uint8_t* __restrict__ out)
+{
+    const long long row = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= (long long) ny * nz) return;
+    const int j = (int) (row % ny), k = (int) (row / ny);
+    const float* o = fg.origin;
+    const float* st = fg.step;
+    float acc[3];
+    acc[0] = __fadd_rn (__fadd_rn (o[0], __fmul_rn ((float) k, st[2])),
+        __fmul_rn ((float) j, st[1]));
+    acc[1] = __fadd_rn (__fadd_rn (o[1], __fmul_rn ((float) k, st[5])),
+        __fmul_rn ((float) j, st[4]));
+    acc[2] = __fadd_rn (__fadd_rn (o[2], __fmul_rn ((float) k, st[8])),
+        __fmul_rn ((float) j, st[7]));
+    uint8_t* dst = out + row * nx;
+    for (int i = 0; i < nx; i++) {
+        float p[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            p[d] = __fadd_rn (__fadd_rn (__fadd_rn (o[d],
+                __fmul_rn ((float) i, st[3 * d])),
+                __fmul_rn ((float) j, st[3 * d + 1])),
+                __fmul_rn ((float) k, st[3 * d + 2]));
+        }
+        const bool b0 = inside_roi_dev (roi, rg.dim, rg.origin, rg.proj, p);
+        const bool b1 = inside_roi_dev (roi, rg.dim, rg.origin, rg.proj, acc);
+        dst[i] = (uint8_t) ((b0 ? 1 : 0) | (b1 ? 2 : 0));
+#pragma unroll
+        for (int d = 0; d < 3; d++) acc[d] = __fadd_rn (acc[d], st[3 * d]);
+    }
+}
+
+cudaError_t
+launch_fixed_roi_mask (const int fdim[3], const RoiGeom& fixed,
+    const RoiGeom& roi_geom, const uint8_t* roi, uint8_t* out,
+    cudaStream_t st)
+{
+    const long long rows = (long long) fdim[1] * fdim[2];
+    const int threads = 128;
+    fixed_roi_mask_kernel<<<(unsigned) ((rows + threads - 1) / threads),
+        threads, 0, st>>> (fdim[0], fdim[1], fdim[2], fixed, roi_geom, roi, out);
+    return cudaGetLastError ();
+}
+
+} // namespace b200

@@ -59,8 +59,9 @@ fp32_tile_kernel (BspGeom g, F fn, const float* __restrict__ mimg,
         int fj = g.roi_off[1] + vy * ty + ly;
         int fk = g.roi_off[2] + vz * tz + lz;
         float dc[3] = {0.f, 0.f, 0.f};
+        const int fidx = fi + g.fdim[0] * (fj + g.fdim[1] * fk);
         if (fi < g.roi_off[0] + g.roi_dim[0] && fj < g.roi_off[1] + g.roi_dim[1]
-            && fk < g.roi_off[2] + g.roi_dim[2]) {
+            && fk < g.roi_off[2] + g.roi_dim[2] && roi_fixed_ok (g, fidx)) {
             float fxyz[3], d[3] = {0.f, 0.f, 0.f};
             fixed_position (g, fi, fj, fk, fxyz);
             int m = 0;
@@ -80,10 +81,9 @@ fp32_tile_kernel (BspGeom g, F fn, const float* __restrict__ mimg,
                 }
             }
             Sample s;
-            if (locate (g, fxyz, d, s)) {
+            if (locate (g, fxyz, d, s) && roi_moving_ok (g, fxyz, d)) {
                 Corners cr = F::kNeedCorners
                     ? load_corners (mimg, s.mvf, dx, dxy) : Corners ();
-                int fidx = fi + g.fdim[0] * (fj + g.fdim[1] * fk);
                 if (fn.voxel (g, fidx, s, cr, dc, sc)) cnt++;
             }
         }

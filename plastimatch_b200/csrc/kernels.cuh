@@ -56,6 +56,29 @@ cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
     float* part, double* score_part, int* count_part, int* err_flag,
     cudaStream_t st);
 
+// Tensor-core form, x-lane kernel (mse_xl.cu): one batch is a row of T
+// tiles along x with TMEM lane = voxel x; rows of the batch in chunks of
+// whole z planes (at most 32 rows).  Supports 3 <= vox_per_rgn[1] <= 10.
+struct XlPlan {
+    int T;               // tiles per batch along x
+    int nbx;             // batches per row of tiles
+    int nbatches;
+    int nlz, nch;        // z planes per chunk, chunks per batch
+    size_t smem;
+    int threads;
+    int grid;
+    int score_parts;     // per batch and compute warp
+};
+bool xl_plan (const BspGeom& g, XlPlan* plan, int sm_count);
+int xl_build_table (const BspGeom& g, const XlPlan& plan, const float* bx_lut,
+    void** d_tab);
+constexpr unsigned XL_DEFAULT_WAIT_LIMIT = 1u << 22;
+cudaError_t launch_mse_xl (const BspGeom& g, const XlPlan& plan,
+    int grad_mode, const float* fimg, const float* mimg, const float* mgrad,
+    const float* coeff, const void* tab, const float* luts, float* part,
+    double* score_part, int* count_part, int* err, unsigned wait_limit,
+    cudaStream_t st);
+
 // Mattes MI on the tensor-core kernel (axis-aligned geometry, tiles of at
 // most 128 voxels, histograms that fit the adjoint operand's area): pass 1
 // (hist_pass: PVI-8 or Parzen histograms into mi.hist, integer 2^-24 units,
@@ -106,6 +129,20 @@ cudaError_t launch_gather_grad (const BspGeom& g, const PartLayout& lay,
     long long* nvox_out, cudaStream_t st);
 cudaError_t launch_volume_grad (const int dim[3], const float spacing[3],
     const float inv_dc[9], const float* img, float* grad, cudaStream_t st);
+
+// Geometry of an image or ROI volume for the ROI tests: dims, origin,
+// step (dcos * spacing) and proj (inv(dcos) / spacing), row-major.
+struct RoiGeom {
+    int dim[3];
+    float origin[3];
+    float step[9];
+    float proj[9];
+};
+// Fixed ROI test of every fixed voxel into out[fdim] (bit 0 at the
+// voxel's position, bit 1 at the whole-image scan's accumulated position).
+cudaError_t launch_fixed_roi_mask (const int fdim[3], const RoiGeom& fixed,
+    const RoiGeom& roi_geom, const uint8_t* roi, uint8_t* out,
+    cudaStream_t st);
 
 // Landmark term (landmarks.cu): n landmarks with tiles p[3n], q_lut rows
 // w[64n], fixed/moving xyz fm[6n]; scratch dc[4n]; ADDS the gradient into

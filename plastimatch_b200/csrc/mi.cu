@@ -73,6 +73,124 @@ bin_image_kernel (const float* __restrict__ img, long long n, float offset,
     }
 }
 
+// V-optimal bins: key = floor((v - offset) / delta) over MI_VOPT_KEYS fine
+// keys, bin = key_lut[key] (the reference's lookup, bspline_mi.cxx:565-579).
+__global__ void
+bin_image_vopt_kernel (const float* __restrict__ img, long long n,
+    float offset, float delta, const int* __restrict__ key_lut,
+    uint8_t* __restrict__ out)
+{
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        float b = floorf (__fdiv_rn (img[i] - offset, delta));
+        int k = (int) fminf (fmaxf (b, 0.f), (float) (MI_VOPT_KEYS - 1));
+        out[i] = (uint8_t) __ldg (key_lut + k);
+    }
+}
+
+// The V-optimal histogram of one image (the reference's
+// bspline_initialize_mi_hist_vopt, src/register/joint_histogram.cxx:
+// 195-324, restated): MI_VOPT_KEYS equal keys over the value range, each
+// key's voxel count and mean, and the split of the keys into `bins`
+// contiguous bins that minimises the summed within-bin squared error of
+// the key means (dynamic programme over prefix sums; ties go to the later
+// split, as the reference's "<=" does).  Host code in double, in the
+// reference's operation order, so the key table is the reference's.
+static void
+vopt_table (const float* img, size_t n, int bins, float* offset_out,
+    float* delta_out, std::vector<int>& key_lut)
+{
+    const int K = MI_VOPT_KEYS;
+    std::vector<double> hist (K, 0.0), avg (K, 0.0), s (K), ssq (K), cnt (K);
+    float mn = img[0], mx = img[0];
+    for (size_t i = 1; i < n; i++) {
+        if (img[i] < mn) mn = img[i];
+        else if (img[i] > mx) mx = img[i];
+    }
+    const float delta = (mx - mn) / (K - 1);
+    const float offset = (float) (mn - 0.5 * delta);
+    for (size_t i = 0; i < n; i++) {
+        const float v = img[i] - offset;
+        const int b = (int) std::floor (v / delta);
+        hist[b] += 1.0;
+        avg[b] += v;
+    }
+    for (int i = 0; i < K; i++) {
+        if (hist[i] > 0) avg[i] = avg[i] / hist[i];
+        else if (i > 0) avg[i] = avg[i - 1];
+    }
+    s[0] = avg[0];
+    ssq[0] = avg[0] * avg[0];
+    cnt[0] = hist[0];
+    for (int i = 1; i < K; i++) {
+        s[i] = s[i - 1] + avg[i];
+        ssq[i] = ssq[i - 1] + avg[i] * avg[i];
+        cnt[i] = cnt[i - 1] + hist[i];
+    }
+    auto bin_err = [&](int a, int b) {
+        const double d = s[b] - s[a];
+        const double v = (ssq[b] - ssq[a]) - (d * d) / ((double) b - (double) a + 1.0);
+        return cnt[b] - cnt[a] < 1.0 ? DBL_MAX : v;
+    };
+    std::vector<double> err ((size_t) bins * K);
+    std::vector<int> trk ((size_t) bins * K, 0);
+    for (int i = 0; i < K; i++) err[i] = bin_err (0, i);
+    for (int j = 1; j < bins; j++) {
+        const double* prev = err.data () + (size_t) K * (j - 1);
+        double* cur = err.data () + (size_t) K * j;
+        int* tj = trk.data () + (size_t) K * j;
+        for (int i = 0; i < K; i++) {
+            double best = DBL_MAX;
+            int arg = 0;
+            for (int k = 0; k < i; k++) {
+                const double c = prev[k] + bin_err (k + 1, i);
+                if (c <= best) {
+                    best = c;
+                    arg = k;
+                }
+            }
+            cur[i] = best;
+            tj[i] = arg;
+        }
+    }
+    key_lut.assign (K, 0);
+    int curr = K - 1;
+    for (int j = bins - 1; j >= 0; j--) {
+        const int next = trk[(size_t) K * j + curr];
+        const int bottom = j == 0 ? 0 : next + 1;
+        for (int i = bottom; i <= curr; i++) key_lut[i] = j;
+        curr = next;
+    }
+    *offset_out = offset;
+    *delta_out = delta;
+}
+
+static int
+vopt_bins (const float* d_img, size_t n, int bins, float* offset,
+    float* delta, int* d_key, uint8_t* d_bin, cudaStream_t st)
+{
+    std::vector<float> h (n);
+    std::vector<int> lut;
+    if (cudaMemcpyAsync (h.data (), d_img, n * sizeof (float),
+            cudaMemcpyDeviceToHost, st) != cudaSuccess
+        || cudaStreamSynchronize (st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    vopt_table (h.data (), n, bins, offset, delta, lut);
+    if (!(*delta > 0.f)) return B200BSP_E_BADARG;     // constant image
+    if (cudaMemcpyAsync (d_key, lut.data (), MI_VOPT_KEYS * sizeof (int),
+            cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    bin_image_vopt_kernel<<<1184, 256, 0, st>>> (d_img, (long long) n, *offset,
+        *delta, d_key, d_bin);
+    if (cudaGetLastError () != cudaSuccess
+        || cudaStreamSynchronize (st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    return B200BSP_OK;
+}
+
 static int
 image_range (const float* d_img, size_t n, float* d_scratch, float* mn_out,
     float* mx_out, cudaStream_t st)
@@ -124,10 +242,17 @@ eqsp_range (const float* d_img, size_t n, int bins, float* d_scratch,
 }
 
 int
-mi_alloc (MiState* s, const BspGeom& g, int bins, int window)
+mi_alloc (MiState* s, const BspGeom& g, int bins, int window, int hist)
 {
     s->bins = bins;
     s->window = window;
+    s->hist = hist;
+    if (hist == B200BSP_MI_HIST_VOPT
+        && (cudaMalloc (&s->d_fkey, MI_VOPT_KEYS * sizeof (int)) != cudaSuccess
+            || cudaMalloc (&s->d_mkey, MI_VOPT_KEYS * sizeof (int)) != cudaSuccess)) {
+        cudaGetLastError ();
+        return B200BSP_E_OOM;
+    }
     size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
     size_t nm = (size_t) g.mdim[0] * g.mdim[1] * g.mdim[2];
     size_t nh = 2 * bins + bins * bins + 1;
@@ -157,6 +282,7 @@ mi_free (MiState* s)
     cudaFree (s->d_histd); cudaFree (s->d_lut); cudaFree (s->d_nvf);
     cudaFree (s->d_minmax); cudaFree (s->d_part); cudaFree (s->d_score_part);
     cudaFree (s->d_count_part);
+    cudaFree (s->d_fkey); cudaFree (s->d_mkey);
     cudaFreeHost (s->h_histd); cudaFreeHost (s->h_res);
     *s = MiState ();
 }
@@ -179,6 +305,15 @@ mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
         parzen_bin_kernel<<<1184, 256, 0, st>>> (d_fixed, (long long) nf,
             s->pz_fmin, s->pz_fdelta, s->bins, s->d_fbin);
         if (cudaGetLastError () != cudaSuccess) return B200BSP_E_CUDA;
+        s->ready = true;
+        return B200BSP_OK;
+    }
+    if (s->hist == B200BSP_MI_HIST_VOPT) {
+        int rc = vopt_bins (d_fixed, nf, s->bins, &s->f_offset, &s->f_delta,
+            s->d_fkey, s->d_fbin, st);
+        if (!rc) rc = vopt_bins (d_moving, nm, s->bins, &s->m_offset,
+            &s->m_delta, s->d_mkey, s->d_mbin, st);
+        if (rc) return rc;
         s->ready = true;
         return B200BSP_OK;
     }
@@ -261,6 +396,7 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
                 && fk < g.roi_off[2] + g.roi_dim[2];
             int fb = 0, mb[8];
             unsigned int q[8];
+            live = live && roi_fixed_ok (g, fi + g.fdim[0] * (fj + g.fdim[1] * fk), 2);
             if (live) {
                 float fxyz[3], d[3] = {0.f, 0.f, 0.f};
                 fixed_position (g, fi, fj, fk, fxyz);
@@ -281,7 +417,7 @@ mi_hist_kernel (BspGeom g, const float* __restrict__ coeff,
                     }
                 }
                 Sample s;
-                live = locate (g, fxyz, d, s);
+                live = locate (g, fxyz, d, s) && roi_moving_ok (g, fxyz, d);
                 if (live) {
                     const float* l1 = s.w1;
                     const float* l2 = s.w2;
@@ -437,6 +573,7 @@ parzen_hist_kernel (BspGeom g, const float* __restrict__ coeff,
                 && fk < g.roi_off[2] + g.roi_dim[2];
             int fb = 0;
             float u = 2.f;
+            live = live && roi_fixed_ok (g, fi + g.fdim[0] * (fj + g.fdim[1] * fk));
             if (live) {
                 float fxyz[3], d[3] = {0.f, 0.f, 0.f};
                 fixed_position (g, fi, fj, fk, fxyz);
@@ -457,7 +594,7 @@ parzen_hist_kernel (BspGeom g, const float* __restrict__ coeff,
                     }
                 }
                 Sample s;
-                live = locate (g, fxyz, d, s);
+                live = locate (g, fxyz, d, s) && roi_moving_ok (g, fxyz, d);
                 if (live) {
                     const Corners cr = load_corners (mimg, s.mvf, dx, dxy);
                     u = parzen_centre (trilinear (s, cr), m_min, m_delta);

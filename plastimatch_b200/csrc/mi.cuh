@@ -18,9 +18,15 @@ struct MiResult {
     long long num_vox;
 };
 
+constexpr int MI_VOPT_KEYS = 1000;            // VOPT_RES, src/register/histogram.h:12
+
 struct MiState {
     int bins = 0;
     int window = 0;                           // B200BSP_MI_PVI8 / _PARZEN
+    int hist = 0;                             // B200BSP_MI_HIST_EQSP / _VOPT
+    // V-optimal bins: offset/delta span the fine keys, key -> bin tables
+    int* d_fkey = nullptr;
+    int* d_mkey = nullptr;
     bool ready = false;
     // Parzen: fixed bin = floor((v - pz_fmin) / pz_fdelta) + 2; moving
     // window centre (v - pz_mmin) / pz_mdelta + 2
@@ -41,7 +47,8 @@ struct MiState {
     DevResult* h_res = nullptr;
 };
 
-int mi_alloc (MiState* s, const BspGeom& g, int bins, int window);
+int mi_alloc (MiState* s, const BspGeom& g, int bins, int window,
+    int hist = 0);
 void mi_free (MiState* s);
 int mi_set_images (MiState* s, const BspGeom& g, const float* d_fixed,
     const float* d_moving, size_t nf, size_t nm, cudaStream_t st);

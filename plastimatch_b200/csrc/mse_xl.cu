@@ -1,0 +1,787 @@
+// Tensor-core (tcgen05) form of the MSE score + gradient, x-lane layout.
+//
+// One batch is a row of T tiles along x at tile coordinates (ty, tz): its
+// voxels are the block x in [0, T vx) x rows rho = (ly, lz).  The B-spline
+// field there factors into two contractions (the basis is a tensor product,
+// src/base/bspline_interpolate.cxx:78-110):
+//   R_c[xk][rho]  = sum_{j,k} by[ly][j] bz[lz][k] C_c[xk][j][k]   (y and z)
+//   D[x][(c,rho)] = sum_xk   Bx[x][xk] R_c[xk][rho]               (x)
+// with xk the T + 3 knots of the batch along x and Bx the banded x basis
+// (bx[x mod vx][xk - x div vx], zero off the band), shared by every batch.
+// The x contraction runs on the tensor cores with the voxel x as the MMA's
+// M dimension, so TMEM lane = voxel x: each thread of a warp owns one x of
+// 32 consecutive ones and walks the rows rho of the batch, reading its
+// field values straight from TMEM (no transposition through shared memory)
+// while a warp's trilinear gathers and fixed-image reads stay coalesced.
+// The adjoint of the condense (bspline_update_sets_b,
+// src/register/bspline.cxx:347-374) runs the other way:
+//   Rg[(c,xk)][rho] = sum_x Bx[x][xk] DCDV_c[x][rho]               (tensor cores)
+//   G_c[xk][j][k]   = sum_rho by[ly][j] bz[lz][k] Rg[(c,xk)][rho]  (CUDA cores)
+// The adjoint's M dimension is (c, xk): the basis table holds four copies
+// of Bx side by side, so the MMA's rows c*32 + xk land in TMEM lane quarter
+// c and every lane of a quarter owns one knot of one component for the
+// y/z contraction.  G_c is the batch's partial gradient of its
+// (T + 3) x 4 x 4 knot footprint; the finish kernel sums the partials of
+// each knot in a fixed order (no float atomics).
+//
+// Precision: every tensor-core operand is split x = hi + lo (two bf16) and
+// each product takes hi*hi + hi*lo + lo*hi with f32 accumulation in TMEM
+// (~16 significant bits); the y/z contractions, positions, trilinear
+// samples and differences are f32 on the CUDA cores.
+//
+// CTA (one per SM): 16 compute warps + 1 tensor-core warp.  Warp w reads
+// TMEM lane quarter w % 4 (x = 32 (w % 4) + lane); the four warps of a
+// quarter split the batch's rows.  The fourth quarter's warps also compute
+// the y/z contraction of the batch two steps ahead; the other three do the
+// adjoint y/z contraction of the previous step.  Steps (batch, chunk of
+// rows) are software-pipelined through double-buffered operands and TMEM
+// accumulators, with mbarrier handshakes:
+//   B2 ready (R of step s)  -> MMA x-forward(s)  -> D full(s)
+//   D full(s)               -> voxel phase(s)    -> DC ready(s)
+//   DC ready(s)             -> MMA x-adjoint(s)  -> Rg full(s)
+//   Rg full(s)              -> y/z adjoint(s) during step s + 1.
+// Every wait is bounded (a runtime poll limit); on expiry the kernel raises
+// the context's error flag and every warp leaves its loop.
+#include <algorithm>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "bsp_common.cuh"
+#include "kernels.cuh"
+#include "tc_ptx.cuh"
+#include "../../include/plastimatch_b200.h"
+
+namespace b200 {
+
+namespace {
+
+constexpr int XL_CW = 16;                    // compute warps
+constexpr int XL_THREADS = 32 * XL_CW;
+constexpr int XL_BLOCK = XL_THREADS + 32;    // + the tensor-core warp
+constexpr int XL_KMAX = 32;                  // knots per batch along x
+constexpr int XL_RC = 32;                    // rows per component block
+constexpr int XL_N = 3 * XL_RC;              // MMA N: (c, rho)
+
+// Shared memory (offsets from a 1024-byte aligned base).
+constexpr int XS_TAB = 0;          // basis table, bf16 hi (32 KB) then lo
+constexpr int XS_TAB_LO = 32768;
+constexpr int XS_B2 = 65536;       // R operand, 2 buffers x (hi 8 KB, lo 8 KB)
+constexpr int XS_B2_BUF = 16384;
+constexpr int XS_B2_LO = 8192;
+constexpr int XS_DC = XS_B2 + 2 * XS_B2_BUF;   // dc/dv operand, 2 x (hi, lo)
+constexpr int XS_DC_BUF = 49152;
+constexpr int XS_DC_LO = 24576;
+constexpr int XS_DC_ATOM = XL_N * 128;         // 64-voxel K atom of one half
+constexpr int XS_ROWS = XS_DC + 2 * XS_DC_BUF; // per-warp row table
+constexpr int XS_ROWS_BYTES = XL_CW * 8 * 16;
+constexpr int XS_LUT = XS_ROWS + XS_ROWS_BYTES;   // by[vy][4], bz[vz][4]
+constexpr int XS_LUT_FLOATS = 2 * 64 * 4;
+constexpr int XS_TOTAL = XS_LUT + XS_LUT_FLOATS * 4;
+static_assert (XS_TOTAL + 1024 <= 227 * 1024, "shared memory");
+
+// TMEM columns: D[buf] at 128 buf, Rg[buf] at 256 + 128 buf.
+constexpr int XT_COLS = 512;
+constexpr int XT_D = 0;
+constexpr int XT_RG = 256;
+
+// Barriers.
+constexpr int XB_B2 = 0;       // + buf: R operand written (4 warp arrivals)
+constexpr int XB_DC = 2;       // + buf: dc/dv written, D read (16 arrivals)
+constexpr int XB_D = 4;        // + buf: x-forward MMA done (commit)
+constexpr int XB_RG = 6;       // + buf: x-adjoint MMA done (commit)
+
+}  // namespace
+
+struct XlArgs {
+    BspGeom g;
+    int T, KX, nbx, nbatches;
+    int nlz, nch;            // z planes per row chunk, chunks per batch
+    unsigned wait_limit;
+    const float* fimg;
+    const float* mimg;
+    const float* mgrad;      // xyz interleaved (nearest-voxel mode)
+    const float* coeff;
+    const uint4* tab;        // the basis table image (64 KB)
+    const float* luts;       // bx[vx][4], by[vy][4], bz[vz][4]
+    float* part;             // [batch][c][xk + KX (j + 4 k)]
+    double* score_part;      // [batch][warp]
+    int* count_part;         // [batch][warp]
+    int* err;
+};
+
+namespace {
+
+struct XlCtx {
+    uint8_t* sm;
+    uint32_t sm_base;
+    uint32_t taddr;
+    int warp, lane, q, j4;
+};
+
+__device__ __forceinline__ uint32_t
+split_word (float x)
+{
+    // bf16 hi in the low half-word, bf16 lo (x - hi) in the high one
+    __nv_bfloat16 h = __float2bfloat16_rn (x);
+    __nv_bfloat16 l = __float2bfloat16_rn (x - __bfloat162float (h));
+    return (uint32_t) __bfloat16_as_ushort (h)
+        | ((uint32_t) __bfloat16_as_ushort (l) << 16);
+}
+
+// Bounded wait of one warp on an mbarrier phase: lane 0 polls, gives up
+// after the limit or once another warp has given up.
+__device__ __forceinline__ bool
+xl_wait (const XlArgs& a, const XlCtx& x, uint64_t* bar, uint32_t ph,
+    volatile int* s_abort, int code)
+{
+    if (x.lane == 0) {
+        bool ok = false;
+        for (uint32_t n = 0; n < a.wait_limit && !*s_abort; n++) {
+            if (mbar_try_wait (bar, ph)) { ok = true; break; }
+        }
+        if (!ok) {
+            *s_abort = 1;
+            atomicExch (a.err, code);
+        }
+    }
+    __syncwarp ();
+    return *s_abort == 0;
+}
+
+// Step s -> batch, chunk and the batch's tile coordinates.
+struct XlStep {
+    int b, ch, tx0, ty, tz, lz0, nlz;
+};
+
+__device__ __forceinline__ XlStep
+xl_step (const XlArgs& a, int s)
+{
+    XlStep t;
+    const int i = s / a.nch;
+    t.ch = s - i * a.nch;
+    t.b = blockIdx.x + i * gridDim.x;
+    t.tx0 = (t.b % a.nbx) * a.T;
+    t.ty = (t.b / a.nbx) % a.g.rdims[1];
+    t.tz = t.b / (a.nbx * a.g.rdims[1]);
+    t.lz0 = t.ch * a.nlz;
+    t.nlz = min (a.nlz, a.g.vpr[2] - t.lz0);
+    return t;
+}
+
+// y/z forward contraction of one step into the R operand buffer (K = xk
+// rows, N = (c, rho) columns, MN-major, 128-byte swizzle): thread (c, xk)
+// of the fourth lane quarter's warps 0..2.
+__device__ __forceinline__ void
+xl_yz_forward (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf)
+{
+    const BspGeom& g = a.g;
+    const int c = x.j4, xk = x.lane;
+    if (c >= 3) return;
+    const float* by = (const float*) (x.sm + XS_LUT);
+    const float* bz = by + 4 * g.vpr[1];
+    const int kx = t.tx0 + xk;
+    const bool live = xk < a.KX && kx < g.cdims[0];
+    float cf[16];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int knot = ((t.tz + k) * g.cdims[1] + t.ty + j) * g.cdims[0]
+                + (live ? kx : 0);
+            cf[4 * k + j] = live ? __ldg (a.coeff + 3 * knot + c) : 0.f;
+        }
+    }
+    uint8_t* hi = x.sm + XS_B2 + buf * XS_B2_BUF;
+    const int vy = g.vpr[1];
+    const uint32_t rowoff = (uint32_t) ((xk >> 3) * 1024 + (xk & 7) * 128);
+    for (int l = 0; l < t.nlz; l++) {
+        const float* bzl = bz + 4 * (t.lz0 + l);
+        float z[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            z[j] = bzl[0] * cf[j] + bzl[1] * cf[4 + j] + bzl[2] * cf[8 + j]
+                + bzl[3] * cf[12 + j];
+        }
+        for (int ly = 0; ly < vy; ly++) {
+            const float* byl = by + 4 * ly;
+            const float r = byl[0] * z[0] + byl[1] * z[1] + byl[2] * z[2]
+                + byl[3] * z[3];
+            const int n = c * XL_RC + ly + vy * l;
+            const uint32_t off = (uint32_t) ((n >> 6) * 4096) + rowoff
+                + (uint32_t) ((((n & 63) >> 3) ^ (xk & 7)) << 4)
+                + (uint32_t) ((n & 7) * 2);
+            const uint32_t w = split_word (r);
+            *(unsigned short*) (hi + off) = (unsigned short) w;
+            *(unsigned short*) (hi + XS_B2_LO + off) = (unsigned short) (w >> 16);
+        }
+    }
+}
+
+// y/z adjoint contraction of one step: thread (c, xk) of lane quarter c,
+// warp j4 = knot plane k; accumulates G[j] over the batch's chunks.
+template <int VY>
+__device__ __forceinline__ void
+xl_yz_adjoint_t (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
+    float G[4])
+{
+    constexpr int NLZ = XL_RC / VY;
+    const float* by = (const float*) (x.sm + XS_LUT);
+    const float* bz = by + 4 * VY;
+    const int c = x.q, k = x.j4;
+    float rg[32];
+    tmem_ld32_wait (x.taddr + ((uint32_t) (32 * c) << 16) + XT_RG + 128 * buf
+        + XL_RC * c, rg);
+    float z[VY];
+#pragma unroll
+    for (int ly = 0; ly < VY; ly++) z[ly] = 0.f;
+#pragma unroll
+    for (int l = 0; l < NLZ; l++) {
+        if (l < t.nlz) {
+            const float w = bz[4 * (t.lz0 + l) + k];
+#pragma unroll
+            for (int ly = 0; ly < VY; ly++) z[ly] = fmaf (w, rg[ly + VY * l], z[ly]);
+        }
+    }
+#pragma unroll
+    for (int ly = 0; ly < VY; ly++) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) G[j] = fmaf (by[4 * ly + j], z[ly], G[j]);
+    }
+}
+
+__device__ __forceinline__ void
+xl_yz_adjoint (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
+    float G[4])
+{
+    switch (a.g.vpr[1]) {
+    case 3: xl_yz_adjoint_t<3> (a, x, t, buf, G); break;
+    case 4: xl_yz_adjoint_t<4> (a, x, t, buf, G); break;
+    case 5: xl_yz_adjoint_t<5> (a, x, t, buf, G); break;
+    case 6: xl_yz_adjoint_t<6> (a, x, t, buf, G); break;
+    case 7: xl_yz_adjoint_t<7> (a, x, t, buf, G); break;
+    case 8: xl_yz_adjoint_t<8> (a, x, t, buf, G); break;
+    case 9: xl_yz_adjoint_t<9> (a, x, t, buf, G); break;
+    case 10: xl_yz_adjoint_t<10> (a, x, t, buf, G); break;
+    default: break;                  // the plan admits no other vy
+    }
+}
+
+// The voxel phase of one step for warp (quarter q, rows part j4): the
+// warp's rows [ra, rb) of the chunk, four at a time (their field values as
+// three 4-column TMEM loads), two samples in flight per thread.
+template <int MODE, bool AXIS, bool ROI>
+__device__ __forceinline__ void
+xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
+    float& scf, int& cnt)
+{
+    const BspGeom& g = a.g;
+    const int vy = g.vpr[1];
+    const int nrc = vy * t.nlz;
+    const int ra = (nrc * x.j4) >> 2, rb = (nrc * (x.j4 + 1)) >> 2;
+    const int nr = rb - ra;
+    if (nr <= 0) return;
+    // one row per lane: (y, z) part of the world position and the fixed
+    // image's row index (-1: row outside the ROI)
+    float4* rows = (float4*) (x.sm + XS_ROWS) + 8 * x.warp;
+    if (x.lane < nr) {
+        const int rho = ra + x.lane;
+        const int ly = rho % vy, lz = t.lz0 + rho / vy;
+        const int fj = g.roi_off[1] + vy * t.ty + ly;
+        const int fk = g.roi_off[2] + g.vpr[2] * t.tz + lz;
+        const bool live = fj < g.roi_off[1] + g.roi_dim[1]
+            && fk < g.roi_off[2] + g.roi_dim[2];
+        const float ffj = (float) fj, ffk = (float) fk;
+        float p[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            p[d] = __fadd_rn (__fadd_rn (g.img_origin[d],
+                __fmul_rn (g.fstep[3 * d + 1], ffj)),
+                __fmul_rn (g.fstep[3 * d + 2], ffk));
+        }
+        rows[x.lane] = make_float4 (p[0], p[1], p[2],
+            __int_as_float (live ? g.fdim[0] * (fj + g.fdim[1] * fk) : -1));
+    }
+    __syncwarp ();
+
+    const int X = 32 * x.q + x.lane;
+    const int fi = g.roi_off[0] + g.vpr[0] * t.tx0 + X;
+    const bool xlive = X < min (a.T, g.rdims[0] - t.tx0) * g.vpr[0]
+        && fi < g.roi_off[0] + g.roi_dim[0];
+    const int fic = min (fi, g.fdim[0] - 1);
+    const float ffi = (float) fi;
+    const float xp[3] = {__fmul_rn (g.fstep[0], ffi), __fmul_rn (g.fstep[3], ffi),
+        __fmul_rn (g.fstep[6], ffi)};
+    const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
+    // adjoint operand: row n = c * 32 + rho, column (K) x
+    uint8_t* dcb = x.sm + XS_DC + buf * XS_DC_BUF + (X >> 6) * XS_DC_ATOM
+        + (X & 7) * 2;
+    const int xch = (X & 63) >> 3;
+    const uint32_t tl = x.taddr + ((uint32_t) (32 * x.q) << 16) + XT_D
+        + 128 * buf;
+
+    for (int r0 = ra; r0 < rb; r0 += 4) {
+        float dv[12];
+        tmem_ld4x3_wait (tl + r0, tl + XL_RC + r0, tl + 2 * XL_RC + r0, dv);
+#pragma unroll
+        for (int u0 = 0; u0 < 4; u0 += 2) {
+            bool ok[2], rowv[2];
+            int mvf[2], mvr[2], fidx[2];
+            float w2[2][3];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int u = u0 + h;
+                const int rho = r0 + u;
+                rowv[h] = rho < rb;
+                const float4 rw = rows[rowv[h] ? rho - ra : 0];
+                const int frow = __float_as_int (rw.w);
+                const float d[3] = {dv[u], dv[4 + u], dv[8 + u]};
+                const float fxyz[3] = {__fadd_rn (rw.x, xp[0]),
+                    __fadd_rn (rw.y, xp[1]), __fadd_rn (rw.z, xp[2])};
+                float tt[3];
+#pragma unroll
+                for (int e = 0; e < 3; e++) {
+                    tt[e] = __fsub_rn (__fadd_rn (fxyz[e], d[e]), g.morigin[e]);
+                }
+                bool in = rowv[h] && xlive && frow >= 0;
+                int f[3];
+                bool up[3];
+#pragma unroll
+                for (int e = 0; e < 3; e++) {
+                    float ma;
+                    if (AXIS) {
+                        ma = __fmul_rn (tt[e], g.mproj[4 * e]);
+                    } else {
+                        ma = __fadd_rn (__fadd_rn (__fmul_rn (tt[0], g.mproj[3 * e]),
+                            __fmul_rn (tt[1], g.mproj[3 * e + 1])),
+                            __fmul_rn (tt[2], g.mproj[3 * e + 2]));
+                    }
+                    in = in && ma > -0.5f && ma < g.m_hi[e];
+                    // li_clamp without conversions: floor(max(ma, 0)) from
+                    // an add rounded down to 2^23, corner clamped to dim - 2,
+                    // fraction saturated to [0, 1]
+                    const float big = __fadd_rd (fmaxf (ma, 0.f), 8388608.f);
+                    f[e] = min (__float_as_int (big) - 0x4B000000, g.mdim[e] - 2);
+                    const float fc = fminf (big - 8388608.f, g.m_fmax[e]);
+                    const float w = __saturatef (ma - fc);
+                    w2[h][e] = w;
+                    up[e] = w >= 0.5f;
+                }
+                fidx[h] = max (frow, 0) + fic;
+                if (ROI) {
+                    // the image ROIs (flavour i): fixed at the voxel,
+                    // moving at the moving position
+                    in = in && roi_fixed_ok (g, fidx[h])
+                        && roi_moving_ok (g, fxyz, d);
+                }
+                ok[h] = in;
+                mvf[h] = f[0] + dxm * (f[1] + g.mdim[1] * f[2]);
+                mvr[h] = mvf[h] + (up[0] ? 1 : 0) + (up[1] ? dxm : 0)
+                    + (up[2] ? dxym : 0);
+            }
+            float cr[2][8], fv[2], gr[2][3];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float* mp = a.mimg + mvf[h];
+                cr[h][0] = __ldg (mp);
+                cr[h][1] = __ldg (mp + 1);
+                cr[h][2] = __ldg (mp + dxm);
+                cr[h][3] = __ldg (mp + dxm + 1);
+                cr[h][4] = __ldg (mp + dxym);
+                cr[h][5] = __ldg (mp + dxym + 1);
+                cr[h][6] = __ldg (mp + dxym + dxm);
+                cr[h][7] = __ldg (mp + dxym + dxm + 1);
+                fv[h] = __ldg (a.fimg + fidx[h]);
+                if (MODE == 0) {
+                    const float* gp = a.mgrad + 3 * mvr[h];
+                    gr[h][0] = __ldg (gp);
+                    gr[h][1] = __ldg (gp + 1);
+                    gr[h][2] = __ldg (gp + 2);
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                float diff = trilinear_lerp (w2[h], cr[h]) - fv[h];
+                diff = ok[h] ? diff : 0.f;
+                scf = fmaf (diff, diff, scf);
+                cnt += ok[h] ? 1 : 0;
+                float dc[3];
+                if (MODE == 0) {
+                    dc[0] = diff * gr[h][0];
+                    dc[1] = diff * gr[h][1];
+                    dc[2] = diff * gr[h][2];
+                } else {
+                    float gl[3];
+                    trilinear_lerp_grad (g, w2[h], cr[h], gl);
+                    dc[0] = diff * gl[0];
+                    dc[1] = diff * gl[1];
+                    dc[2] = diff * gl[2];
+                }
+                if (rowv[h]) {
+                    const int rho = r0 + u0 + h;
+                    uint8_t* p = dcb + (rho >> 3) * 1024 + (rho & 7) * 128
+                        + ((xch ^ (rho & 7)) << 4);
+#pragma unroll
+                    for (int e = 0; e < 3; e++) {
+                        const uint32_t w = split_word (dc[e]);
+                        *(unsigned short*) (p + 4096 * e) = (unsigned short) w;
+                        *(unsigned short*) (p + XS_DC_LO + 4096 * e)
+                            = (unsigned short) (w >> 16);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// x-forward MMA of a step: D[x][(c, rho)] = Bx[x][xk] R[xk][(c, rho)],
+// K = 32 knots, three split terms; one thread.
+__device__ __forceinline__ void
+xl_issue_forward (const XlCtx& x, int buf, uint64_t* bar)
+{
+    const uint32_t idesc = idesc_bf16_f32 (128, XL_N, 0, 1);
+    const uint32_t ta = x.sm_base + XS_TAB;
+    const uint32_t tb = x.sm_base + XS_B2 + buf * XS_B2_BUF;
+#pragma unroll
+    for (int term = 0; term < 3; term++) {
+        const uint32_t A = term == 2 ? ta + XS_TAB_LO : ta;     // hi, hi, lo
+        const uint32_t B = term == 1 ? tb + XS_B2_LO : tb;      // hi, lo, hi
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+            tc_mma_bf16 (x.taddr + XT_D + 128 * buf,
+                smem_desc_sw128 (A + ks * 32, 16, 1024),
+                smem_desc_sw128 (B + ks * 2048, 4096, 1024), idesc,
+                (term > 0 || ks > 0) ? 1u : 0u);
+        }
+    }
+    tc_commit (bar);
+}
+
+// x-adjoint MMA of a step: Rg[(c, xk)][(c', rho)] = Bx[x][xk] DC[x][(c', rho)]
+// (the table read MN-major: M = four copies of the 32 knots), K = 128
+// voxels, three split terms; one thread.
+__device__ __forceinline__ void
+xl_issue_adjoint (const XlCtx& x, int buf, uint64_t* bar)
+{
+    const uint32_t idesc = idesc_bf16_f32 (128, XL_N, 1, 0);
+    const uint32_t ta = x.sm_base + XS_TAB;
+    const uint32_t td = x.sm_base + XS_DC + buf * XS_DC_BUF;
+#pragma unroll
+    for (int term = 0; term < 3; term++) {
+        const uint32_t A = term == 2 ? ta + XS_TAB_LO : ta;
+        const uint32_t B = term == 1 ? td + XS_DC_LO : td;
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) {
+            tc_mma_bf16 (x.taddr + XT_RG + 128 * buf,
+                smem_desc_sw128 (A + ks * 2048, 16384, 1024),
+                smem_desc_sw128 (B + (ks >> 2) * XS_DC_ATOM + (ks & 3) * 32,
+                    16, 1024), idesc, (term > 0 || ks > 0) ? 1u : 0u);
+        }
+    }
+    tc_commit (bar);
+}
+
+}  // namespace
+
+template <int MODE, bool AXIS, bool ROI>
+__global__ void __launch_bounds__ (XL_BLOCK, 1)
+mse_xl_kernel (XlArgs a)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint64_t s_bar[8];
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_abort;
+
+    const BspGeom& g = a.g;
+    XlCtx x;
+    x.sm = smem_raw + ((1024u - (smem_addr (smem_raw) & 1023u)) & 1023u);
+    x.sm_base = smem_addr (x.sm);
+    const int tid = threadIdx.x;
+    x.warp = tid >> 5;
+    x.lane = tid & 31;
+    x.q = x.warp & 3;
+    x.j4 = x.warp >> 2;
+    const bool mma_warp = x.warp == XL_CW;
+
+    if (tid == 0) {
+        mbar_init (&s_bar[XB_B2], 4);
+        mbar_init (&s_bar[XB_B2 + 1], 4);
+        mbar_init (&s_bar[XB_DC], XL_CW);
+        mbar_init (&s_bar[XB_DC + 1], XL_CW);
+        mbar_init (&s_bar[XB_D], 1);
+        mbar_init (&s_bar[XB_D + 1], 1);
+        mbar_init (&s_bar[XB_RG], 1);
+        mbar_init (&s_bar[XB_RG + 1], 1);
+        fence_barrier_init ();
+        s_abort = 0;
+    }
+    if (mma_warp) {
+        tmem_alloc (&s_taddr, XT_COLS);
+        tmem_relinquish ();
+    } else {
+        // the basis table; both dc/dv buffers zeroed (entries the voxel
+        // phase never writes stay zero); the y and z basis values
+        uint4* tab = (uint4*) (x.sm + XS_TAB);
+        for (int o = tid; o < 65536 / 16; o += XL_THREADS) tab[o] = a.tab[o];
+        uint4* dcz = (uint4*) (x.sm + XS_DC);
+        for (int o = tid; o < 2 * XS_DC_BUF / 16; o += XL_THREADS) {
+            dcz[o] = make_uint4 (0, 0, 0, 0);
+        }
+        float* lut = (float*) (x.sm + XS_LUT);
+        const int nby = 4 * g.vpr[1], nbz = 4 * g.vpr[2];
+        for (int o = tid; o < nby + nbz; o += XL_THREADS) {
+            lut[o] = a.luts[4 * g.vpr[0] + o];
+        }
+        fence_proxy_async_smem ();
+    }
+    tc_fence_before ();
+    __syncthreads ();
+    tc_fence_after ();
+    x.taddr = s_taddr;
+    volatile int* abort_flag = &s_abort;
+    const int nb_local = (a.nbatches - (int) blockIdx.x + (int) gridDim.x - 1)
+        / (int) gridDim.x;
+    const int S = nb_local * a.nch;
+
+    if (mma_warp) {
+        if (x.lane == 0) {
+            // phase parities, bit buf of each word (no local arrays)
+            uint32_t ph_b2 = 0, ph_dc = 0;
+            auto wait = [&](uint64_t* bar, uint32_t& ph, int buf, int code) {
+                for (uint32_t n = 0; n < a.wait_limit && !*abort_flag; n++) {
+                    if (mbar_try_wait (bar, (ph >> buf) & 1u)) {
+                        ph ^= 1u << buf;
+                        return true;
+                    }
+                }
+                *abort_flag = 1;
+                atomicExch (a.err, code);
+                return false;
+            };
+            for (int s = 0; s <= S; s++) {
+                if (s < S) {
+                    const int buf = s & 1;
+                    if (!wait (&s_bar[XB_B2 + buf], ph_b2, buf, 3)) break;
+                    tc_fence_after ();
+                    xl_issue_forward (x, buf, &s_bar[XB_D + buf]);
+                }
+                if (s >= 1) {
+                    const int pb = (s - 1) & 1;
+                    if (!wait (&s_bar[XB_DC + pb], ph_dc, pb, 4)) break;
+                    tc_fence_after ();
+                    xl_issue_adjoint (x, pb, &s_bar[XB_RG + pb]);
+                }
+            }
+        }
+        __syncwarp ();
+    } else {
+        uint32_t ph_d = 0, ph_rg = 0;       // phase parity of buffer b: bit b
+        const bool yz_fwd_warp = x.q == 3;
+        const bool vox_live = 32 * x.q < a.T * g.vpr[0];
+        float G[4] = {0.f, 0.f, 0.f, 0.f};
+        double sc = 0.0;
+        int cnt = 0;
+        bool ok = true;
+        if (yz_fwd_warp) {
+            for (int s = 0; s < 2 && s < S; s++) {
+                xl_yz_forward (a, x, xl_step (a, s), s);
+                fence_proxy_async_smem ();
+                __syncwarp ();
+                if (x.lane == 0) mbar_arrive (&s_bar[XB_B2 + s]);
+            }
+        }
+        // adjoint y/z of step sp (quarters 0..2): accumulate, and write
+        // the batch's partial gradient at its last chunk
+        auto yz_adjoint = [&](int sp) {
+            const int pb = sp & 1;
+            if (!xl_wait (a, x, &s_bar[XB_RG + pb], (ph_rg >> pb) & 1u,
+                    abort_flag, 2)) {
+                return false;
+            }
+            ph_rg ^= 1u << pb;
+            tc_fence_after ();
+            const XlStep t = xl_step (a, sp);
+            if (t.ch == 0) G[0] = G[1] = G[2] = G[3] = 0.f;
+            xl_yz_adjoint (a, x, t, pb, G);
+            tc_fence_before ();
+            if (t.ch == a.nch - 1 && x.lane < a.KX) {
+                const int KF = 16 * a.KX;
+                float* dst = a.part + ((size_t) t.b * 3 + x.q) * KF + x.lane
+                    + a.KX * 4 * x.j4;
+#pragma unroll
+                for (int j = 0; j < 4; j++) dst[a.KX * j] = G[j];
+            }
+            return true;
+        };
+        for (int s = 0; s < S && ok; s++) {
+            const int buf = s & 1;
+            if (!xl_wait (a, x, &s_bar[XB_D + buf], (ph_d >> buf) & 1u,
+                    abort_flag, 1)) {
+                ok = false;
+                break;
+            }
+            ph_d ^= 1u << buf;
+            tc_fence_after ();
+            const XlStep t = xl_step (a, s);
+            if (vox_live) {
+                float scf = 0.f;
+                xl_voxel<MODE, AXIS, ROI> (a, x, t, buf, scf, cnt);
+                sc += (double) scf;
+            }
+            if (t.ch == a.nch - 1) {
+                // the warp's score and count of the batch, fixed tree order
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sc += __shfl_down_sync (0xffffffffu, sc, o);
+                    cnt += __shfl_down_sync (0xffffffffu, cnt, o);
+                }
+                if (x.lane == 0) {
+                    a.score_part[(size_t) t.b * XL_CW + x.warp] = sc;
+                    a.count_part[(size_t) t.b * XL_CW + x.warp] = cnt;
+                }
+                sc = 0.0;
+                cnt = 0;
+            }
+            fence_proxy_async_smem ();
+            tc_fence_before ();
+            __syncwarp ();
+            if (x.lane == 0) mbar_arrive (&s_bar[XB_DC + buf]);
+            if (yz_fwd_warp) {
+                if (s + 2 < S) {
+                    xl_yz_forward (a, x, xl_step (a, s + 2), buf);
+                    fence_proxy_async_smem ();
+                    __syncwarp ();
+                    if (x.lane == 0) mbar_arrive (&s_bar[XB_B2 + buf]);
+                }
+            } else if (s >= 1) {
+                ok = yz_adjoint (s - 1);
+            }
+        }
+        if (ok && !yz_fwd_warp && S >= 1) yz_adjoint (S - 1);
+    }
+
+    tc_fence_before ();
+    __syncthreads ();
+    if (mma_warp) tmem_dealloc (x.taddr, XT_COLS);
+}
+
+// ------------------------------------------------------------------ host --
+
+bool
+xl_plan (const BspGeom& g, XlPlan* p, int sm_count)
+{
+    const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
+    if (vy < 3 || vy > 10 || vx < 1 || vz < 1) return false;
+    // tiles per batch: T vx <= 128 voxels and T + 3 <= 32 knots along x;
+    // the fewest batches per row, balanced; a split row needs T >= 3 (the
+    // finish kernel's gather assumes a knot meets at most two batches)
+    const int tmax = std::min (128 / vx, XL_KMAX - 3);
+    if (tmax < 1) return false;
+    const int nb_row = (g.rdims[0] + tmax - 1) / tmax;
+    const int T = (g.rdims[0] + nb_row - 1) / nb_row;
+    if (nb_row > 1 && T < 3) return false;
+    p->T = T;
+    p->nbx = nb_row;
+    p->nbatches = nb_row * g.rdims[1] * g.rdims[2];
+    // rows per chunk: whole z planes of vy rows, at most 32 rows
+    const int nlz_max = XL_RC / vy;
+    p->nch = (vz + nlz_max - 1) / nlz_max;
+    p->nlz = (vz + p->nch - 1) / p->nch;
+    p->smem = XS_TOTAL + 1024;
+    p->threads = XL_BLOCK;
+    p->grid = std::min (p->nbatches, sm_count);
+    p->score_parts = p->nbatches * XL_CW;
+    return true;
+}
+
+// The basis table image: 128 voxel rows x 128 columns m = c * 32 + xk
+// (c = 0..2 copies of the 32 knot columns, c = 3 zero), bf16 hi then lo,
+// each the exact 128-byte-swizzled shared-memory image (32 KB).  Row x of a
+// batch, x < T vx, holds bx[x mod vx][xk - x div vx] on the band.
+int
+xl_build_table (const BspGeom& g, const XlPlan& p, const float* bx_lut,
+    void** d_tab)
+{
+    const int vx = g.vpr[0];
+    std::vector<uint8_t> img (65536, 0);
+    for (int xr = 0; xr < 128; xr++) {
+        for (int m = 0; m < 128; m++) {
+            const int c = m >> 5, xk = m & 31;
+            float v = 0.f;
+            if (c < 3 && xr < p.T * vx) {
+                const int i = xk - xr / vx;
+                if (i >= 0 && i < 4) v = bx_lut[4 * (xr % vx) + i];
+            }
+            __nv_bfloat16 h = __float2bfloat16_rn (v);
+            __nv_bfloat16 l = __float2bfloat16_rn (v - __bfloat162float (h));
+            const uint32_t off = sw128_offset (xr, m, 128);
+            *(unsigned short*) (img.data () + off) = __bfloat16_as_ushort (h);
+            *(unsigned short*) (img.data () + 32768 + off) = __bfloat16_as_ushort (l);
+        }
+    }
+    if (cudaMalloc (d_tab, img.size ()) != cudaSuccess) return B200BSP_E_OOM;
+    if (cudaMemcpy (*d_tab, img.data (), img.size (), cudaMemcpyHostToDevice)
+        != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    return B200BSP_OK;
+}
+
+template <int MODE, bool AXIS, bool ROI>
+static cudaError_t
+xl_launch_t (const XlPlan& p, const XlArgs& a, cudaStream_t st)
+{
+    auto k = mse_xl_kernel<MODE, AXIS, ROI>;
+    cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int) p.smem);
+    k<<<p.grid, XL_BLOCK, p.smem, st>>> (a);
+    return cudaGetLastError ();
+}
+
+cudaError_t
+launch_mse_xl (const BspGeom& g, const XlPlan& p, int grad_mode,
+    const float* fimg, const float* mimg, const float* mgrad,
+    const float* coeff, const void* tab, const float* luts, float* part,
+    double* score_part, int* count_part, int* err, unsigned wait_limit,
+    cudaStream_t st)
+{
+    XlArgs a;
+    a.g = g;
+    a.T = p.T;
+    a.KX = p.T + 3;
+    a.nbx = p.nbx;
+    a.nbatches = p.nbatches;
+    a.nlz = p.nlz;
+    a.nch = p.nch;
+    a.wait_limit = wait_limit;
+    a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;
+    a.tab = (const uint4*) tab;
+    a.luts = luts;
+    a.part = part; a.score_part = score_part; a.count_part = count_part;
+    a.err = err;
+    bool axis = true;
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            if (i != j && (g.fstep[3 * i + j] != 0.f || g.mproj[3 * i + j] != 0.f)) {
+                axis = false;
+            }
+        }
+    }
+    const bool roi = g.fmask || g.mroi;
+    if (roi) {
+        if (grad_mode == 0) {
+            return axis ? xl_launch_t<0, true, true> (p, a, st)
+                        : xl_launch_t<0, false, true> (p, a, st);
+        }
+        return axis ? xl_launch_t<1, true, true> (p, a, st)
+                    : xl_launch_t<1, false, true> (p, a, st);
+    }
+    if (grad_mode == 0) {
+        return axis ? xl_launch_t<0, true, false> (p, a, st)
+                    : xl_launch_t<0, false, false> (p, a, st);
+    }
+    return axis ? xl_launch_t<1, true, false> (p, a, st)
+                : xl_launch_t<1, false, false> (p, a, st);
+}
+
+}  // namespace b200

@@ -104,7 +104,7 @@ b200bsp_score_mse_static (const b200bsp_volume* fixed,
         && mse_grad != B200BSP_MSE_GRAD_TRILINEAR) {
         return static_fail (B200BSP_E_BADARG, "unknown mse_grad");
     }
-    BspGeom g;
+    BspGeom g = {};
     float luts[4 * 3 * 64];
     int nlut = 0;
     int rc = static_geometry (fixed, moving, grid, &g, luts, &nlut);

@@ -60,6 +60,14 @@ struct b200bsp_ctx {
 
     PartLayout lay;
     TcPlan plan;
+    // the x-lane tensor-core MSE kernel (mse_xl.cu) where its plan exists
+    // and the autotuner has not preferred the tile kernel
+    bool use_xl = false;
+    bool has_xl = false;
+    XlPlan xplan;
+    PartLayout xlay;
+    void* d_xtab = nullptr;
+    unsigned wait_limit = XL_DEFAULT_WAIT_LIMIT;
     int tc_grid = 0;          // CTAs of the tile kernel; 0: plan.grid
     // the optimiser's device workspace, kept between runs (optimize.cu)
     void* opt_ws = nullptr;
@@ -69,6 +77,11 @@ struct b200bsp_ctx {
 
     MiState mi;
     RegState reg;
+
+    // image ROIs (b200bsp_set_roi): the fixed ROI's test per fixed voxel,
+    // the moving ROI's mask; geom.fmask / geom.mroi point at them
+    uint8_t* d_fmask = nullptr;
+    uint8_t* d_mroi = nullptr;
 
     // landmark pairs (b200bsp_set_landmarks)
     int lm_n = 0;
@@ -242,9 +255,10 @@ free_all (b200bsp_ctx* c)
     cudaFree (c->d_coeff); cudaFree (c->d_luts); cudaFree (c->d_grad);
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
     cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
-    cudaFree (c->d_qlut); cudaFree (c->d_inv_dc);
+    cudaFree (c->d_qlut); cudaFree (c->d_xtab); cudaFree (c->d_inv_dc);
     cudaFree (c->d_lm_p); cudaFree (c->d_lm_w); cudaFree (c->d_lm_fm);
     cudaFree (c->d_lm_dc);
+    cudaFree (c->d_fmask); cudaFree (c->d_mroi);
     cudaFreeHost (c->h_res); cudaFreeHost (c->h_scalar);
     mi_free (&c->mi);
     reg_free (&c->reg);
@@ -281,7 +295,7 @@ static_geometry (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         return fail (nullptr, B200BSP_E_BADARG,
             "singular matrix of direction cosines");
     }
-    BspGeom g;
+    BspGeom g = {};
     long long ntiles = 1, nknots = 1;
     for (int d = 0; d < 3; d++) {
         g.fdim[d] = (int) fixed->dim[d];
@@ -426,6 +440,13 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         return fail (nullptr, B200BSP_E_BADARG,
             "Parzen-window MI needs at least 5 bins");
     }
+    if (o.mi_hist != B200BSP_MI_HIST_EQSP && o.mi_hist != B200BSP_MI_HIST_VOPT) {
+        return fail (nullptr, B200BSP_E_BADARG, "unknown mi_hist %d", o.mi_hist);
+    }
+    if (o.mi_hist == B200BSP_MI_HIST_VOPT && o.mi_window != B200BSP_MI_PVI8) {
+        return fail (nullptr, B200BSP_E_BADARG,
+            "V-optimal bins are a PVI-8 histogram type");
+    }
     if (o.mi_bins < 2 || o.mi_bins > MI_MAX_BINS) {
         return fail (nullptr, B200BSP_E_BADARG, "mi_bins must be in [2, %d]",
             MI_MAX_BINS);
@@ -508,7 +529,19 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     alloc ((void**) &c->d_fixed, nf * sizeof (float));
     alloc ((void**) &c->d_moving, nm * sizeof (float));
     if (o.mse_grad == 0) alloc ((void**) &c->d_mgrad, 3 * nm * sizeof (float));
-    if (o.mse_grad == 0 && o.form == B200BSP_FORM_TC) {
+    int sm_count = 148;
+    cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount, o.device);
+    if (o.form == B200BSP_FORM_TC) {
+        c->has_xl = c->use_xl = xl_plan (g, &c->xplan, sm_count);
+    }
+    if (o.wait_limit < 0) {
+        rc2 = fail (c, B200BSP_E_BADARG, "wait_limit must be >= 0");
+    } else if (o.wait_limit > 0) {
+        c->wait_limit = (unsigned) o.wait_limit;
+    }
+    // the tile kernel's 16-byte moving-gradient copy, only where the x-lane
+    // kernel does not apply
+    if (o.mse_grad == 0 && o.form == B200BSP_FORM_TC && !c->has_xl) {
         alloc ((void**) &c->d_mgrad4, nm * sizeof (float4));
     }
     alloc ((void**) &c->d_coeff, c->num_coeff * sizeof (float));
@@ -531,8 +564,6 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     }
 
     // Tile partial-gradient layout of the chosen form.
-    int sm_count = 148;
-    cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount, o.device);
     size_t part_elems = 0;
     size_t score_parts = 0;
     if (!rc2 && o.form == B200BSP_FORM_TC) {
@@ -550,6 +581,17 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
                 score_parts = std::max (score_parts, (size_t) p.nbatches);
             }
             use_tc_plan (c, c->plan);
+            if (c->has_xl) {
+                const XlPlan& xp = c->xplan;
+                part_elems = std::max (part_elems,
+                    (size_t) xp.nbatches * (xp.T + 3) * 16 * 3);
+                score_parts = std::max (score_parts, (size_t) xp.score_parts);
+                PartLayout& L = c->xlay;
+                L.bx = xp.T; L.by = 1; L.bz = 1;
+                L.nbx = xp.nbx; L.nby = g.rdims[1]; L.nbz = g.rdims[2];
+                L.kx = xp.T + 3; L.ky = 4; L.kz = 4;
+                L.slots = 1;
+            }
         }
     } else if (!rc2) {
         if (mse_fp32_smem_bytes (g) > 200 * 1024) {
@@ -571,7 +613,8 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
         if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
     }
-    if (!rc2 && mi_alloc (&c->mi, c->geom, o.mi_bins, o.mi_window)) {
+    if (!rc2 && mi_alloc (&c->mi, c->geom, o.mi_bins, o.mi_window,
+            o.mi_hist)) {
         rc2 = fail (c, B200BSP_E_OOM, "MI buffers: out of device memory");
     }
     if (!rc2) {
@@ -604,6 +647,15 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     basis_lut (luts.data (), g.vpr[0]);
     basis_lut (luts.data () + 4 * g.vpr[0], g.vpr[1]);
     basis_lut (luts.data () + 4 * (g.vpr[0] + g.vpr[1]), g.vpr[2]);
+    if (c->has_xl) {
+        int rt = xl_build_table (g, c->xplan, luts.data (), &c->d_xtab);
+        if (rt) {
+            cudaGetLastError ();
+            free_all (c);
+            delete c;
+            return fail (nullptr, rt, "tensor-core x-lane table");
+        }
+    }
     cudaMemcpy (c->d_luts, luts.data (), nlut * sizeof (float),
         cudaMemcpyHostToDevice);
     cudaMemcpy (c->d_inv_dc, minv, 9 * sizeof (float), cudaMemcpyHostToDevice);
@@ -761,6 +813,17 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
         CK (launch_mse_fp32 (g, c->opts.mse_grad, c->d_fixed, c->d_moving,
             c->d_mgrad, dcoeff, c->d_luts, c->d_part, c->d_score_part,
             c->d_count_part, c->stream));
+    } else if (c->use_xl) {
+        XlPlan plan = c->xplan;
+        // a batch's share of the SMs' CTA slots counts two per SM (the
+        // tile kernel's); this kernel runs one CTA per SM
+        if (c->tc_grid > 0) {
+            plan.grid = std::min (std::max (1, c->tc_grid / 2), plan.nbatches);
+        }
+        CK (launch_mse_xl (g, plan, c->opts.mse_grad, c->d_fixed,
+            c->d_moving, c->d_mgrad, dcoeff, c->d_xtab, c->d_luts,
+            c->d_part, c->d_score_part, c->d_count_part, c->d_err,
+            c->wait_limit, c->stream));
     } else {
         TcPlan plan = c->plan;
         if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
@@ -772,8 +835,10 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     c->last_launches++;
     int rc = mark_main_done (c);
     if (rc) return rc;
-    CK (launch_finish_mse (g, c->lay, c->d_part, c->d_score_part,
-        c->d_count_part, c->nscore_parts,
+    const bool xl = c->opts.form == B200BSP_FORM_TC && c->use_xl;
+    CK (launch_finish_mse (g, xl ? c->xlay : c->lay, c->d_part,
+        c->d_score_part, c->d_count_part,
+        xl ? c->xplan.score_parts : c->nscore_parts,
         c->opts.form == B200BSP_FORM_TC ? c->d_err : nullptr, c->d_res,
         res_host, grad_out, grad64_out, score_out, score64_out, nvox_out,
         c->stream));
@@ -882,58 +947,115 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     CK (cudaEventCreate (&e0));
     CK (cudaEventCreate (&e1));
     const TcPlan start = c->plan;
+    const bool start_xl = c->use_xl;
     TcPlan best = start;
+    bool best_xl = start_xl;
     float best_ms = 0.f;
-    for (int e = 0; e <= TC_TUNE_MAX_EXTRA && !rc; e++) {
+    auto time_it = [&](float* ms) {
+        int r = run_mse (c, dcoeff, c->d_grad, nullptr, nullptr, nullptr,
+            nullptr);                                    // warm-up
+        if (!r && cudaEventRecord (e0, c->stream) != cudaSuccess) r = B200BSP_E_CUDA;
+        for (int i = 0; i < evals && !r; i++) {
+            r = run_mse (c, dcoeff, c->d_grad, nullptr, nullptr, nullptr,
+                nullptr);
+        }
+        if (!r && (cudaEventRecord (e1, c->stream) != cudaSuccess
+                || cudaEventSynchronize (e1) != cudaSuccess
+                || cudaEventElapsedTime (ms, e0, e1) != cudaSuccess)) {
+            r = B200BSP_E_CUDA;
+        }
+        return r;
+    };
+    // candidates: the x-lane kernel, then each batch split of the tile
+    // kernel; ties keep the earlier candidate
+    if (c->has_xl) {
+        c->use_xl = true;
+        float ms = 0.f;
+        rc = time_it (&ms);
+        if (!rc) {
+            best_ms = ms;
+            best_xl = true;
+        }
+    }
+    c->use_xl = false;
+    const bool roi = c->geom.fmask || c->geom.mroi;
+    for (int e = 0; e <= TC_TUNE_MAX_EXTRA && !rc && !roi; e++) {
         TcPlan p;
         if (!tc_plan (c->geom, &p, 2, sm_count, e)) continue;
         use_tc_plan (c, p);
-        rc = run_mse (c, dcoeff, c->d_grad, nullptr, nullptr, nullptr,
-            nullptr);                                    // warm-up
-        if (!rc && cudaEventRecord (e0, c->stream) != cudaSuccess) rc = B200BSP_E_CUDA;
-        for (int i = 0; i < evals && !rc; i++) {
-            rc = run_mse (c, dcoeff, c->d_grad, nullptr, nullptr, nullptr,
-                nullptr);
-        }
         float ms = 0.f;
-        if (!rc && (cudaEventRecord (e1, c->stream) != cudaSuccess
-                || cudaEventSynchronize (e1) != cudaSuccess
-                || cudaEventElapsedTime (&ms, e0, e1) != cudaSuccess)) {
-            rc = B200BSP_E_CUDA;
-        }
+        rc = time_it (&ms);
         if (!rc && (best_ms == 0.f || ms < best_ms)) {
             best_ms = ms;
             best = p;
+            best_xl = false;
         }
     }
     cudaEventDestroy (e0);
     cudaEventDestroy (e1);
     use_tc_plan (c, rc ? start : best);
+    c->use_xl = rc ? start_xl : best_xl;
     if (rc) {
         cudaGetLastError ();
         return fail (c, rc, "autotuning failed");
     }
-    if (tiles) *tiles = best.bx;
+    if (tiles) *tiles = c->use_xl ? c->xplan.T : best.bx;
     return check_device_error (c);
 }
 
 // One or both MI passes on the context's form (tensor-core modes where they
 // apply); gradients to grad (float) or grad64 (double), device pointers.
 static int
-mi_passes (b200bsp_ctx* c, const float* dcoeff, float* grad, double* grad64,
-    int passes)
+mi_passes_on (b200bsp_ctx* c, const BspGeom& g, const float* dcoeff,
+    float* grad, double* grad64, int passes)
 {
-    if (c->opts.form == B200BSP_FORM_TC
-        && tc_mi_supported (c->geom, c->plan, c->mi.bins)) {
+    const bool roi = g.fmask || g.mroi;
+    if (c->opts.form == B200BSP_FORM_TC && !roi
+        && tc_mi_supported (g, c->plan, c->mi.bins)) {
         TcPlan plan = c->plan;
         if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
-        return mi_run_tc (&c->mi, c->geom, plan, c->lay, c->d_qlut,
+        return mi_run_tc (&c->mi, g, plan, c->lay, c->d_qlut,
             c->d_part, c->d_score_part, c->d_count_part, c->d_err, dcoeff,
             c->d_moving, c->d_res, grad, grad64, c->stream,
             &c->last_launches, passes);
     }
-    return mi_run (&c->mi, c->geom, dcoeff, c->d_moving, c->d_luts, c->d_res,
+    return mi_run (&c->mi, g, dcoeff, c->d_moving, c->d_luts, c->d_res,
         grad, grad64, c->stream, &c->last_launches, passes);
+}
+
+// Whether the PVI-8 histogram pass must scan more than the ROI: the
+// reference's flavours g/h scan the whole fixed image with tile index
+// ijk / vox_per_rgn (bspline_mi.cxx:1562-1620), which is in range only when
+// the grid starts at voxel 0 and its tiles cover the image.  Returns 1
+// (whole image differs from the ROI), 0 (ROI is the image) or -1
+// (unsupported).
+static int
+mi_whole_image_pass1 (const b200bsp_ctx* c)
+{
+    const BspGeom& g = c->geom;
+    int differs = 0;
+    for (int d = 0; d < 3; d++) {
+        if (g.roi_off[d] != 0 || g.rdims[d] * g.vpr[d] < g.fdim[d]) return -1;
+        if (g.roi_dim[d] != g.fdim[d]) differs = 1;
+    }
+    return differs;
+}
+
+static int
+mi_passes (b200bsp_ctx* c, const float* dcoeff, float* grad, double* grad64,
+    int passes)
+{
+    if (c->opts.mi_window == B200BSP_MI_PVI8 && (passes & MI_PASS_HIST)
+        && mi_whole_image_pass1 (c) == 1) {
+        // pass 1 over the whole image with the same tile grid, pass 2
+        // over the ROI
+        BspGeom g1 = c->geom;
+        for (int d = 0; d < 3; d++) g1.roi_dim[d] = g1.fdim[d];
+        int rc = mi_passes_on (c, g1, dcoeff, grad, grad64, MI_PASS_HIST);
+        if (rc || !(passes & MI_PASS_GRAD)) return rc;
+        passes = MI_PASS_GRAD;
+    }
+    return mi_passes_on (c, c->geom, dcoeff, grad, grad64, passes);
 }
 
 extern "C" int
@@ -942,15 +1064,14 @@ b200bsp_score_mi (b200bsp_ctx* c, const float* coeff, float* score,
     double* j_hist)
 {
     if (!c) return B200BSP_E_BADARG;
-    for (int d = 0; d < 3 && c->opts.mi_window == B200BSP_MI_PVI8; d++) {
-        if (c->geom.roi_off[d] != 0 || c->geom.roi_dim[d] != c->geom.fdim[d]) {
-            // The reference's histogram pass scans the whole fixed image
-            // while its gradient pass scans the ROI; the two agree only
-            // when the ROI is the whole image.  (The Parzen variant scans
-            // the ROI in both passes.)
-            return fail (c, B200BSP_E_UNSUPPORTED,
-                "MI needs the ROI to cover the whole fixed image");
-        }
+    if (c->opts.mi_window == B200BSP_MI_PVI8 && mi_whole_image_pass1 (c) < 0) {
+        // The reference's histogram pass scans the whole fixed image with
+        // tile index ijk / vox_per_rgn; unless the grid starts at voxel 0
+        // and covers the image it reads past its tile tables.  (The Parzen
+        // variant scans the ROI in both passes.)
+        return fail (c, B200BSP_E_UNSUPPORTED,
+            "PVI-8 MI needs the grid to start at voxel 0 and its tiles to "
+            "cover the fixed image");
     }
     const float* dcoeff = nullptr;
     int rc = begin_eval (c, coeff, &dcoeff);
@@ -983,7 +1104,8 @@ b200bsp_mi_hist (b200bsp_ctx* c, const float* coeff, int64_t* hist)
     const float* dcoeff = nullptr;
     int rc = begin_eval (c, coeff, &dcoeff);
     if (rc) return rc;
-    rc = mi_passes (c, dcoeff, nullptr, nullptr, MI_PASS_HIST);
+    // over the context's ROI (a slab's pass 1; see the header)
+    rc = mi_passes_on (c, c->geom, dcoeff, nullptr, nullptr, MI_PASS_HIST);
     if (rc) return fail (c, rc, "MI pass 1 failed: %s",
         cudaGetErrorString (cudaGetLastError ()));
     const int B = c->mi.bins;
@@ -1011,8 +1133,8 @@ b200bsp_mi_grad (b200bsp_ctx* c, const float* coeff, const int64_t* hist,
         is_device_ptr (hist) ? cudaMemcpyDeviceToDevice
                              : cudaMemcpyHostToDevice, c->stream));
     const bool dev_grad = is_device_ptr (grad);
-    rc = mi_passes (c, dcoeff, nullptr, dev_grad ? grad : c->d_grad64,
-        MI_PASS_GRAD);
+    rc = mi_passes_on (c, c->geom, dcoeff, nullptr,
+        dev_grad ? grad : c->d_grad64, MI_PASS_GRAD);
     if (rc) return fail (c, rc, "MI pass 2 failed: %s",
         cudaGetErrorString (cudaGetLastError ()));
     CK (cudaMemcpyAsync (c->h_res, c->d_res, sizeof (DevResult),
@@ -1103,6 +1225,106 @@ free_landmarks (b200bsp_ctx* c)
     c->d_lm_p = nullptr; c->d_lm_w = nullptr; c->d_lm_fm = nullptr;
     c->d_lm_dc = nullptr;
     c->lm_n = 0;
+}
+
+static bool
+roi_geom (const b200bsp_volume* v, RoiGeom* o)
+{
+    float inv[9];
+    if (!inv3f (inv, v->dcos)) return false;
+    for (int d = 0; d < 3; d++) {
+        if (v->dim[d] < 1 || v->dim[d] > (1 << 30) || !(v->spacing[d] != 0.f)
+            || !std::isfinite (v->spacing[d])) {
+            return false;
+        }
+        o->dim[d] = (int) v->dim[d];
+        o->origin[d] = v->origin[d];
+    }
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            o->step[3*i+j] = v->dcos[3*i+j] * v->spacing[j];
+            o->proj[3*i+j] = inv[3*i+j] / v->spacing[i];
+        }
+    }
+    return (long long) o->dim[0] * o->dim[1] * o->dim[2] < (1LL << 31);
+}
+
+extern "C" int
+b200bsp_set_roi (b200bsp_ctx* c, const b200bsp_volume* fixed_roi,
+    const uint8_t* fixed_mask, const b200bsp_volume* moving_roi,
+    const uint8_t* moving_mask)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (!fixed_roi != !fixed_mask || !moving_roi != !moving_mask) {
+        return fail (c, B200BSP_E_BADARG,
+            "an ROI needs both its geometry and its mask");
+    }
+    RoiGeom fr, mr;
+    if ((fixed_roi && !roi_geom (fixed_roi, &fr))
+        || (moving_roi && !roi_geom (moving_roi, &mr))) {
+        return fail (c, B200BSP_E_BADARG,
+            "ROI geometry: need dims >= 1 (< 2^31 voxels), finite nonzero "
+            "spacing and invertible direction cosines");
+    }
+    const bool any = fixed_roi || moving_roi;
+    if (any && c->opts.form == B200BSP_FORM_TC && !c->has_xl) {
+        return fail (c, B200BSP_E_UNSUPPORTED,
+            "image ROIs in the tensor-core form need its x-lane kernel "
+            "(3 <= vox_per_rgn[1] <= 10); use B200BSP_FORM_FP32");
+    }
+    CK (cudaSetDevice (c->device));
+    CK (cudaStreamSynchronize (c->stream));
+    cudaFree (c->d_fmask);
+    cudaFree (c->d_mroi);
+    c->d_fmask = nullptr;
+    c->d_mroi = nullptr;
+    BspGeom& g = c->geom;
+    g.fmask = nullptr;
+    g.mroi = nullptr;
+    if (fixed_roi) {
+        const size_t nr = (size_t) fr.dim[0] * fr.dim[1] * fr.dim[2];
+        const size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
+        uint8_t* d_roi = nullptr;
+        const bool dev = is_device_ptr (fixed_mask);
+        if (!dev) CK (cudaMalloc ((void**) &d_roi, nr));
+        CK (cudaMalloc ((void**) &c->d_fmask, nf));
+        cudaError_t e = cudaSuccess;
+        if (!dev) {
+            e = cudaMemcpyAsync (d_roi, fixed_mask, nr, cudaMemcpyHostToDevice,
+                c->stream);
+        }
+        RoiGeom fg;
+        for (int d = 0; d < 3; d++) {
+            fg.dim[d] = g.fdim[d];
+            fg.origin[d] = g.img_origin[d];
+        }
+        for (int i = 0; i < 9; i++) fg.step[i] = g.fstep[i];
+        if (e == cudaSuccess) {
+            e = launch_fixed_roi_mask (g.fdim, fg, fr, dev ? fixed_mask : d_roi,
+                c->d_fmask, c->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize (c->stream);
+        cudaFree (d_roi);
+        if (e != cudaSuccess) {
+            return fail (c, B200BSP_E_CUDA, "fixed ROI: %s",
+                cudaGetErrorString (e));
+        }
+        g.fmask = c->d_fmask;
+    }
+    if (moving_roi) {
+        const size_t nr = (size_t) mr.dim[0] * mr.dim[1] * mr.dim[2];
+        CK (cudaMalloc ((void**) &c->d_mroi, nr));
+        CK (cudaMemcpy (c->d_mroi, moving_mask, nr, cudaMemcpyDefault));
+        for (int d = 0; d < 3; d++) {
+            g.mroi_dim[d] = mr.dim[d];
+            g.mroi_origin[d] = mr.origin[d];
+        }
+        for (int i = 0; i < 9; i++) g.mroi_proj[i] = mr.proj[i];
+        g.mroi = c->d_mroi;
+    }
+    // the tile kernel has no ROI tests: MSE stays on the x-lane kernel
+    if (any && c->opts.form == B200BSP_FORM_TC) c->use_xl = true;
+    return B200BSP_OK;
 }
 
 extern "C" int

@@ -75,6 +75,41 @@ class Volume:
 
 
 @dataclass
+class Roi:
+    """An image region of interest: a uint8 mask (nonzero = inside) shaped
+    (nz, ny, nx) with its own geometry, as Plastimatch's fixed_roi /
+    moving_roi volumes (src/register/bspline_state.h:44-45)."""
+    mask: np.ndarray
+    origin: tuple = (0.0, 0.0, 0.0)
+    spacing: tuple = (1.0, 1.0, 1.0)
+    dcos: tuple = IDENTITY_DCOS
+
+    def __post_init__(self):
+        self.mask = np.ascontiguousarray(self.mask, dtype=np.uint8)
+        self.origin = tuple(float(v) for v in self.origin)
+        self.spacing = tuple(float(v) for v in self.spacing)
+        self.dcos = tuple(float(v) for v in self.dcos)
+
+    @property
+    def dim(self) -> tuple:
+        nz, ny, nx = self.mask.shape
+        return (nx, ny, nz)
+
+    @classmethod
+    def like(cls, vol: Volume, mask) -> "Roi":
+        """A mask on the voxel grid of `vol`."""
+        return cls(mask, vol.origin, vol.spacing, vol.dcos)
+
+    @classmethod
+    def from_window(cls, vol: Volume, lo: float, hi: float) -> "Roi":
+        """Voxels of `vol` with lo <= value <= hi: the mask a registration
+        stage builds from its MI intensity window on an image without a
+        ROI (update_roi, src/register/bspline_stage.cxx:72-95)."""
+        img = vol.img
+        return cls.like(vol, ((img >= lo) & (img <= hi)).astype(np.uint8))
+
+
+@dataclass
 class BsplineGrid:
     """The B-spline control grid over a fixed image's ROI."""
     img_origin: tuple

@@ -41,3 +41,21 @@ def rel_err(a, b):
     b = np.asarray(b, np.float64)
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def load_rois(rec):
+    """The (fixed, moving) image ROIs stored in a roimask_* golden case."""
+    from plastimatch_b200.geometry import Roi
+
+    def mk(p):
+        return Roi(rec[f"{p}_mask"], origin=tuple(float(v) for v in rec[f"{p}_origin"]),
+                   spacing=tuple(float(v) for v in rec[f"{p}_spacing"]),
+                   dcos=tuple(float(v) for v in rec[f"{p}_dcos"]))
+    return mk("froi"), mk("mroi")
+
+
+ROI_TAGS = ("f", "m", "fm")
+
+
+def pick_rois(tag, froi, mroi):
+    return (froi if "f" in tag else None), (mroi if "m" in tag else None)

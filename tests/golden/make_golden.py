@@ -23,7 +23,7 @@ sys.path.insert(0, ROOT)
 
 import oracle as O  # noqa: E402
 from plastimatch_b200 import synth  # noqa: E402
-from plastimatch_b200.geometry import BsplineGrid, Volume  # noqa: E402
+from plastimatch_b200.geometry import BsplineGrid, Roi, Volume  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
@@ -81,6 +81,52 @@ RESAMPLE_CASES = {
 # its whole bspline_score (MSE flavour g + curvature 0.005 + landmarks).
 LANDMARK_CASES = {"landmarks_small": ("mse_small", 0.8, 17),
                   "landmarks_dcos": ("mse_dcos", 2.5, 23)}
+
+
+# Image-ROI fixtures (Bspline_state::fixed_roi / moving_roi): the inputs of
+# a case, a fixed ROI from an intensity window on the fixed image (as a
+# registration stage builds it from its MI window) and a moving ROI on its
+# own coarser, shifted grid (a box minus a slab), and the reference's ROI
+# flavours on them: MSE i (via 'g') and k (via 'c'), MI h (via 'g').
+# Names: roimask_<base>.
+ROI_CASES = {"roimask_mse_small": "mse_small", "roimask_mse_roi": "mse_roi",
+             "roimask_mse_dcos": "mse_dcos", "roimask_mi_small": "mi_small",
+             "roimask_mi_dcos": "mi_dcos"}
+
+# MI with a grid that starts at voxel 0 and covers the image with fewer
+# ROI voxels than the image (the reference's histogram pass still scans
+# the whole image): name -> (base, roi_dim).
+MI_PARTIAL_CASES = {"mi_partial": ("mi_small", (22, 19, 17))}
+
+
+# V-optimal histogram fixtures: the inputs of an MI case and the reference's
+# MI flavour g with Bspline_parms::mi_hist_type = HIST_VOPT.
+VOPT_CASES = {"vopt_mi_small": "mi_small", "vopt_mi_dcos": "mi_dcos"}
+
+
+def roi_pair(fixed, moving, seed):
+    lo = float(np.percentile(fixed.img, 35))
+    froi = Roi.from_window(fixed, lo, 1e30)
+    rng = np.random.default_rng(seed)
+    sp = tuple(1.7 * s for s in moving.spacing)
+    dim = tuple(int(np.ceil(d * s0 / s)) + 2 for d, s0, s in
+                zip(moving.dim, moving.spacing, sp))
+    m = np.zeros(dim[::-1], np.uint8)
+    m[1:-2, 2:-1, 1:-3] = 1
+    m[:, :, dim[0] // 2: dim[0] // 2 + 2] = 0
+    org = tuple(o - 0.6 * s + float(rng.uniform(-0.3, 0.3))
+                for o, s in zip(moving.origin, sp))
+    mroi = Roi(m, origin=org, spacing=sp, dcos=moving.dcos)
+    return froi, mroi
+
+
+def roi_record(froi, mroi):
+    return dict(froi_mask=froi.mask, froi_origin=np.array(froi.origin, np.float32),
+                froi_spacing=np.array(froi.spacing, np.float32),
+                froi_dcos=np.array(froi.dcos, np.float32),
+                mroi_mask=mroi.mask, mroi_origin=np.array(mroi.origin, np.float32),
+                mroi_spacing=np.array(mroi.spacing, np.float32),
+                mroi_dcos=np.array(mroi.dcos, np.float32))
 
 
 def landmark_points(fixed, n, seed):
@@ -202,6 +248,96 @@ def main(force=False):
             lm_score=np.float32(rl.score), lm_grad=rl.grad,
             total_score=np.float32(rt.score), total_grad=rt.grad,
             total_lm_score=np.float32(rs.score), total_lm_grad=rs.grad)
+        print("wrote", name)
+
+    for name, base in ROI_CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
+        dim, sp, vpr, roff, rdim, seed, dcos, remap, csig = CASES[base]
+        fixed, moving = make_pair(dim, sp, seed, dcos, remap)
+        grid = BsplineGrid.for_volume(fixed, vpr, roi_offset=roff,
+                                      roi_dim=rdim)
+        coeff = synth.random_coeff(grid, csig, seed=seed + 3)
+        froi, mroi = roi_pair(fixed, moving, seed + 5)
+        rec = dict(
+            fixed=fixed.img, moving=moving.img,
+            f_origin=np.array(fixed.origin, np.float32),
+            f_spacing=np.array(fixed.spacing, np.float32),
+            m_origin=np.array(moving.origin, np.float32),
+            m_spacing=np.array(moving.spacing, np.float32),
+            dcos=np.array(fixed.dcos, np.float32),
+            roi_offset=np.array(grid.roi_offset), roi_dim=np.array(grid.roi_dim),
+            vpr=np.array(grid.vox_per_rgn), coeff=coeff, **roi_record(froi, mroi))
+        rec["moving_grad"] = O.ref_volume_grad(moving)
+        for tag, fr, mr in (("f", froi, None), ("m", None, mroi),
+                            ("fm", froi, mroi)):
+            if base.startswith("mse"):
+                # flavour k (chosen for 'c') scans the whole fixed image,
+                # defined only when the grid's ROI is the image
+                for fl in ("gc" if rdim is None else "g"):
+                    r = O.ref_metric(grid, fixed, moving, coeff, flavor=fl,
+                                     fixed_roi=fr, moving_roi=mr)
+                    rec[f"{tag}_{fl}_score"] = np.float32(r.score)
+                    rec[f"{tag}_{fl}_grad"] = r.grad
+                    rec[f"{tag}_{fl}_num_vox"] = np.int64(r.num_vox)
+            else:
+                r = O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                                 metric="mi", bins=32, fixed_roi=fr,
+                                 moving_roi=mr)
+                rec[f"{tag}_mi_score"] = np.float32(r.score)
+                rec[f"{tag}_mi_grad"] = r.grad
+                rec[f"{tag}_mi_num_vox"] = np.int64(r.num_vox)
+                rec[f"{tag}_j_hist"] = r.j_hist
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **rec)
+        print("wrote", name)
+
+    for name, base in VOPT_CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
+        dim, sp, vpr, roff, rdim, seed, dcos, remap, csig = CASES[base]
+        fixed, moving = make_pair(dim, sp, seed, dcos, remap)
+        grid = BsplineGrid.for_volume(fixed, vpr, roi_offset=roff,
+                                      roi_dim=rdim)
+        coeff = synth.random_coeff(grid, csig, seed=seed + 3)
+        r = O.ref_metric(grid, fixed, moving, coeff, flavor="g", metric="mi",
+                         bins=32, hist="vopt")
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            fixed=fixed.img, moving=moving.img,
+            f_origin=np.array(fixed.origin, np.float32),
+            f_spacing=np.array(fixed.spacing, np.float32),
+            m_origin=np.array(moving.origin, np.float32),
+            m_spacing=np.array(moving.spacing, np.float32),
+            dcos=np.array(fixed.dcos, np.float32),
+            roi_offset=np.array(grid.roi_offset), roi_dim=np.array(grid.roi_dim),
+            vpr=np.array(grid.vox_per_rgn), coeff=coeff,
+            mi_score=np.float32(r.score), mi_grad=r.grad,
+            mi_num_vox=np.int64(r.num_vox), f_hist=r.f_hist, m_hist=r.m_hist,
+            j_hist=r.j_hist)
+        print("wrote", name)
+
+    for name, (base, rdim) in MI_PARTIAL_CASES.items():
+        if not force and os.path.exists(os.path.join(OUT, f"{name}.npz")):
+            continue
+        dim, sp, vpr, roff, _, seed, dcos, remap, csig = CASES[base]
+        fixed, moving = make_pair(dim, sp, seed, dcos, remap)
+        grid = BsplineGrid.for_volume(fixed, vpr, roi_dim=rdim)
+        coeff = synth.random_coeff(grid, csig, seed=seed + 3)
+        r = O.ref_metric(grid, fixed, moving, coeff, flavor="g", metric="mi",
+                         bins=32)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            fixed=fixed.img, moving=moving.img,
+            f_origin=np.array(fixed.origin, np.float32),
+            f_spacing=np.array(fixed.spacing, np.float32),
+            m_origin=np.array(moving.origin, np.float32),
+            m_spacing=np.array(moving.spacing, np.float32),
+            dcos=np.array(fixed.dcos, np.float32),
+            roi_offset=np.array(grid.roi_offset), roi_dim=np.array(grid.roi_dim),
+            vpr=np.array(grid.vox_per_rgn), coeff=coeff,
+            mi_score=np.float32(r.score), mi_grad=r.grad,
+            mi_num_vox=np.int64(r.num_vox), f_hist=r.f_hist, m_hist=r.m_hist,
+            j_hist=r.j_hist)
         print("wrote", name)
 
     for name, (mode, rate) in RESAMPLE_CASES.items():

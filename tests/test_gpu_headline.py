@@ -1,0 +1,69 @@
+"""Parity at the benchmark's own workload: the 256x256x128 CT-like phantom
+(0.98 x 0.98 x 2.5 mm), vox_per_rgn 5, coefficients N(0, 3 mm), exactly as
+bench.py times it (bench.make_workload), for both device forms.
+
+Bars (stated here):
+  score     relative 1e-5 against the double-precision oracle
+  gradient  relative 1e-3 (L2 norm of the difference over the norm of the
+            reference) against the double-precision oracle and against the
+            reference's own float flavour g (compiled in place,
+            oracle/_ref) on the same inputs
+  num_vox   within 0.01 % (+2) of the reference's count
+
+The phantom's +-1000..2000 HU edges make this the hardest case for the
+tensor-core form's 3-term bf16 split: its products are f32-accurate to
+about 2^-16, and every MSE gradient entry is a sum of ~8000 such products
+with cancellation across tissue edges.
+"""
+import numpy as np
+import pytest
+
+import bench
+import oracle as O
+import plastimatch_b200 as P
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2():
+    fixed, moving, grid, coeff = bench.make_workload()
+    mg = O.port_volume_grad(moving)
+    f64 = O.port_mse(grid, fixed, moving, coeff, moving_grad=mg,
+                     precision="f64")
+    ref = (O.ref_metric(grid, fixed, moving, coeff, flavor="g", threads=8)
+           if O.ref_available() else None)
+    return fixed, moving, grid, coeff, mg, f64, ref
+
+
+@pytest.mark.parametrize("form", ["tc", "fp32"])
+def test_headline_workload_parity(form, c2):
+    fixed, moving, grid, coeff, mg, f64, ref = c2
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images()
+        s, g, n = ctx.score_mse(coeff)
+        s2, g2, n2 = ctx.score_mse(coeff)
+    assert s == s2 and n == n2 and np.array_equal(g, g2)   # deterministic
+    assert abs(s - f64.score) <= 1e-5 * abs(f64.score), (s, f64.score)
+    e64 = rel_err(g, f64.grad)
+    assert e64 < 1e-3, e64
+    if ref is not None:
+        assert abs(n - ref.num_vox) <= 1e-4 * ref.num_vox + 2, (n, ref.num_vox)
+        eref = rel_err(g, ref.grad)
+        assert eref < 1e-3, eref
+        assert abs(s - ref.score) <= 1e-5 * abs(ref.score), (s, ref.score)
+
+
+@pytest.mark.parametrize("form", ["tc", "fp32"])
+def test_headline_workload_trilinear_gradient(form, c2):
+    fixed, moving, grid, coeff, _, _, _ = c2
+    with P.Context(fixed, moving, grid, form=form,
+                   mse_grad="trilinear") as ctx:
+        ctx.set_images()
+        s, g, n = ctx.score_mse(coeff)
+    f64 = O.port_mse(grid, fixed, moving, coeff, grad_mode=1,
+                     precision="f64")
+    assert abs(s - f64.score) <= 1e-5 * abs(f64.score), (s, f64.score)
+    assert rel_err(g, f64.grad) < 1e-3, rel_err(g, f64.grad)
+    assert abs(n - f64.num_vox) <= 1e-4 * f64.num_vox + 2

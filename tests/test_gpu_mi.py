@@ -108,3 +108,20 @@ def test_mi_no_overlap_and_roi_rejected(form):
         with pytest.raises(P.B200Error) as e:
             ctx.score_mi(np.zeros(roi.num_coeff, np.float32))
         assert e.value.code == -6
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("name", golden_names("vopt_mi"))
+def test_mi_vopt_golden(form, name):
+    """V-optimal bins: the device's bin images come from the restated
+    dynamic programme; the passes are those of equal spacing."""
+    fixed, moving, grid, coeff, rec = load_golden(name)
+    with P.Context(fixed, moving, grid, form=form, mi_bins=32,
+                   mi_hist="vopt") as ctx:
+        ctx.set_images()
+        s, g, n, (fh, mh, jh) = ctx.score_mi(coeff, with_hist=True)
+    f64 = O.port_mi(grid, fixed, moving, coeff, bins=32, precision="f64",
+                    hist="vopt")
+    _check(s, g, n, f64, rec["mi_grad"], int(rec["mi_num_vox"]))
+    assert rel_err(fh, rec["f_hist"]) < 1e-5
+    assert rel_err(jh, rec["j_hist"]) < 1e-5
