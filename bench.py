@@ -398,12 +398,17 @@ def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
     import torch
     lib = P.lib()
     reg = P.reg_parms(curvature=0.005)
-    s_c, n_c, r_c = C.c_float(), C.c_int64(), C.c_float()
+    s_c, n_c = C.c_float(), C.c_int64()
+
+    d_total = torch.zeros(4, device=d_grad.device)
 
     def mse_reg():
-        ctx.score_mse(d_coeff, grad_out=d_grad)
-        rc = lib.b200bsp_regularize(ctx._h, d_coeff.data_ptr(), C.byref(reg),
-                                    C.addressof(r_c), d_grad.data_ptr())
+        # bspline_score with device outputs: the regulariser overlaps the
+        # tile kernel on the context's second stream
+        rc = lib.b200bsp_score(ctx._h, d_coeff.data_ptr(), 0, C.c_float(1.0),
+                               C.byref(reg), d_total.data_ptr(),
+                               d_grad.data_ptr(), d_total[1:].data_ptr(),
+                               None)
         if rc:
             raise RuntimeError(lib.b200bsp_last_error(ctx._h))
 

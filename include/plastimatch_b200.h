@@ -216,6 +216,21 @@ int b200bsp_set_landmarks (b200bsp_ctx* ctx, const float* fixed_xyz,
     int64_t n_fixed, const float* moving_xyz, int64_t n_moving,
     float stiffness);
 
+/* Bounded device-side waits of the tensor-core MSE kernel (no reference
+ * counterpart; the reference exits on failures): `polls` mbarrier polls
+ * before a wait gives up and the call returns B200BSP_E_TIMEOUT (0: the
+ * default, 1 << 22, or opts.wait_limit).  withhold_mma != 0 is a testing
+ * aid: the kernel's tensor-core warp then issues no MMA, so the compute
+ * warps' first wait runs out after `polls` polls -- the failure path, on a
+ * GPU, without a fault.  On expiry every warp leaves its loop, the issued
+ * MMAs are drained and TMEM is released; the context stays usable. */
+int b200bsp_set_wait_limit (b200bsp_ctx* ctx, int polls, int withhold_mma);
+
+/* Testing aid: the nth device allocation made by the next b200bsp_create
+ * calls of this thread fails as if the device were full (0 disables).  The
+ * create returns B200BSP_E_OOM and releases everything it allocated. */
+void b200bsp_debug_fail_alloc (int nth);
+
 /* Image ROIs of the cost function: Bspline_state::fixed_roi and
  * ::moving_roi (src/register/bspline_state.h:44-45), uchar mask volumes
  * (x fastest, nonzero = inside) with their own geometry.  A fixed voxel
@@ -424,10 +439,13 @@ int b200bsp_lbfgs_minimize (int64_t n, double* x, b200bsp_eval_fn fn,
  * the current device (moving_grad only for B200BSP_MSE_GRAD_NEAREST;
  * score and num_vox may be NULL); the call is ordered on `stream` and
  * returns without waiting.  Grids of more than B200BSP_STATIC_MAX_TILES
- * tiles are rejected (B200BSP_E_UNSUPPORTED).  The first call on each
- * device looks up the array's address; make it before any stream capture.
- * Calls whose device work overlaps race on the shared array: issue them on
- * one stream.  Errors are reported through b200bsp_last_error (NULL). */
+ * tiles are rejected (B200BSP_E_UNSUPPORTED).  Every call looks up the
+ * array's address in the current context (the first one on a device also
+ * loads the library's module there); make the first call before any
+ * stream capture.  A CUDA error already pending when the call starts is
+ * reported (B200BSP_E_CUDA) and left pending.  Calls whose device work
+ * overlaps race on the shared array: issue them on one stream.  Errors
+ * are reported through b200bsp_last_error (NULL). */
 int b200bsp_score_mse_static (const b200bsp_volume* fixed,
     const b200bsp_volume* moving, const b200bsp_grid* grid, int mse_grad,
     const float* fixed_img, const float* moving_img, const float* moving_grad,

@@ -742,3 +742,43 @@ def ref_lbfgs(fn, x0, max_its=1000):
     rc = ref().lbfgs(C.c_int(n), x.ctypes.data_as(C.POINTER(C.c_double)),
                      C.byref(fx), cb_e, cb_p, None, None)
     return x, fx.value, rc, state["k"], state["fe"]
+
+
+# ------------------------------------------------------------- adapter ---
+
+ADAPTER_SO = os.path.join(HERE, "_ref", "libb200adapter.so")
+
+
+def adapter_available() -> bool:
+    return os.path.exists(ADAPTER_SO)
+
+
+def adapter_compare(grid, fixed, moving, coeff, flavor="g", metric="mse",
+                    bins=32, hist="eqsp", threads=8, fixed_roi=None,
+                    moving_roi=None):
+    """Score the reference's own objects through the reference-side
+    drop-in (oracle/ref/b200_adapter.cxx: bspline_b200_state_create +
+    bspline_score_b200, linked with the reference build and the product
+    library) and through the reference's CPU flavour: (b200 Result,
+    reference Result).  Needs a GPU for the first."""
+    lib = C.CDLL(ADAPTER_SO)
+    n = grid.num_coeff
+    g_b, g_r = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    s_b, s_r = C.c_float(), C.c_float()
+    n_b, n_r = C.c_int64(), C.c_int64()
+    u8 = C.POINTER(C.c_uint8)
+    rois = []
+    for r in (fixed_roi, moving_roi):
+        rois += ([None, None] if r is None
+                 else [C.byref(_ref_geom(r)), r.mask.ctypes.data_as(u8)])
+    rc = lib.adapter_compare(
+        C.byref(_ref_geom(fixed)), _p(fixed.img), C.byref(_ref_geom(moving)),
+        _p(moving.img), C.byref(_ref_grid(grid)),
+        _p(np.ascontiguousarray(coeff, np.float32)), C.c_char(flavor.encode()),
+        C.c_int(1 if metric == "mi" else 0), C.c_int(bins),
+        C.c_int(1 if hist == "vopt" else 0), C.c_int(threads), *rois,
+        C.byref(s_b), C.byref(n_b), _p(g_b), C.byref(s_r), C.byref(n_r),
+        _p(g_r))
+    if rc:
+        raise RuntimeError(f"adapter failed with status {rc}")
+    return Result(s_b.value, g_b, n_b.value), Result(s_r.value, g_r, n_r.value)

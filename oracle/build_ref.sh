@@ -9,10 +9,15 @@
 # headers on the path, and oracle/ref/ holds stand-ins for the two
 # cmake-generated headers (plm_config.h, plm_version.h).
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or PLM_REFERENCE in the
+# environment)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${PLM_REFERENCE:-}}"
+if [ -z "$REF" ]; then
+    echo "build_ref: give the reference tree as an argument or PLM_REFERENCE" >&2
+    exit 1
+fi
 SRC="$REF/src"
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"
@@ -68,3 +73,15 @@ for p in "${pids[@]}"; do wait "$p"; done
 $CXX -shared -fopenmp -Wl,--no-undefined -o "$OUT/libplmref.so" \
     "${OBJS[@]}" "$OBJ/lbfgs.o" "$OBJ/ref_driver.o" -lm
 echo "build_ref: wrote $OUT/libplmref.so"
+
+# The reference-side drop-in (oracle/ref/b200_adapter.cxx): the adapter a
+# maintainer would add, compiled against the reference headers and linked
+# with both libraries, for the tests that drive the product through it.
+B200="$HERE/../plastimatch_b200"
+if [ -f "$B200/libplastimatch_b200.so" ]; then
+    $CXX $CXXFLAGS -c "$HERE/ref/b200_adapter.cxx" -o "$OBJ/b200_adapter.o"
+    $CXX -shared -fopenmp -o "$OUT/libb200adapter.so" "$OBJ/b200_adapter.o" \
+        -L"$OUT" -lplmref -L"$B200" -lplastimatch_b200 \
+        -Wl,-rpath,'$ORIGIN' -Wl,-rpath,'$ORIGIN/../../plastimatch_b200'
+    echo "build_ref: wrote $OUT/libb200adapter.so"
+fi

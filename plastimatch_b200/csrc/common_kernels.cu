@@ -190,8 +190,15 @@ finish_mse_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
     const int* __restrict__ err, DevResult* __restrict__ res,
     DevResult* __restrict__ res_host, float* __restrict__ grad_out,
     double* __restrict__ grad64_out, float* __restrict__ score_out,
-    double* __restrict__ score64_out, long long* __restrict__ nvox_out)
+    double* __restrict__ score64_out, long long* __restrict__ nvox_out,
+    unsigned* __restrict__ clear, int nclear, FinishCombine cb)
 {
+    // the tile kernel's per-batch arrival counters start the next
+    // evaluation at zero, also after a tile kernel that gave up early
+    for (int i = blockIdx.x * FIN_THREADS + threadIdx.x; i < nclear;
+         i += gridDim.x * FIN_THREADS) {
+        clear[i] = 0u;
+    }
     __shared__ double sh_v[FIN_THREADS / 32];
     __shared__ int sh_n[FIN_THREADS / 32];
     __shared__ long long s_n;
@@ -234,6 +241,14 @@ finish_mse_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
             }
             *res = r;
             if (res_host) *res_host = r;
+            if (cb.total_score) {
+                // Bspline_score::accumulate then the regulariser's score
+                // (src/register/bspline.cxx:595-622), in float
+                float total = 0.f;
+                total += cb.lambda * r.score_f;
+                if (cb.reg_score) total += (float) *cb.reg_score;
+                *cb.total_score = total;
+            }
             if (score_out) *score_out = r.score_f;
             if (score64_out) *score64_out = r.score;
             if (nvox_out) *nvox_out = r.num_vox;
@@ -312,6 +327,18 @@ finish_mse_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
     s_g[3 * threadIdx.x] = s0 * scale;
     s_g[3 * threadIdx.x + 1] = s1 * scale;
     s_g[3 * threadIdx.x + 2] = s2 * scale;
+    if (cb.total_score && knot < g.nknots) {
+        // total_grad = 0 + lambda * smetric_grad (float), then the
+        // regulariser's double gradient added with one rounding, as the
+        // separate calls would leave it
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            float t = 0.f + cb.lambda * (float) s_g[3 * threadIdx.x + c];
+            s_g[3 * threadIdx.x + c] = cb.reg_grad
+                ? (double) (float) ((double) t + cb.reg_grad[3 * (size_t) knot + c])
+                : (double) t;
+        }
+    }
     __syncthreads ();
     const int n = 3 * min (FIN_THREADS, g.nknots - knot0);
     if (grad_out) store_run<float> (grad_out + 3 * (size_t) knot0, s_g, n);
@@ -323,12 +350,13 @@ launch_finish_mse (const BspGeom& g, const PartLayout& lay, const float* part,
     const double* score_part, const int* count_part, int nparts,
     const int* err, DevResult* res, DevResult* res_host, float* grad_out,
     double* grad64_out, float* score_out, double* score64_out,
-    long long* nvox_out, cudaStream_t st)
+    long long* nvox_out, cudaStream_t st, unsigned* clear, int nclear,
+    const FinishCombine& cb)
 {
     const int blocks = std::max (1, (g.nknots + FIN_THREADS - 1) / FIN_THREADS);
     finish_mse_kernel<<<blocks, FIN_THREADS, 0, st>>> (g, lay, part,
         score_part, count_part, nparts, err, res, res_host, grad_out,
-        grad64_out, score_out, score64_out, nvox_out);
+        grad64_out, score_out, score64_out, nvox_out, clear, nclear, cb);
     return cudaGetLastError ();
 }
 

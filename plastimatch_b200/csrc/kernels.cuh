@@ -73,11 +73,20 @@ bool xl_plan (const BspGeom& g, XlPlan* plan, int sm_count);
 int xl_build_table (const BspGeom& g, const XlPlan& plan, const float* bx_lut,
     void** d_tab);
 constexpr unsigned XL_DEFAULT_WAIT_LIMIT = 1u << 22;
+// Per-warp score partials and per-batch arrival counters (the last warp of
+// a batch to finish sums the batch's partials in a fixed order); arrive
+// must be zero before a launch (the finish kernel clears it).
+struct XlScratch {
+    double* wscore;      // [batch][compute warp]
+    int* wcount;
+    unsigned* arrive;    // [batch]
+};
+constexpr int XL_COMPUTE_WARPS = 16;
 cudaError_t launch_mse_xl (const BspGeom& g, const XlPlan& plan,
     int grad_mode, const float* fimg, const float* mimg, const float* mgrad,
     const float* coeff, const void* tab, const float* luts, float* part,
     double* score_part, int* count_part, int* err, unsigned wait_limit,
-    cudaStream_t st);
+    int withhold, const XlScratch& scratch, cudaStream_t st);
 
 // Mattes MI on the tensor-core kernel (axis-aligned geometry, tiles of at
 // most 128 voxels, histograms that fit the adjoint operand's area): pass 1
@@ -97,6 +106,13 @@ struct TcMiArgs {
     float m_min, m_delta;        // Parzen: moving value -> window centre
 };
 bool tc_mi_supported (const BspGeom& g, const TcPlan& p, int bins);
+// The same passes on the x-lane kernel (mse_xl.cu): pass 1 into mi.hist,
+// pass 2's partial gradients into part (the x-lane batch layout).
+bool xl_mi_supported (int bins);
+cudaError_t launch_mi_xl (const BspGeom& g, const XlPlan& p, bool hist_pass,
+    const TcMiArgs& mi, const float* coeff, const void* tab,
+    const float* luts, float* part, int* err, unsigned wait_limit,
+    cudaStream_t st);
 cudaError_t launch_mi_tc (const BspGeom& g, const TcPlan& p, bool hist_pass,
     const TcMiArgs& mi, const float* coeff, const void* qimg, float* part,
     double* score_part, int* count_part, int* err, cudaStream_t st);
@@ -110,6 +126,16 @@ cudaError_t launch_field_warp (const BspGeom& g, const float* coeff,
     const float* luts, const float* mimg, float default_value, float* vf,
     float* warped, cudaStream_t st);
 
+// bspline_score's combination done by the finish kernel (all device
+// pointers; total_score null: plain metric output): total score = lambda *
+// score + reg score, gradient = lambda * metric gradient + reg gradient.
+struct FinishCombine {
+    float lambda = 1.f;
+    const double* reg_grad = nullptr;    // [num_coeff] or null
+    const double* reg_score = nullptr;   // or null
+    float* total_score = nullptr;
+};
+
 // Score reduction + per-knot gradient gather, MSE normalisation, one
 // launch.  err (may be null): the tile kernel's error flag, copied into the
 // result block; res_host (may be null): a second copy of the result block,
@@ -118,7 +144,9 @@ cudaError_t launch_finish_mse (const BspGeom& g, const PartLayout& lay,
     const float* part, const double* score_part, const int* count_part,
     int nparts, const int* err, DevResult* res, DevResult* res_host,
     float* grad_out, double* grad64_out, float* score_out,
-    double* score64_out, long long* nvox_out, cudaStream_t st);
+    double* score64_out, long long* nvox_out, cudaStream_t st,
+    unsigned* clear = nullptr, int nclear = 0,
+    const FinishCombine& combine = FinishCombine ());
 
 cudaError_t launch_reduce_score (const double* score_part,
     const int* count_part, int n, DevResult* res, int mode,

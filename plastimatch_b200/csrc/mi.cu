@@ -941,6 +941,61 @@ mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
 }
 
+// The two passes on the x-lane tensor-core kernel (any geometry; tiles
+// with 3 <= vox_per_rgn[1] <= 10); the caller has checked
+// xl_mi_supported.
+int
+mi_run_xl (MiState* s, const BspGeom& g, const XlPlan& plan,
+    const PartLayout& lay, const void* tab, const float* luts, float* part,
+    int* err, unsigned wait_limit, const float* d_coeff,
+    const float* d_moving, DevResult* d_res, float* grad_out,
+    double* grad64_out, cudaStream_t st, int* launches, int passes)
+{
+    if (!s->ready) return B200BSP_E_STATE;
+    const int B = s->bins;
+    const int nh = 2 * B + B * B;
+    if ((passes & MI_PASS_HIST)
+        && cudaMemsetAsync (s->d_hist, 0, (nh + 1) * sizeof (unsigned long long),
+            st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    TcMiArgs mi;
+    mi.fbin = s->d_fbin;
+    mi.mbin = s->d_mbin;
+    mi.bins = B;
+    mi.lut = s->d_lut;
+    mi.nvf = s->d_nvf;
+    mi.hist = s->d_hist;
+    mi.parzen = s->window == B200BSP_MI_PARZEN;
+    mi.mimg = d_moving;
+    mi.m_min = s->pz_mmin;
+    mi.m_delta = s->pz_mdelta;
+    if ((passes & MI_PASS_HIST)
+        && launch_mi_xl (g, plan, true, mi, d_coeff, tab, luts, part, err,
+            wait_limit, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    if (!(passes & MI_PASS_GRAD)) {
+        if (launches) *launches += 1;
+        return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+    }
+    if (mi.parzen) {
+        parzen_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->pz_mdelta,
+            s->d_histd, s->d_lut, s->d_nvf, d_res);
+    } else {
+        mi_score_kernel<<<1, 1024, 0, st>>> (s->d_hist, B, s->d_histd,
+            s->d_lut, s->d_nvf, d_res);
+    }
+    if (launch_mi_xl (g, plan, false, mi, d_coeff, tab, luts, part, err,
+            wait_limit, st) != cudaSuccess
+        || launch_gather_grad (g, lay, part, d_res, 1, grad_out, grad64_out,
+            nullptr, nullptr, nullptr, st) != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    if (launches) *launches += 4;
+    return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
+}
+
 int
 mi_fetch (MiState* s, const DevResult* d_res, double* f_hist, double* m_hist,
     double* j_hist, cudaStream_t st)

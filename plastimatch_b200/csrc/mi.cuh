@@ -65,6 +65,12 @@ int mi_run_tc (MiState* s, const BspGeom& g, const TcPlan& plan,
     int* count_part, int* err, const float* d_coeff, const float* d_moving,
     DevResult* d_res, float* grad_out, double* grad64_out, cudaStream_t st,
     int* launches, int passes = MI_PASS_HIST | MI_PASS_GRAD);
+int mi_run_xl (MiState* s, const BspGeom& g, const XlPlan& plan,
+    const PartLayout& lay, const void* tab, const float* luts, float* part,
+    int* err, unsigned wait_limit, const float* d_coeff,
+    const float* d_moving, DevResult* d_res, float* grad_out,
+    double* grad64_out, cudaStream_t st, int* launches,
+    int passes = MI_PASS_HIST | MI_PASS_GRAD);
 int mi_fetch (MiState* s, const DevResult* d_res, double* f_hist,
     double* m_hist, double* j_hist, cudaStream_t st);
 void mi_finish (MiState* s, MiResult* r);

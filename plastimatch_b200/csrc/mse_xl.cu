@@ -56,7 +56,7 @@ namespace b200 {
 
 namespace {
 
-constexpr int XL_CW = 16;                    // compute warps
+constexpr int XL_CW = XL_COMPUTE_WARPS;      // compute warps
 constexpr int XL_THREADS = 32 * XL_CW;
 constexpr int XL_BLOCK = XL_THREADS + 32;    // + the tensor-core warp
 constexpr int XL_KMAX = 32;                  // knots per batch along x
@@ -85,6 +85,28 @@ constexpr int XT_COLS = 512;
 constexpr int XT_D = 0;
 constexpr int XT_RG = 256;
 
+// What the kernel computes (template argument MODE).
+constexpr int XM_MSE_NEAREST = 0;   // MSE, moving gradient at the nearest voxel
+constexpr int XM_MSE_LINEAR = 1;    // MSE, trilinear moving gradient
+constexpr int XM_MI_GRAD = 2;       // Mattes MI pass 2, PVI-8 factor table
+constexpr int XM_MI_HIST = 3;       // Mattes MI pass 1, PVI-8 histograms
+constexpr int XM_PZ_GRAD = 4;       // Parzen-window MI pass 2
+constexpr int XM_PZ_HIST = 5;       // Parzen-window MI pass 1
+
+__host__ __device__ constexpr bool
+xl_hist_mode (int m)
+{
+    return m == XM_MI_HIST || m == XM_PZ_HIST;
+}
+
+__host__ __device__ constexpr bool
+xl_mse_mode (int m)
+{
+    return m == XM_MSE_NEAREST || m == XM_MSE_LINEAR;
+}
+
+constexpr float XL_MI_WUNIT = 16777216.0f;   // histogram weights in 2^-24
+
 // Barriers.
 constexpr int XB_B2 = 0;       // + buf: R operand written (4 warp arrivals)
 constexpr int XB_DC = 2;       // + buf: dc/dv written, D read (16 arrivals)
@@ -98,6 +120,8 @@ struct XlArgs {
     int T, KX, nbx, nbatches;
     int nlz, nch;            // z planes per row chunk, chunks per batch
     unsigned wait_limit;
+    int withhold;            // testing aid: the tensor-core warp issues
+                             // nothing, so the first waits run out
     const float* fimg;
     const float* mimg;
     const float* mgrad;      // xyz interleaved (nearest-voxel mode)
@@ -105,9 +129,21 @@ struct XlArgs {
     const uint4* tab;        // the basis table image (64 KB)
     const float* luts;       // bx[vx][4], by[vy][4], bz[vz][4]
     float* part;             // [batch][c][xk + KX (j + 4 k)]
-    double* score_part;      // [batch][warp]
-    int* count_part;         // [batch][warp]
+    double* score_part;      // [batch]
+    int* count_part;         // [batch]
+    XlScratch sx;            // per-warp partials, arrival counters
     int* err;
+    // Mattes MI modes: bin images, bins, the pass-2 factor table [fixed
+    // bin][moving bin], the voxel count (float; Parzen: [1] the pass-2
+    // scale), the global histograms f[B], m[B], j[B*B], count; Parzen's
+    // moving value -> window centre
+    const uint8_t* fbin;
+    const uint8_t* mbin;
+    int bins;
+    const float* mi_lut;
+    const float* mi_nvf;
+    unsigned long long* hist;
+    float pz_mmin, pz_mdelta;
 };
 
 namespace {
@@ -267,6 +303,185 @@ xl_yz_adjoint (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
     }
 }
 
+// Mattes MI pass 2 at one sample (bspline_mi_pvi_8_dc_dv_dcos,
+// src/register/bspline_mi.txx:9-120): the derivative of each PVI-8 corner
+// weight along x, y, z times that corner's factor f[fixed bin][corner bin],
+// negated, divided by the voxel count, then projected by the moving
+// image's projection matrix in place (each row sees the rows above already
+// updated, as the reference does).  w2: the upper-corner fractions.
+__device__ __forceinline__ void
+xl_mi_dc_dv (const XlArgs& a, const float w2[3], int fb, const int mb[8],
+    float nv, float dc[3])
+{
+    const float* l2 = w2;
+    const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
+    const float dw[24] = {
+        (-1) * l1[1] * l1[2], l1[0] * (-1) * l1[2], l1[0] * l1[1] * (-1),
+        (+1) * l1[1] * l1[2], l2[0] * (-1) * l1[2], l2[0] * l1[1] * (-1),
+        (-1) * l2[1] * l1[2], l1[0] * (+1) * l1[2], l1[0] * l2[1] * (-1),
+        (+1) * l2[1] * l1[2], l2[0] * (+1) * l1[2], l2[0] * l2[1] * (-1),
+        (-1) * l1[1] * l2[2], l1[0] * (-1) * l2[2], l1[0] * l1[1] * (+1),
+        (+1) * l1[1] * l2[2], l2[0] * (-1) * l2[2], l2[0] * l1[1] * (+1),
+        (-1) * l2[1] * l2[2], l1[0] * (+1) * l2[2], l1[0] * l2[1] * (+1),
+        (+1) * l2[1] * l2[2], l2[0] * (+1) * l2[2], l2[0] * l2[1] * (+1)};
+    const float* lut = a.mi_lut + fb * a.bins;
+    float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const float f = __ldg (lut + mb[k]);
+        d0 -= dw[3 * k + 0] * f;
+        d1 -= dw[3 * k + 1] * f;
+        d2 -= dw[3 * k + 2] * f;
+    }
+    d0 = d0 / nv;
+    d1 = d1 / nv;
+    d2 = d2 / nv;
+    const float* p = a.g.mproj;
+    d0 = d0 * p[0] + d1 * p[1] + d2 * p[2];
+    d1 = d0 * p[3] + d1 * p[4] + d2 * p[5];
+    d2 = d0 * p[6] + d1 * p[7] + d2 * p[8];
+    dc[0] = d0;
+    dc[1] = d1;
+    dc[2] = d2;
+}
+
+// Mattes MI pass 1 at one sample: the PVI-8 corner weights as integers in
+// 2^-24 units (sums independent of their order), corners with equal moving
+// bins merged; the first two (fixed, moving) pairs of every lane combine
+// across the warp (match + reduce) so one lane per distinct pair updates
+// the shared joint histogram, further pairs go straight to the shared
+// atomics; the fixed histogram counts each first-pair group's voxels (the
+// moving one is the joint's column sums, taken at the flush).  Every lane
+// of the warp calls this (warp collectives).
+__device__ __forceinline__ void
+xl_mi_hist_add (const XlArgs& a, unsigned long long* hf, bool live,
+    const float w2[3], int fb, const int mb[8], int lane, int& cnt)
+{
+    const int B = a.bins;
+    unsigned long long* hj = hf + 2 * B;
+    const float* l2 = w2;
+    const float l1[3] = {1.f - w2[0], 1.f - w2[1], 1.f - w2[2]};
+    const float w[8] = {l1[0] * l1[1] * l1[2], l2[0] * l1[1] * l1[2],
+        l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
+        l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
+    unsigned int q[8];
+    bool first[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        q[k] = __float2uint_rn (w[k] * XL_MI_WUNIT);
+        first[k] = live;
+    }
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+#pragma unroll
+        for (int k2 = 0; k2 < k; k2++) {
+            if (first[k] && first[k2] && mb[k2] == mb[k]) {
+                q[k2] += q[k];
+                first[k] = false;
+            }
+        }
+    }
+    bool two = false, many = false;
+    int mb2 = 0;
+    unsigned int q2 = 0;
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+        many = many || (first[k] && two);
+        mb2 = (first[k] && !two) ? mb[k] : mb2;
+        q2 = (first[k] && !two) ? q[k] : q2;
+        two = two || first[k];
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        cnt++;
+        const int key = fb * B + mb[0];
+        const unsigned peers = __match_any_sync (live_mask, key);
+        const unsigned sum = __reduce_add_sync (peers, q[0]);
+        if (lane == __ffs (peers) - 1) {
+            atomicAdd (&hj[key], (unsigned long long) sum);
+            atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
+        }
+    }
+    const unsigned two_mask = __ballot_sync (0xffffffffu, two);
+    if (two) {
+        const int key = fb * B + mb2;
+        const unsigned peers = __match_any_sync (two_mask, key);
+        const unsigned sum = __reduce_add_sync (peers, q2);
+        if (lane == __ffs (peers) - 1) {
+            atomicAdd (&hj[key], (unsigned long long) sum);
+        }
+    }
+    if (many) {
+        bool seen = false;
+#pragma unroll
+        for (int k = 1; k < 8; k++) {
+            if (first[k] && seen) {
+                atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
+            }
+            seen = seen || first[k];
+        }
+    }
+}
+
+// Parzen-window MI pass 1 at one sample: the cubic window's four weights
+// at the moving value's window centre u (2^-24 units) into the fixed bin's
+// row of the shared joint histogram; lanes with the same (fixed bin, first
+// window bin) combine across the warp first.  Every lane calls this.
+__device__ __forceinline__ void
+xl_pz_hist_add (const XlArgs& a, unsigned long long* hf, bool live, int fb,
+    float u, int lane, int& cnt)
+{
+    const int B = a.bins;
+    unsigned long long* hj = hf + 2 * B;
+    const int k0 = parzen_first_bin (u, B);
+    unsigned int q[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        q[j] = __float2uint_rn (bspline3f ((float) (k0 + j) - u) * XL_MI_WUNIT);
+    }
+    const unsigned live_mask = __ballot_sync (0xffffffffu, live);
+    if (live) {
+        cnt++;
+        const int key = fb * B + k0;
+        const unsigned peers = __match_any_sync (live_mask, key);
+        unsigned sum[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) sum[j] = __reduce_add_sync (peers, q[j]);
+        if (lane == __ffs (peers) - 1) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (sum[j]) atomicAdd (&hj[key + j], (unsigned long long) sum[j]);
+            }
+        }
+    }
+}
+
+// Parzen-window MI pass 2 at one sample: 1/(N delta_m) times the sum over
+// the window's bins of beta3'(k - u) log(p(f, k) / p_m(k)) (the factor
+// table), times the world gradient of the trilinear interpolant (proj^T
+// times the index gradient; 0 along an axis the clamp holds).
+__device__ __forceinline__ void
+xl_pz_dc_dv (const XlArgs& a, float u, int fb, const float w2[3],
+    const float m[8], int clamp, float dc[3])
+{
+    const int B = a.bins;
+    const int k0 = parzen_first_bin (u, B);
+    const float* row = a.mi_lut + fb * B;
+    float sum = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        sum += bspline3f_d ((float) (k0 + j) - u) * __ldg (row + k0 + j);
+    }
+    float gi[3];
+    trilinear_igrad (w2, m, clamp, gi);
+    const float sc = __ldg (a.mi_nvf + 1) * sum;
+    const float* p = a.g.mproj;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        dc[c] = sc * (p[c] * gi[0] + p[3 + c] * gi[1] + p[6 + c] * gi[2]);
+    }
+}
+
 // The voxel phase of one step for warp (quarter q, rows part j4): the
 // warp's rows [ra, rb) of the chunk, four at a time (their field values as
 // three 4-column TMEM loads), two samples in flight per thread.
@@ -326,7 +541,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
 #pragma unroll
         for (int u0 = 0; u0 < 4; u0 += 2) {
             bool ok[2], rowv[2];
-            int mvf[2], mvr[2], fidx[2];
+            int mvf[2], mvr[2], fidx[2], clampb[2];
             float w2[2][3];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
@@ -346,6 +561,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                 bool in = rowv[h] && xlive && frow >= 0;
                 int f[3];
                 bool up[3];
+                clampb[h] = 0;
 #pragma unroll
                 for (int e = 0; e < 3; e++) {
                     float ma;
@@ -357,6 +573,10 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                             __fmul_rn (tt[2], g.mproj[3 * e + 2]));
                     }
                     in = in && ma > -0.5f && ma < g.m_hi[e];
+                    if (MODE == XM_PZ_GRAD
+                        && (ma < 0.f || ma >= g.m_fmax[e] + 1.f)) {
+                        clampb[h] |= 1 << e;      // li_clamp holds this axis
+                    }
                     // li_clamp without conversions: floor(max(ma, 0)) from
                     // an add rounded down to 2^23, corner clamped to dim - 2,
                     // fraction saturated to [0, 1]
@@ -379,44 +599,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                 mvr[h] = mvf[h] + (up[0] ? 1 : 0) + (up[1] ? dxm : 0)
                     + (up[2] ? dxym : 0);
             }
-            float cr[2][8], fv[2], gr[2][3];
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const float* mp = a.mimg + mvf[h];
-                cr[h][0] = __ldg (mp);
-                cr[h][1] = __ldg (mp + 1);
-                cr[h][2] = __ldg (mp + dxm);
-                cr[h][3] = __ldg (mp + dxm + 1);
-                cr[h][4] = __ldg (mp + dxym);
-                cr[h][5] = __ldg (mp + dxym + 1);
-                cr[h][6] = __ldg (mp + dxym + dxm);
-                cr[h][7] = __ldg (mp + dxym + dxm + 1);
-                fv[h] = __ldg (a.fimg + fidx[h]);
-                if (MODE == 0) {
-                    const float* gp = a.mgrad + 3 * mvr[h];
-                    gr[h][0] = __ldg (gp);
-                    gr[h][1] = __ldg (gp + 1);
-                    gr[h][2] = __ldg (gp + 2);
-                }
-            }
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                float diff = trilinear_lerp (w2[h], cr[h]) - fv[h];
-                diff = ok[h] ? diff : 0.f;
-                scf = fmaf (diff, diff, scf);
-                cnt += ok[h] ? 1 : 0;
-                float dc[3];
-                if (MODE == 0) {
-                    dc[0] = diff * gr[h][0];
-                    dc[1] = diff * gr[h][1];
-                    dc[2] = diff * gr[h][2];
-                } else {
-                    float gl[3];
-                    trilinear_lerp_grad (g, w2[h], cr[h], gl);
-                    dc[0] = diff * gl[0];
-                    dc[1] = diff * gl[1];
-                    dc[2] = diff * gl[2];
-                }
+            auto store_dc = [&](int h, const float dc[3]) {
                 if (rowv[h]) {
                     const int rho = r0 + u0 + h;
                     uint8_t* p = dcb + (rho >> 3) * 1024 + (rho & 7) * 128
@@ -427,6 +610,113 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                         *(unsigned short*) (p + 4096 * e) = (unsigned short) w;
                         *(unsigned short*) (p + XS_DC_LO + 4096 * e)
                             = (unsigned short) (w >> 16);
+                    }
+                }
+            };
+            if constexpr (xl_mse_mode (MODE)) {
+                float cr[2][8], fv[2], gr[2][3];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const float* mp = a.mimg + mvf[h];
+                    cr[h][0] = __ldg (mp);
+                    cr[h][1] = __ldg (mp + 1);
+                    cr[h][2] = __ldg (mp + dxm);
+                    cr[h][3] = __ldg (mp + dxm + 1);
+                    cr[h][4] = __ldg (mp + dxym);
+                    cr[h][5] = __ldg (mp + dxym + 1);
+                    cr[h][6] = __ldg (mp + dxym + dxm);
+                    cr[h][7] = __ldg (mp + dxym + dxm + 1);
+                    fv[h] = __ldg (a.fimg + fidx[h]);
+                    if (MODE == XM_MSE_NEAREST) {
+                        const float* gp = a.mgrad + 3 * mvr[h];
+                        gr[h][0] = __ldg (gp);
+                        gr[h][1] = __ldg (gp + 1);
+                        gr[h][2] = __ldg (gp + 2);
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float diff = trilinear_lerp (w2[h], cr[h]) - fv[h];
+                    diff = ok[h] ? diff : 0.f;
+                    scf = fmaf (diff, diff, scf);
+                    cnt += ok[h] ? 1 : 0;
+                    float dc[3];
+                    if (MODE == XM_MSE_NEAREST) {
+                        dc[0] = diff * gr[h][0];
+                        dc[1] = diff * gr[h][1];
+                        dc[2] = diff * gr[h][2];
+                    } else {
+                        float gl[3];
+                        trilinear_lerp_grad (g, w2[h], cr[h], gl);
+                        dc[0] = diff * gl[0];
+                        dc[1] = diff * gl[1];
+                        dc[2] = diff * gl[2];
+                    }
+                    store_dc (h, dc);
+                }
+            } else if constexpr (MODE == XM_MI_GRAD || MODE == XM_MI_HIST) {
+                // PVI-8: the fixed voxel's bin and the bins of the eight
+                // trilinear corners, in li_value's order
+                int fb[2], mb[2][8];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint8_t* mp = a.mbin + mvf[h];
+                    mb[h][0] = __ldg (mp);
+                    mb[h][1] = __ldg (mp + 1);
+                    mb[h][2] = __ldg (mp + dxm);
+                    mb[h][3] = __ldg (mp + dxm + 1);
+                    mb[h][4] = __ldg (mp + dxym);
+                    mb[h][5] = __ldg (mp + dxym + 1);
+                    mb[h][6] = __ldg (mp + dxym + dxm);
+                    mb[h][7] = __ldg (mp + dxym + dxm + 1);
+                    fb[h] = __ldg (a.fbin + fidx[h]);
+                }
+                if constexpr (MODE == XM_MI_GRAD) {
+                    const float nv = __ldg (a.mi_nvf);
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        float dc[3] = {0.f, 0.f, 0.f};
+                        if (ok[h]) xl_mi_dc_dv (a, w2[h], fb[h], mb[h], nv, dc);
+                        store_dc (h, dc);
+                    }
+                } else {
+                    unsigned long long* hsm = (unsigned long long*) (x.sm + XS_DC);
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        xl_mi_hist_add (a, hsm, ok[h], w2[h], fb[h], mb[h],
+                            x.lane, cnt);
+                    }
+                }
+            } else {
+                // Parzen windows: the trilinear moving value's window
+                float cr[2][8];
+                int fb[2];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const float* mp = a.mimg + mvf[h];
+                    cr[h][0] = __ldg (mp);
+                    cr[h][1] = __ldg (mp + 1);
+                    cr[h][2] = __ldg (mp + dxm);
+                    cr[h][3] = __ldg (mp + dxm + 1);
+                    cr[h][4] = __ldg (mp + dxym);
+                    cr[h][5] = __ldg (mp + dxym + 1);
+                    cr[h][6] = __ldg (mp + dxym + dxm);
+                    cr[h][7] = __ldg (mp + dxym + dxm + 1);
+                    fb[h] = __ldg (a.fbin + fidx[h]);
+                }
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const float u = parzen_centre (trilinear_lerp (w2[h], cr[h]),
+                        a.pz_mmin, a.pz_mdelta);
+                    if constexpr (MODE == XM_PZ_HIST) {
+                        unsigned long long* hsm = (unsigned long long*) (x.sm + XS_DC);
+                        xl_pz_hist_add (a, hsm, ok[h], fb[h], u, x.lane, cnt);
+                    } else {
+                        float dc[3] = {0.f, 0.f, 0.f};
+                        if (ok[h]) {
+                            xl_pz_dc_dv (a, u, fb[h], w2[h], cr[h], clampb[h], dc);
+                        }
+                        store_dc (h, dc);
                     }
                 }
             }
@@ -488,7 +778,7 @@ __global__ void __launch_bounds__ (XL_BLOCK, 1)
 mse_xl_kernel (XlArgs a)
 {
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t s_bar[8];
+    __shared__ uint64_t s_bar[9];      // + drain: every issued MMA done
     __shared__ uint32_t s_taddr;
     __shared__ int s_abort;
 
@@ -512,6 +802,7 @@ mse_xl_kernel (XlArgs a)
         mbar_init (&s_bar[XB_D + 1], 1);
         mbar_init (&s_bar[XB_RG], 1);
         mbar_init (&s_bar[XB_RG + 1], 1);
+        mbar_init (&s_bar[8], 1);
         fence_barrier_init ();
         s_abort = 0;
     }
@@ -544,7 +835,7 @@ mse_xl_kernel (XlArgs a)
     const int S = nb_local * a.nch;
 
     if (mma_warp) {
-        if (x.lane == 0) {
+        if (x.lane == 0 && !a.withhold) {
             // phase parities, bit buf of each word (no local arrays)
             uint32_t ph_b2 = 0, ph_dc = 0;
             auto wait = [&](uint64_t* bar, uint32_t& ph, int buf, int code) {
@@ -566,10 +857,14 @@ mse_xl_kernel (XlArgs a)
                     xl_issue_forward (x, buf, &s_bar[XB_D + buf]);
                 }
                 if (s >= 1) {
+                    // the voxel phase of step s - 1 is done with D (and
+                    // has written dc/dv, except in the histogram passes)
                     const int pb = (s - 1) & 1;
                     if (!wait (&s_bar[XB_DC + pb], ph_dc, pb, 4)) break;
                     tc_fence_after ();
-                    xl_issue_adjoint (x, pb, &s_bar[XB_RG + pb]);
+                    if (!xl_hist_mode (MODE)) {
+                        xl_issue_adjoint (x, pb, &s_bar[XB_RG + pb]);
+                    }
                 }
             }
         }
@@ -628,16 +923,37 @@ mse_xl_kernel (XlArgs a)
                 xl_voxel<MODE, AXIS, ROI> (a, x, t, buf, scf, cnt);
                 sc += (double) scf;
             }
-            if (t.ch == a.nch - 1) {
-                // the warp's score and count of the batch, fixed tree order
+            if (xl_mse_mode (MODE) && t.ch == a.nch - 1) {
+                // the warp's score and count of the batch (fixed tree
+                // order), then the batch's: the last of its 16 warps to
+                // get here sums their partials in warp order
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {
                     sc += __shfl_down_sync (0xffffffffu, sc, o);
                     cnt += __shfl_down_sync (0xffffffffu, cnt, o);
                 }
+                const size_t wb = (size_t) t.b * XL_CW;
+                unsigned arrived = 0;
                 if (x.lane == 0) {
-                    a.score_part[(size_t) t.b * XL_CW + x.warp] = sc;
-                    a.count_part[(size_t) t.b * XL_CW + x.warp] = cnt;
+                    a.sx.wscore[wb + x.warp] = sc;
+                    a.sx.wcount[wb + x.warp] = cnt;
+                    __threadfence ();
+                    arrived = atomicAdd (a.sx.arrive + t.b, 1u);
+                }
+                arrived = __shfl_sync (0xffffffffu, arrived, 0);
+                if (arrived == XL_CW - 1) {
+                    __threadfence ();
+                    double v = x.lane < XL_CW ? __ldcg (a.sx.wscore + wb + x.lane) : 0.0;
+                    int n = x.lane < XL_CW ? __ldcg (a.sx.wcount + wb + x.lane) : 0;
+#pragma unroll
+                    for (int o = XL_CW / 2; o > 0; o >>= 1) {
+                        v += __shfl_down_sync (0xffffffffu, v, o);
+                        n += __shfl_down_sync (0xffffffffu, n, o);
+                    }
+                    if (x.lane == 0) {
+                        a.score_part[t.b] = v;
+                        a.count_part[t.b] = n;
+                    }
                 }
                 sc = 0.0;
                 cnt = 0;
@@ -653,13 +969,49 @@ mse_xl_kernel (XlArgs a)
                     __syncwarp ();
                     if (x.lane == 0) mbar_arrive (&s_bar[XB_B2 + buf]);
                 }
-            } else if (s >= 1) {
+            } else if (s >= 1 && !xl_hist_mode (MODE)) {
                 ok = yz_adjoint (s - 1);
             }
         }
-        if (ok && !yz_fwd_warp && S >= 1) yz_adjoint (S - 1);
+        if (ok && !yz_fwd_warp && S >= 1 && !xl_hist_mode (MODE)) {
+            yz_adjoint (S - 1);
+        }
+        if constexpr (xl_hist_mode (MODE)) {
+            // the CTA's histograms and voxel count into the global ones
+            // (integer sums: the order does not matter); the moving
+            // histogram is the joint one's column sums; Parzen keeps the
+            // joint one only (its score kernel forms the marginals)
+            named_bar_sync (1, XL_THREADS);
+            const int B = a.bins, nh = 2 * B + B * B;
+            const unsigned long long* h = (const unsigned long long*) (x.sm + XS_DC);
+            for (int i = tid; i < nh; i += XL_THREADS) {
+                unsigned long long v = h[i];
+                if (MODE == XM_PZ_HIST && i < 2 * B) {
+                    v = 0;
+                } else if (i >= B && i < 2 * B) {
+                    v = 0;
+                    for (int fb = 0; fb < B; fb++) v += h[2 * B + fb * B + (i - B)];
+                }
+                if (v) atomicAdd (&a.hist[i], v);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cnt += __shfl_down_sync (0xffffffffu, cnt, o);
+            }
+            if (x.lane == 0 && cnt) {
+                atomicAdd (&a.hist[nh], (unsigned long long) cnt);
+            }
+        }
     }
 
+    if (mma_warp && x.lane == 0 && !a.withhold) {
+        // every MMA this thread issued completes before TMEM is released,
+        // also when a wait gave up (the MMAs themselves wait on nothing)
+        tc_commit (&s_bar[8]);
+        for (uint32_t n = 0; n < a.wait_limit + 1000000u; n++) {
+            if (mbar_try_wait (&s_bar[8], 0)) break;
+        }
+    }
     tc_fence_before ();
     __syncthreads ();
     if (mma_warp) tmem_dealloc (x.taddr, XT_COLS);
@@ -690,7 +1042,7 @@ xl_plan (const BspGeom& g, XlPlan* p, int sm_count)
     p->smem = XS_TOTAL + 1024;
     p->threads = XL_BLOCK;
     p->grid = std::min (p->nbatches, sm_count);
-    p->score_parts = p->nbatches * XL_CW;
+    p->score_parts = p->nbatches;
     return true;
 }
 
@@ -738,14 +1090,26 @@ xl_launch_t (const XlPlan& p, const XlArgs& a, cudaStream_t st)
     return cudaGetLastError ();
 }
 
+static bool
+xl_axis_aligned (const BspGeom& g)
+{
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) {
+            if (i != j && (g.fstep[3 * i + j] != 0.f || g.mproj[3 * i + j] != 0.f)) {
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
 cudaError_t
-launch_mse_xl (const BspGeom& g, const XlPlan& p, int grad_mode,
-    const float* fimg, const float* mimg, const float* mgrad,
-    const float* coeff, const void* tab, const float* luts, float* part,
-    double* score_part, int* count_part, int* err, unsigned wait_limit,
+launch_mi_xl (const BspGeom& g, const XlPlan& p, bool hist_pass,
+    const TcMiArgs& mi, const float* coeff, const void* tab,
+    const float* luts, float* part, int* err, unsigned wait_limit,
     cudaStream_t st)
 {
-    XlArgs a;
+    XlArgs a = {};
     a.g = g;
     a.T = p.T;
     a.KX = p.T + 3;
@@ -754,19 +1118,63 @@ launch_mse_xl (const BspGeom& g, const XlPlan& p, int grad_mode,
     a.nlz = p.nlz;
     a.nch = p.nch;
     a.wait_limit = wait_limit;
+    a.coeff = coeff;
+    a.tab = (const uint4*) tab;
+    a.luts = luts;
+    a.part = part;
+    a.err = err;
+    a.fbin = mi.fbin; a.mbin = mi.mbin; a.bins = mi.bins;
+    a.mi_lut = mi.lut; a.mi_nvf = mi.nvf; a.hist = mi.hist;
+    a.mimg = mi.mimg;
+    a.pz_mmin = mi.m_min;
+    a.pz_mdelta = mi.m_delta;
+    const bool axis = xl_axis_aligned (g);
+    if (mi.parzen) {
+        if (hist_pass) {
+            return axis ? xl_launch_t<XM_PZ_HIST, true, false> (p, a, st)
+                        : xl_launch_t<XM_PZ_HIST, false, false> (p, a, st);
+        }
+        return axis ? xl_launch_t<XM_PZ_GRAD, true, false> (p, a, st)
+                    : xl_launch_t<XM_PZ_GRAD, false, false> (p, a, st);
+    }
+    if (hist_pass) {
+        return axis ? xl_launch_t<XM_MI_HIST, true, false> (p, a, st)
+                    : xl_launch_t<XM_MI_HIST, false, false> (p, a, st);
+    }
+    return axis ? xl_launch_t<XM_MI_GRAD, true, false> (p, a, st)
+                : xl_launch_t<XM_MI_GRAD, false, false> (p, a, st);
+}
+
+bool
+xl_mi_supported (int bins)
+{
+    return (size_t) (2 * bins + bins * bins) * 8 <= 2 * XS_DC_BUF;
+}
+
+cudaError_t
+launch_mse_xl (const BspGeom& g, const XlPlan& p, int grad_mode,
+    const float* fimg, const float* mimg, const float* mgrad,
+    const float* coeff, const void* tab, const float* luts, float* part,
+    double* score_part, int* count_part, int* err, unsigned wait_limit,
+    int withhold, const XlScratch& scratch, cudaStream_t st)
+{
+    XlArgs a = {};
+    a.g = g;
+    a.T = p.T;
+    a.KX = p.T + 3;
+    a.nbx = p.nbx;
+    a.nbatches = p.nbatches;
+    a.nlz = p.nlz;
+    a.nch = p.nch;
+    a.wait_limit = wait_limit;
+    a.withhold = withhold;
     a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;
     a.tab = (const uint4*) tab;
     a.luts = luts;
     a.part = part; a.score_part = score_part; a.count_part = count_part;
+    a.sx = scratch;
     a.err = err;
-    bool axis = true;
-    for (int i = 0; i < 3; i++) {
-        for (int j = 0; j < 3; j++) {
-            if (i != j && (g.fstep[3 * i + j] != 0.f || g.mproj[3 * i + j] != 0.f)) {
-                axis = false;
-            }
-        }
-    }
+    const bool axis = xl_axis_aligned (g);
     const bool roi = g.fmask || g.mroi;
     if (roi) {
         if (grad_mode == 0) {

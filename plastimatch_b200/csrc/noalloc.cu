@@ -21,7 +21,6 @@
 // overlaps (different streams, or different host threads) race on it.
 // Callers serialise them, e.g. by issuing all calls on one stream.
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/plastimatch_b200.h"
 #include "kernels.cuh"
@@ -55,23 +54,19 @@ fill_luts_kernel (LutArg a, int n, float* __restrict__ dst)
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = a.v[i];
 }
 
-// Device address of the static array, looked up once per device.
+// Device address of the static array in the current device's context.
+// Looked up on every call (a cheap query) rather than cached: after a
+// cudaDeviceReset, or under another driver context on the same ordinal,
+// the module is loaded afresh and the array has a new address.
 static unsigned char*
-scratch_base (int dev)
+scratch_base ()
 {
-    static std::mutex mu;
-    static unsigned char* addr[64] = {};
-    if (dev < 0 || dev >= 64) return nullptr;
-    std::lock_guard<std::mutex> lock (mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress (&p, g_scratch) != cudaSuccess) {
-            cudaGetLastError ();
-            return nullptr;
-        }
-        addr[dev] = (unsigned char*) p;
+    void* p = nullptr;
+    if (cudaGetSymbolAddress (&p, g_scratch) != cudaSuccess) {
+        cudaGetLastError ();             // this call's own lookup error
+        return nullptr;
     }
-    return addr[dev];
+    return (unsigned char*) p;
 }
 
 static bool
@@ -118,6 +113,15 @@ b200bsp_score_mse_static (const b200bsp_volume* fixed,
     if (mse_fp32_smem_bytes (g) > 200 * 1024) {
         return static_fail (B200BSP_E_UNSUPPORTED, "tile too large");
     }
+    // an error the caller's own earlier work left pending is reported, not
+    // cleared (and not blamed on this call's launches below)
+    const cudaError_t pending = cudaPeekAtLastError ();
+    if (pending != cudaSuccess) {
+        char msg[200];
+        snprintf (msg, sizeof msg, "a CUDA error is already pending: %s",
+            cudaGetErrorString (pending));
+        return static_fail (B200BSP_E_CUDA, msg);
+    }
     int dev = 0;
     if (cudaGetDevice (&dev) != cudaSuccess) {
         cudaGetLastError ();
@@ -133,7 +137,7 @@ b200bsp_score_mse_static (const b200bsp_volume* fixed,
             "moving gradient (nearest mode) and outputs must be device "
             "memory on the current device");
     }
-    unsigned char* base = scratch_base (dev);
+    unsigned char* base = scratch_base ();
     if (!base) return static_fail (B200BSP_E_CUDA, "static scratch lookup failed");
     DevResult* res = (DevResult*) (base + OFF_RES);
     float* d_luts = (float*) (base + OFF_LUT);

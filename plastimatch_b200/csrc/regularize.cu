@@ -236,7 +236,7 @@ __global__ void __launch_bounds__ (REG_THREADS)
 reg_pass_z (RegPlan plan, int cx, int cy, int cz, int nk,
     const double* __restrict__ hz, const double* __restrict__ t2,
     const float* __restrict__ coeff, float* __restrict__ grad,
-    double* __restrict__ part)
+    double* __restrict__ grad64, double* __restrict__ part)
 {
     __shared__ double sh_v[REG_THREADS / 32];
     __shared__ int sh_n[REG_THREADS / 32];
@@ -268,10 +268,15 @@ reg_pass_z (RegPlan plan, int cx, int cy, int cz, int nk,
         double c2 = coeff[3 * knot + 2];
         S = c0 * out[O_DX] + c1 * out[O_DY] + c2 * out[O_DZ]
             + c1 * out[O_CXY] + c2 * out[O_CXZ] + c2 * out[O_CYZ];
-        if (grad) {
-            double g0 = 2.0 * out[O_DX] + out[O_CYX] + out[O_CZX];
-            double g1 = 2.0 * out[O_DY] + out[O_CXY] + out[O_CZY];
-            double g2 = 2.0 * out[O_DZ] + out[O_CXZ] + out[O_CYZ];
+        const double g0 = 2.0 * out[O_DX] + out[O_CYX] + out[O_CZX];
+        const double g1 = 2.0 * out[O_DY] + out[O_CXY] + out[O_CZY];
+        const double g2 = 2.0 * out[O_DZ] + out[O_CXZ] + out[O_CYZ];
+        if (grad64) {
+            // stored for a later kernel to add (b200bsp_score's overlap)
+            grad64[3 * knot + 0] = g0;
+            grad64[3 * knot + 1] = g1;
+            grad64[3 * knot + 2] = g2;
+        } else if (grad) {
             grad[3 * knot + 0] = (float) ((double) grad[3 * knot + 0] + g0);
             grad[3 * knot + 1] = (float) ((double) grad[3 * knot + 1] + g1);
             grad[3 * knot + 2] = (float) ((double) grad[3 * knot + 2] + g2);
@@ -426,7 +431,7 @@ reg_prepare (RegState* s, const b200bsp_reg_parms* p, cudaStream_t st)
 
 int
 reg_run (RegState* s, const BspGeom& g, const b200bsp_reg_parms* p,
-    const float* d_coeff, float* d_grad, cudaStream_t st)
+    const float* d_coeff, float* d_grad, cudaStream_t st, double* d_grad64)
 {
     if (!s->have_parms || memcmp (&s->parms, p, sizeof *p) != 0) {
         int rc = reg_prepare (s, p, st);
@@ -442,7 +447,7 @@ reg_run (RegState* s, const BspGeom& g, const b200bsp_reg_parms* p,
             s->d_t1, s->d_t2);
     }
     reg_pass_z<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, cy, cz, nk, s->d_hz,
-        s->d_t2, d_coeff, d_grad, s->d_part);
+        s->d_t2, d_coeff, d_grad, d_grad64, s->d_part);
     reg_reduce<<<1, 1024, 0, st>>> (s->d_part, nb, s->d_score);
     return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
 }

@@ -45,8 +45,12 @@ struct RegState {
 
 int reg_alloc (RegState* s, const BspGeom& g, const float grid_spac[3]);
 void reg_free (RegState* s);
+// d_grad: the gradient is added into it (float, one double rounding per
+// entry); d_grad64 (instead): stored there in double.  The score goes to
+// s->d_score (double).
 int reg_run (RegState* s, const BspGeom& g, const b200bsp_reg_parms* p,
-    const float* d_coeff, float* d_grad, cudaStream_t st);
+    const float* d_coeff, float* d_grad, cudaStream_t st,
+    double* d_grad64 = nullptr);
 int reg_fetch (RegState* s, double* score, cudaStream_t st);
 
 } // namespace b200

@@ -27,6 +27,9 @@
 using namespace b200;
 
 static thread_local std::string g_create_error;
+// b200bsp_debug_fail_alloc: the n-th device allocation of the next
+// b200bsp_create calls on this thread fails as if the device were full
+static thread_local int g_fail_alloc = 0;
 
 struct b200bsp_ctx {
     int device = 0;
@@ -64,10 +67,19 @@ struct b200bsp_ctx {
     // and the autotuner has not preferred the tile kernel
     bool use_xl = false;
     bool has_xl = false;
+    bool use_xl_mi = true;    // MI on the x-lane kernel where it applies
     XlPlan xplan;
     PartLayout xlay;
     void* d_xtab = nullptr;
+    XlScratch xs = {nullptr, nullptr, nullptr};
     unsigned wait_limit = XL_DEFAULT_WAIT_LIMIT;
+    int withhold_mma = 0;     // b200bsp_set_wait_limit's testing aid
+    // b200bsp_score's device path: the regulariser on a second stream,
+    // overlapping the tile kernel, its gradient kept in double
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    double* d_reg_grad64 = nullptr;
+    float* d_total = nullptr;
     int tc_grid = 0;          // CTAs of the tile kernel; 0: plan.grid
     // the optimiser's device workspace, kept between runs (optimize.cu)
     void* opt_ws = nullptr;
@@ -256,6 +268,7 @@ free_all (b200bsp_ctx* c)
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
     cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
     cudaFree (c->d_qlut); cudaFree (c->d_xtab); cudaFree (c->d_inv_dc);
+    cudaFree (c->xs.wscore); cudaFree (c->xs.wcount); cudaFree (c->xs.arrive);
     cudaFree (c->d_lm_p); cudaFree (c->d_lm_w); cudaFree (c->d_lm_fm);
     cudaFree (c->d_lm_dc);
     cudaFree (c->d_fmask); cudaFree (c->d_mroi);
@@ -265,6 +278,11 @@ free_all (b200bsp_ctx* c)
     if (c->opt_ws_free) c->opt_ws_free (c->opt_ws);
     c->opt_ws = nullptr;
     for (auto& e : c->ev) if (e) cudaEventDestroy (e);
+    if (c->ev_fork) cudaEventDestroy (c->ev_fork);
+    if (c->ev_join) cudaEventDestroy (c->ev_join);
+    if (c->aux_stream) cudaStreamDestroy (c->aux_stream);
+    cudaFree (c->d_reg_grad64);
+    cudaFree (c->d_total);
     if (c->own_stream) cudaStreamDestroy (c->own_stream);
 }
 
@@ -519,6 +537,11 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     int rc2 = B200BSP_OK;
     auto alloc = [&](void** p, size_t bytes) {
         if (rc2) return;
+        if (g_fail_alloc > 0 && --g_fail_alloc == 0) {
+            rc2 = fail (c, B200BSP_E_OOM, "cudaMalloc(%zu): injected failure",
+                bytes);
+            return;
+        }
         cudaError_t e = cudaMalloc (p, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError ();
@@ -547,6 +570,8 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     alloc ((void**) &c->d_coeff, c->num_coeff * sizeof (float));
     alloc ((void**) &c->d_grad, c->num_coeff * sizeof (float));
     alloc ((void**) &c->d_grad64, c->num_coeff * sizeof (double));
+    alloc ((void**) &c->d_reg_grad64, c->num_coeff * sizeof (double));
+    alloc ((void**) &c->d_total, sizeof (float));
     alloc ((void**) &c->d_res, sizeof (DevResult));
     alloc ((void**) &c->d_err, sizeof (int));
     alloc ((void**) &c->d_inv_dc, 9 * sizeof (float));
@@ -609,6 +634,16 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     score_parts = std::max (score_parts, (size_t) std::max (c->nscore_parts, 1));
     alloc ((void**) &c->d_score_part, score_parts * sizeof (double));
     alloc ((void**) &c->d_count_part, score_parts * sizeof (int));
+    if (c->has_xl) {
+        const size_t nb = (size_t) c->xplan.nbatches;
+        alloc ((void**) &c->xs.wscore, nb * XL_COMPUTE_WARPS * sizeof (double));
+        alloc ((void**) &c->xs.wcount, nb * XL_COMPUTE_WARPS * sizeof (int));
+        alloc ((void**) &c->xs.arrive, nb * sizeof (unsigned));
+        if (!rc2 && cudaMemset (c->xs.arrive, 0, nb * sizeof (unsigned))
+            != cudaSuccess) {
+            rc2 = fail (c, B200BSP_E_CUDA, "memset failed");
+        }
+    }
     if (!rc2 && o.form == B200BSP_FORM_TC) {
         rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
         if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
@@ -635,6 +670,12 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     }
 
     if (cudaStreamCreateWithFlags (&c->own_stream, cudaStreamNonBlocking)
+        != cudaSuccess
+        || cudaStreamCreateWithFlags (&c->aux_stream, cudaStreamNonBlocking)
+        != cudaSuccess
+        || cudaEventCreateWithFlags (&c->ev_fork, cudaEventDisableTiming)
+        != cudaSuccess
+        || cudaEventCreateWithFlags (&c->ev_join, cudaEventDisableTiming)
         != cudaSuccess) {
         cudaGetLastError ();
         free_all (c);
@@ -668,6 +709,22 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     }
     *out = c;
     return B200BSP_OK;
+}
+
+extern "C" int
+b200bsp_set_wait_limit (b200bsp_ctx* c, int polls, int withhold_mma)
+{
+    if (!c) return B200BSP_E_BADARG;
+    if (polls < 0) return fail (c, B200BSP_E_BADARG, "polls must be >= 0");
+    c->wait_limit = polls > 0 ? (unsigned) polls : XL_DEFAULT_WAIT_LIMIT;
+    c->withhold_mma = withhold_mma ? 1 : 0;
+    return B200BSP_OK;
+}
+
+extern "C" void
+b200bsp_debug_fail_alloc (int nth)
+{
+    g_fail_alloc = nth > 0 ? nth : 0;
 }
 
 extern "C" int
@@ -806,7 +863,9 @@ end_eval (b200bsp_ctx* c, bool wait)
 static int
 run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     double* grad64_out, float* score_out, double* score64_out,
-    long long* nvox_out, DevResult* res_host = nullptr)
+    long long* nvox_out, DevResult* res_host = nullptr,
+    const FinishCombine& combine = FinishCombine (),
+    cudaEvent_t before_finish = nullptr)
 {
     const BspGeom& g = c->geom;
     if (c->opts.form == B200BSP_FORM_FP32) {
@@ -823,7 +882,7 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
         CK (launch_mse_xl (g, plan, c->opts.mse_grad, c->d_fixed,
             c->d_moving, c->d_mgrad, dcoeff, c->d_xtab, c->d_luts,
             c->d_part, c->d_score_part, c->d_count_part, c->d_err,
-            c->wait_limit, c->stream));
+            c->wait_limit, c->withhold_mma, c->xs, c->stream));
     } else {
         TcPlan plan = c->plan;
         if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
@@ -836,12 +895,14 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     int rc = mark_main_done (c);
     if (rc) return rc;
     const bool xl = c->opts.form == B200BSP_FORM_TC && c->use_xl;
+    if (before_finish) CK (cudaStreamWaitEvent (c->stream, before_finish, 0));
     CK (launch_finish_mse (g, xl ? c->xlay : c->lay, c->d_part,
         c->d_score_part, c->d_count_part,
         xl ? c->xplan.score_parts : c->nscore_parts,
         c->opts.form == B200BSP_FORM_TC ? c->d_err : nullptr, c->d_res,
         res_host, grad_out, grad64_out, score_out, score64_out, nvox_out,
-        c->stream));
+        c->stream, xl ? c->xs.arrive : nullptr, xl ? c->xplan.nbatches : 0,
+        combine));
     c->last_launches += 1;
     return B200BSP_OK;
 }
@@ -1010,6 +1071,16 @@ mi_passes_on (b200bsp_ctx* c, const BspGeom& g, const float* dcoeff,
     float* grad, double* grad64, int passes)
 {
     const bool roi = g.fmask || g.mroi;
+    if (c->opts.form == B200BSP_FORM_TC && !roi && c->has_xl && c->use_xl_mi
+        && xl_mi_supported (c->mi.bins)) {
+        XlPlan plan = c->xplan;
+        if (c->tc_grid > 0) {
+            plan.grid = std::min (std::max (1, c->tc_grid / 2), plan.nbatches);
+        }
+        return mi_run_xl (&c->mi, g, plan, c->xlay, c->d_xtab, c->d_luts,
+            c->d_part, c->d_err, c->wait_limit, dcoeff, c->d_moving,
+            c->d_res, grad, grad64, c->stream, &c->last_launches, passes);
+    }
     if (c->opts.form == B200BSP_FORM_TC && !roi
         && tc_mi_supported (g, c->plan, c->mi.bins)) {
         TcPlan plan = c->plan;
@@ -1464,12 +1535,52 @@ b200bsp_landmarks_score (b200bsp_ctx* c, const float* coeff, float* lmetric,
     return B200BSP_OK;
 }
 
+// bspline_score with MSE and device outputs, stream-ordered: the
+// regulariser runs on the context's second stream while the tile kernel
+// runs on the first, and the finish kernel combines them (lambda times the
+// metric, plus the regulariser's score and double gradient).
+static int
+score_mse_device (b200bsp_ctx* c, const float* coeff, float lambda,
+    const b200bsp_reg_parms* reg, float* total_score, float* total_grad,
+    float* smetric, int64_t* num_vox)
+{
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    FinishCombine cb;
+    cb.lambda = lambda;
+    cb.total_score = total_score ? total_score : c->d_total;
+    if (reg) {
+        CK (cudaEventRecord (c->ev_fork, c->stream));
+        CK (cudaStreamWaitEvent (c->aux_stream, c->ev_fork, 0));
+        rc = reg_run (&c->reg, c->geom, reg, dcoeff, nullptr, c->aux_stream,
+            c->d_reg_grad64);
+        if (rc) return fail (c, rc, "regulariser failed: %s",
+            cudaGetErrorString (cudaGetLastError ()));
+        CK (cudaEventRecord (c->ev_join, c->aux_stream));
+        cb.reg_grad = c->d_reg_grad64;
+        cb.reg_score = c->reg.d_score;
+        c->last_launches += c->reg.plan.n1 ? 4 : 2;
+    }
+    rc = run_mse (c, dcoeff, total_grad, nullptr, smetric, nullptr,
+        (long long*) num_vox, nullptr, cb, reg ? c->ev_join : nullptr);
+    if (rc) return rc;
+    return end_eval (c, false);
+}
+
 extern "C" int
 b200bsp_score (b200bsp_ctx* c, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
     float* total_grad, float* smetric, int64_t* num_vox)
 {
     if (!c || !total_grad) return fail (c, B200BSP_E_BADARG, "null argument");
+    if (metric_type == 0 && c->lm_n == 0 && is_device_ptr (total_grad)
+        && (!total_score || is_device_ptr (total_score))
+        && (!smetric || is_device_ptr (smetric))
+        && (!num_vox || is_device_ptr (num_vox))) {
+        return score_mse_device (c, coeff, lambda, reg, total_score,
+            total_grad, smetric, num_vox);
+    }
     std::vector<float> g ((size_t) c->num_coeff);
     float s = 0.f;
     int64_t nv = 0;

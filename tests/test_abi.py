@@ -43,3 +43,14 @@ def test_null_arguments_are_rejected_without_crash():
     assert L.b200bsp_destroy(None) == 0
     assert L.b200bsp_score_mse(None, None, None, None, None) == -1
     assert b"null" in L.b200bsp_last_error(None)
+
+
+def test_reference_side_adapter_links():
+    """The reference-side drop-in (oracle/ref/b200_adapter.cxx) resolves
+    every symbol against the reference build and this library."""
+    import ctypes
+    import oracle as O
+    if not O.adapter_available():
+        pytest.skip("reference-side adapter not built")
+    lib = ctypes.CDLL(O.ADAPTER_SO, mode=ctypes.RTLD_GLOBAL)
+    assert hasattr(lib, "adapter_compare")

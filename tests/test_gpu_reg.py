@@ -75,3 +75,34 @@ def test_total_score_golden(form, name):
                                   P.reg_parms(curvature=0.005))
     assert abs(ts - rec["total_score"]) <= 1e-5 * abs(rec["total_score"])
     assert rel_err(tg, rec["total_grad"]) < 1e-3
+
+
+@pytest.mark.parametrize("form", ["tc", "fp32"])
+@pytest.mark.parametrize("with_reg", [True, False])
+def test_score_device_path_matches_host_path(form, with_reg):
+    """b200bsp_score with device outputs (the regulariser on a second
+    stream, overlapping the tile kernel, combined by the finish kernel) is
+    bit-identical to the host-output path (metric, then regulariser, in
+    sequence)."""
+    import torch
+    fixed, moving, grid, coeff, rec = load_golden("mse_small")
+    reg = P.reg_parms(curvature=0.005, diffusion=0.1) if with_reg else None
+    with P.Context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images(moving_grad=rec["moving_grad"])
+        ts, g, sm, n = ctx.score(coeff, lam=0.7, reg=reg)
+        d_c = torch.from_numpy(coeff).cuda()
+        d_g = torch.zeros(grid.num_coeff, device="cuda")
+        d_ts = torch.zeros(1, device="cuda")
+        d_sm = torch.zeros(1, device="cuda")
+        d_n = torch.zeros(1, dtype=torch.int64, device="cuda")
+        import ctypes as C
+        for _ in range(2):
+            rc = P.lib().b200bsp_score(
+                ctx._h, d_c.data_ptr(), 0, C.c_float(0.7),
+                C.byref(reg) if reg is not None else None, d_ts.data_ptr(),
+                d_g.data_ptr(), d_sm.data_ptr(), d_n.data_ptr())
+            assert rc == 0
+            torch.cuda.synchronize()
+            assert float(d_ts.item()) == ts and float(d_sm.item()) == sm
+            assert int(d_n.item()) == n
+            assert np.array_equal(d_g.cpu().numpy(), g)
