@@ -69,7 +69,10 @@ struct XlPlan {
     int grid;
     int score_parts;     // per batch and compute warp
 };
-bool xl_plan (const BspGeom& g, XlPlan* plan, int sm_count);
+// extra_row_batches: more batches per row of tiles than the fewest (the
+// autotuner's knob).  The basis table of the fewest serves every split.
+bool xl_plan (const BspGeom& g, XlPlan* plan, int sm_count,
+    int extra_row_batches = 0);
 int xl_build_table (const BspGeom& g, const XlPlan& plan, const float* bx_lut,
     void** d_tab);
 constexpr unsigned XL_DEFAULT_WAIT_LIMIT = 1u << 22;

@@ -540,6 +540,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
         tmem_ld4x3_wait (tl + r0, tl + XL_RC + r0, tl + 2 * XL_RC + r0, dv);
 #pragma unroll
         for (int u0 = 0; u0 < 4; u0 += 2) {
+            if (r0 + u0 >= rb) break;          // both rows past the warp's
             bool ok[2], rowv[2];
             int mvf[2], mvr[2], fidx[2], clampb[2];
             float w2[2][3];
@@ -1020,7 +1021,7 @@ mse_xl_kernel (XlArgs a)
 // ------------------------------------------------------------------ host --
 
 bool
-xl_plan (const BspGeom& g, XlPlan* p, int sm_count)
+xl_plan (const BspGeom& g, XlPlan* p, int sm_count, int extra_row_batches)
 {
     const int vx = g.vpr[0], vy = g.vpr[1], vz = g.vpr[2];
     if (vy < 3 || vy > 10 || vx < 1 || vz < 1) return false;
@@ -1029,7 +1030,8 @@ xl_plan (const BspGeom& g, XlPlan* p, int sm_count)
     // finish kernel's gather assumes a knot meets at most two batches)
     const int tmax = std::min (128 / vx, XL_KMAX - 3);
     if (tmax < 1) return false;
-    const int nb_row = (g.rdims[0] + tmax - 1) / tmax;
+    const int nb_row = (g.rdims[0] + tmax - 1) / tmax + extra_row_batches;
+    if (nb_row > g.rdims[0]) return false;
     const int T = (g.rdims[0] + nb_row - 1) / nb_row;
     if (nb_row > 1 && T < 3) return false;
     p->T = T;

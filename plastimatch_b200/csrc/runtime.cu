@@ -68,6 +68,7 @@ struct b200bsp_ctx {
     bool use_xl = false;
     bool has_xl = false;
     bool use_xl_mi = true;    // MI on the x-lane kernel where it applies
+    int xl_max_batches = 0;   // over the autotuner's x-lane splits
     XlPlan xplan;
     PartLayout xlay;
     void* d_xtab = nullptr;
@@ -176,6 +177,19 @@ use_tc_plan (b200bsp_ctx* c, const TcPlan& p)
     L.kx = L.bx + 3; L.ky = 4; L.kz = 4;
     L.slots = 1;
     c->nscore_parts = p.nbatches;
+}
+
+// Make `p` the context's x-lane plan and batch layout.
+static void
+use_xl_plan (b200bsp_ctx* c, const XlPlan& p)
+{
+    const BspGeom& g = c->geom;
+    c->xplan = p;
+    PartLayout& L = c->xlay;
+    L.bx = p.T; L.by = 1; L.bz = 1;
+    L.nbx = p.nbx; L.nby = g.rdims[1]; L.nbz = g.rdims[2];
+    L.kx = p.T + 3; L.ky = 4; L.kz = 4;
+    L.slots = 1;
 }
 
 // Cofactor inverse in float (Plastimatch src/base/direction_cosines.cxx:
@@ -607,15 +621,17 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
             }
             use_tc_plan (c, c->plan);
             if (c->has_xl) {
-                const XlPlan& xp = c->xplan;
-                part_elems = std::max (part_elems,
-                    (size_t) xp.nbatches * (xp.T + 3) * 16 * 3);
-                score_parts = std::max (score_parts, (size_t) xp.score_parts);
-                PartLayout& L = c->xlay;
-                L.bx = xp.T; L.by = 1; L.bz = 1;
-                L.nbx = xp.nbx; L.nby = g.rdims[1]; L.nbz = g.rdims[2];
-                L.kx = xp.T + 3; L.ky = 4; L.kz = 4;
-                L.slots = 1;
+                for (int e = 0; e <= TC_TUNE_MAX_EXTRA; e++) {
+                    XlPlan xp;
+                    if (!xl_plan (g, &xp, sm_count, e)) continue;
+                    part_elems = std::max (part_elems,
+                        (size_t) xp.nbatches * (xp.T + 3) * 16 * 3);
+                    score_parts = std::max (score_parts,
+                        (size_t) xp.score_parts);
+                    c->xl_max_batches = std::max (c->xl_max_batches,
+                        xp.nbatches);
+                }
+                use_xl_plan (c, c->xplan);
             }
         }
     } else if (!rc2) {
@@ -635,7 +651,7 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     alloc ((void**) &c->d_score_part, score_parts * sizeof (double));
     alloc ((void**) &c->d_count_part, score_parts * sizeof (int));
     if (c->has_xl) {
-        const size_t nb = (size_t) c->xplan.nbatches;
+        const size_t nb = (size_t) c->xl_max_batches;
         alloc ((void**) &c->xs.wscore, nb * XL_COMPUTE_WARPS * sizeof (double));
         alloc ((void**) &c->xs.wcount, nb * XL_COMPUTE_WARPS * sizeof (int));
         alloc ((void**) &c->xs.arrive, nb * sizeof (unsigned));
@@ -1029,13 +1045,19 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     };
     // candidates: the x-lane kernel, then each batch split of the tile
     // kernel; ties keep the earlier candidate
-    if (c->has_xl) {
+    const XlPlan xstart = c->xplan;
+    XlPlan xbest = xstart;
+    for (int e = 0; e <= TC_TUNE_MAX_EXTRA && c->has_xl && !rc; e++) {
+        XlPlan xp;
+        if (!xl_plan (c->geom, &xp, sm_count, e)) continue;
+        use_xl_plan (c, xp);
         c->use_xl = true;
         float ms = 0.f;
         rc = time_it (&ms);
-        if (!rc) {
+        if (!rc && (best_ms == 0.f || ms < best_ms)) {
             best_ms = ms;
             best_xl = true;
+            xbest = xp;
         }
     }
     c->use_xl = false;
@@ -1055,6 +1077,7 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     cudaEventDestroy (e0);
     cudaEventDestroy (e1);
     use_tc_plan (c, rc ? start : best);
+    if (c->has_xl) use_xl_plan (c, rc ? xstart : xbest);
     c->use_xl = rc ? start_xl : best_xl;
     if (rc) {
         cudaGetLastError ();
