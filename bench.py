@@ -440,7 +440,8 @@ def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
     return out
 
 
-def measure_form(P, form, args, workload, local_rank, dist, flush):
+def measure_form(P, form, args, workload, local_rank, dist, flush,
+                 tc_kernel="auto"):
     """Device and end-to-end throughput of one form on the workload.
 
     Returns a dict: device ms per evaluation (CUDA events on the context's
@@ -453,7 +454,8 @@ def measure_form(P, form, args, workload, local_rank, dist, flush):
     import torch
     fixed, moving, grid, coeff = workload
     dev = f"cuda:{local_rank}"
-    ctx = P.Context(fixed, moving, grid, form=form, device=local_rank)
+    ctx = P.Context(fixed, moving, grid, form=form, device=local_rank,
+                    tc_kernel=tc_kernel if form == "tc" else "auto")
     stream = torch.cuda.Stream(device=local_rank)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_images()
@@ -538,8 +540,40 @@ def measure_form(P, form, args, workload, local_rank, dist, flush):
     return {"ctx": ctx, "stream": stream, "d_coeff": d_coeff,
             "d_grad": d_grad, "dev_ms": dev_ms, "e2e_ms": e2e_ms,
             "kernel_ms": float(np.median(main_ms)), "launches": launches,
-            "tiles": tiles, "score": s_h, "grad": g_h, "num_vox": n_h,
-            "clocks": clk.summary()}
+            "tiles": tiles, "kernel": ctx.mse_kernel(), "score": s_h,
+            "grad": g_h, "num_vox": n_h, "clocks": clk.summary()}
+
+
+def tc_kernel_probe(P, workload, local_rank, flush, probes=5):
+    """Each tensor-core MSE kernel pinned in turn on the workload (x-lane:
+    voxel x on the TMEM lanes; tile: one tile's 125 voxels on the lanes),
+    autotuned over its batch splits: its own kernel time (the library's
+    events, L2 flushed before each probe, median)."""
+    import torch
+    fixed, moving, grid, coeff = workload
+    out = {}
+    for k in ("xlane", "tile"):
+        try:
+            ctx = P.Context(fixed, moving, grid, form="tc", device=local_rank,
+                            tc_kernel=k)
+        except P.B200Error as e:
+            out[k] = {"unsupported": str(e)}
+            continue
+        with ctx:
+            ctx.set_images()
+            ctx.autotune(coeff, evals=3)
+            d_coeff = torch.from_numpy(coeff).to(f"cuda:{local_rank}")
+            ctx.enable_timing(True)
+            ms = []
+            for _ in range(probes):
+                flush.fill_(1)
+                torch.cuda.synchronize()
+                ctx.score_mse(d_coeff)
+                ms.append(ctx.last_timing()[1])
+            name, tiles, batches = ctx.mse_kernel()
+            out[k] = {"kernel_ms": float(np.median(ms)), "tiles": tiles,
+                      "batches": batches}
+    return out
 
 
 def accuracy_block(workload, score, grad, num_vox, threads):
@@ -561,14 +595,22 @@ def accuracy_block(workload, score, grad, num_vox, threads):
                "score_rel": abs(score - f64.score) / abs(f64.score),
                "grad_rel_l2": rel(grad, f64.grad),
                "num_vox": int(f64.num_vox)},
-           "bars": {"score_rel": 1e-5, "grad_rel_l2": 1e-3}}
-    if O.ref_available():
-        r = O.ref_metric(grid, fixed, moving, coeff, flavor="g",
-                         threads=threads)
-        out["vs_reference_flavour_g"] = {
-            "score_rel": abs(score - r.score) / abs(r.score),
-            "grad_rel_l2": rel(grad, r.grad),
-            "num_vox": int(r.num_vox)}
+           "bars": {"score_rel": 1e-5,
+                    "grad_rel_l2_vs_reference": 1e-3,
+                    "grad_rel_l2_vs_fp64": "the reference float flavour's "
+                                           "own error + 1e-4"}}
+    r = (O.ref_metric(grid, fixed, moving, coeff, flavor="g",
+                      threads=threads) if O.ref_available()
+         else O.port_mse(grid, fixed, moving, coeff, moving_grad=mg))
+    out["vs_reference_flavour_g"] = {
+        "score_rel": abs(score - r.score) / abs(r.score),
+        "grad_rel_l2": rel(grad, r.grad),
+        "num_vox": int(r.num_vox)}
+    # the reference's own float evaluation against double precision on
+    # the same inputs (the floor any float implementation shares)
+    out["reference_float_vs_fp64"] = {
+        "score_rel": abs(r.score - f64.score) / abs(f64.score),
+        "grad_rel_l2": rel(r.grad, f64.grad)}
     out["device_num_vox"] = int(num_vox)
     return out
 
@@ -579,6 +621,8 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--form", default="tc", choices=["tc", "fp32"])
+    ap.add_argument("--tc-kernel", default="auto",
+                    choices=["auto", "xlane", "tile"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-evals", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -611,7 +655,8 @@ def main():
     fixed, moving, grid, coeff = workload
     flush = torch.empty(256 << 20, dtype=torch.uint8,
                         device=f"cuda:{local_rank}")
-    m = measure_form(P, args.form, args, workload, local_rank, dist, flush)
+    m = measure_form(P, args.form, args, workload, local_rank, dist, flush,
+                     args.tc_kernel)
     ctx, stream = m["ctx"], m["stream"]
     # the other form, timed the same way in the same run (the metric's
     # comparison); replicas time it too so every rank takes the same
@@ -622,8 +667,9 @@ def main():
 
     extra = {}
     if not args.no_extra:
-        extra = extra_metrics(P, ctx, stream, flush, m["d_coeff"],
-                              m["d_grad"], grid.num_roi_voxels, args.warmup)
+        extra["tc_kernels"] = tc_kernel_probe(P, workload, local_rank, flush)
+        extra.update(extra_metrics(P, ctx, stream, flush, m["d_coeff"],
+                              m["d_grad"], grid.num_roi_voxels, args.warmup))
     if rank == 0 and world == 1 and not args.no_extra:
         # one-GPU workloads, measured at N = 1 only (the other ranks would
         # idle meanwhile); the device-only ones first: the reference's
@@ -701,7 +747,10 @@ def main():
                            l2="inputs 167 MB > L2 and 256 MiB flush write "
                               "before every timed step (excluded)",
                            parallelism=f"replicas x{world}",
-                           tiles_per_batch=m["tiles"]),
+                           tc_kernel=m["kernel"][0] if args.form == "tc"
+                           else None,
+                           tiles_per_batch=m["kernel"][1],
+                           batches=m["kernel"][2]),
             "e2e": {"value": e2e_value, "unit": "Gvox/s",
                     "h2d_bytes_per_step": 4 * grid.num_coeff,
                     "d2h_bytes_per_step": 4 * grid.num_coeff + 32},

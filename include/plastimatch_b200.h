@@ -80,8 +80,18 @@ typedef struct {
                            MSE kernel gives up with B200BSP_E_TIMEOUT
                            (0: the default, 1 << 22) */
     int mi_hist;        /* B200BSP_MI_HIST_* (0: equal spacing) */
-    int reserved;       /* zero */
+    int tc_kernel;      /* B200BSP_TC_KERNEL_* (0: chosen per context) */
 } b200bsp_opts;
+
+/* The tensor-core form's MSE kernel.  AUTO starts on the x-lane kernel
+ * (voxel x on the TMEM lanes, 3 <= vox_per_rgn[1] <= 10) where the grid
+ * allows it, else the tile kernel (125 voxels of one tile on the lanes),
+ * and b200bsp_autotune may move between them; XLANE and TILE pin one (XLANE
+ * on a grid it cannot take is B200BSP_E_UNSUPPORTED; TILE has no image
+ * ROIs and runs MI on its FP32 kernels). */
+#define B200BSP_TC_KERNEL_AUTO   0
+#define B200BSP_TC_KERNEL_XLANE  1
+#define B200BSP_TC_KERNEL_TILE   2
 
 /* Mattes MI histogram windows: PVI-8 partial-volume binning (the
  * reference's, bspline_mi.cxx) or cubic B-spline Parzen windows on the
@@ -281,6 +291,12 @@ int b200bsp_mi_grad (b200bsp_ctx* ctx, const float* coeff,
  * deterministic for a given split. */
 int b200bsp_autotune (b200bsp_ctx* ctx, const float* coeff, int evals,
     int* tiles);
+
+/* The MSE kernel the context's next evaluation runs: *kernel receives
+ * B200BSP_TC_KERNEL_XLANE or _TILE (AUTO never; 0 for the FP32 form),
+ * *tiles its tiles per batch and *batches the batches it launches. */
+int b200bsp_mse_kernel (const b200bsp_ctx* ctx, int* kernel, int* tiles,
+    int* batches);
 
 /* Dense displacement field over the ROI (bspline_interpolate_vf,
  * src/base/bspline_interpolate.cxx:112-142): vf is dim[0]*dim[1]*dim[2]*3

@@ -53,11 +53,12 @@ class Opts(C.Structure):
     _fields_ = [("form", C.c_int), ("mse_grad", C.c_int), ("mi_bins", C.c_int),
                 ("device", C.c_int), ("mi_window", C.c_int),
                 ("wait_limit", C.c_int), ("mi_hist", C.c_int),
-                ("reserved", C.c_int)]
+                ("tc_kernel", C.c_int)]
 
 
 MI_WINDOW = {"pvi8": 0, "parzen": 1}
 MI_HIST = {"eqsp": 0, "vopt": 1}
+TC_KERNEL = {"auto": 0, "xlane": 1, "tile": 2}
 
 
 class RegParms(C.Structure):
@@ -174,6 +175,7 @@ _SIGS = {
     "b200bsp_score_mse_static": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP,
                                            _VP, _VP, _VP, _VP, _VP, _VP]),
     "b200bsp_autotune": (C.c_int, [_VP, _VP, C.c_int, _VP]),
+    "b200bsp_mse_kernel": (C.c_int, [_VP, _VP, _VP, _VP]),
     "b200bsp_mi_hist": (C.c_int, [_VP, _VP, _VP]),
     "b200bsp_mi_grad": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "b200bsp_batch_create": (C.c_int, [_VP, C.c_int, _VP]),
@@ -352,7 +354,8 @@ class Context:
     def __init__(self, fixed: Volume, moving: Volume, grid: BsplineGrid,
                  form: str = "tc", mse_grad: str = "nearest",
                  mi_bins: int = 32, device: int = 0, mi_window: str = "pvi8",
-                 mi_hist: str = "eqsp", wait_limit: int = 0):
+                 mi_hist: str = "eqsp", wait_limit: int = 0,
+                 tc_kernel: str = "auto"):
         L = lib()
         self.fixed, self.moving, self.grid = fixed, moving, grid
         self.form = form
@@ -365,6 +368,7 @@ class Context:
         o.mi_window = MI_WINDOW[mi_window]
         o.mi_hist = MI_HIST[mi_hist]
         o.wait_limit = wait_limit
+        o.tc_kernel = TC_KERNEL[tc_kernel]
         o.device = device
         self._fd, self._md = _vol_desc(fixed), _vol_desc(moving)
         self._gd = GridDesc((C.c_int64 * 3)(*grid.roi_offset),
@@ -444,6 +448,15 @@ class Context:
         _check(lib().b200bsp_autotune(self._h, _ptr(coeff), evals,
                                       C.byref(t)), self._h)
         return t.value
+
+    def mse_kernel(self):
+        """b200bsp_mse_kernel: ("xlane" | "tile" | "fp32", tiles per
+        batch, batches) of the next MSE evaluation."""
+        k, t, b = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().b200bsp_mse_kernel(self._h, C.byref(k), C.byref(t),
+                                        C.byref(b)), self._h)
+        name = {0: "fp32", 1: "xlane", 2: "tile"}[k.value]
+        return name, t.value, b.value
 
     def score_mse_f64(self, coeff):
         g = np.zeros(self.num_coeff, np.float64)

@@ -67,7 +67,7 @@ struct XlPlan {
     size_t smem;
     int threads;
     int grid;
-    int score_parts;     // per batch and compute warp
+    int score_parts;     // one per batch
 };
 // extra_row_batches: more batches per row of tiles than the fewest (the
 // autotuner's knob).  The basis table of the fewest serves every split.
@@ -75,21 +75,14 @@ bool xl_plan (const BspGeom& g, XlPlan* plan, int sm_count,
     int extra_row_batches = 0);
 int xl_build_table (const BspGeom& g, const XlPlan& plan, const float* bx_lut,
     void** d_tab);
+// Polls before a device-side wait gives up (between polls the waiting
+// thread sleeps up to about 1 us).
 constexpr unsigned XL_DEFAULT_WAIT_LIMIT = 1u << 22;
-// Per-warp score partials and per-batch arrival counters (the last warp of
-// a batch to finish sums the batch's partials in a fixed order); arrive
-// must be zero before a launch (the finish kernel clears it).
-struct XlScratch {
-    double* wscore;      // [batch][compute warp]
-    int* wcount;
-    unsigned* arrive;    // [batch]
-};
-constexpr int XL_COMPUTE_WARPS = 16;
 cudaError_t launch_mse_xl (const BspGeom& g, const XlPlan& plan,
     int grad_mode, const float* fimg, const float* mimg, const float* mgrad,
     const float* coeff, const void* tab, const float* luts, float* part,
     double* score_part, int* count_part, int* err, unsigned wait_limit,
-    int withhold, const XlScratch& scratch, cudaStream_t st);
+    int withhold, cudaStream_t st);
 
 // Mattes MI on the tensor-core kernel (axis-aligned geometry, tiles of at
 // most 128 voxels, histograms that fit the adjoint operand's area): pass 1

@@ -29,13 +29,15 @@
 // (~16 significant bits); the y/z contractions, positions, trilinear
 // samples and differences are f32 on the CUDA cores.
 //
-// CTA (one per SM): 16 compute warps + 1 tensor-core warp.  Warp w reads
-// TMEM lane quarter w % 4 (x = 32 (w % 4) + lane); the four warps of a
-// quarter split the batch's rows.  The fourth quarter's warps also compute
-// the y/z contraction of the batch two steps ahead; the other three do the
-// adjoint y/z contraction of the previous step.  Steps (batch, chunk of
-// rows) are software-pipelined through double-buffered operands and TMEM
-// accumulators, with mbarrier handshakes:
+// CTA (one per SM): 15 compute warps + 1 tensor-core warp (warp 15).  Warp
+// w reads TMEM lane quarter w % 4 (x = 32 (w % 4) + lane); the warps of a
+// quarter (four, three in the last) split the batch's rows.  The fourth
+// quarter's compute warps also compute the y/z contraction of the step
+// three ahead; the other three quarters' warps do the adjoint y/z
+// contraction of the previous step.  Steps (batch, chunk of
+// rows) are software-pipelined through triple-buffered R operands and
+// double-buffered dc/dv operands and TMEM accumulators, with mbarrier
+// handshakes:
 //   B2 ready (R of step s)  -> MMA x-forward(s)  -> D full(s)
 //   D full(s)               -> voxel phase(s)    -> DC ready(s)
 //   DC ready(s)             -> MMA x-adjoint(s)  -> Rg full(s)
@@ -56,7 +58,9 @@ namespace b200 {
 
 namespace {
 
-constexpr int XL_CW = XL_COMPUTE_WARPS;      // compute warps
+// 16 warps: warp 15 (lane quarter 3, the fourth warp of it) issues the
+// MMAs, warps 0..14 compute; 512 threads leave 128 registers a thread
+constexpr int XL_CW = 15;                    // compute warps
 constexpr int XL_THREADS = 32 * XL_CW;
 constexpr int XL_BLOCK = XL_THREADS + 32;    // + the tensor-core warp
 constexpr int XL_KMAX = 32;                  // knots per batch along x
@@ -66,15 +70,17 @@ constexpr int XL_N = 3 * XL_RC;              // MMA N: (c, rho)
 // Shared memory (offsets from a 1024-byte aligned base).
 constexpr int XS_TAB = 0;          // basis table, bf16 hi (32 KB) then lo
 constexpr int XS_TAB_LO = 32768;
-constexpr int XS_B2 = 65536;       // R operand, 2 buffers x (hi 8 KB, lo 8 KB)
+constexpr int XL_NB2 = 3;          // R operand buffers (steps of look-ahead)
+constexpr int XS_B2 = 65536;       // R operand, XL_NB2 x (hi 8 KB, lo 8 KB)
 constexpr int XS_B2_BUF = 16384;
 constexpr int XS_B2_LO = 8192;
-constexpr int XS_DC = XS_B2 + 2 * XS_B2_BUF;   // dc/dv operand, 2 x (hi, lo)
+constexpr int XS_DC = XS_B2 + XL_NB2 * XS_B2_BUF;  // dc/dv operand, 2 x (hi, lo)
 constexpr int XS_DC_BUF = 49152;
 constexpr int XS_DC_LO = 24576;
 constexpr int XS_DC_ATOM = XL_N * 128;         // 64-voxel K atom of one half
 constexpr int XS_ROWS = XS_DC + 2 * XS_DC_BUF; // per-warp row table
-constexpr int XS_ROWS_BYTES = XL_CW * 8 * 16;
+constexpr int XL_ROWS_MAX = 12;    // rows of a warp (groups of four, 3-way split)
+constexpr int XS_ROWS_BYTES = XL_CW * XL_ROWS_MAX * 16;
 constexpr int XS_LUT = XS_ROWS + XS_ROWS_BYTES;   // by[vy][4], bz[vz][4]
 constexpr int XS_LUT_FLOATS = 2 * 64 * 4;
 constexpr int XS_TOTAL = XS_LUT + XS_LUT_FLOATS * 4;
@@ -108,17 +114,51 @@ xl_mse_mode (int m)
 constexpr float XL_MI_WUNIT = 16777216.0f;   // histogram weights in 2^-24
 
 // Barriers.
-constexpr int XB_B2 = 0;       // + buf: R operand written (4 warp arrivals)
-constexpr int XB_DC = 2;       // + buf: dc/dv written, D read (16 arrivals)
-constexpr int XB_D = 4;        // + buf: x-forward MMA done (commit)
-constexpr int XB_RG = 6;       // + buf: x-adjoint MMA done (commit)
+constexpr int XB_B2 = 0;       // + buf: R operand written (3 warp arrivals)
+constexpr int XB_DC = XL_NB2;  // + buf: dc/dv written, D read (15 arrivals)
+constexpr int XB_D = XB_DC + 2;    // + buf: x-forward MMA done (commit)
+constexpr int XB_RG = XB_D + 2;    // + buf: x-adjoint MMA done (commit)
+constexpr int XB_DRAIN = XB_RG + 2;    // every issued MMA done
+// Longest sleep between two polls of a wait (the sleeps double from 32 ns):
+// the compute warps' waits, the look-ahead warps', the tensor-core
+// thread's wait for an R operand and for a step's dc/dv.
+constexpr unsigned XL_SLEEP_COMPUTE = 128;
+constexpr unsigned XL_SLEEP_AHEAD = 1024;
+constexpr unsigned XL_SLEEP_B2 = 64;
+constexpr unsigned XL_SLEEP_DC = 256;
 
 }  // namespace
+
+// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994, round-up multiplier m = floor(2^32 (2^l - d) / d) + 1 with
+// l = ceil(log2 d)).
+struct XlDiv {
+    uint32_t mul, shift;
+};
+
+static XlDiv
+xl_div (uint32_t d)
+{
+    uint32_t l = 0;
+    while ((1ull << l) < d) l++;
+    XlDiv v;
+    v.mul = (uint32_t) ((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    v.shift = l;
+    return v;
+}
+
+__device__ __forceinline__ int
+xl_q (int n, XlDiv v)
+{
+    return (int) ((__umulhi ((uint32_t) n, v.mul) + (uint32_t) n) >> v.shift);
+}
 
 struct XlArgs {
     BspGeom g;
     int T, KX, nbx, nbatches;
     int nlz, nch;            // z planes per row chunk, chunks per batch
+    XlDiv d_nch, d_nbx, d_rdy, d_vy;   // by nch, nbx, rdims[1], vpr[1]
     unsigned wait_limit;
     int withhold;            // testing aid: the tensor-core warp issues
                              // nothing, so the first waits run out
@@ -131,7 +171,6 @@ struct XlArgs {
     float* part;             // [batch][c][xk + KX (j + 4 k)]
     double* score_part;      // [batch]
     int* count_part;         // [batch]
-    XlScratch sx;            // per-warp partials, arrival counters
     int* err;
     // Mattes MI modes: bin images, bins, the pass-2 factor table [fixed
     // bin][moving bin], the voxel count (float; Parzen: [1] the pass-2
@@ -165,17 +204,30 @@ split_word (float x)
         | ((uint32_t) __bfloat16_as_ushort (l) << 16);
 }
 
+// Polls of one thread on an mbarrier phase with exponential back-off
+// (sleeps of 32, 64, ... ns, at most cap): true once the phase completes,
+// false after `limit` polls or once another warp has given up.
+__device__ __forceinline__ bool
+xl_poll (uint64_t* bar, uint32_t ph, unsigned cap, unsigned limit,
+    volatile int* s_abort)
+{
+    unsigned t = 32;
+    for (uint32_t n = 0; n < limit && !*s_abort; n++) {
+        if (mbar_try_wait (bar, ph)) return true;
+        __nanosleep (t);
+        t = min (2 * t, cap);
+    }
+    return false;
+}
+
 // Bounded wait of one warp on an mbarrier phase: lane 0 polls, gives up
 // after the limit or once another warp has given up.
 __device__ __forceinline__ bool
 xl_wait (const XlArgs& a, const XlCtx& x, uint64_t* bar, uint32_t ph,
-    volatile int* s_abort, int code)
+    volatile int* s_abort, int code, unsigned cap)
 {
     if (x.lane == 0) {
-        bool ok = false;
-        for (uint32_t n = 0; n < a.wait_limit && !*s_abort; n++) {
-            if (mbar_try_wait (bar, ph)) { ok = true; break; }
-        }
+        const bool ok = xl_poll (bar, ph, cap, a.wait_limit, s_abort);
         if (!ok) {
             *s_abort = 1;
             atomicExch (a.err, code);
@@ -194,12 +246,13 @@ __device__ __forceinline__ XlStep
 xl_step (const XlArgs& a, int s)
 {
     XlStep t;
-    const int i = s / a.nch;
+    const int i = xl_q (s, a.d_nch);
     t.ch = s - i * a.nch;
     t.b = blockIdx.x + i * gridDim.x;
-    t.tx0 = (t.b % a.nbx) * a.T;
-    t.ty = (t.b / a.nbx) % a.g.rdims[1];
-    t.tz = t.b / (a.nbx * a.g.rdims[1]);
+    const int q1 = xl_q (t.b, a.d_nbx);         // row of tiles
+    t.tx0 = (t.b - q1 * a.nbx) * a.T;
+    t.tz = xl_q (q1, a.d_rdy);
+    t.ty = q1 - t.tz * a.g.rdims[1];
     t.lz0 = t.ch * a.nlz;
     t.nlz = min (a.nlz, a.g.vpr[2] - t.lz0);
     return t;
@@ -207,15 +260,19 @@ xl_step (const XlArgs& a, int s)
 
 // y/z forward contraction of one step into the R operand buffer (K = xk
 // rows, N = (c, rho) columns, MN-major, 128-byte swizzle): thread (c, xk)
-// of the fourth lane quarter's warps 0..2.
+// of the fourth lane quarter's warps 0..2.  The rows are unrolled (VY
+// known at compile time) and stored two at a time (rows rho, rho + 1 of
+// one component share a 32-bit word of the operand).
+template <int VY>
 __device__ __forceinline__ void
-xl_yz_forward (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf)
+xl_yz_forward_t (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf)
 {
+    constexpr int NLZ = XL_RC / VY;
     const BspGeom& g = a.g;
     const int c = x.j4, xk = x.lane;
     if (c >= 3) return;
     const float* by = (const float*) (x.sm + XS_LUT);
-    const float* bz = by + 4 * g.vpr[1];
+    const float* bz = by + 4 * VY;
     const int kx = t.tx0 + xk;
     const bool live = xk < a.KX && kx < g.cdims[0];
     float cf[16];
@@ -229,28 +286,97 @@ xl_yz_forward (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf)
         }
     }
     uint8_t* hi = x.sm + XS_B2 + buf * XS_B2_BUF;
-    const int vy = g.vpr[1];
     const uint32_t rowoff = (uint32_t) ((xk >> 3) * 1024 + (xk & 7) * 128);
-    for (int l = 0; l < t.nlz; l++) {
-        const float* bzl = bz + 4 * (t.lz0 + l);
-        float z[4];
+    const int nrc = VY * t.nlz;
+    auto word_off = [&](int n) {
+        return (uint32_t) ((n >> 6) * 4096) + rowoff
+            + (uint32_t) ((((n & 63) >> 3) ^ (xk & 7)) << 4)
+            + (uint32_t) ((n & 7) * 2);
+    };
+    uint32_t w_even = 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            z[j] = bzl[0] * cf[j] + bzl[1] * cf[4 + j] + bzl[2] * cf[8 + j]
-                + bzl[3] * cf[12 + j];
+    for (int l = 0; l < NLZ; l++) {
+        if (l < t.nlz) {
+            const float* bzl = bz + 4 * (t.lz0 + l);
+            float z[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                z[j] = bzl[0] * cf[j] + bzl[1] * cf[4 + j] + bzl[2] * cf[8 + j]
+                    + bzl[3] * cf[12 + j];
+            }
+#pragma unroll
+            for (int ly = 0; ly < VY; ly++) {
+                const int rho = ly + VY * l;
+                const float r = by[4 * ly] * z[0] + by[4 * ly + 1] * z[1]
+                    + by[4 * ly + 2] * z[2] + by[4 * ly + 3] * z[3];
+                const uint32_t w = split_word (r);
+                if ((rho & 1) == 0) {
+                    w_even = w;
+                    if (rho + 1 == nrc) {          // a last, unpaired row
+                        const uint32_t off = word_off (c * XL_RC + rho);
+                        *(unsigned short*) (hi + off) = (unsigned short) w;
+                        *(unsigned short*) (hi + XS_B2_LO + off)
+                            = (unsigned short) (w >> 16);
+                    }
+                } else {
+                    const uint32_t off = word_off (c * XL_RC + rho - 1);
+                    *(uint32_t*) (hi + off) = __byte_perm (w_even, w, 0x5410);
+                    *(uint32_t*) (hi + XS_B2_LO + off)
+                        = __byte_perm (w_even, w, 0x7632);
+                }
+            }
         }
-        for (int ly = 0; ly < vy; ly++) {
-            const float* byl = by + 4 * ly;
-            const float r = byl[0] * z[0] + byl[1] * z[1] + byl[2] * z[2]
-                + byl[3] * z[3];
-            const int n = c * XL_RC + ly + vy * l;
-            const uint32_t off = (uint32_t) ((n >> 6) * 4096) + rowoff
-                + (uint32_t) ((((n & 63) >> 3) ^ (xk & 7)) << 4)
-                + (uint32_t) ((n & 7) * 2);
-            const uint32_t w = split_word (r);
-            *(unsigned short*) (hi + off) = (unsigned short) w;
-            *(unsigned short*) (hi + XS_B2_LO + off) = (unsigned short) (w >> 16);
+    }
+}
+
+// The look-ahead warps' L2 prefetch of step t's fixed-image rows (the only
+// reads of the voxel phase whose addresses do not depend on the
+// displacement), one 128-byte line a thread: thread i of the 96 takes
+// lines i, i + 96, ...
+__device__ __forceinline__ void
+xl_prefetch_fixed (const XlArgs& a, const XlCtx& x, const XlStep& t)
+{
+    const BspGeom& g = a.g;
+    const int i = 32 * x.j4 + x.lane;
+    const int x0 = g.roi_off[0] + g.vpr[0] * t.tx0;
+    const int x1 = min (x0 + a.T * g.vpr[0], g.roi_off[0] + g.roi_dim[0]);
+    const int y0 = g.roi_off[1] + g.vpr[1] * t.ty;
+    const int y1 = min (y0 + g.vpr[1], g.roi_off[1] + g.roi_dim[1]);
+    const int z0 = g.roi_off[2] + g.vpr[2] * t.tz + t.lz0;
+    const int z1 = min (z0 + t.nlz, g.roi_off[2] + g.roi_dim[2]);
+    if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
+    const size_t fdx = g.fdim[0], fdxy = (size_t) g.fdim[0] * g.fdim[1];
+    // lines of a row: from the line holding x0 to the one holding x1 - 1
+    const uintptr_t base = (uintptr_t) a.fimg;
+    const int ny = y1 - y0;
+    const int nrow = ny * (z1 - z0);
+    // every row spans the same number of lines or one more; take the most
+    const int nl = (int) ((4 * (x1 - x0) + 127) >> 7) + 1;
+    for (int r = i; r < nrow * nl; r += 96) {
+        const int row = r / nl, l = r - row * nl;
+        const size_t o = ((size_t) (z0 + row / ny) * fdxy
+            + (size_t) (y0 + row % ny) * fdx + x0) * 4;
+        const uintptr_t first = (base + o) & ~(uintptr_t) 127;
+        const uintptr_t line = first + 128 * (uintptr_t) l;
+        if (line < base + o + 4 * (size_t) (x1 - x0)) {
+            asm volatile ("prefetch.global.L2 [%0];" :: "l"(line));
         }
+    }
+}
+
+__device__ __forceinline__ void
+xl_yz_forward (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf)
+{
+    switch (a.g.vpr[1]) {
+    case 3: xl_yz_forward_t<3> (a, x, t, buf); break;
+    case 4: xl_yz_forward_t<4> (a, x, t, buf); break;
+    case 5: xl_yz_forward_t<5> (a, x, t, buf); break;
+    case 6: xl_yz_forward_t<6> (a, x, t, buf); break;
+    case 7: xl_yz_forward_t<7> (a, x, t, buf); break;
+    case 8: xl_yz_forward_t<8> (a, x, t, buf); break;
+    case 9: xl_yz_forward_t<9> (a, x, t, buf); break;
+    case 10: xl_yz_forward_t<10> (a, x, t, buf); break;
+    default: break;                  // the plan admits no other vy
     }
 }
 
@@ -484,24 +610,32 @@ xl_pz_dc_dv (const XlArgs& a, float u, int fb, const float w2[3],
 
 // The voxel phase of one step for warp (quarter q, rows part j4): the
 // warp's rows [ra, rb) of the chunk, four at a time (their field values as
-// three 4-column TMEM loads), two samples in flight per thread.
+// three 4-column TMEM loads); the MSE modes issue the gathers of all four
+// samples before using any, the MI modes two at a time.
 template <int MODE, bool AXIS, bool ROI>
 __device__ __forceinline__ void
 xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
     float& scf, int& cnt)
 {
+    constexpr int NS = xl_mse_mode (MODE) ? 4 : 2;
     const BspGeom& g = a.g;
     const int vy = g.vpr[1];
     const int nrc = vy * t.nlz;
-    const int ra = (nrc * x.j4) >> 2, rb = (nrc * (x.j4 + 1)) >> 2;
+    // the quarter's rows split among its compute warps (three in quarter
+    // 3) in whole groups of four, so that one group at most is partial
+    const int parts = x.q == 3 ? 3 : 4;
+    const int ng = (nrc + 3) >> 2;
+    const int ra = 4 * (ng * x.j4 / parts);
+    const int rb = min (4 * (ng * (x.j4 + 1) / parts), nrc);
     const int nr = rb - ra;
     if (nr <= 0) return;
     // one row per lane: (y, z) part of the world position and the fixed
     // image's row index (-1: row outside the ROI)
-    float4* rows = (float4*) (x.sm + XS_ROWS) + 8 * x.warp;
+    float4* rows = (float4*) (x.sm + XS_ROWS) + XL_ROWS_MAX * x.warp;
     if (x.lane < nr) {
         const int rho = ra + x.lane;
-        const int ly = rho % vy, lz = t.lz0 + rho / vy;
+        const int qy = xl_q (rho, a.d_vy);
+        const int ly = rho - qy * vy, lz = t.lz0 + qy;
         const int fj = g.roi_off[1] + vy * t.ty + ly;
         const int fk = g.roi_off[2] + g.vpr[2] * t.tz + lz;
         const bool live = fj < g.roi_off[1] + g.roi_dim[1]
@@ -528,6 +662,17 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
     const float xp[3] = {__fmul_rn (g.fstep[0], ffi), __fmul_rn (g.fstep[3], ffi),
         __fmul_rn (g.fstep[6], ffi)};
     const int dxm = g.mdim[0], dxym = g.mdim[0] * g.mdim[1];
+    // the moving geometry in registers for the row loop
+    float m_org[3], m_prj[3], m_hi[3], m_fmax[3];
+    int m_cmax[3];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+        m_org[e] = g.morigin[e];
+        m_prj[e] = g.mproj[4 * e];
+        m_hi[e] = g.m_hi[e];
+        m_fmax[e] = g.m_fmax[e];
+        m_cmax[e] = g.mdim[e] - 2;
+    }
     // adjoint operand: row n = c * 32 + rho, column (K) x
     uint8_t* dcb = x.sm + XS_DC + buf * XS_DC_BUF + (X >> 6) * XS_DC_ATOM
         + (X & 7) * 2;
@@ -539,13 +684,13 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
         float dv[12];
         tmem_ld4x3_wait (tl + r0, tl + XL_RC + r0, tl + 2 * XL_RC + r0, dv);
 #pragma unroll
-        for (int u0 = 0; u0 < 4; u0 += 2) {
-            if (r0 + u0 >= rb) break;          // both rows past the warp's
-            bool ok[2], rowv[2];
-            int mvf[2], mvr[2], fidx[2], clampb[2];
-            float w2[2][3];
+        for (int u0 = 0; u0 < 4; u0 += NS) {
+            if (r0 + u0 >= rb) break;          // all rows past the warp's
+            bool ok[NS], rowv[NS];
+            int mvf[NS], mvr[NS], fidx[NS], clampb[NS];
+            float w2[NS][3];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
+            for (int h = 0; h < NS; h++) {
                 const int u = u0 + h;
                 const int rho = r0 + u;
                 rowv[h] = rho < rb;
@@ -557,7 +702,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                 float tt[3];
 #pragma unroll
                 for (int e = 0; e < 3; e++) {
-                    tt[e] = __fsub_rn (__fadd_rn (fxyz[e], d[e]), g.morigin[e]);
+                    tt[e] = __fsub_rn (__fadd_rn (fxyz[e], d[e]), m_org[e]);
                 }
                 bool in = rowv[h] && xlive && frow >= 0;
                 int f[3];
@@ -567,23 +712,23 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                 for (int e = 0; e < 3; e++) {
                     float ma;
                     if (AXIS) {
-                        ma = __fmul_rn (tt[e], g.mproj[4 * e]);
+                        ma = __fmul_rn (tt[e], m_prj[e]);
                     } else {
                         ma = __fadd_rn (__fadd_rn (__fmul_rn (tt[0], g.mproj[3 * e]),
                             __fmul_rn (tt[1], g.mproj[3 * e + 1])),
                             __fmul_rn (tt[2], g.mproj[3 * e + 2]));
                     }
-                    in = in && ma > -0.5f && ma < g.m_hi[e];
+                    in = in && ma > -0.5f && ma < m_hi[e];
                     if (MODE == XM_PZ_GRAD
-                        && (ma < 0.f || ma >= g.m_fmax[e] + 1.f)) {
+                        && (ma < 0.f || ma >= m_fmax[e] + 1.f)) {
                         clampb[h] |= 1 << e;      // li_clamp holds this axis
                     }
                     // li_clamp without conversions: floor(max(ma, 0)) from
                     // an add rounded down to 2^23, corner clamped to dim - 2,
                     // fraction saturated to [0, 1]
                     const float big = __fadd_rd (fmaxf (ma, 0.f), 8388608.f);
-                    f[e] = min (__float_as_int (big) - 0x4B000000, g.mdim[e] - 2);
-                    const float fc = fminf (big - 8388608.f, g.m_fmax[e]);
+                    f[e] = min (__float_as_int (big) - 0x4B000000, m_cmax[e]);
+                    const float fc = fminf (big - 8388608.f, m_fmax[e]);
                     const float w = __saturatef (ma - fc);
                     w2[h][e] = w;
                     up[e] = w >= 0.5f;
@@ -605,19 +750,27 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                     const int rho = r0 + u0 + h;
                     uint8_t* p = dcb + (rho >> 3) * 1024 + (rho & 7) * 128
                         + ((xch ^ (rho & 7)) << 4);
-#pragma unroll
-                    for (int e = 0; e < 3; e++) {
-                        const uint32_t w = split_word (dc[e]);
-                        *(unsigned short*) (p + 4096 * e) = (unsigned short) w;
-                        *(unsigned short*) (p + XS_DC_LO + 4096 * e)
-                            = (unsigned short) (w >> 16);
-                    }
+                    // hi = bf16(v), lo = bf16(v - hi), two values a convert
+                    const __nv_bfloat162 h01 = __floats2bfloat162_rn (dc[0], dc[1]);
+                    const __nv_bfloat162 h22 = __floats2bfloat162_rn (dc[2], dc[2]);
+                    const float2 f01 = __bfloat1622float2 (h01);
+                    const __nv_bfloat162 l01 = __floats2bfloat162_rn (
+                        dc[0] - f01.x, dc[1] - f01.y);
+                    const float f2 = __low2float (h22);
+                    const __nv_bfloat162 l22 = __floats2bfloat162_rn (
+                        dc[2] - f2, dc[2] - f2);
+                    *(__nv_bfloat16*) (p) = __low2bfloat16 (h01);
+                    *(__nv_bfloat16*) (p + 4096) = __high2bfloat16 (h01);
+                    *(__nv_bfloat16*) (p + 8192) = __low2bfloat16 (h22);
+                    *(__nv_bfloat16*) (p + XS_DC_LO) = __low2bfloat16 (l01);
+                    *(__nv_bfloat16*) (p + XS_DC_LO + 4096) = __high2bfloat16 (l01);
+                    *(__nv_bfloat16*) (p + XS_DC_LO + 8192) = __low2bfloat16 (l22);
                 }
             };
             if constexpr (xl_mse_mode (MODE)) {
-                float cr[2][8], fv[2], gr[2][3];
+                float cr[NS][8], fv[NS], gr[NS][3];
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int h = 0; h < NS; h++) {
                     const float* mp = a.mimg + mvf[h];
                     cr[h][0] = __ldg (mp);
                     cr[h][1] = __ldg (mp + 1);
@@ -636,7 +789,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                     }
                 }
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int h = 0; h < NS; h++) {
                     float diff = trilinear_lerp (w2[h], cr[h]) - fv[h];
                     diff = ok[h] ? diff : 0.f;
                     scf = fmaf (diff, diff, scf);
@@ -658,9 +811,9 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
             } else if constexpr (MODE == XM_MI_GRAD || MODE == XM_MI_HIST) {
                 // PVI-8: the fixed voxel's bin and the bins of the eight
                 // trilinear corners, in li_value's order
-                int fb[2], mb[2][8];
+                int fb[NS], mb[NS][8];
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int h = 0; h < NS; h++) {
                     const uint8_t* mp = a.mbin + mvf[h];
                     mb[h][0] = __ldg (mp);
                     mb[h][1] = __ldg (mp + 1);
@@ -675,7 +828,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                 if constexpr (MODE == XM_MI_GRAD) {
                     const float nv = __ldg (a.mi_nvf);
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
+                    for (int h = 0; h < NS; h++) {
                         float dc[3] = {0.f, 0.f, 0.f};
                         if (ok[h]) xl_mi_dc_dv (a, w2[h], fb[h], mb[h], nv, dc);
                         store_dc (h, dc);
@@ -683,17 +836,17 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                 } else {
                     unsigned long long* hsm = (unsigned long long*) (x.sm + XS_DC);
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
+                    for (int h = 0; h < NS; h++) {
                         xl_mi_hist_add (a, hsm, ok[h], w2[h], fb[h], mb[h],
                             x.lane, cnt);
                     }
                 }
             } else {
                 // Parzen windows: the trilinear moving value's window
-                float cr[2][8];
-                int fb[2];
+                float cr[NS][8];
+                int fb[NS];
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int h = 0; h < NS; h++) {
                     const float* mp = a.mimg + mvf[h];
                     cr[h][0] = __ldg (mp);
                     cr[h][1] = __ldg (mp + 1);
@@ -706,7 +859,7 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
                     fb[h] = __ldg (a.fbin + fidx[h]);
                 }
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int h = 0; h < NS; h++) {
                     const float u = parzen_centre (trilinear_lerp (w2[h], cr[h]),
                         a.pz_mmin, a.pz_mdelta);
                     if constexpr (MODE == XM_PZ_HIST) {
@@ -726,13 +879,14 @@ xl_voxel (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
 }
 
 // x-forward MMA of a step: D[x][(c, rho)] = Bx[x][xk] R[xk][(c, rho)],
-// K = 32 knots, three split terms; one thread.
+// K = 32 knots, three split terms; one thread.  buf: the D accumulator,
+// rbuf: the R operand buffer.
 __device__ __forceinline__ void
-xl_issue_forward (const XlCtx& x, int buf, uint64_t* bar)
+xl_issue_forward (const XlCtx& x, int buf, int rbuf, uint64_t* bar)
 {
     const uint32_t idesc = idesc_bf16_f32 (128, XL_N, 0, 1);
     const uint32_t ta = x.sm_base + XS_TAB;
-    const uint32_t tb = x.sm_base + XS_B2 + buf * XS_B2_BUF;
+    const uint32_t tb = x.sm_base + XS_B2 + rbuf * XS_B2_BUF;
 #pragma unroll
     for (int term = 0; term < 3; term++) {
         const uint32_t A = term == 2 ? ta + XS_TAB_LO : ta;     // hi, hi, lo
@@ -772,6 +926,23 @@ xl_issue_adjoint (const XlCtx& x, int buf, uint64_t* bar)
     tc_commit (bar);
 }
 
+// A look-ahead warp's share of step sn: its component of the R operand into
+// buffer rbuf, then (MSE) its share of the L2 prefetch of the step's fixed
+// rows.
+template <int MODE>
+__device__ __forceinline__ bool
+xl_produce (const XlArgs& a, const XlCtx& x, uint64_t* s_bar, int sn,
+    int rbuf)
+{
+    const XlStep tn = xl_step (a, sn);
+    xl_yz_forward (a, x, tn, rbuf);
+    fence_proxy_async_smem ();
+    __syncwarp ();
+    if (x.lane == 0) mbar_arrive (&s_bar[XB_B2 + rbuf]);
+    if (xl_mse_mode (MODE)) xl_prefetch_fixed (a, x, tn);
+    return true;
+}
+
 }  // namespace
 
 template <int MODE, bool AXIS, bool ROI>
@@ -779,9 +950,13 @@ __global__ void __launch_bounds__ (XL_BLOCK, 1)
 mse_xl_kernel (XlArgs a)
 {
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t s_bar[9];      // + drain: every issued MMA done
+    __shared__ uint64_t s_bar[XB_DRAIN + 1];
     __shared__ uint32_t s_taddr;
     __shared__ int s_abort;
+    // each compute warp's score and count of the batch that ends at a
+    // step, by step parity (summed by the tensor-core thread)
+    __shared__ double s_wsc[2][XL_CW];
+    __shared__ int s_wcnt[2][XL_CW];
 
     const BspGeom& g = a.g;
     XlCtx x;
@@ -795,15 +970,14 @@ mse_xl_kernel (XlArgs a)
     const bool mma_warp = x.warp == XL_CW;
 
     if (tid == 0) {
-        mbar_init (&s_bar[XB_B2], 4);
-        mbar_init (&s_bar[XB_B2 + 1], 4);
+        for (int i = 0; i < XL_NB2; i++) mbar_init (&s_bar[XB_B2 + i], 3);
         mbar_init (&s_bar[XB_DC], XL_CW);
         mbar_init (&s_bar[XB_DC + 1], XL_CW);
         mbar_init (&s_bar[XB_D], 1);
         mbar_init (&s_bar[XB_D + 1], 1);
         mbar_init (&s_bar[XB_RG], 1);
         mbar_init (&s_bar[XB_RG + 1], 1);
-        mbar_init (&s_bar[8], 1);
+        mbar_init (&s_bar[XB_DRAIN], 1);
         fence_barrier_init ();
         s_abort = 0;
     }
@@ -839,32 +1013,52 @@ mse_xl_kernel (XlArgs a)
         if (x.lane == 0 && !a.withhold) {
             // phase parities, bit buf of each word (no local arrays)
             uint32_t ph_b2 = 0, ph_dc = 0;
-            auto wait = [&](uint64_t* bar, uint32_t& ph, int buf, int code) {
-                for (uint32_t n = 0; n < a.wait_limit && !*abort_flag; n++) {
-                    if (mbar_try_wait (bar, (ph >> buf) & 1u)) {
-                        ph ^= 1u << buf;
-                        return true;
-                    }
+            auto wait = [&](uint64_t* bar, uint32_t& ph, int buf, int code,
+                    unsigned cap) {
+                if (xl_poll (bar, (ph >> buf) & 1u, cap, a.wait_limit,
+                        abort_flag)) {
+                    ph ^= 1u << buf;
+                    return true;
                 }
                 *abort_flag = 1;
                 atomicExch (a.err, code);
                 return false;
             };
+            int rb = 0;                      // s % XL_NB2
             for (int s = 0; s <= S; s++) {
                 if (s < S) {
-                    const int buf = s & 1;
-                    if (!wait (&s_bar[XB_B2 + buf], ph_b2, buf, 3)) break;
+                    if (!wait (&s_bar[XB_B2 + rb], ph_b2, rb, 3, XL_SLEEP_B2)) {
+                        break;
+                    }
                     tc_fence_after ();
-                    xl_issue_forward (x, buf, &s_bar[XB_D + buf]);
+                    xl_issue_forward (x, s & 1, rb, &s_bar[XB_D + (s & 1)]);
+                    rb = rb + 1 == XL_NB2 ? 0 : rb + 1;
                 }
                 if (s >= 1) {
                     // the voxel phase of step s - 1 is done with D (and
                     // has written dc/dv, except in the histogram passes)
                     const int pb = (s - 1) & 1;
-                    if (!wait (&s_bar[XB_DC + pb], ph_dc, pb, 4)) break;
+                    if (!wait (&s_bar[XB_DC + pb], ph_dc, pb, 4, XL_SLEEP_DC)) {
+                        break;
+                    }
                     tc_fence_after ();
                     if (!xl_hist_mode (MODE)) {
                         xl_issue_adjoint (x, pb, &s_bar[XB_RG + pb]);
+                    }
+                    if (xl_mse_mode (MODE)) {
+                        // the batch's score and count, warps in order
+                        const XlStep tp = xl_step (a, s - 1);
+                        if (tp.ch == a.nch - 1) {
+                            double v = 0.0;
+                            int n = 0;
+#pragma unroll
+                            for (int w = 0; w < XL_CW; w++) {
+                                v += s_wsc[pb][w];
+                                n += s_wcnt[pb][w];
+                            }
+                            a.score_part[tp.b] = v;
+                            a.count_part[tp.b] = n;
+                        }
                     }
                 }
             }
@@ -879,11 +1073,8 @@ mse_xl_kernel (XlArgs a)
         int cnt = 0;
         bool ok = true;
         if (yz_fwd_warp) {
-            for (int s = 0; s < 2 && s < S; s++) {
-                xl_yz_forward (a, x, xl_step (a, s), s);
-                fence_proxy_async_smem ();
-                __syncwarp ();
-                if (x.lane == 0) mbar_arrive (&s_bar[XB_B2 + s]);
+            for (int s = 0; s < XL_NB2 && s < S && ok; s++) {
+                ok = xl_produce<MODE> (a, x, s_bar, s, s);
             }
         }
         // adjoint y/z of step sp (quarters 0..2): accumulate, and write
@@ -891,7 +1082,7 @@ mse_xl_kernel (XlArgs a)
         auto yz_adjoint = [&](int sp) {
             const int pb = sp & 1;
             if (!xl_wait (a, x, &s_bar[XB_RG + pb], (ph_rg >> pb) & 1u,
-                    abort_flag, 2)) {
+                    abort_flag, 2, XL_SLEEP_COMPUTE)) {
                 return false;
             }
             ph_rg ^= 1u << pb;
@@ -912,7 +1103,8 @@ mse_xl_kernel (XlArgs a)
         for (int s = 0; s < S && ok; s++) {
             const int buf = s & 1;
             if (!xl_wait (a, x, &s_bar[XB_D + buf], (ph_d >> buf) & 1u,
-                    abort_flag, 1)) {
+                    abort_flag, 1,
+                    yz_fwd_warp ? XL_SLEEP_AHEAD : XL_SLEEP_COMPUTE)) {
                 ok = false;
                 break;
             }
@@ -926,35 +1118,16 @@ mse_xl_kernel (XlArgs a)
             }
             if (xl_mse_mode (MODE) && t.ch == a.nch - 1) {
                 // the warp's score and count of the batch (fixed tree
-                // order), then the batch's: the last of its 16 warps to
-                // get here sums their partials in warp order
+                // order), for the tensor-core thread once this step's
+                // dc/dv barrier completes
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {
                     sc += __shfl_down_sync (0xffffffffu, sc, o);
                     cnt += __shfl_down_sync (0xffffffffu, cnt, o);
                 }
-                const size_t wb = (size_t) t.b * XL_CW;
-                unsigned arrived = 0;
                 if (x.lane == 0) {
-                    a.sx.wscore[wb + x.warp] = sc;
-                    a.sx.wcount[wb + x.warp] = cnt;
-                    __threadfence ();
-                    arrived = atomicAdd (a.sx.arrive + t.b, 1u);
-                }
-                arrived = __shfl_sync (0xffffffffu, arrived, 0);
-                if (arrived == XL_CW - 1) {
-                    __threadfence ();
-                    double v = x.lane < XL_CW ? __ldcg (a.sx.wscore + wb + x.lane) : 0.0;
-                    int n = x.lane < XL_CW ? __ldcg (a.sx.wcount + wb + x.lane) : 0;
-#pragma unroll
-                    for (int o = XL_CW / 2; o > 0; o >>= 1) {
-                        v += __shfl_down_sync (0xffffffffu, v, o);
-                        n += __shfl_down_sync (0xffffffffu, n, o);
-                    }
-                    if (x.lane == 0) {
-                        a.score_part[t.b] = v;
-                        a.count_part[t.b] = n;
-                    }
+                    s_wsc[buf][x.warp] = sc;
+                    s_wcnt[buf][x.warp] = cnt;
                 }
                 sc = 0.0;
                 cnt = 0;
@@ -964,11 +1137,11 @@ mse_xl_kernel (XlArgs a)
             __syncwarp ();
             if (x.lane == 0) mbar_arrive (&s_bar[XB_DC + buf]);
             if (yz_fwd_warp) {
-                if (s + 2 < S) {
-                    xl_yz_forward (a, x, xl_step (a, s + 2), buf);
-                    fence_proxy_async_smem ();
-                    __syncwarp ();
-                    if (x.lane == 0) mbar_arrive (&s_bar[XB_B2 + buf]);
+                // the forward MMA of step s has read R buffer s % XL_NB2:
+                // step s + XL_NB2 goes there
+                if (s + XL_NB2 < S) {
+                    ok = xl_produce<MODE> (a, x, s_bar, s + XL_NB2,
+                        s % XL_NB2);
                 }
             } else if (s >= 1 && !xl_hist_mode (MODE)) {
                 ok = yz_adjoint (s - 1);
@@ -1008,10 +1181,10 @@ mse_xl_kernel (XlArgs a)
     if (mma_warp && x.lane == 0 && !a.withhold) {
         // every MMA this thread issued completes before TMEM is released,
         // also when a wait gave up (the MMAs themselves wait on nothing)
-        tc_commit (&s_bar[8]);
-        for (uint32_t n = 0; n < a.wait_limit + 1000000u; n++) {
-            if (mbar_try_wait (&s_bar[8], 0)) break;
-        }
+        tc_commit (&s_bar[XB_DRAIN]);
+        int never = 0;
+        xl_poll (&s_bar[XB_DRAIN], 0, XL_SLEEP_AHEAD, a.wait_limit + 1000u,
+            &never);
     }
     tc_fence_before ();
     __syncthreads ();
@@ -1119,6 +1292,10 @@ launch_mi_xl (const BspGeom& g, const XlPlan& p, bool hist_pass,
     a.nbatches = p.nbatches;
     a.nlz = p.nlz;
     a.nch = p.nch;
+    a.d_nch = xl_div (p.nch);
+    a.d_nbx = xl_div (p.nbx);
+    a.d_rdy = xl_div (g.rdims[1]);
+    a.d_vy = xl_div (g.vpr[1]);
     a.wait_limit = wait_limit;
     a.coeff = coeff;
     a.tab = (const uint4*) tab;
@@ -1158,7 +1335,7 @@ launch_mse_xl (const BspGeom& g, const XlPlan& p, int grad_mode,
     const float* fimg, const float* mimg, const float* mgrad,
     const float* coeff, const void* tab, const float* luts, float* part,
     double* score_part, int* count_part, int* err, unsigned wait_limit,
-    int withhold, const XlScratch& scratch, cudaStream_t st)
+    int withhold, cudaStream_t st)
 {
     XlArgs a = {};
     a.g = g;
@@ -1168,13 +1345,16 @@ launch_mse_xl (const BspGeom& g, const XlPlan& p, int grad_mode,
     a.nbatches = p.nbatches;
     a.nlz = p.nlz;
     a.nch = p.nch;
+    a.d_nch = xl_div (p.nch);
+    a.d_nbx = xl_div (p.nbx);
+    a.d_rdy = xl_div (g.rdims[1]);
+    a.d_vy = xl_div (g.vpr[1]);
     a.wait_limit = wait_limit;
     a.withhold = withhold;
     a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;
     a.tab = (const uint4*) tab;
     a.luts = luts;
     a.part = part; a.score_part = score_part; a.count_part = count_part;
-    a.sx = scratch;
     a.err = err;
     const bool axis = xl_axis_aligned (g);
     const bool roi = g.fmask || g.mroi;

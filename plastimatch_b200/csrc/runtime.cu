@@ -68,11 +68,9 @@ struct b200bsp_ctx {
     bool use_xl = false;
     bool has_xl = false;
     bool use_xl_mi = true;    // MI on the x-lane kernel where it applies
-    int xl_max_batches = 0;   // over the autotuner's x-lane splits
     XlPlan xplan;
     PartLayout xlay;
     void* d_xtab = nullptr;
-    XlScratch xs = {nullptr, nullptr, nullptr};
     unsigned wait_limit = XL_DEFAULT_WAIT_LIMIT;
     int withhold_mma = 0;     // b200bsp_set_wait_limit's testing aid
     // b200bsp_score's device path: the regulariser on a second stream,
@@ -282,7 +280,6 @@ free_all (b200bsp_ctx* c)
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
     cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
     cudaFree (c->d_qlut); cudaFree (c->d_xtab); cudaFree (c->d_inv_dc);
-    cudaFree (c->xs.wscore); cudaFree (c->xs.wcount); cudaFree (c->xs.arrive);
     cudaFree (c->d_lm_p); cudaFree (c->d_lm_w); cudaFree (c->d_lm_fm);
     cudaFree (c->d_lm_dc);
     cudaFree (c->d_fmask); cudaFree (c->d_mroi);
@@ -568,17 +565,25 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     if (o.mse_grad == 0) alloc ((void**) &c->d_mgrad, 3 * nm * sizeof (float));
     int sm_count = 148;
     cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount, o.device);
-    if (o.form == B200BSP_FORM_TC) {
+    if (o.tc_kernel < 0 || o.tc_kernel > B200BSP_TC_KERNEL_TILE) {
+        rc2 = fail (c, B200BSP_E_BADARG, "tc_kernel %d unknown", o.tc_kernel);
+    } else if (o.form == B200BSP_FORM_TC
+               && o.tc_kernel != B200BSP_TC_KERNEL_TILE) {
         c->has_xl = c->use_xl = xl_plan (g, &c->xplan, sm_count);
+        if (!c->has_xl && o.tc_kernel == B200BSP_TC_KERNEL_XLANE) {
+            rc2 = fail (c, B200BSP_E_UNSUPPORTED,
+                "x-lane kernel: vox_per_rgn[1] = %d outside 3..10", g.vpr[1]);
+        }
     }
     if (o.wait_limit < 0) {
         rc2 = fail (c, B200BSP_E_BADARG, "wait_limit must be >= 0");
     } else if (o.wait_limit > 0) {
         c->wait_limit = (unsigned) o.wait_limit;
     }
-    // the tile kernel's 16-byte moving-gradient copy, only where the x-lane
-    // kernel does not apply
-    if (o.mse_grad == 0 && o.form == B200BSP_FORM_TC && !c->has_xl) {
+    // the tile kernel's 16-byte moving-gradient copy, wherever the tile
+    // kernel may run
+    if (o.mse_grad == 0 && o.form == B200BSP_FORM_TC
+        && !(c->has_xl && o.tc_kernel == B200BSP_TC_KERNEL_XLANE)) {
         alloc ((void**) &c->d_mgrad4, nm * sizeof (float4));
     }
     alloc ((void**) &c->d_coeff, c->num_coeff * sizeof (float));
@@ -628,8 +633,6 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
                         (size_t) xp.nbatches * (xp.T + 3) * 16 * 3);
                     score_parts = std::max (score_parts,
                         (size_t) xp.score_parts);
-                    c->xl_max_batches = std::max (c->xl_max_batches,
-                        xp.nbatches);
                 }
                 use_xl_plan (c, c->xplan);
             }
@@ -650,16 +653,6 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     score_parts = std::max (score_parts, (size_t) std::max (c->nscore_parts, 1));
     alloc ((void**) &c->d_score_part, score_parts * sizeof (double));
     alloc ((void**) &c->d_count_part, score_parts * sizeof (int));
-    if (c->has_xl) {
-        const size_t nb = (size_t) c->xl_max_batches;
-        alloc ((void**) &c->xs.wscore, nb * XL_COMPUTE_WARPS * sizeof (double));
-        alloc ((void**) &c->xs.wcount, nb * XL_COMPUTE_WARPS * sizeof (int));
-        alloc ((void**) &c->xs.arrive, nb * sizeof (unsigned));
-        if (!rc2 && cudaMemset (c->xs.arrive, 0, nb * sizeof (unsigned))
-            != cudaSuccess) {
-            rc2 = fail (c, B200BSP_E_CUDA, "memset failed");
-        }
-    }
     if (!rc2 && o.form == B200BSP_FORM_TC) {
         rc2 = tc_build_tables (c->geom, c->plan, &c->d_qlut);
         if (rc2) rc2 = fail (c, rc2, "tensor-core tables: %s", cudaGetErrorString (cudaGetLastError ()));
@@ -898,7 +891,7 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
         CK (launch_mse_xl (g, plan, c->opts.mse_grad, c->d_fixed,
             c->d_moving, c->d_mgrad, dcoeff, c->d_xtab, c->d_luts,
             c->d_part, c->d_score_part, c->d_count_part, c->d_err,
-            c->wait_limit, c->withhold_mma, c->xs, c->stream));
+            c->wait_limit, c->withhold_mma, c->stream));
     } else {
         TcPlan plan = c->plan;
         if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
@@ -917,8 +910,7 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
         xl ? c->xplan.score_parts : c->nscore_parts,
         c->opts.form == B200BSP_FORM_TC ? c->d_err : nullptr, c->d_res,
         res_host, grad_out, grad64_out, score_out, score64_out, nvox_out,
-        c->stream, xl ? c->xs.arrive : nullptr, xl ? c->xplan.nbatches : 0,
-        combine));
+        c->stream, nullptr, 0, combine));
     c->last_launches += 1;
     return B200BSP_OK;
 }
@@ -1062,7 +1054,9 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     }
     c->use_xl = false;
     const bool roi = c->geom.fmask || c->geom.mroi;
-    for (int e = 0; e <= TC_TUNE_MAX_EXTRA && !rc && !roi; e++) {
+    const bool tile_ok = !roi && !(c->has_xl
+        && c->opts.tc_kernel == B200BSP_TC_KERNEL_XLANE);
+    for (int e = 0; e <= TC_TUNE_MAX_EXTRA && !rc && tile_ok; e++) {
         TcPlan p;
         if (!tc_plan (c->geom, &p, 2, sm_count, e)) continue;
         use_tc_plan (c, p);
@@ -1085,6 +1079,27 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     }
     if (tiles) *tiles = c->use_xl ? c->xplan.T : best.bx;
     return check_device_error (c);
+}
+
+extern "C" int
+b200bsp_mse_kernel (const b200bsp_ctx* c, int* kernel, int* tiles,
+    int* batches)
+{
+    if (!c) return B200BSP_E_BADARG;
+    int k = 0, t = 1, b = c->geom.ntiles;
+    if (c->opts.form == B200BSP_FORM_TC && c->use_xl) {
+        k = B200BSP_TC_KERNEL_XLANE;
+        t = c->xplan.T;
+        b = c->xplan.nbatches;
+    } else if (c->opts.form == B200BSP_FORM_TC) {
+        k = B200BSP_TC_KERNEL_TILE;
+        t = c->plan.bx;
+        b = c->plan.nbatches;
+    }
+    if (kernel) *kernel = k;
+    if (tiles) *tiles = t;
+    if (batches) *batches = b;
+    return B200BSP_OK;
 }
 
 // One or both MI passes on the context's form (tensor-core modes where they
@@ -1364,7 +1379,8 @@ b200bsp_set_roi (b200bsp_ctx* c, const b200bsp_volume* fixed_roi,
     if (any && c->opts.form == B200BSP_FORM_TC && !c->has_xl) {
         return fail (c, B200BSP_E_UNSUPPORTED,
             "image ROIs in the tensor-core form need its x-lane kernel "
-            "(3 <= vox_per_rgn[1] <= 10); use B200BSP_FORM_FP32");
+            "(3 <= vox_per_rgn[1] <= 10, tc_kernel not TILE); use "
+            "B200BSP_FORM_FP32");
     }
     CK (cudaSetDevice (c->device));
     CK (cudaStreamSynchronize (c->stream));

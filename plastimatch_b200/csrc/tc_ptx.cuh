@@ -38,6 +38,20 @@ mbar_try_wait (uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
+// One poll that may suspend the thread for up to `ns` nanoseconds while
+// the phase is incomplete (it resumes as soon as the phase completes).
+__device__ __forceinline__ bool
+mbar_try_wait_sleep (uint64_t* bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t ok;
+    asm volatile (
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(smem_addr (bar)), "r"(parity), "r"(ns) : "memory");
+    return ok != 0;
+}
+
 // Bounded wait: returns false after `limit` unsuccessful polls (each poll
 // may itself suspend for a hardware-chosen time).
 __device__ __forceinline__ bool

@@ -13,7 +13,10 @@
 * Non-finite coefficients: the voxels whose displacement is not finite
   fail the inside test and drop out; the call succeeds with a finite score
   and gradient.  (The reference's is_inside lets NaN through and then
-  reads outside its image; a defined result is the library's choice.)
+  reads outside its image; a defined result is the library's choice.)  The
+  FP32 form loses the knot's 64 tiles; the tensor-core form's x contraction
+  is one dense product per row of tiles, whose zeros off the band times a
+  NaN are NaN, so it loses every row of tiles that holds the knot.
 """
 import ctypes as C
 
@@ -108,5 +111,7 @@ def test_nonfinite_coefficient_drops_its_voxels(form, bad):
         c[3 * k] = bad
         s, g, n = ctx.score_mse(c)
     assert np.isfinite(s) and np.all(np.isfinite(g))
-    # the knot's 64 tiles of 125 voxels drop out (some may lie outside anyway)
-    assert 0 < n0 - n <= 64 * 125
+    # the knot's 64 tiles of 125 voxels drop out (FP32 form), or the 16
+    # rows of tiles along x through them (tensor-core form)
+    limit = 64 * 125 if form == "fp32" else 16 * grid.rdims[0] * 125
+    assert 0 < n0 - n <= limit, (n0 - n, limit)

@@ -64,6 +64,7 @@ def test_registration_64cubed_matches_reference(form):
     mse_ref = float(np.mean((w_ref.reshape(fixed.img.shape).astype(np.float64)
                              - fixed.img) ** 2))
     assert abs(mse - mse_ref) <= 2e-2 * mse_ref, (mse, mse_ref)
-    # and the registration did register: the warped image is far closer
+    # and the registration did register: the warped image is closer (the
+    # reference's own 30 iterations leave about a third of the start)
     mse0 = float(np.mean((moving.img.astype(np.float64) - fixed.img) ** 2))
-    assert mse < 0.2 * mse0
+    assert mse < 0.5 * mse0
