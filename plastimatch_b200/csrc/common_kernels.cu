@@ -10,6 +10,9 @@
 //                    the result is deterministic without atomics.
 //   volume_grad   -- volume_calc_grad (src/base/volume_grad.cxx:9-76)
 #include <cfloat>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "kernels.cuh"
 
@@ -184,6 +187,24 @@ store_run (T* __restrict__ dst, const double* __restrict__ src, int n)
     }
 }
 
+cudaError_t
+set_max_dynamic_smem (const void* kernel, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;   // -> bytes set
+    int dev = 0;
+    cudaError_t e = cudaGetDevice (&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock (mu);
+    const auto key = std::make_pair (kernel, dev);
+    const auto it = done.find (key);
+    if (it != done.end () && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute (kernel,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done[key] = bytes;
+    return e;
+}
+
 __global__ void __launch_bounds__ (FIN_THREADS)
 finish_mse_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
     const double* __restrict__ sp, const int* __restrict__ cp, int nparts,
@@ -298,7 +319,9 @@ finish_mse_kernel (BspGeom g, PartLayout lay, const float* __restrict__ part,
             // the 8 x 3 loads first, then the sums in ascending batch order
             const int KF = lay.kx * lay.ky * lay.kz;
             const int bi1 = min (lay.nbx - 1, kx / lay.bx);
-#pragma unroll 1
+            // all 4 x 8 x 3 loads in flight (the sums stay in ascending
+            // batch order)
+#pragma unroll
             for (int dk = 0; dk < 4; dk++) {
                 const int bk = kz - 3 + dk, lz = kz - bk * lay.bz;
                 const bool okz = bk >= 0 && bk < lay.nbz && lz < lay.kz;

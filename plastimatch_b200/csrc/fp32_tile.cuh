@@ -10,6 +10,7 @@
 #pragma once
 
 #include "bsp_common.cuh"
+#include "kernels.cuh"
 
 namespace b200 {
 
@@ -137,8 +138,8 @@ launch_fp32_tile (const BspGeom& g, const F& fn, const float* mimg,
     size_t smem = fp32_tile_smem_bytes (g);
     auto k = fp32_tile_kernel<F>;
     if (smem > 48 * 1024) {
-        cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int) smem);
+        cudaError_t e = set_max_dynamic_smem ((const void*) k, (int) smem);
+        if (e != cudaSuccess) return e;
     }
     k<<<g.ntiles, FP32_THREADS, smem, st>>> (g, fn, mimg, coeff, luts, part,
         score_part, count_part);

@@ -56,6 +56,11 @@ cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
     float* part, double* score_part, int* count_part, int* err_flag,
     cudaStream_t st);
 
+// cudaFuncAttributeMaxDynamicSharedMemorySize for a kernel on the current
+// device, set once per (kernel, device) and size: the attribute call is a
+// host round trip that would otherwise precede every launch.
+cudaError_t set_max_dynamic_smem (const void* kernel, int bytes);
+
 // Tensor-core form, x-lane kernel (mse_xl.cu): one batch is a row of T
 // tiles along x with TMEM lane = voxel x; rows of the batch in chunks of
 // whole z planes (at most 32 rows).  Supports 3 <= vox_per_rgn[1] <= 10.

@@ -859,9 +859,9 @@ mi_run (MiState* s, const BspGeom& g, const float* d_coeff,
     }
     size_t hsmem = (size_t) nh * sizeof (unsigned long long);
     auto hk = mi_hist_kernel;
-    if (hsmem > 48 * 1024) {
-        cudaFuncSetAttribute (hk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int) hsmem);
+    if (hsmem > 48 * 1024
+        && set_max_dynamic_smem ((const void*) hk, (int) hsmem) != cudaSuccess) {
+        return B200BSP_E_CUDA;
     }
     int grid = std::min (g.ntiles, 8 * sms);
     if (passes & MI_PASS_HIST) {

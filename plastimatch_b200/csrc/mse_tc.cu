@@ -1543,8 +1543,8 @@ static cudaError_t
 launch_mode (const TcPlan& p, const TcArgs& a, cudaStream_t st)
 {
     auto k = mse_tc_kernel<MODE>;
-    cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int) p.smem);
+    cudaError_t e = set_max_dynamic_smem ((const void*) k, (int) p.smem);
+    if (e != cudaSuccess) return e;
     k<<<p.grid, TC_BLOCK, p.smem, st>>> (a);
     return cudaGetLastError ();
 }

@@ -1259,8 +1259,8 @@ static cudaError_t
 xl_launch_t (const XlPlan& p, const XlArgs& a, cudaStream_t st)
 {
     auto k = mse_xl_kernel<MODE, AXIS, ROI>;
-    cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int) p.smem);
+    cudaError_t e = set_max_dynamic_smem ((const void*) k, (int) p.smem);
+    if (e != cudaSuccess) return e;
     k<<<p.grid, XL_BLOCK, p.smem, st>>> (a);
     return cudaGetLastError ();
 }

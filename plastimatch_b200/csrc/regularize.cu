@@ -14,7 +14,8 @@
 //   pass 2  knot-y bands applied to the pass-1 fields
 //   pass 3  weighted knot-z bands, summed into the nine outputs below; the
 //           gradient and the per-knot score follow, and the score is
-//           reduced per block in a fixed order.
+//           reduced per block, then over the blocks by the last block to
+//           finish, in a fixed order.
 // Outputs of pass 3 (input component in brackets):
 //   Dx[x] Dy[y] Dz[z]   same-component terms: V0..V8, V21..V31 on every
 //                       component, V15..V20 on the components the elastic
@@ -27,9 +28,11 @@
 //   S = sum over knots of cx Dx + cy Dy + cz Dz + cy Cxy + cz Cxz + cz Cyz.
 // All arithmetic is double; the gradient is added into the float gradient
 // once per knot component.
+#include <algorithm>
 #include <cstring>
 #include <map>
 
+#include "kernels.cuh"
 #include "regularize.cuh"
 
 namespace b200 {
@@ -188,23 +191,49 @@ term_outputs (int t, int out[3])
 }
 
 // ---- device passes ----------------------------------------------------------
+//
+// Each block covers 32 knots along x times REG_TY knots along the pass's
+// axis (256 threads: x fastest).  The pass's input fields over the block's
+// knots and a halo of 3 on either side of that axis are staged in shared
+// memory once, so the 7-tap stencils read each value from L2 once instead
+// of seven times.  Taps outside the grid read zeros (the reference's sums
+// skip them; adding a zero product leaves every sum unchanged).
+
+constexpr int REG_TY = 8;                    // knots along the pass axis
+constexpr int REG_TH = REG_TY + 6;           // with the halo
 
 __global__ void __launch_bounds__ (REG_THREADS)
-reg_pass_x (RegPlan plan, int cx, int nk, const double* __restrict__ gx,
+reg_pass_x (RegPlan plan, int cx, int cy, int nk, const double* __restrict__ gx,
     const float* __restrict__ coeff, double* __restrict__ t1)
 {
-    int knot = blockIdx.x * REG_THREADS + threadIdx.x;
-    if (knot >= nk) return;
-    int kx = knot % cx;
+    // block: knots kx0 .. kx0 + 31 (+ 3 either side) of rows ky0 .. ky0 + 7
+    __shared__ float sc[3][REG_TY][32 + 6];
+    __shared__ double sb[6][32][7];          // the six x bands of the block
+    const int kx0 = blockIdx.x * 32, ky0 = blockIdx.y * REG_TY;
+    const int kz = blockIdx.z;
+    for (int i = threadIdx.x; i < 3 * REG_TY * 38; i += REG_THREADS) {
+        const int c = i / (REG_TY * 38), r = (i / 38) % REG_TY, j = i % 38;
+        const int kx = kx0 - 3 + j, ky = ky0 + r;
+        sc[c][r][j] = kx >= 0 && kx < cx && ky < cy
+            ? coeff[3 * (kx + cx * (ky + cy * kz)) + c] : 0.f;
+    }
+    for (int i = threadIdx.x; i < 6 * 32 * 7; i += REG_THREADS) {
+        const int f = i / (32 * 7), j = i % (32 * 7);
+        (&sb[0][0][0])[i] = kx0 + j / 7 < cx
+            ? gx[((size_t) f * cx + kx0) * 7 + j] : 0.0;
+    }
+    __syncthreads ();
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int kx = kx0 + tx, ky = ky0 + ty;
+    if (kx >= cx || ky >= cy) return;
+    const int knot = kx + cx * (ky + cy * kz);
     for (int s = 0; s < plan.n1; s++) {
-        int c = plan.t1_c[s];
-        const double* band = gx + ((size_t) plan.t1_xf[s] * cx + kx) * 7;
+        const int c = plan.t1_c[s];
+        const double* band = sb[plan.t1_xf[s]][tx];
         double acc = 0.0;
 #pragma unroll
         for (int d = -3; d <= 3; d++) {
-            if (kx + d >= 0 && kx + d < cx) {
-                acc += band[d + 3] * (double) coeff[3 * (knot + d) + c];
-            }
+            acc += band[d + 3] * (double) sc[c][ty][tx + 3 + d];
         }
         t1[(size_t) s * nk + knot] = acc;
     }
@@ -215,18 +244,35 @@ reg_pass_y (RegPlan plan, int cx, int cy, int nk,
     const double* __restrict__ gy, const double* __restrict__ t1,
     double* __restrict__ t2)
 {
-    int knot = blockIdx.x * REG_THREADS + threadIdx.x;
-    if (knot >= nk) return;
-    int ky = (knot / cx) % cy;
+    // block: knots kx0 .. kx0 + 31 of rows ky0 - 3 .. ky0 + 10, every
+    // pass-1 field
+    extern __shared__ double st[];           // [n1][REG_TH][32]
+    __shared__ double sb[6][REG_TY][7];      // the six y bands of the block
+    const int kx0 = blockIdx.x * 32, ky0 = blockIdx.y * REG_TY;
+    const int kz = blockIdx.z;
+    for (int i = threadIdx.x; i < plan.n1 * REG_TH * 32; i += REG_THREADS) {
+        const int s = i / (REG_TH * 32), r = (i / 32) % REG_TH, j = i % 32;
+        const int kx = kx0 + j, ky = ky0 - 3 + r;
+        st[i] = kx < cx && ky >= 0 && ky < cy
+            ? t1[(size_t) s * nk + kx + cx * (ky + cy * kz)] : 0.0;
+    }
+    for (int i = threadIdx.x; i < 6 * REG_TY * 7; i += REG_THREADS) {
+        const int f = i / (REG_TY * 7), j = i % (REG_TY * 7);
+        (&sb[0][0][0])[i] = ky0 + j / 7 < cy
+            ? gy[((size_t) f * cy + ky0) * 7 + j] : 0.0;
+    }
+    __syncthreads ();
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int kx = kx0 + tx, ky = ky0 + ty;
+    if (kx >= cx || ky >= cy) return;
+    const int knot = kx + cx * (ky + cy * kz);
     for (int s = 0; s < plan.n2; s++) {
-        const double* src = t1 + (size_t) plan.t2_src[s] * nk;
-        const double* band = gy + ((size_t) plan.t2_yf[s] * cy + ky) * 7;
+        const double* src = st + plan.t2_src[s] * (REG_TH * 32) + tx;
+        const double* band = sb[plan.t2_yf[s]][ty];
         double acc = 0.0;
 #pragma unroll
         for (int d = -3; d <= 3; d++) {
-            if (ky + d >= 0 && ky + d < cy) {
-                acc += band[d + 3] * src[knot + d * cx];
-            }
+            acc += band[d + 3] * src[(ty + 3 + d) * 32];
         }
         t2[(size_t) s * nk + knot] = acc;
     }
@@ -236,33 +282,52 @@ __global__ void __launch_bounds__ (REG_THREADS)
 reg_pass_z (RegPlan plan, int cx, int cy, int cz, int nk,
     const double* __restrict__ hz, const double* __restrict__ t2,
     const float* __restrict__ coeff, float* __restrict__ grad,
-    double* __restrict__ grad64, double* __restrict__ part)
+    double* __restrict__ grad64, double* __restrict__ part,
+    unsigned* __restrict__ arrive, double* __restrict__ score)
 {
+    // block: knots kx0 .. kx0 + 31 of row ky, planes kz0 - 3 .. kz0 + 10,
+    // every pass-2 field
+    // [n2][REG_TH][32] pass-2 fields, then [ne][REG_TY][7] z bands
+    extern __shared__ double st[];
     __shared__ double sh_v[REG_THREADS / 32];
     __shared__ int sh_n[REG_THREADS / 32];
-    int knot = blockIdx.x * REG_THREADS + threadIdx.x;
+    __shared__ bool s_last;
+    const int kx0 = blockIdx.x * 32, ky = blockIdx.y;
+    const int kz0 = blockIdx.z * REG_TY;
+    const int plane = cx * cy;
+    for (int i = threadIdx.x; i < plan.n2 * REG_TH * 32; i += REG_THREADS) {
+        const int s = i / (REG_TH * 32), r = (i / 32) % REG_TH, j = i % 32;
+        const int kx = kx0 + j, kz = kz0 - 3 + r;
+        st[i] = kx < cx && kz >= 0 && kz < cz
+            ? t2[(size_t) s * nk + kx + cx * ky + (size_t) plane * kz] : 0.0;
+    }
+    double* sb = st + plan.n2 * REG_TH * 32;
+    for (int i = threadIdx.x; i < plan.ne * REG_TY * 7; i += REG_THREADS) {
+        const int e = i / (REG_TY * 7), j = i % (REG_TY * 7);
+        sb[i] = kz0 + j / 7 < cz ? hz[((size_t) e * cz + kz0) * 7 + j] : 0.0;
+    }
+    __syncthreads ();
+    const int tx = threadIdx.x & 31, tz = threadIdx.x >> 5;
+    const int kx = kx0 + tx, kz = kz0 + tz;
     double S = 0.0;
-    if (knot < nk) {
-        int kz = knot / (cx * cy);
-        int plane = cx * cy;
+    if (kx < cx && kz < cz) {
+        const int knot = kx + cx * ky + plane * kz;
+        // each output sums its entries in the order they were formed
         double out[O_N];
 #pragma unroll
-        for (int o = 0; o < O_N; o++) out[o] = 0.0;
-        for (int e = 0; e < plan.ne; e++) {
-            const double* src = t2 + (size_t) plan.e_src[e] * nk;
-            const double* band = hz + ((size_t) e * cz + kz) * 7;
-            double acc = 0.0;
+        for (int o = 0; o < O_N; o++) {
+            double v = 0.0;
+            for (int e = plan.e_off[o]; e < plan.e_off[o + 1]; e++) {
+                const double* src = st + plan.e_src[e] * (REG_TH * 32) + tx;
+                const double* band = sb + (e * REG_TY + tz) * 7;
+                double acc = 0.0;
 #pragma unroll
-            for (int d = -3; d <= 3; d++) {
-                if (kz + d >= 0 && kz + d < cz) {
-                    acc += band[d + 3] * src[knot + d * plane];
+                for (int d = -3; d <= 3; d++) {
+                    acc += band[d + 3] * src[(tz + 3 + d) * 32];
                 }
+                v += acc;
             }
-            // out[e_out] += acc, with a compile-time index
-#pragma unroll
-            for (int o = 0; o < O_N; o++) {
-                if (plan.e_out[e] == o) out[o] += acc;
-            }
+            out[o] = v;
         }
         double c0 = coeff[3 * knot + 0], c1 = coeff[3 * knot + 1];
         double c2 = coeff[3 * knot + 2];
@@ -272,7 +337,7 @@ reg_pass_z (RegPlan plan, int cx, int cy, int cz, int nk,
         const double g1 = 2.0 * out[O_DY] + out[O_CXY] + out[O_CZY];
         const double g2 = 2.0 * out[O_DZ] + out[O_CXZ] + out[O_CYZ];
         if (grad64) {
-            // stored for a later kernel to add (b200bsp_score's overlap)
+            // stored for a later kernel to add (b200bsp_score)
             grad64[3 * knot + 0] = g0;
             grad64[3 * knot + 1] = g1;
             grad64[3 * knot + 2] = g2;
@@ -284,19 +349,27 @@ reg_pass_z (RegPlan plan, int cx, int cy, int cz, int nk,
     }
     int dummy = 0;
     block_sum<REG_THREADS> (S, dummy, sh_v, sh_n);
-    if (threadIdx.x == 0) part[blockIdx.x] = S;
-}
-
-__global__ void __launch_bounds__ (1024)
-reg_reduce (const double* __restrict__ part, int n, double* __restrict__ out)
-{
-    __shared__ double sh_v[32];
-    __shared__ int sh_n[32];
+    // the last block to finish sums the block partials in block order
+    // (the same order whichever block is last) and re-arms the counter
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (threadIdx.x == 0) {
+        part[bid] = S;
+        __threadfence ();
+        s_last = atomicAdd (arrive, 1u) == (unsigned) nb - 1;
+    }
+    __syncthreads ();
+    if (!s_last) return;
+    __threadfence ();
     double v = 0.0;
-    for (int i = threadIdx.x; i < n; i += 1024) v += part[i];
-    int dummy = 0;
-    block_sum<1024> (v, dummy, sh_v, sh_n);
-    if (threadIdx.x == 0) *out = v;
+    for (int i = threadIdx.x; i < nb; i += REG_THREADS) v += __ldcg (part + i);
+    dummy = 0;
+    __syncthreads ();
+    block_sum<REG_THREADS> (v, dummy, sh_v, sh_n);
+    if (threadIdx.x == 0) {
+        *score = v;
+        *arrive = 0u;
+    }
 }
 
 // ---- host -------------------------------------------------------------------
@@ -309,7 +382,19 @@ reg_alloc (RegState* s, const BspGeom& g, const float grid_spac[3])
         s->gs[d] = (double) grid_spac[d];
     }
     s->nknots = g.nknots;
-    s->nblocks = (g.nknots + REG_THREADS - 1) / REG_THREADS;
+    // the staged fields exceed the default 48 KB of shared memory for the
+    // larger plans (set once per context, on its device)
+    const size_t slot = REG_TH * 32 * sizeof (double);
+    if (set_max_dynamic_smem ((const void*) reg_pass_y,
+            (int) (REG_T1_MAX * slot)) != cudaSuccess
+        || set_max_dynamic_smem ((const void*) reg_pass_z,
+            (int) (REG_T2_MAX * slot + REG_E_MAX * REG_TY * 7 * sizeof (double)))
+            != cudaSuccess) {
+        return B200BSP_E_CUDA;
+    }
+    // pass z's grid: 32 knots along x x one y row x REG_TY planes
+    s->nblocks = ((g.cdims[0] + 31) / 32) * g.cdims[1]
+        * ((g.cdims[2] + REG_TY - 1) / REG_TY);
     const int cx = g.cdims[0], cy = g.cdims[1], cz = g.cdims[2];
     if (cudaMalloc (&s->d_gx, sizeof (double) * 6 * cx * 7) != cudaSuccess
         || cudaMalloc (&s->d_gy, sizeof (double) * 6 * cy * 7) != cudaSuccess
@@ -319,6 +404,8 @@ reg_alloc (RegState* s, const BspGeom& g, const float grid_spac[3])
         || cudaMalloc (&s->d_t2, sizeof (double) * REG_T2_MAX * (size_t) g.nknots)
             != cudaSuccess
         || cudaMalloc (&s->d_part, sizeof (double) * s->nblocks) != cudaSuccess
+        || cudaMalloc (&s->d_arrive, sizeof (unsigned)) != cudaSuccess
+        || cudaMemset (s->d_arrive, 0, sizeof (unsigned)) != cudaSuccess
         || cudaMalloc (&s->d_score, sizeof (double)) != cudaSuccess
         || cudaMallocHost (&s->h_score, sizeof (double)) != cudaSuccess) {
         cudaGetLastError ();
@@ -358,6 +445,7 @@ reg_free (RegState* s)
 {
     cudaFree (s->d_gx); cudaFree (s->d_gy); cudaFree (s->d_hz);
     cudaFree (s->d_t1); cudaFree (s->d_t2); cudaFree (s->d_part);
+    cudaFree (s->d_arrive);
     cudaFree (s->d_score); cudaFreeHost (s->h_score);
     *s = RegState ();
 }
@@ -415,6 +503,27 @@ reg_prepare (RegState* s, const b200bsp_reg_parms* p, cudaStream_t st)
             }
         }
     }
+    {
+        // pass 3's entries grouped by output, in their order within each
+        RegPlan q = plan;
+        std::vector<double> hz2 (hz.size ());
+        int n = 0;
+        for (int o = 0; o < O_N; o++) {
+            q.e_off[o] = (unsigned char) n;
+            for (int e = 0; e < plan.ne; e++) {
+                if (plan.e_out[e] != o) continue;
+                q.e_src[n] = plan.e_src[e];
+                q.e_out[n] = plan.e_out[e];
+                std::copy (hz.begin () + (size_t) e * cz * 7,
+                    hz.begin () + (size_t) (e + 1) * cz * 7,
+                    hz2.begin () + (size_t) n * cz * 7);
+                n++;
+            }
+        }
+        q.e_off[O_N] = (unsigned char) n;
+        plan = q;
+        hz.swap (hz2);
+    }
     if (!hz.empty ()
         && cudaMemcpyAsync (s->d_hz, hz.data (), hz.size () * sizeof (double),
             cudaMemcpyHostToDevice, st) != cudaSuccess) {
@@ -439,16 +548,21 @@ reg_run (RegState* s, const BspGeom& g, const b200bsp_reg_parms* p,
     }
     const int cx = g.cdims[0], cy = g.cdims[1], cz = g.cdims[2];
     const int nk = g.nknots;
-    const int nb = s->nblocks;
+    const int bx = (cx + 31) / 32;
+    const size_t slot = REG_TH * 32 * sizeof (double);
+    const size_t zbands = REG_TY * 7 * sizeof (double);
     if (s->plan.n1) {
-        reg_pass_x<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, nk, s->d_gx,
-            d_coeff, s->d_t1);
-        reg_pass_y<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, cy, nk, s->d_gy,
-            s->d_t1, s->d_t2);
+        const dim3 gxy (bx, (cy + REG_TY - 1) / REG_TY, cz);
+        reg_pass_x<<<gxy, REG_THREADS, 0, st>>> (s->plan, cx, cy, nk,
+            s->d_gx, d_coeff, s->d_t1);
+        reg_pass_y<<<gxy, REG_THREADS, s->plan.n1 * slot, st>>> (s->plan, cx,
+            cy, nk, s->d_gy, s->d_t1, s->d_t2);
     }
-    reg_pass_z<<<nb, REG_THREADS, 0, st>>> (s->plan, cx, cy, cz, nk, s->d_hz,
-        s->d_t2, d_coeff, d_grad, d_grad64, s->d_part);
-    reg_reduce<<<1, 1024, 0, st>>> (s->d_part, nb, s->d_score);
+    const dim3 gz (bx, cy, (cz + REG_TY - 1) / REG_TY);
+    reg_pass_z<<<gz, REG_THREADS, s->plan.n2 * slot + s->plan.ne * zbands,
+        st>>> (s->plan, cx, cy,
+        cz, nk, s->d_hz, s->d_t2, d_coeff, d_grad, d_grad64, s->d_part,
+        s->d_arrive, s->d_score);
     return cudaGetLastError () == cudaSuccess ? B200BSP_OK : B200BSP_E_CUDA;
 }
 

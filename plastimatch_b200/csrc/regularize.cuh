@@ -22,6 +22,10 @@ struct RegPlan {
     unsigned char t2_src[REG_T2_MAX], t2_yf[REG_T2_MAX];
     int ne;                         // pass 3: z-axis bands into outputs
     unsigned char e_src[REG_E_MAX], e_out[REG_E_MAX];
+    // pass 3's entries grouped by output (stable, so each output sums its
+    // entries in the order they were formed): output o takes entries
+    // e_off[o] .. e_off[o + 1] - 1 of the nine
+    unsigned char e_off[10];
 };
 
 struct RegState {
@@ -34,6 +38,7 @@ struct RegState {
     double* d_t1 = nullptr;         // [REG_T1_MAX][nknots]
     double* d_t2 = nullptr;         // [REG_T2_MAX][nknots]
     double* d_part = nullptr;       // per-block score partials
+    unsigned* d_arrive = nullptr;   // blocks of pass 3 done (zero between runs)
     double* d_score = nullptr;
     double* h_score = nullptr;
     int nblocks = 0;

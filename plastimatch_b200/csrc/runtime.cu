@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -67,7 +68,6 @@ struct b200bsp_ctx {
     // and the autotuner has not preferred the tile kernel
     bool use_xl = false;
     bool has_xl = false;
-    bool use_xl_mi = true;    // MI on the x-lane kernel where it applies
     XlPlan xplan;
     PartLayout xlay;
     void* d_xtab = nullptr;
@@ -75,11 +75,14 @@ struct b200bsp_ctx {
     int withhold_mma = 0;     // b200bsp_set_wait_limit's testing aid
     // b200bsp_score's device path: the regulariser on a second stream,
     // overlapping the tile kernel, its gradient kept in double
-    cudaStream_t aux_stream = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     double* d_reg_grad64 = nullptr;
     float* d_total = nullptr;
     int tc_grid = 0;          // CTAs of the tile kernel; 0: plan.grid
+    int sm_count = 148;
+    // b200bsp_score's regulariser: a second stream, and the fork and join
+    // of it around the MSE kernel
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // the optimiser's device workspace, kept between runs (optimize.cu)
     void* opt_ws = nullptr;
     void (*opt_ws_free) (void*) = nullptr;
@@ -122,6 +125,9 @@ fail (b200bsp_ctx* c, int code, const char* fmt, ...)
     if (c) c->err = buf; else g_create_error = buf;
     return code;
 }
+
+// SMs left to b200bsp_score's regulariser beside the MSE kernel
+constexpr int REG_SIDE_SMS = 12;
 
 #define CK(call)                                                        \
     do {                                                                \
@@ -276,6 +282,9 @@ free_all (b200bsp_ctx* c)
     cudaFree (c->d_fixed); cudaFree (c->d_moving); cudaFree (c->d_mgrad);
     cudaFree (c->d_out);
     cudaFree (c->d_mgrad4);
+    if (c->ev_fork) cudaEventDestroy (c->ev_fork);
+    if (c->ev_join) cudaEventDestroy (c->ev_join);
+    if (c->aux_stream) cudaStreamDestroy (c->aux_stream);
     cudaFree (c->d_coeff); cudaFree (c->d_luts); cudaFree (c->d_grad);
     cudaFree (c->d_grad64); cudaFree (c->d_part); cudaFree (c->d_score_part);
     cudaFree (c->d_count_part); cudaFree (c->d_res); cudaFree (c->d_err);
@@ -289,9 +298,6 @@ free_all (b200bsp_ctx* c)
     if (c->opt_ws_free) c->opt_ws_free (c->opt_ws);
     c->opt_ws = nullptr;
     for (auto& e : c->ev) if (e) cudaEventDestroy (e);
-    if (c->ev_fork) cudaEventDestroy (c->ev_fork);
-    if (c->ev_join) cudaEventDestroy (c->ev_join);
-    if (c->aux_stream) cudaStreamDestroy (c->aux_stream);
     cudaFree (c->d_reg_grad64);
     cudaFree (c->d_total);
     if (c->own_stream) cudaStreamDestroy (c->own_stream);
@@ -565,6 +571,7 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
     if (o.mse_grad == 0) alloc ((void**) &c->d_mgrad, 3 * nm * sizeof (float));
     int sm_count = 148;
     cudaDeviceGetAttribute (&sm_count, cudaDevAttrMultiProcessorCount, o.device);
+    c->sm_count = sm_count;
     if (o.tc_kernel < 0 || o.tc_kernel > B200BSP_TC_KERNEL_TILE) {
         rc2 = fail (c, B200BSP_E_BADARG, "tc_kernel %d unknown", o.tc_kernel);
     } else if (o.form == B200BSP_FORM_TC
@@ -874,7 +881,8 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     double* grad64_out, float* score_out, double* score64_out,
     long long* nvox_out, DevResult* res_host = nullptr,
     const FinishCombine& combine = FinishCombine (),
-    cudaEvent_t before_finish = nullptr)
+    cudaEvent_t before_finish = nullptr,
+    const std::function<int ()>& after_main = nullptr)
 {
     const BspGeom& g = c->geom;
     if (c->opts.form == B200BSP_FORM_FP32) {
@@ -903,6 +911,10 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
     c->last_launches++;
     int rc = mark_main_done (c);
     if (rc) return rc;
+    if (after_main) {
+        rc = after_main ();
+        if (rc) return rc;
+    }
     const bool xl = c->opts.form == B200BSP_FORM_TC && c->use_xl;
     if (before_finish) CK (cudaStreamWaitEvent (c->stream, before_finish, 0));
     CK (launch_finish_mse (g, xl ? c->xlay : c->lay, c->d_part,
@@ -1109,7 +1121,13 @@ mi_passes_on (b200bsp_ctx* c, const BspGeom& g, const float* dcoeff,
     float* grad, double* grad64, int passes)
 {
     const bool roi = g.fmask || g.mroi;
-    if (c->opts.form == B200BSP_FORM_TC && !roi && c->has_xl && c->use_xl_mi
+    // the tile kernel's MI passes are the faster ones where both apply
+    // (PVI-8, 32 bins, 256x256x128 at vpr 5: 332 + 179 us against 532 +
+    // 223 us); the x-lane kernel's when pinned or the tile kernel cannot
+    const bool tile_mi = c->opts.form == B200BSP_FORM_TC && !roi
+        && c->opts.tc_kernel != B200BSP_TC_KERNEL_XLANE
+        && tc_mi_supported (g, c->plan, c->mi.bins);
+    if (c->opts.form == B200BSP_FORM_TC && !roi && c->has_xl && !tile_mi
         && xl_mi_supported (c->mi.bins)) {
         XlPlan plan = c->xplan;
         if (c->tc_grid > 0) {
@@ -1119,8 +1137,7 @@ mi_passes_on (b200bsp_ctx* c, const BspGeom& g, const float* dcoeff,
             c->d_part, c->d_err, c->wait_limit, dcoeff, c->d_moving,
             c->d_res, grad, grad64, c->stream, &c->last_launches, passes);
     }
-    if (c->opts.form == B200BSP_FORM_TC && !roi
-        && tc_mi_supported (g, c->plan, c->mi.bins)) {
+    if (tile_mi) {
         TcPlan plan = c->plan;
         if (c->tc_grid > 0) plan.grid = std::min (c->tc_grid, plan.nbatches);
         return mi_run_tc (&c->mi, g, plan, c->lay, c->d_qlut,
@@ -1574,10 +1591,13 @@ b200bsp_landmarks_score (b200bsp_ctx* c, const float* coeff, float* lmetric,
     return B200BSP_OK;
 }
 
-// bspline_score with MSE and device outputs, stream-ordered: the
-// regulariser runs on the context's second stream while the tile kernel
-// runs on the first, and the finish kernel combines them (lambda times the
-// metric, plus the regulariser's score and double gradient).
+// bspline_score with MSE and device outputs, stream-ordered: the MSE
+// kernel, the regulariser's passes beside it on the context's second
+// stream, then the finish kernel that combines them (lambda times the
+// metric, plus the regulariser's score and double gradient).  The MSE
+// kernel holds every register of the SMs it runs on, so it is launched on
+// all but REG_SIDE_SMS of them and the passes (a few microseconds of work
+// each, but three dependent launches) run on the rest meanwhile.
 static int
 score_mse_device (b200bsp_ctx* c, const float* coeff, float lambda,
     const b200bsp_reg_parms* reg, float* total_score, float* total_grad,
@@ -1589,20 +1609,31 @@ score_mse_device (b200bsp_ctx* c, const float* coeff, float lambda,
     FinishCombine cb;
     cb.lambda = lambda;
     cb.total_score = total_score ? total_score : c->d_total;
+    const int grid0 = c->tc_grid;
     if (reg) {
         CK (cudaEventRecord (c->ev_fork, c->stream));
         CK (cudaStreamWaitEvent (c->aux_stream, c->ev_fork, 0));
-        rc = reg_run (&c->reg, c->geom, reg, dcoeff, nullptr, c->aux_stream,
-            c->d_reg_grad64);
-        if (rc) return fail (c, rc, "regulariser failed: %s",
-            cudaGetErrorString (cudaGetLastError ()));
-        CK (cudaEventRecord (c->ev_join, c->aux_stream));
         cb.reg_grad = c->d_reg_grad64;
         cb.reg_score = c->reg.d_score;
-        c->last_launches += c->reg.plan.n1 ? 4 : 2;
+        if (c->opts.form == B200BSP_FORM_TC && grid0 == 0
+            && c->sm_count > 2 * REG_SIDE_SMS) {
+            c->tc_grid = 2 * (c->sm_count - REG_SIDE_SMS);
+        }
     }
     rc = run_mse (c, dcoeff, total_grad, nullptr, smetric, nullptr,
-        (long long*) num_vox, nullptr, cb, reg ? c->ev_join : nullptr);
+        (long long*) num_vox, nullptr, cb, reg ? c->ev_join : nullptr,
+        [&] () {
+            // between the MSE kernel's launch and the finish kernel's
+            if (!reg) return B200BSP_OK;
+            int r = reg_run (&c->reg, c->geom, reg, dcoeff, nullptr,
+                c->aux_stream, c->d_reg_grad64);
+            if (r) return fail (c, r, "regulariser failed: %s",
+                cudaGetErrorString (cudaGetLastError ()));
+            CK (cudaEventRecord (c->ev_join, c->aux_stream));
+            c->last_launches += c->reg.plan.n1 ? 3 : 1;
+            return B200BSP_OK;
+        });
+    c->tc_grid = grid0;
     if (rc) return rc;
     return end_eval (c, false);
 }
