@@ -389,7 +389,7 @@ def mi_registration_c4(P, its=50):
 
 
 def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
-                  evals=50):
+                  evals=50, which=("mse_reg", "mi")):
     """The same workload with the curvature regulariser added (lambda 0.005)
     and with Mattes MI (PVI-8, 32 bins) instead of MSE: device time per
     evaluation (CUDA events on the context stream, L2 flushed before each),
@@ -420,8 +420,10 @@ def extra_metrics(P, ctx, stream, flush, d_coeff, d_grad, nvox, warmup,
             raise RuntimeError(lib.b200bsp_last_error(ctx._h))
 
     out = {}
-    for name, fn in (("mse_plus_curvature_regularizer", mse_reg),
-                     ("mattes_mi_pvi8_32bins", mi)):
+    for key, name, fn in (("mse_reg", "mse_plus_curvature_regularizer", mse_reg),
+                          ("mi", "mattes_mi_pvi8_32bins", mi)):
+        if key not in which:
+            continue
         ts = []
         for i in range(warmup + evals):
             with torch.cuda.stream(stream):
@@ -629,7 +631,17 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip also_measured (regulariser, MI, the "
                          "registration workloads)")
+    ap.add_argument("--extras", default="all",
+                    help="comma-separated also_measured entries to run: "
+                         "kernels (both tensor-core kernels pinned), "
+                         "mse_reg, mi, batched, mi_pyramid, registration "
+                         "(default all)")
     args = ap.parse_args()
+    extras = ({"kernels", "mse_reg", "mi", "batched", "mi_pyramid",
+               "registration"} if args.extras == "all"
+              else set(args.extras.split(",")))
+    if args.no_extra:
+        extras = set()
     if args.warmup < 3:
         args.warmup = 3
 
@@ -666,21 +678,25 @@ def main():
     mo["ctx"].close()
 
     extra = {}
-    if not args.no_extra:
+    if "kernels" in extras:
         extra["tc_kernels"] = tc_kernel_probe(P, workload, local_rank, flush)
-        extra.update(extra_metrics(P, ctx, stream, flush, m["d_coeff"],
-                              m["d_grad"], grid.num_roi_voxels, args.warmup))
-    if rank == 0 and world == 1 and not args.no_extra:
+    extra.update(extra_metrics(P, ctx, stream, flush, m["d_coeff"],
+                               m["d_grad"], grid.num_roi_voxels, args.warmup,
+                               which=extras))
+    if rank == 0 and world == 1:
         # one-GPU workloads, measured at N = 1 only (the other ranks would
         # idle meanwhile); the device-only ones first: the reference's
         # OpenMP threads (registration_c1's CPU leg) keep host cores busy
         # for a while after they finish, which would slow the host-side
         # line searches
-        extra["batched_16_registrations_40_lbfgs_its"] = batched_c5(P)
-        extra["mi_parzen_registration_512x512x160_pyramid_4_2_1"] = \
-            mi_registration_c4(P)
-        extra["registration_64cubed_vpr8_30_lbfgs_its"] = registration_c1(
-            P, not args.no_cpu_baseline and world == 1)
+        if "batched" in extras:
+            extra["batched_16_registrations_40_lbfgs_its"] = batched_c5(P)
+        if "mi_pyramid" in extras:
+            extra["mi_parzen_registration_512x512x160_pyramid_4_2_1"] = \
+                mi_registration_c4(P)
+        if "registration" in extras:
+            extra["registration_64cubed_vpr8_30_lbfgs_its"] = \
+                registration_c1(P, not args.no_cpu_baseline and world == 1)
 
     nvox = grid.num_roi_voxels
     peak, peak_kind = measured_peaks()
@@ -728,7 +744,7 @@ def main():
                    "kind": kind,
                    "sample": f"{args.cpu_evals} full evaluations of the same "
                              "256x256x128 workload (median)"}
-            if not args.no_extra:
+            if extras and args.extras == "all":
                 extra["cpu_reference_other_paths"] = cpu_reference_others(
                     fixed, moving, grid, coeff, host_threads())
         acc = accuracy_block(workload, m["score"], m["grad"], m["num_vox"],

@@ -389,41 +389,38 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
         l1[0] * l2[1] * l1[2], l2[0] * l2[1] * l1[2], l1[0] * l1[1] * l2[2],
         l2[0] * l1[1] * l2[2], l1[0] * l2[1] * l2[2], l2[0] * l2[1] * l2[2]};
     unsigned int q[8];
-    bool first[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        q[k] = __float2uint_rn (w[k] * TC_MI_WUNIT);
-        first[k] = live;
-    }
-#pragma unroll
-    for (int k = 1; k < 8; k++) {
-#pragma unroll
-        for (int k2 = 0; k2 < k; k2++) {
-            if (first[k] && first[k2] && mb[k2] == mb[k]) {
-                q[k2] += q[k];
-                first[k] = false;
-            }
-        }
-    }
-    // second pair: the first remaining corner after corner 0
-    bool two = false, many = false;
-    int mb2 = 0;
-    unsigned int q2 = 0;
+    for (int k = 0; k < 8; k++) q[k] = __float2uint_rn (w[k] * TC_MI_WUNIT);
+    // the first pair: corner 0's bin with the weights of every corner in
+    // it; the second: the first other bin in corner order, likewise; any
+    // further bins (rare) go corner by corner to the atomics below (integer
+    // sums, so grouping them does not change the histogram)
+    const int mb1 = mb[0];
+    int mb2 = mb1;
+    bool two = false;
 #pragma unroll
     for (int k = 1; k < 8; k++) {
-        many = many || (first[k] && two);
-        mb2 = (first[k] && !two) ? mb[k] : mb2;
-        q2 = (first[k] && !two) ? q[k] : q2;
-        two = two || first[k];
+        mb2 = (!two && mb[k] != mb1) ? mb[k] : mb2;
+        two = two || mb[k] != mb1;
     }
+    unsigned int q1 = q[0], q2 = 0;
+    bool many = false;
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+        q1 += mb[k] == mb1 ? q[k] : 0u;
+        q2 += mb[k] == mb2 && mb[k] != mb1 ? q[k] : 0u;
+        many = many || (mb[k] != mb1 && mb[k] != mb2);
+    }
+    two = two && live;
+    many = many && live;
     const unsigned live_mask = __ballot_sync (0xffffffffu, live);
     if (live) {
         cnt++;
         // first pair (a warp's sum stays below 32 * (2^24 + 8) < 2^32); its
         // leader also counts the group's voxels into the fixed histogram
-        const int key = fb * B + mb[0];
+        const int key = fb * B + mb1;
         const unsigned peers = __match_any_sync (live_mask, key);
-        const unsigned sum = __reduce_add_sync (peers, q[0]);
+        const unsigned sum = __reduce_add_sync (peers, q1);
         if (x.lane == __ffs (peers) - 1) {
             atomicAdd (&hj[key], (unsigned long long) sum);
             atomicAdd (&hf[fb], (unsigned long long) __popc (peers));
@@ -439,13 +436,11 @@ mi_hist_add (const TcArgs& a, const TcCtx& x, bool live, const float w2[3],
         }
     }
     if (many) {
-        bool seen = false;
 #pragma unroll
         for (int k = 1; k < 8; k++) {
-            if (first[k] && seen) {
+            if (mb[k] != mb1 && mb[k] != mb2) {
                 atomicAdd (&hj[fb * B + mb[k]], (unsigned long long) q[k]);
             }
-            seen = seen || first[k];
         }
     }
 }
