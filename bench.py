@@ -617,6 +617,91 @@ def accuracy_block(workload, score, grad, num_vox, threads):
     return out
 
 
+def run_slab(args, rank, world, local_rank):
+    """--mode slab: one 256x256x128 volume sharded by z-slab over the
+    process group (plastimatch_b200.shard.SlabScorer): each rank evaluates
+    its slab through a context on its GPU, then one NCCL all-reduce of the
+    raw sums (FP64) assembles the global score and gradient on every rank.
+    Strong scaling (the volume is fixed); one step = one global evaluation
+    from host coefficients to the host gradient, so value and e2e are the
+    same measurement."""
+    import torch
+    import plastimatch_b200 as P
+    from plastimatch_b200 import shard
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    fixed, moving, grid, coeff = make_workload()
+    dev = torch.device("cuda", local_rank)
+    mg = P.volume_grad(moving)
+    evaluate = shard.context_evaluator(fixed, moving, form=args.form,
+                                       device=local_rank, moving_grad=mg)
+    if world > 1:
+        scorer = shard.SlabScorer(grid, evaluate, device=dev)
+        step = lambda: scorer.score_mse(coeff)
+    else:
+        # one rank: the whole grid is the one slab, no collective
+        def step():
+            s, g, nv = evaluate(grid, coeff)
+            return (float(np.float32(s / nv)),
+                    (2.0 * g / nv).astype(np.float32), nv)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    ev = [(torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.fill_(1)
+            ev[i][0].record(stream)
+            res = step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    nvox = grid.num_roi_voxels
+    value = nvox / (ms * 1e-3) / 1e9
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "Gvox/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, form=args.form, mode="slab",
+                           l2="256 MiB flush write before every timed step",
+                           parallelism=f"z-slabs x{world}, NCCL all-reduce "
+                                       "of the raw sums (FP64)"),
+            "e2e": {"value": value, "unit": "Gvox/s",
+                    "h2d_bytes_per_step": 4 * grid.num_coeff,
+                    "d2h_bytes_per_step": 8 * grid.num_coeff},
+            # per step and rank: the slab's MSE kernel and finish kernel
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk.summary(),
+            "score": res[0], "num_vox": res[2],
+        }
+        print(json.dumps(out), flush=True)
+    for c in evaluate.contexts.values():
+        c.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -626,6 +711,10 @@ def main():
     ap.add_argument("--tc-kernel", default="auto",
                     choices=["auto", "xlane", "tile"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "slab"],
+                    help="replicas: one evaluation stream per GPU (the "
+                         "headline); slab: one volume sharded by z-slab "
+                         "with an NCCL all-reduce")
     ap.add_argument("--cpu-evals", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
@@ -651,6 +740,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.mode == "slab":
+        run_slab(args, rank, world, local_rank)
         return
 
     import torch
