@@ -25,6 +25,9 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+# per-source flags: the optimiser's device controller rounds as its host
+# counterpart does (no multiply-add contraction)
+FILE_FLAGS = {"lbfgs_graph.cu": ["-fmad=false"]}
 
 
 def nvcc_path() -> str:
@@ -59,6 +62,7 @@ def build(verbose: bool = False, force: bool = False, extra_flags=()) -> str:
         objs.append(obj)
         if force or not _newer(obj, [src] + headers):
             cmd = ([nvcc, "-ccbin", host_cxx()] + ARCH + NVCC_FLAGS
+                   + FILE_FLAGS.get(os.path.basename(src), [])
                    + list(extra_flags) + ["-I", CSRC, "-I",
                                           os.path.join(ROOT, "include"),
                                           "-c", src, "-o", obj])

@@ -11,13 +11,12 @@
 // persistent kernel over the union of the work.  Graphs are captured once
 // per set of participating contexts and replayed.
 //
-// The batched L-BFGS runs one host thread per registration with the
-// device-side L-BFGS of optimize.cu; their function evaluations meet at a
-// barrier, and the last thread to arrive launches the batch evaluation of
-// everyone waiting (registrations that have finished drop out of the set).
-// Each registration's trial sequence is that of b200bsp_optimize_lbfgs.
+// The batched L-BFGS runs every registration's graph-resident optimiser
+// (b200bsp_optimize_lbfgs, optimize.cu) at once, each on its context's
+// stream: the kernels of all registrations share the GPU through the same
+// CTA split, and no trial point waits for the host.  Each registration's
+// trial sequence is that of b200bsp_optimize_lbfgs.
 #include <algorithm>
-#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -35,9 +34,6 @@ long long ctx_work (const b200bsp_ctx* c, bool* persistent);
 void ctx_set_tc_grid (b200bsp_ctx* c, int ctas);
 int* ctx_err_flag (b200bsp_ctx* c);
 int ctx_report_device_error (b200bsp_ctx* c, int e);
-int lbfgs_optimize_batched (b200bsp_ctx* ctx, float lambda,
-    const b200bsp_lbfgs_parms* parms, float* coeff, b200bsp_lbfgs_result* res,
-    void* member, int (*eval) (void*, int, const float*, float*, float*)); // optimize.cu
 
 // Largest error flag over the participating contexts.
 __global__ void
@@ -71,17 +67,9 @@ struct b200bsp_batch {
     std::vector<Graph> graphs;
     std::string err;
 
-    // batched L-BFGS state
-    std::mutex mu;
-    std::condition_variable cv;
-    int active = 0, waiting = 0;
-    long long generation = 0;
-    std::vector<char> want;
-    std::vector<const float*> lb_coeff;
-    std::vector<float*> lb_grad;
+    std::mutex mu;                      // one batch evaluation at a time
     float* d_scores = nullptr;
     float* h_scores = nullptr;
-    int lb_status = 0;
 };
 
 static int
@@ -193,9 +181,6 @@ b200bsp_batch_create (b200bsp_ctx* const* ctxs, int n, b200bsp_batch** out)
     b->ctx.assign (ctxs, ctxs + n);
     b->device = dev;
     b->join.assign (n, nullptr);
-    b->want.assign (n, 0);
-    b->lb_coeff.assign (n, nullptr);
-    b->lb_grad.assign (n, nullptr);
     int rc = B200BSP_OK;
     if (cudaSetDevice (dev) != cudaSuccess
         || cudaStreamCreateWithFlags (&b->st, cudaStreamNonBlocking) != cudaSuccess
@@ -299,71 +284,11 @@ b200bsp_batch_score_mse (b200bsp_batch* b, const float* const* coeffs,
 }
 
 // ---- batched L-BFGS ---------------------------------------------------------
-
-// Called by a registration's thread with its trial coefficients (device,
-// float) ready: waits until the batch evaluation that includes it is done;
-// the score comes back in *score and the gradient in its device buffer.
-static int
-batch_member_eval (void* user, int i, const float* coeff, float* grad,
-    float* score)
-{
-    auto* b = (b200bsp_batch*) user;
-    std::unique_lock<std::mutex> lk (b->mu);
-    b->want[i] = 1;
-    b->lb_coeff[i] = coeff;
-    b->lb_grad[i] = grad;
-    b->waiting++;
-    const long long gen = b->generation;
-    if (b->waiting == b->active) {
-        std::vector<int> sel;
-        std::vector<const float*> cs (b->ctx.size (), nullptr);
-        std::vector<float*> gs (b->ctx.size (), nullptr);
-        for (int k = 0; k < (int) b->ctx.size (); k++) {
-            if (b->want[k]) {
-                sel.push_back (k);
-                cs[k] = b->lb_coeff[k];
-                gs[k] = b->lb_grad[k];
-            }
-        }
-        b->lb_status = launch_eval (b, sel, cs.data (), gs.data (),
-            b->d_scores, nullptr);
-        std::fill (b->want.begin (), b->want.end (), 0);
-        b->waiting = 0;
-        b->generation++;
-        b->cv.notify_all ();
-    } else {
-        b->cv.wait (lk, [&] { return b->generation != gen; });
-    }
-    *score = b->h_scores[i];
-    return b->lb_status;
-}
-
-// A registration's thread is done: the others no longer wait for it.
-static void
-batch_member_leave (b200bsp_batch* b)
-{
-    std::unique_lock<std::mutex> lk (b->mu);
-    b->active--;
-    if (b->active > 0 && b->waiting == b->active) {
-        // everyone left is waiting: evaluate them
-        std::vector<int> sel;
-        std::vector<const float*> cs (b->ctx.size (), nullptr);
-        std::vector<float*> gs (b->ctx.size (), nullptr);
-        for (int k = 0; k < (int) b->ctx.size (); k++) {
-            if (b->want[k]) {
-                sel.push_back (k);
-                cs[k] = b->lb_coeff[k];
-                gs[k] = b->lb_grad[k];
-            }
-        }
-        b->lb_status = launch_eval (b, sel, cs.data (), gs.data (),
-            b->d_scores, nullptr);
-        std::fill (b->want.begin (), b->want.end (), 0);
-        b->waiting = 0;
-        b->generation++;
-        b->cv.notify_all ();
-    }
-}
+//
+// Every registration runs the graph-resident optimiser on its own context
+// and stream, all at once from one host thread each: no trial waits for
+// the host, and the persistent kernels of different registrations share
+// the SMs through the CTA split set at batch creation.
 
 extern "C" int
 b200bsp_batch_optimize_lbfgs (b200bsp_batch* b, float lambda,
@@ -375,29 +300,14 @@ b200bsp_batch_optimize_lbfgs (b200bsp_batch* b, float lambda,
     for (int i = 0; i < n; i++) {
         if (!coeffs[i]) return bfail (b, B200BSP_E_BADARG, "null coefficients");
     }
-    {
-        std::lock_guard<std::mutex> lk (b->mu);
-        b->active = n;
-        b->waiting = 0;
-        std::fill (b->want.begin (), b->want.end (), 0);
-    }
     std::vector<int> rcs (n, B200BSP_OK);
     std::vector<std::thread> th;
     th.reserve (n);
     for (int i = 0; i < n; i++) {
         th.emplace_back ([&, i] {
             cudaSetDevice (b->device);
-            struct Member {
-                b200bsp_batch* b;
-                int i;
-            } m{b, i};
-            rcs[i] = lbfgs_optimize_batched (b->ctx[i], lambda, parms,
-                coeffs[i], &results[i], &m,
-                [] (void* u, int, const float* c, float* g, float* s) {
-                    auto* mm = (Member*) u;
-                    return batch_member_eval (mm->b, mm->i, c, g, s);
-                });
-            batch_member_leave (b);
+            rcs[i] = b200bsp_optimize_lbfgs (b->ctx[i], 0, lambda, nullptr,
+                parms, coeffs[i], &results[i]);
         });
     }
     for (auto& t : th) t.join ();

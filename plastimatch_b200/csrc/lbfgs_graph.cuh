@@ -1,0 +1,23 @@
+// The graph-resident L-BFGS controller kernels (lbfgs_graph.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/plastimatch_b200.h"
+#include "lbfgs_logic.cuh"
+
+namespace b200 {
+
+// Start of a line search (after the correction pair, the two-loop
+// recursion and dginit = gp.d): the search's state and its first trial
+// step; ends the run (h_while) when the step or the direction is unusable.
+__global__ void lb_begin_search_kernel (LbDev* s,
+    cudaGraphConditionalHandle h_while);
+
+// After an evaluation and its dot products: the progress rule, the line
+// search's tests, and either the next trial step, a new line search
+// (h_new) or the end of the run (h_while).
+__global__ void lb_after_eval_kernel (LbDev* s,
+    cudaGraphConditionalHandle h_while, cudaGraphConditionalHandle h_new);
+
+}  // namespace b200

@@ -21,10 +21,13 @@
 // line-search logic runs.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "../../include/plastimatch_b200.h"
 #include "kernels.cuh"
+#include "lbfgs_graph.cuh"
+#include "lbfgs_logic.cuh"
 
 namespace b200 {
 
@@ -33,12 +36,14 @@ cudaStream_t ctx_stream (const b200bsp_ctx* c); // runtime.cu
 void* ctx_opt_ws (const b200bsp_ctx* c);
 int ctx_landmarks (const b200bsp_ctx* c, float* stiffness);
 void ctx_set_opt_ws (b200bsp_ctx* c, void* ws, void (*release) (void*));
+unsigned ctx_generation (const b200bsp_ctx* c);                // runtime.cu
 
 constexpr int OPT_THREADS = 256;
 constexpr int OPT_BLOCKS = 296;
 
-__global__ void __launch_bounds__ (OPT_THREADS)
-dot_partial_kernel (const double* __restrict__ a, const double* __restrict__ b,
+// one block's partial sum of a . b (blocks stride the vector)
+__device__ __forceinline__ void
+dot_partial_body (const double* __restrict__ a, const double* __restrict__ b,
     long long n, double* __restrict__ part)
 {
     __shared__ double sh[OPT_THREADS];
@@ -54,6 +59,13 @@ dot_partial_kernel (const double* __restrict__ a, const double* __restrict__ b,
         __syncthreads ();
     }
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void __launch_bounds__ (OPT_THREADS)
+dot_partial_kernel (const double* __restrict__ a, const double* __restrict__ b,
+    long long n, double* __restrict__ part)
+{
+    dot_partial_body (a, b, n, part);
 }
 
 __global__ void
@@ -284,124 +296,19 @@ struct Objective {
     int fevals = 0;
 };
 
-// Moré-Thuente trial-interval update (the cstep of MINPACK): x = best
-// step so far (fx, dx), y = other end of the interval (fy, dy), t = trial
-// step (ft, dt).  Returns 0, or an error code when the inputs are
-// inconsistent (rounding errors).
 static int
 update_interval (double* x, double* fx, double* dx, double* y, double* fy,
     double* dy, double* t, double ft, double dt, double tmin, double tmax,
     int* brackt)
 {
-    if (*brackt) {
-        if (*t <= std::min (*x, *y) || std::max (*x, *y) <= *t) return 1;
-        if (0.0 <= *dx * (*t - *x)) return 2;
-        if (tmax < tmin) return 3;
-    }
-    // the derivatives differ in sign (dt * sign(dx) < 0)
-    const bool dsign = dt * (*dx / std::fabs (*dx)) < 0.0;
-    bool bound;
-    double newt;
-    // Minimiser of the cubic interpolating (u, fu, du) and (v, fv, dv),
-    // written from u's side: returns r with minimiser u + r (v - u), and
-    // gamma (zero when the cubic has no minimiser there and clamp_zero).
-    auto cubic = [](double u, double fu, double du, double v, double fv,
-                     double dv, bool clamp_zero, double* gamma_out) {
-        const double theta = 3.0 * (fu - fv) / (v - u) + du + dv;
-        const double s = std::max (std::fabs (theta),
-            std::max (std::fabs (du), std::fabs (dv)));
-        const double a = theta / s;
-        double gamma2 = a * a - (du / s) * (dv / s);
-        if (clamp_zero && gamma2 < 0) gamma2 = 0;
-        double gamma = s * std::sqrt (gamma2);
-        if (v < u) gamma = -gamma;
-        const double p = (gamma - du) + theta;
-        const double q = ((gamma - du) + gamma) + dv;
-        if (gamma_out) *gamma_out = gamma;
-        return p / q;
-    };
-    if (*fx < ft) {
-        // case 1: higher function value; the minimum is bracketed
-        *brackt = 1;
-        bound = true;
-        const double mc = *x + cubic (*x, *fx, *dx, *t, ft, dt, false,
-            nullptr) * (*t - *x);
-        const double mq = *x + (*dx / ((*fx - ft) / (*t - *x) + *dx)) / 2.0
-            * (*t - *x);
-        if (std::fabs (mc - *x) < std::fabs (mq - *x)) newt = mc;
-        else newt = mc + 0.5 * (mq - mc);
-    } else if (dsign) {
-        // case 2: lower value, derivatives of opposite sign; bracketed
-        *brackt = 1;
-        bound = false;
-        const double mc = *t + cubic (*t, ft, dt, *x, *fx, *dx, false,
-            nullptr) * (*x - *t);
-        const double mq = *t + (dt / (dt - *dx)) * (*x - *t);
-        if (std::fabs (mc - *t) > std::fabs (mq - *t)) newt = mc;
-        else newt = mq;
-    } else if (std::fabs (dt) < std::fabs (*dx)) {
-        // case 3: lower value, same sign, smaller derivative magnitude
-        bound = true;
-        double gamma;
-        const double r = cubic (*t, ft, dt, *x, *fx, *dx, true, &gamma);
-        double mc;
-        // the cubic may have no minimiser beyond t
-        if (r < 0.0 && gamma != 0.0) mc = *t + r * (*x - *t);
-        else if (*x < *t) mc = tmax;
-        else mc = tmin;
-        const double mq = *t + (dt / (dt - *dx)) * (*x - *t);
-        if (*brackt) {
-            newt = std::fabs (*t - mc) < std::fabs (*t - mq) ? mc : mq;
-        } else {
-            newt = std::fabs (*t - mc) > std::fabs (*t - mq) ? mc : mq;
-        }
-    } else {
-        // case 4: lower value, same sign, derivative does not decrease
-        bound = false;
-        if (*brackt) {
-            newt = *t + cubic (*t, ft, dt, *y, *fy, *dy, false, nullptr)
-                * (*y - *t);
-        } else if (*x < *t) {
-            newt = tmax;
-        } else {
-            newt = tmin;
-        }
-    }
-    // update the interval
-    if (*fx < ft) {
-        *y = *t; *fy = ft; *dy = dt;
-    } else {
-        if (dsign) {
-            *y = *x; *fy = *fx; *dy = *dx;
-        }
-        *x = *t; *fx = ft; *dx = dt;
-    }
-    newt = std::min (tmax, newt);
-    newt = std::max (tmin, newt);
-    if (*brackt && bound) {
-        const double mq = *x + 0.66 * (*y - *x);
-        if (*x < *y) newt = std::min (mq, newt);
-        else newt = std::max (mq, newt);
-    }
-    *t = newt;
-    return 0;
+    return lb_update_interval (x, fx, dx, y, fy, dy, t, ft, dt, tmin, tmax,
+        brackt);
 }
 
-enum {
-    LS_ROUNDING = -1001, LS_MAXSTEP = -1002, LS_MINSTEP = -1003,
-    LS_WIDTH = -1004, LS_MAXLS = -1005, LS_INCREASE = -1006, LS_BADSTEP = -1007,
-    LS_STOPPED = -1100      // the progress rule stopped the run mid-search
-};
-
-// Plastimatch's progress rule (src/register/bspline_optimize_liblbfgs.cxx:
-// 53-79): stop once the iteration number exceeds max_its or the function
-// evaluations exceed max_feval.  The liblbfgs it links consults the rule
-// after every evaluation inside a line search (with the current iteration
-// number) and once more after each completed line search.
 static bool
 stop_rule (const b200bsp_lbfgs_parms& p, int k, int fevals)
 {
-    return k > p.max_its || fevals > p.max_feval;
+    return lb_stop_rule (p.max_its, p.max_feval, k, fevals);
 }
 
 // Moré-Thuente line search from xp along d; on return x, f, g are the last
@@ -481,15 +388,17 @@ line_search (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
     }
 }
 
+// The start of a run: the objective at x0, the gradient test, d = -g and
+// the first step 1/|d|.  Returns a status; *more is false when the run is
+// already over (res holds its outcome).
 static int
-lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
-    b200bsp_lbfgs_result* res)
+lbfgs_prologue (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
+    b200bsp_lbfgs_result* res, double* f, double* step, bool* more)
 {
-    const int m = p.m;
-    double f = 0.0;
-    int rc = obj.eval (w.x, w.g, &f);
+    *more = false;
+    int rc = obj.eval (w.x, w.g, f);
     if (rc) return rc;
-    res->score = f;
+    res->score = *f;
     res->iterations = 0;
     double xnorm, gnorm;
     w.norms2 (w.x, w.g, &xnorm, &gnorm);
@@ -502,7 +411,19 @@ lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
         return B200BSP_OK;
     }
     w.axpby (-1.0, w.g, 0.0, w.d);                // d = -g
-    double step = 1.0 / std::sqrt (w.dot (w.d, w.d));
+    *step = 1.0 / std::sqrt (w.dot (w.d, w.d));
+    if (w.err) return w.err;
+    *more = true;
+    return B200BSP_OK;
+}
+
+// The iterations after the prologue, driven from the host.
+static int
+lbfgs_loop (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
+    b200bsp_lbfgs_result* res, double f, double step)
+{
+    const int m = p.m;
+    double xnorm, gnorm;
     int k = 1, end = 0;
     while (true) {
         w.copy (w.xp, w.x);
@@ -570,6 +491,17 @@ lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
     }
 }
 
+static int
+lbfgs_run (Lbfgs& w, Objective& obj, const b200bsp_lbfgs_parms& p,
+    b200bsp_lbfgs_result* res)
+{
+    double f = 0.0, step = 0.0;
+    bool more = false;
+    int rc = lbfgs_prologue (w, obj, p, res, &f, &step, &more);
+    if (rc || !more) return rc;
+    return lbfgs_loop (w, obj, p, res, f, step);
+}
+
 // ---- objectives -----------------------------------------------------------
 
 // bspline_score() on the context: lambda * metric (+ regulariser, +
@@ -584,10 +516,6 @@ struct ContextObjective : Objective {
     float* grad_f;
     long long n;
     cudaStream_t st;
-    // batched evaluation (a registration of a batch): the score and the
-    // gradient come from the batch's graph launch instead
-    void* member = nullptr;
-    int (*batch_eval) (void*, int, const float*, float*, float*) = nullptr;
     int eval (const double* x, double* g, double* f) override
     {
         const unsigned grid = (unsigned) std::min<long long> ((n + 255) / 256,
@@ -596,15 +524,10 @@ struct ContextObjective : Objective {
         float s = 0.f;
         int64_t nv = 0;
         int rc;
-        if (batch_eval) {
-            rc = cudaStreamSynchronize (st) == cudaSuccess
-                ? batch_eval (member, 0, coeff_f, grad_f, &s) : B200BSP_E_CUDA;
-        } else {
-            rc = metric == 0
-                ? b200bsp_score_mse (ctx, coeff_f, &s, grad_f, &nv)
-                : b200bsp_score_mi (ctx, coeff_f, &s, grad_f, &nv, nullptr,
-                    nullptr, nullptr);
-        }
+        rc = metric == 0
+            ? b200bsp_score_mse (ctx, coeff_f, &s, grad_f, &nv)
+            : b200bsp_score_mi (ctx, coeff_f, &s, grad_f, &nv, nullptr,
+                nullptr, nullptr);
         if (rc) return rc;
         // Bspline_score::accumulate: total = lambda * smetric, total_grad =
         // lambda * smetric_grad (src/register/bspline_score.cxx:63-74)
@@ -634,6 +557,377 @@ struct ContextObjective : Objective {
     }
     float last = 0.f;     // score of the last evaluation
 };
+
+// ---- the graph-resident run --------------------------------------------------
+//
+// For MSE on a context (with or without the regulariser, no landmarks) the
+// iterations after the prologue run as one CUDA graph: a while node over
+// trial points whose body is [new line search?] -> x = xp + stp d ->
+// evaluation (the context's MSE kernel and finish kernel, the regulariser
+// beside them) -> g.d, x.x, g.g -> the controller (lbfgs_graph.cu).  The
+// "new line search" branch (an if node) forms the correction pair, runs the
+// two-loop recursion with its indices read on the device, copies xp, gp and
+// takes dginit.  Only the outcome comes back to the host.
+
+namespace {
+
+__device__ __forceinline__ bool
+lb_skip (const LbDev* s, int i)
+{
+    return s->first || i >= s->bound;
+}
+
+// the i-th pair of the first loop (newest first) and of the second
+__device__ __forceinline__ int
+lb_j1 (const LbDev* s, int i)
+{
+    return (s->end - 1 - i + 2 * s->m) % s->m;
+}
+
+__device__ __forceinline__ int
+lb_j2 (const LbDev* s, int i)
+{
+    return (s->end - s->bound + i + 2 * s->m) % s->m;
+}
+
+// s[newest] = x - xp, y[newest] = g - gp
+__global__ void
+lb_pair_kernel (const LbDev* __restrict__ st, double* __restrict__ S,
+    double* __restrict__ Y, const double* __restrict__ x,
+    const double* __restrict__ xp, const double* __restrict__ g,
+    const double* __restrict__ gp, long long n)
+{
+    if (st->first) return;
+    double* sj = S + (size_t) st->newest * n;
+    double* yj = Y + (size_t) st->newest * n;
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        sj[i] = x[i] - xp[i];
+        yj[i] = g[i] - gp[i];
+    }
+}
+
+enum { LB_YS, LB_YY, LB_ALPHA, LB_BETA };
+
+// a block's partial dot product of the recursion: ys = y.s and yy = y.y of
+// the newest pair, s_j.d of the first loop, y_j.d of the second
+__global__ void __launch_bounds__ (OPT_THREADS)
+lb_dot_partial_kernel (const LbDev* __restrict__ st, int op, int i,
+    const double* __restrict__ S, const double* __restrict__ Y,
+    const double* __restrict__ d, long long n, double* __restrict__ part)
+{
+    const double *a, *b;
+    if (op == LB_YS || op == LB_YY) {
+        if (st->first) return;
+        a = Y + (size_t) st->newest * n;
+        b = op == LB_YS ? S + (size_t) st->newest * n : a;
+    } else {
+        if (lb_skip (st, i)) return;
+        a = op == LB_ALPHA ? S + (size_t) lb_j1 (st, i) * n
+                           : Y + (size_t) lb_j2 (st, i) * n;
+        b = d;
+    }
+    dot_partial_body (a, b, n, part);
+}
+
+// the partial sums in block order (dot_final_div_kernel's), into the
+// recursion's scalars: ys[newest], yy, alpha[j] = s_j.d / ys[j],
+// beta = y_j.d / ys[j]
+__global__ void
+lb_dot_final_kernel (const LbDev* __restrict__ st, int op, int i,
+    const double* __restrict__ part, int nparts, double* __restrict__ dsc)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int m = st->m;
+    if (op == LB_YS || op == LB_YY) {
+        if (st->first) return;
+    } else if (lb_skip (st, i)) {
+        return;
+    }
+    double s = 0.0;
+    for (int k = 0; k < nparts; k++) s += part[k];
+    if (op == LB_YS) {
+        dsc[st->newest] = s;
+    } else if (op == LB_YY) {
+        dsc[2 * m + 1] = s;
+    } else if (op == LB_ALPHA) {
+        const int j = lb_j1 (st, i);
+        dsc[m + j] = s / dsc[j];
+    } else {
+        dsc[2 * m] = s / dsc[lb_j2 (st, i)];
+    }
+}
+
+// d = -alpha[j] y_j + d (first loop)
+__global__ void
+lb_axpy1_kernel (const LbDev* __restrict__ st, int i,
+    const double* __restrict__ Y, const double* __restrict__ dsc,
+    double* __restrict__ d, long long n)
+{
+    if (lb_skip (st, i)) return;
+    const int j = lb_j1 (st, i);
+    const double av = -1.0 * dsc[st->m + j];
+    const double* yj = Y + (size_t) j * n;
+    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long) gridDim.x * blockDim.x) {
+        d[k] = av * yj[k] + 1.0 * d[k];
+    }
+}
+
+// d = (ys / yy) d
+__global__ void
+lb_scale_kernel (const LbDev* __restrict__ st, const double* __restrict__ dsc,
+    double* __restrict__ d, long long n)
+{
+    if (st->first) return;
+    const double bv = dsc[st->newest] / dsc[2 * st->m + 1];
+    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long) gridDim.x * blockDim.x) {
+        d[k] = 0.0 * d[k] + bv * d[k];
+    }
+}
+
+// d = (alpha[j] - beta) s_j + d (second loop)
+__global__ void
+lb_axpy2_kernel (const LbDev* __restrict__ st, int i,
+    const double* __restrict__ S, const double* __restrict__ dsc,
+    double* __restrict__ d, long long n)
+{
+    if (lb_skip (st, i)) return;
+    const int j = lb_j2 (st, i);
+    const double av = dsc[st->m + j] - dsc[2 * st->m];
+    const double* sj = S + (size_t) j * n;
+    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long) gridDim.x * blockDim.x) {
+        d[k] = av * sj[k] + 1.0 * d[k];
+    }
+}
+
+// The whole new-line-search branch in one block, for vectors of at most
+// LB_FUSED_MAX entries: correction pair, the two-loop recursion, xp = x,
+// gp = g and dginit = gp.d, each dot product a block reduction in a fixed
+// order (one launch instead of some fifty for small registrations).
+constexpr long long LB_FUSED_MAX = 1 << 17;
+constexpr int LB_FUSED_THREADS = 1024;
+
+__device__ double
+lb_block_dot (const double* __restrict__ a, const double* __restrict__ b,
+    long long n, double* red)
+{
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < n; i += LB_FUSED_THREADS) s += a[i] * b[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync (0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads ();
+    if (threadIdx.x < 32) {
+        double v = red[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync (0xffffffffu, v, o);
+        if (threadIdx.x == 0) red[32] = v;
+    }
+    __syncthreads ();
+    const double r = red[32];
+    __syncthreads ();
+    return r;
+}
+
+__global__ void __launch_bounds__ (LB_FUSED_THREADS)
+lb_branch_fused_kernel (const LbDev* __restrict__ st, double* __restrict__ S,
+    double* __restrict__ Y, const double* __restrict__ x,
+    double* __restrict__ xp, const double* __restrict__ g,
+    double* __restrict__ gp, double* __restrict__ d,
+    double* __restrict__ dsc, double* __restrict__ dginit, long long n)
+{
+    __shared__ double red[33];
+    const int m = st->m;
+    const bool first = st->first;
+    const int t = threadIdx.x;
+    if (!first) {
+        double* sn = S + (size_t) st->newest * n;
+        double* yn = Y + (size_t) st->newest * n;
+        for (long long i = t; i < n; i += LB_FUSED_THREADS) {
+            sn[i] = x[i] - xp[i];
+            yn[i] = g[i] - gp[i];
+        }
+        __syncthreads ();
+        const double ys = lb_block_dot (yn, sn, n, red);
+        const double yy = lb_block_dot (yn, yn, n, red);
+        if (t == 0) {
+            dsc[st->newest] = ys;
+            dsc[2 * m + 1] = yy;
+        }
+    }
+    for (long long i = t; i < n; i += LB_FUSED_THREADS) d[i] = -1.0 * g[i] + 0.0 * d[i];
+    __syncthreads ();
+    if (!first) {
+        const int bound = st->bound;
+        int j = st->end;
+        for (int k = 0; k < bound; k++) {
+            j = (j + m - 1) % m;
+            const double* sj = S + (size_t) j * n;
+            const double* yj = Y + (size_t) j * n;
+            const double alpha = lb_block_dot (sj, d, n, red) / dsc[j];
+            if (t == 0) dsc[m + j] = alpha;
+            for (long long i = t; i < n; i += LB_FUSED_THREADS) {
+                d[i] = (-1.0 * alpha) * yj[i] + 1.0 * d[i];
+            }
+            __syncthreads ();
+        }
+        const double bv = dsc[st->newest] / dsc[2 * m + 1];
+        for (long long i = t; i < n; i += LB_FUSED_THREADS) d[i] = 0.0 * d[i] + bv * d[i];
+        __syncthreads ();
+        for (int k = 0; k < bound; k++) {
+            const double* sj = S + (size_t) j * n;
+            const double* yj = Y + (size_t) j * n;
+            const double beta = lb_block_dot (yj, d, n, red) / dsc[j];
+            const double av = dsc[m + j] - beta;
+            for (long long i = t; i < n; i += LB_FUSED_THREADS) {
+                d[i] = av * sj[i] + 1.0 * d[i];
+            }
+            __syncthreads ();
+            j = (j + 1) % m;
+        }
+    }
+    for (long long i = t; i < n; i += LB_FUSED_THREADS) {
+        xp[i] = x[i];
+        gp[i] = g[i];
+    }
+    __syncthreads ();
+    const double dg0 = lb_block_dot (gp, d, n, red);
+    if (t == 0) *dginit = dg0;
+}
+
+// x = xp + stp d (the trial point; x stays when the run is over)
+__global__ void
+lb_trial_kernel (const LbDev* __restrict__ st, const double* __restrict__ xp,
+    const double* __restrict__ d, double* __restrict__ x, long long n)
+{
+    if (st->done) return;
+    const double a = st->stp;
+    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long) gridDim.x * blockDim.x) {
+        x[k] = xp[k] + a * d[k];
+    }
+}
+
+}  // namespace
+
+// Record the graph of the run's iterations on the context's stream (which
+// must be idle); false when a step of the construction is refused.
+static bool
+build_lbfgs_graph (b200bsp_ctx* ctx, Lbfgs& w, LbDev* dst, float lambda,
+    const b200bsp_reg_parms* reg, float* coeff_f, float* grad_f,
+    cudaGraphExec_t* exec)
+{
+    cudaStream_t st = w.st;
+    const long long n = w.n;
+    const unsigned grid = w.grid ();
+    cudaGraph_t graph = nullptr, out = nullptr;
+    bool ok = cudaGraphCreate (&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h_while = 0, h_new = 0;
+    ok = ok && cudaGraphConditionalHandleCreate (&h_while, graph, 1,
+        cudaGraphCondAssignDefault) == cudaSuccess;
+    ok = ok && cudaGraphConditionalHandleCreate (&h_new, graph, 1,
+        cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t wnode = nullptr, inode = nullptr;
+    cudaGraph_t body = nullptr, branch = nullptr;
+    if (ok) {
+        cudaGraphNodeParams wp = {};
+        wp.type = cudaGraphNodeTypeConditional;
+        wp.conditional.handle = h_while;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        ok = cudaGraphAddNode (&wnode, graph, nullptr, 0, &wp) == cudaSuccess;
+        body = wp.conditional.phGraph_out[0];
+    }
+    if (ok) {
+        cudaGraphNodeParams ip = {};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = h_new;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        ok = cudaGraphAddNode (&inode, body, nullptr, 0, &ip) == cudaSuccess;
+        branch = ip.conditional.phGraph_out[0];
+    }
+    const int m = w.m;
+    double* ys_d = w.dsc;
+    // the new-line-search branch
+    if (ok && n <= LB_FUSED_MAX && cudaStreamBeginCaptureToGraph (st, branch,
+            nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        lb_branch_fused_kernel<<<1, LB_FUSED_THREADS, 0, st>>> (dst, w.s, w.y,
+            w.x, w.xp, w.g, w.gp, w.d, ys_d, &dst->dginit, n);
+        lb_begin_search_kernel<<<1, 32, 0, st>>> (dst, h_while);
+        ok = cudaStreamEndCapture (st, &out) == cudaSuccess && out == branch;
+    } else if (ok && cudaStreamBeginCaptureToGraph (st, branch, nullptr,
+            nullptr, 0, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        lb_pair_kernel<<<grid, 256, 0, st>>> (dst, w.s, w.y, w.x, w.xp, w.g,
+            w.gp, n);
+        lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, LB_YS,
+            0, w.s, w.y, w.d, n, w.part);
+        lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_YS, 0, w.part,
+            OPT_BLOCKS, ys_d);
+        lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, LB_YY,
+            0, w.s, w.y, w.d, n, w.part);
+        lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_YY, 0, w.part,
+            OPT_BLOCKS, ys_d);
+        axpby_kernel<<<grid, 256, 0, st>>> (-1.0, w.g, 0.0, w.d, n);
+        for (int i = 0; i < m; i++) {
+            lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst,
+                LB_ALPHA, i, w.s, w.y, w.d, n, w.part);
+            lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_ALPHA, i, w.part,
+                OPT_BLOCKS, ys_d);
+            lb_axpy1_kernel<<<grid, 256, 0, st>>> (dst, i, w.y, ys_d, w.d, n);
+        }
+        lb_scale_kernel<<<grid, 256, 0, st>>> (dst, ys_d, w.d, n);
+        for (int i = 0; i < m; i++) {
+            lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst,
+                LB_BETA, i, w.s, w.y, w.d, n, w.part);
+            lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_BETA, i, w.part,
+                OPT_BLOCKS, ys_d);
+            lb_axpy2_kernel<<<grid, 256, 0, st>>> (dst, i, w.s, ys_d, w.d, n);
+        }
+        cudaMemcpyAsync (w.xp, w.x, n * sizeof (double),
+            cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync (w.gp, w.g, n * sizeof (double),
+            cudaMemcpyDeviceToDevice, st);
+        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.gp, w.d, n,
+            w.part);
+        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->dginit);
+        lb_begin_search_kernel<<<1, 32, 0, st>>> (dst, h_while);
+        ok = cudaStreamEndCapture (st, &out) == cudaSuccess && out == branch;
+    } else {
+        ok = false;
+    }
+    // the trial: after the branch, every iteration of the loop
+    if (ok && cudaStreamBeginCaptureToGraph (st, body, &inode, nullptr, 1,
+            cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        lb_trial_kernel<<<grid, 256, 0, st>>> (dst, w.xp, w.d, w.x, n);
+        to_float_kernel<<<grid, 256, 0, st>>> (w.x, coeff_f, n);
+        // bspline_score with device outputs: lambda * MSE (+ regulariser)
+        const int rc = b200bsp_score (ctx, coeff_f, 0, lambda, reg,
+            &dst->total, grad_f, nullptr, nullptr);
+        to_double_kernel<<<grid, 256, 0, st>>> (grad_f, w.g, n);
+        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.g, w.d, n,
+            w.part);
+        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->dg);
+        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.x, w.x, n,
+            w.part);
+        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->xx);
+        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.g, w.g, n,
+            w.part);
+        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->gg);
+        lb_after_eval_kernel<<<1, 32, 0, st>>> (dst, h_while, h_new);
+        ok = cudaStreamEndCapture (st, &out) == cudaSuccess && out == body
+            && rc == B200BSP_OK;
+    } else {
+        ok = false;
+    }
+    ok = ok && cudaGraphInstantiate (exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy (graph);
+    if (!ok) cudaGetLastError ();
+    return ok;
+}
 
 // A caller's function on host copies of x and g.
 struct HostObjective : Objective {
@@ -703,7 +997,19 @@ f2d_kernel (const float* __restrict__ a, double* __restrict__ out, long long n)
 struct OptWorkspace {
     Lbfgs w;
     float* buf = nullptr;
-    ~OptWorkspace () { cudaFree (buf); }
+    LbDev* lbdev = nullptr;          // the graph-resident run's state
+    // the recorded graph of the iterations, and what it was recorded for
+    cudaGraphExec_t exec = nullptr;
+    unsigned gen = 0;
+    float lambda = 0.f;
+    bool has_reg = false;
+    b200bsp_reg_parms reg = {};
+    ~OptWorkspace ()
+    {
+        if (exec) cudaGraphExecDestroy (exec);
+        cudaFree (buf);
+        cudaFree (lbdev);
+    }
 };
 
 static void
@@ -719,7 +1025,8 @@ context_workspace (b200bsp_ctx* ctx, int64_t nc, int m)
     if (ws && ws->w.n == nc && ws->w.m == m) return ws;
     ws = new OptWorkspace ();
     if (ws->w.alloc (nc, m)
-        || cudaMalloc (&ws->buf, 2 * nc * sizeof (float)) != cudaSuccess) {
+        || cudaMalloc (&ws->buf, 2 * nc * sizeof (float)) != cudaSuccess
+        || cudaMalloc (&ws->lbdev, sizeof (LbDev)) != cudaSuccess) {
         cudaGetLastError ();
         delete ws;
         return nullptr;
@@ -728,8 +1035,76 @@ context_workspace (b200bsp_ctx* ctx, int64_t nc, int m)
     return ws;
 }
 
+// The iterations after the prologue as one graph launch (MSE on a context);
+// the host-driven loop when the graph cannot be built.
+static int
+lbfgs_graph_run (b200bsp_ctx* ctx, Lbfgs& w, ContextObjective& obj,
+    const b200bsp_lbfgs_parms& p, b200bsp_lbfgs_result* res, double f,
+    double step, OptWorkspace* ws)
+{
+    LbDev* dst = ws->lbdev;
+    LbDev h;
+    memset (&h, 0, sizeof h);
+    h.m = p.m;
+    h.max_its = p.max_its;
+    h.max_feval = p.max_feval;
+    h.max_linesearch = p.max_linesearch;
+    h.epsilon = p.epsilon;
+    h.min_step = p.min_step;
+    h.max_step = p.max_step;
+    h.ftol = p.ftol;
+    h.gtol = p.gtol;
+    h.xtol = p.xtol;
+    h.k = 1;
+    h.fevals = obj.fevals;
+    h.first = 1;
+    h.newiter = 1;
+    h.f = f;
+    h.stp = step;
+    h.last = obj.last;
+    if (cudaMemcpyAsync (dst, &h, sizeof h, cudaMemcpyHostToDevice, w.st)
+            != cudaSuccess
+        || cudaStreamSynchronize (w.st) != cudaSuccess) {
+        cudaGetLastError ();
+        return B200BSP_E_CUDA;
+    }
+    // record the graph once per (context state, lambda, regulariser); the
+    // history length and the buffers are the workspace's own
+    const bool fresh = ws->exec && ws->gen == ctx_generation (ctx)
+        && ws->lambda == obj.lambda && ws->has_reg == (obj.reg != nullptr)
+        && (!obj.reg || memcmp (&ws->reg, obj.reg, sizeof ws->reg) == 0);
+    if (!fresh) {
+        if (ws->exec) cudaGraphExecDestroy (ws->exec);
+        ws->exec = nullptr;
+        if (!build_lbfgs_graph (ctx, w, dst, obj.lambda, obj.reg, obj.coeff_f,
+                obj.grad_f, &ws->exec)) {
+            ws->exec = nullptr;
+            return lbfgs_loop (w, obj, p, res, f, step);
+        }
+        ws->gen = ctx_generation (ctx);
+        ws->lambda = obj.lambda;
+        ws->has_reg = obj.reg != nullptr;
+        if (obj.reg) ws->reg = *obj.reg;
+    }
+    const bool ran = cudaGraphLaunch (ws->exec, w.st) == cudaSuccess
+        && cudaMemcpyAsync (&h, dst, sizeof h, cudaMemcpyDeviceToHost, w.st)
+            == cudaSuccess
+        && cudaStreamSynchronize (w.st) == cudaSuccess;
+    if (!ran) {
+        cudaGetLastError ();
+        return B200BSP_E_CUDA;
+    }
+    obj.fevals = h.fevals;
+    obj.last = h.last;
+    res->iterations = h.iterations;
+    res->status = h.status == LS_STOPPED ? B200BSP_LBFGS_STOPPED : h.status;
+    return B200BSP_OK;
+}
+
 // L-BFGS over a context's coefficients (host or device floats, updated in
-// place with the last evaluated point), evaluations by `obj`.
+// place with the last evaluated point), evaluations by `obj`: MSE without
+// landmarks runs its iterations as one graph launch (lbfgs_graph_run), the
+// rest from the host.
 static int
 optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
     int64_t nc, float* coeff, b200bsp_lbfgs_result* res,
@@ -756,7 +1131,17 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
     f2d_kernel<<<w.grid (), 256, 0, st>>> (buf, w.x, nc);
     res->status = 0;
     res->fevals = 0;
-    rc = lbfgs_run (w, obj, p, res);
+    float stiffness = 0.f;
+    if (obj.metric == 0 && ctx_landmarks (ctx, &stiffness) == 0) {
+        double f = 0.0, step = 0.0;
+        bool more = false;
+        rc = lbfgs_prologue (w, obj, p, res, &f, &step, &more);
+        if (!rc && more) {
+            rc = lbfgs_graph_run (ctx, w, obj, p, res, f, step, ws);
+        }
+    } else {
+        rc = lbfgs_run (w, obj, p, res);
+    }
     res->fevals = obj.fevals;
     if (!rc) {
         // Plastimatch's evaluate callback copies every trial point into the
@@ -773,27 +1158,6 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
         }
     }
     return rc;
-}
-
-// One registration of a batch (batch.cu): MSE, no regulariser, each
-// evaluation through `eval` (the batch's barrier and graph launch).
-int
-lbfgs_optimize_batched (b200bsp_ctx* ctx, float lambda,
-    const b200bsp_lbfgs_parms* parms, float* coeff, b200bsp_lbfgs_result* res,
-    void* member, int (*eval) (void*, int, const float*, float*, float*))
-{
-    b200bsp_lbfgs_parms p;
-    if (parms) p = *parms; else b200bsp_lbfgs_default_parms (&p);
-    int rc = check_parms (&p);
-    if (rc) return rc;
-    int64_t nc = 0;
-    rc = b200bsp_grid_info (ctx, nullptr, nullptr, &nc);
-    if (rc) return rc;
-    ContextObjective obj;
-    obj.ctx = ctx; obj.metric = 0; obj.lambda = lambda; obj.reg = nullptr;
-    obj.member = member;
-    obj.batch_eval = eval;
-    return optimize_on_context (ctx, p, nc, coeff, res, obj);
 }
 
 } // namespace b200

@@ -79,6 +79,10 @@ struct b200bsp_ctx {
     float* d_total = nullptr;
     int tc_grid = 0;          // CTAs of the tile kernel; 0: plan.grid
     int sm_count = 148;
+    // bumped by every change to what an evaluation launches (kernel
+    // choice, ROIs, images, wait limit, grid): a recorded graph of
+    // evaluations is stale once it moves
+    unsigned gen = 0;
     // b200bsp_score's regulariser: a second stream, and the fork and join
     // of it around the MSE kernel
     cudaStream_t aux_stream = nullptr;
@@ -392,6 +396,12 @@ ctx_landmarks (const b200bsp_ctx* c, float* stiffness)
     return c->lm_n;
 }
 
+unsigned
+ctx_generation (const b200bsp_ctx* c)
+{
+    return c->gen;
+}
+
 // The optimiser's workspace slot: kept by the context, freed with it.
 void*
 ctx_opt_ws (const b200bsp_ctx* c)
@@ -423,6 +433,7 @@ ctx_work (const b200bsp_ctx* c, bool* persistent)
 void
 ctx_set_tc_grid (b200bsp_ctx* c, int ctas)
 {
+    if (c->tc_grid != ctas) c->gen++;
     c->tc_grid = ctas;
 }
 
@@ -734,6 +745,7 @@ b200bsp_set_wait_limit (b200bsp_ctx* c, int polls, int withhold_mma)
     if (polls < 0) return fail (c, B200BSP_E_BADARG, "polls must be >= 0");
     c->wait_limit = polls > 0 ? (unsigned) polls : XL_DEFAULT_WAIT_LIMIT;
     c->withhold_mma = withhold_mma ? 1 : 0;
+    c->gen++;
     return B200BSP_OK;
 }
 
@@ -789,6 +801,7 @@ b200bsp_set_images (b200bsp_ctx* c, const float* fixed_img,
     if (!c || !fixed_img || !moving_img) {
         return fail (c, B200BSP_E_BADARG, "null image");
     }
+    c->gen++;
     CK (cudaSetDevice (c->device));
     const BspGeom& g = c->geom;
     size_t nf = (size_t) g.fdim[0] * g.fdim[1] * g.fdim[2];
@@ -1014,6 +1027,7 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
 {
     if (!c) return B200BSP_E_BADARG;
     if (evals < 1) return fail (c, B200BSP_E_BADARG, "evals must be >= 1");
+    c->gen++;
     if (c->opts.form != B200BSP_FORM_TC) {
         if (tiles) *tiles = 1;
         return B200BSP_OK;
@@ -1381,6 +1395,7 @@ b200bsp_set_roi (b200bsp_ctx* c, const b200bsp_volume* fixed_roi,
     const uint8_t* moving_mask)
 {
     if (!c) return B200BSP_E_BADARG;
+    c->gen++;
     if (!fixed_roi != !fixed_mask || !moving_roi != !moving_mask) {
         return fail (c, B200BSP_E_BADARG,
             "an ROI needs both its geometry and its mask");
