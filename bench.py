@@ -76,11 +76,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(form):
+def profile_traffic(kernel):
+    """ncu DRAM bytes per launch of the kernel that ran ("tile", "xlane" or
+    "fp32", as b200bsp_mse_kernel names it)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get(form)
+            return json.load(f).get(kernel)
     return None
 
 
@@ -800,7 +802,8 @@ def main():
         return value, e2e_value, {
             "bound": "hbm", "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak,
-            "traffic": profile_traffic(form), "peak_source": peak_kind,
+            "traffic": profile_traffic(r["kernel"][0]),
+            "traffic_kernel": r["kernel"][0], "peak_source": peak_kind,
             "kernel_ms": r["kernel_ms"],
             "algorithmic_bytes_per_launch": ALGO_BYTES_PER_VOXEL * nvox}
 
