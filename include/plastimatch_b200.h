@@ -241,6 +241,12 @@ int b200bsp_set_wait_limit (b200bsp_ctx* ctx, int polls, int withhold_mma);
  * create returns B200BSP_E_OOM and releases everything it allocated. */
 void b200bsp_debug_fail_alloc (int nth);
 
+/* Testing aid: nonzero makes this thread's b200bsp_optimize_lbfgs calls
+ * drive every iteration from the host (one synchronisation per trial)
+ * instead of running them as one graph launch, so the two can be
+ * compared. */
+void b200bsp_debug_host_lbfgs (int on);
+
 /* Image ROIs of the cost function: Bspline_state::fixed_roi and
  * ::moving_roi (src/register/bspline_state.h:44-45), uchar mask volumes
  * (x fastest, nonzero = inside) with their own geometry.  A fixed voxel

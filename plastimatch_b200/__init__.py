@@ -151,6 +151,7 @@ _SIGS = {
     "b200bsp_set_roi": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "b200bsp_set_wait_limit": (C.c_int, [_VP, C.c_int, C.c_int]),
     "b200bsp_debug_fail_alloc": (None, [C.c_int]),
+    "b200bsp_debug_host_lbfgs": (None, [C.c_int]),
     "b200bsp_score": (C.c_int, [_VP, _VP, C.c_int, C.c_float, _VP, _VP, _VP,
                                 _VP, _VP]),
     "b200bsp_interpolate_vf": (C.c_int, [_VP, _VP, _VP]),

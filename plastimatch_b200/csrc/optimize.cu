@@ -1101,6 +1101,9 @@ lbfgs_graph_run (b200bsp_ctx* ctx, Lbfgs& w, ContextObjective& obj,
     return B200BSP_OK;
 }
 
+// b200bsp_debug_host_lbfgs: this thread's runs stay on the host-driven loop
+static thread_local int g_host_lbfgs = 0;
+
 // L-BFGS over a context's coefficients (host or device floats, updated in
 // place with the last evaluated point), evaluations by `obj`: MSE without
 // landmarks runs its iterations as one graph launch (lbfgs_graph_run), the
@@ -1132,7 +1135,8 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
     res->status = 0;
     res->fevals = 0;
     float stiffness = 0.f;
-    if (obj.metric == 0 && ctx_landmarks (ctx, &stiffness) == 0) {
+    if (obj.metric == 0 && ctx_landmarks (ctx, &stiffness) == 0
+        && !g_host_lbfgs) {
         double f = 0.0, step = 0.0;
         bool more = false;
         rc = lbfgs_prologue (w, obj, p, res, &f, &step, &more);
@@ -1163,6 +1167,12 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
 } // namespace b200
 
 using namespace b200;
+
+extern "C" void
+b200bsp_debug_host_lbfgs (int on)
+{
+    g_host_lbfgs = on ? 1 : 0;
+}
 
 extern "C" void
 b200bsp_lbfgs_default_parms (b200bsp_lbfgs_parms* p)

@@ -16,6 +16,8 @@ import pytest
 import oracle as O
 import plastimatch_b200 as P
 from conftest import load_golden
+from plastimatch_b200 import synth
+from plastimatch_b200.geometry import BsplineGrid
 
 pytestmark = pytest.mark.gpu
 
@@ -73,3 +75,43 @@ def test_registration_matches_plastimatch_liblbfgs(form):
     assert abs(res["score"] - s_ref) <= 1e-3 * abs(s_ref), (res["score"], s_ref)
     assert res["score"] < 0.05 * float(rec["g_score"])
     assert np.linalg.norm(c - c_ref) <= 1e-2 * np.linalg.norm(c_ref - coeff)
+
+
+def _blobs_case(seed=20261208):
+    fixed = synth.gaussian_blobs((64, 56, 48), spacing=(1.0, 1.1, 1.3),
+                                 seed=seed)
+    g0 = BsplineGrid.for_volume(fixed, 8)
+    moving = synth.warp_trilinear(fixed, fixed, g0,
+                                  synth.random_coeff(g0, 2.0, seed + 1))
+    return fixed, moving
+
+
+@pytest.mark.parametrize("form", ["fp32", "tc"])
+@pytest.mark.parametrize("vpr, with_reg", [(8, True), (8, False), (4, True)])
+def test_graph_run_matches_host_driven_run(form, vpr, with_reg):
+    """The graph-resident iterations (one launch) against the host-driven
+    loop on the same registration: MSE, optionally with the curvature
+    regulariser.  The controller rounds as the host does; the two differ
+    only in the dot products' summation order of the new-line-search branch
+    for small grids (vpr 8: one block), so the bar is the same trials and
+    scores to 1e-5."""
+    fixed, moving = _blobs_case()
+    grid = BsplineGrid.for_volume(fixed, vpr)
+    reg = P.reg_parms(curvature=0.005) if with_reg else None
+    x0 = np.zeros(grid.num_coeff, np.float32)
+    out = []
+    for host in (1, 0):
+        P.lib().b200bsp_debug_host_lbfgs(host)
+        try:
+            with P.Context(fixed, moving, grid, form=form) as ctx:
+                ctx.set_images()
+                out.append(ctx.optimize_lbfgs(x0, reg=reg, max_its=15,
+                                              max_feval=40))
+        finally:
+            P.lib().b200bsp_debug_host_lbfgs(0)
+    (c_h, r_h), (c_g, r_g) = out
+    assert r_g["fevals"] == r_h["fevals"], (r_g, r_h)
+    assert r_g["iterations"] == r_h["iterations"], (r_g, r_h)
+    assert r_g["status"] == r_h["status"], (r_g, r_h)
+    assert abs(r_g["score"] - r_h["score"]) <= 1e-5 * abs(r_h["score"])
+    assert np.linalg.norm(c_g - c_h) <= 1e-4 * max(np.linalg.norm(c_h), 1.0)
