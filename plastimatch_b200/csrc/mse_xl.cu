@@ -17,10 +17,12 @@
 // src/register/bspline.cxx:347-374) runs the other way:
 //   Rg[(c,xk)][rho] = sum_x Bx[x][xk] DCDV_c[x][rho]               (tensor cores)
 //   G_c[xk][j][k]   = sum_rho by[ly][j] bz[lz][k] Rg[(c,xk)][rho]  (CUDA cores)
-// The adjoint's M dimension is (c, xk): the basis table holds four copies
-// of Bx side by side, so the MMA's rows c*32 + xk land in TMEM lane quarter
-// c and every lane of a quarter owns one knot of one component for the
-// y/z contraction.  G_c is the batch's partial gradient of its
+// The adjoint runs one MMA per component; its M dimension is four copies of
+// the 32 knots (the basis table holds Bx four times side by side), so
+// every TMEM lane quarter receives all of Rg_c and each of its lanes owns
+// one knot for the y/z contraction -- done by lane quarter 3's warps when
+// that quarter has no samples (at vox_per_rgn 5 a batch spans 90 voxels),
+// else by the other quarters'.  G_c is the batch's partial gradient of its
 // (T + 3) x 4 x 4 knot footprint; the finish kernel sums the partials of
 // each knot in a fixed order (no float atomics).
 //
@@ -380,20 +382,17 @@ xl_yz_forward (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf)
     }
 }
 
-// y/z adjoint contraction of one step: thread (c, xk) of lane quarter c,
-// warp j4 = knot plane k; accumulates G[j] over the batch's chunks.
+// y/z adjoint contraction of one step for knot plane k, given the
+// thread's row of Rg_c (rg, 32 columns): accumulates G[j] over the batch's
+// chunks.
 template <int VY>
 __device__ __forceinline__ void
-xl_yz_adjoint_t (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
-    float G[4])
+xl_yz_adjoint_t (const XlArgs& a, const XlCtx& x, const XlStep& t,
+    const float rg[32], int k, float G[4])
 {
     constexpr int NLZ = XL_RC / VY;
     const float* by = (const float*) (x.sm + XS_LUT);
     const float* bz = by + 4 * VY;
-    const int c = x.q, k = x.j4;
-    float rg[32];
-    tmem_ld32_wait (x.taddr + ((uint32_t) (32 * c) << 16) + XT_RG + 128 * buf
-        + XL_RC * c, rg);
     float z[VY];
 #pragma unroll
     for (int ly = 0; ly < VY; ly++) z[ly] = 0.f;
@@ -413,20 +412,29 @@ xl_yz_adjoint_t (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
 }
 
 __device__ __forceinline__ void
-xl_yz_adjoint (const XlArgs& a, const XlCtx& x, const XlStep& t, int buf,
-    float G[4])
+xl_yz_adjoint (const XlArgs& a, const XlCtx& x, const XlStep& t,
+    const float rg[32], int k, float G[4])
 {
     switch (a.g.vpr[1]) {
-    case 3: xl_yz_adjoint_t<3> (a, x, t, buf, G); break;
-    case 4: xl_yz_adjoint_t<4> (a, x, t, buf, G); break;
-    case 5: xl_yz_adjoint_t<5> (a, x, t, buf, G); break;
-    case 6: xl_yz_adjoint_t<6> (a, x, t, buf, G); break;
-    case 7: xl_yz_adjoint_t<7> (a, x, t, buf, G); break;
-    case 8: xl_yz_adjoint_t<8> (a, x, t, buf, G); break;
-    case 9: xl_yz_adjoint_t<9> (a, x, t, buf, G); break;
-    case 10: xl_yz_adjoint_t<10> (a, x, t, buf, G); break;
+    case 3: xl_yz_adjoint_t<3> (a, x, t, rg, k, G); break;
+    case 4: xl_yz_adjoint_t<4> (a, x, t, rg, k, G); break;
+    case 5: xl_yz_adjoint_t<5> (a, x, t, rg, k, G); break;
+    case 6: xl_yz_adjoint_t<6> (a, x, t, rg, k, G); break;
+    case 7: xl_yz_adjoint_t<7> (a, x, t, rg, k, G); break;
+    case 8: xl_yz_adjoint_t<8> (a, x, t, rg, k, G); break;
+    case 9: xl_yz_adjoint_t<9> (a, x, t, rg, k, G); break;
+    case 10: xl_yz_adjoint_t<10> (a, x, t, rg, k, G); break;
     default: break;                  // the plan admits no other vy
     }
+}
+
+// The thread's row of Rg_c from its lane quarter (every quarter holds all
+// of it).
+__device__ __forceinline__ void
+xl_load_rg (const XlCtx& x, int buf, int c, float rg[32])
+{
+    tmem_ld32_wait (x.taddr + ((uint32_t) (32 * x.q) << 16) + XT_RG
+        + 128 * buf + XL_RC * c, rg);
 }
 
 // Mattes MI pass 2 at one sample (bspline_mi_pvi_8_dc_dv_dcos,
@@ -898,25 +906,31 @@ xl_issue_forward (const XlCtx& x, int buf, int rbuf, uint64_t* bar)
     tc_commit (bar);
 }
 
-// x-adjoint MMA of a step: Rg[(c, xk)][(c', rho)] = Bx[x][xk] DC[x][(c', rho)]
-// (the table read MN-major: M = four copies of the 32 knots), K = 128
-// voxels, three split terms; one thread.
+// x-adjoint MMAs of a step, one per component c:
+// Rg_c[(q, xk)][rho] = Bx[x][xk] DC_c[x][rho] (the table read MN-major: M =
+// four identical copies of the 32 knots, so every TMEM lane quarter q holds
+// all of Rg_c), N = the component's 32 rows, K = 128 voxels, three split
+// terms; Rg_c in columns 32 c of the buffer.  One thread.
 __device__ __forceinline__ void
 xl_issue_adjoint (const XlCtx& x, int buf, uint64_t* bar)
 {
-    const uint32_t idesc = idesc_bf16_f32 (128, XL_N, 1, 0);
+    const uint32_t idesc = idesc_bf16_f32 (128, XL_RC, 1, 0);
     const uint32_t ta = x.sm_base + XS_TAB;
     const uint32_t td = x.sm_base + XS_DC + buf * XS_DC_BUF;
 #pragma unroll
-    for (int term = 0; term < 3; term++) {
-        const uint32_t A = term == 2 ? ta + XS_TAB_LO : ta;
-        const uint32_t B = term == 1 ? td + XS_DC_LO : td;
+    for (int c = 0; c < 3; c++) {
 #pragma unroll
-        for (int ks = 0; ks < 8; ks++) {
-            tc_mma_bf16 (x.taddr + XT_RG + 128 * buf,
-                smem_desc_sw128 (A + ks * 2048, 16384, 1024),
-                smem_desc_sw128 (B + (ks >> 2) * XS_DC_ATOM + (ks & 3) * 32,
-                    16, 1024), idesc, (term > 0 || ks > 0) ? 1u : 0u);
+        for (int term = 0; term < 3; term++) {
+            const uint32_t A = term == 2 ? ta + XS_TAB_LO : ta;
+            // the component's 32 rows: four 8-row groups of 1024 bytes
+            const uint32_t B = (term == 1 ? td + XS_DC_LO : td) + 4096 * c;
+#pragma unroll
+            for (int ks = 0; ks < 8; ks++) {
+                tc_mma_bf16 (x.taddr + XT_RG + 128 * buf + XL_RC * c,
+                    smem_desc_sw128 (A + ks * 2048, 16384, 1024),
+                    smem_desc_sw128 (B + (ks >> 2) * XS_DC_ATOM + (ks & 3) * 32,
+                        16, 1024), idesc, (term > 0 || ks > 0) ? 1u : 0u);
+            }
         }
     }
     tc_commit (bar);
@@ -1064,6 +1078,11 @@ mse_xl_kernel (XlArgs a)
         uint32_t ph_d = 0, ph_rg = 0;       // phase parity of buffer b: bit b
         const bool yz_fwd_warp = x.q == 3;
         const bool vox_live = 32 * x.q < a.T * g.vpr[0];
+        // the y/z adjoint: by lane quarter 3's warps (one component each,
+        // every knot plane) when that quarter has no samples, else by the
+        // other quarters' warps (component q, knot plane j4)
+        const bool adj_q3 = 32 * 3 >= a.T * g.vpr[0];
+        const bool adj_warp = adj_q3 ? x.q == 3 : x.q < 3;
         float G[4] = {0.f, 0.f, 0.f, 0.f};
         double sc = 0.0;
         int cnt = 0;
@@ -1084,8 +1103,33 @@ mse_xl_kernel (XlArgs a)
             ph_rg ^= 1u << pb;
             tc_fence_after ();
             const XlStep t = xl_step (a, sp);
+            if (adj_q3) {
+                // component j4, the four knot planes one after another,
+                // added into the batch's partial gradient (stored by the
+                // first chunk; the same thread owns those entries)
+                const int c = x.j4;
+                float* dst = a.part + ((size_t) t.b * 3 + c) * (16 * a.KX)
+                    + x.lane;
+                float rg[32];
+                xl_load_rg (x, pb, c, rg);
+                for (int k = 0; k < 4; k++) {
+                    float Gk[4] = {0.f, 0.f, 0.f, 0.f};
+                    xl_yz_adjoint (a, x, t, rg, k, Gk);
+                    if (x.lane < a.KX) {
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            float* p = dst + a.KX * (j + 4 * k);
+                            *p = t.ch == 0 ? Gk[j] : *p + Gk[j];
+                        }
+                    }
+                }
+                tc_fence_before ();
+                return true;
+            }
             if (t.ch == 0) G[0] = G[1] = G[2] = G[3] = 0.f;
-            xl_yz_adjoint (a, x, t, pb, G);
+            float rg[32];
+            xl_load_rg (x, pb, x.q, rg);
+            xl_yz_adjoint (a, x, t, rg, x.j4, G);
             tc_fence_before ();
             if (t.ch == a.nch - 1 && x.lane < a.KX) {
                 const int KF = 16 * a.KX;
@@ -1139,11 +1183,12 @@ mse_xl_kernel (XlArgs a)
                     ok = xl_produce<MODE> (a, x, s_bar, s + XL_NB2,
                         s % XL_NB2);
                 }
-            } else if (s >= 1 && !xl_hist_mode (MODE)) {
+            }
+            if (ok && adj_warp && s >= 1 && !xl_hist_mode (MODE)) {
                 ok = yz_adjoint (s - 1);
             }
         }
-        if (ok && !yz_fwd_warp && S >= 1 && !xl_hist_mode (MODE)) {
+        if (ok && adj_warp && S >= 1 && !xl_hist_mode (MODE)) {
             yz_adjoint (S - 1);
         }
         if constexpr (xl_hist_mode (MODE)) {
@@ -1217,8 +1262,8 @@ xl_plan (const BspGeom& g, XlPlan* p, int sm_count, int extra_row_batches)
     return true;
 }
 
-// The basis table image: 128 voxel rows x 128 columns m = c * 32 + xk
-// (c = 0..2 copies of the 32 knot columns, c = 3 zero), bf16 hi then lo,
+// The basis table image: 128 voxel rows x 128 columns m = q * 32 + xk
+// (four copies of the 32 knot columns), bf16 hi then lo,
 // each the exact 128-byte-swizzled shared-memory image (32 KB).  Row x of a
 // batch, x < T vx, holds bx[x mod vx][xk - x div vx] on the band.
 int
@@ -1229,9 +1274,9 @@ xl_build_table (const BspGeom& g, const XlPlan& p, const float* bx_lut,
     std::vector<uint8_t> img (65536, 0);
     for (int xr = 0; xr < 128; xr++) {
         for (int m = 0; m < 128; m++) {
-            const int c = m >> 5, xk = m & 31;
+            const int xk = m & 31;
             float v = 0.f;
-            if (c < 3 && xr < p.T * vx) {
+            if (xr < p.T * vx) {
                 const int i = xk - xr / vx;
                 if (i >= 0 && i < 4) v = bx_lut[4 * (xr % vx) + i];
             }
