@@ -467,7 +467,10 @@ int b200bsp_lbfgs_minimize (int64_t n, double* x, b200bsp_eval_fn fn,
  * stream capture.  A CUDA error already pending when the call starts is
  * reported (B200BSP_E_CUDA) and left pending.  Calls whose device work
  * overlaps race on the shared array: issue them on one stream.  Errors
- * are reported through b200bsp_last_error (NULL). */
+ * are reported through b200bsp_last_error (NULL).  The whole fixed image
+ * is the ROI: this entry point takes no fixed or moving ROI mask (a masked
+ * registration, the reference's inside_roi test, needs a context and
+ * b200bsp_set_roi). */
 int b200bsp_score_mse_static (const b200bsp_volume* fixed,
     const b200bsp_volume* moving, const b200bsp_grid* grid, int mse_grad,
     const float* fixed_img, const float* moving_img, const float* moving_grad,
