@@ -45,9 +45,15 @@ finish_run (LbDev* s, int status, cudaGraphConditionalHandle h_while)
 }  // namespace
 
 __global__ void
-lb_begin_search_kernel (LbDev* s, cudaGraphConditionalHandle h_while)
+lb_begin_search_kernel (LbDev* s, cudaGraphConditionalHandle h_while,
+    const double* part, int nparts)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || s->done) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    if (part) {
+        const double dg0 = lb_warp_sum (part + (size_t) LP_DG0 * nparts, nparts);
+        if (threadIdx.x == 0) s->dginit = dg0;
+    }
+    if (threadIdx.x != 0 || s->done) return;
     s->first = 0;
     s->finit = s->f;
     if (s->stp <= 0.0) {
@@ -76,9 +82,20 @@ lb_begin_search_kernel (LbDev* s, cudaGraphConditionalHandle h_while)
 
 __global__ void
 lb_after_eval_kernel (LbDev* s, cudaGraphConditionalHandle h_while,
-    cudaGraphConditionalHandle h_new)
+    cudaGraphConditionalHandle h_new, const double* part, int nparts)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    {
+        const double dg = lb_warp_sum (part + (size_t) LP_GD * nparts, nparts);
+        const double xx = lb_warp_sum (part + (size_t) LP_XX * nparts, nparts);
+        const double gg = lb_warp_sum (part + (size_t) LP_GG * nparts, nparts);
+        if (threadIdx.x == 0) {
+            s->dg = dg;
+            s->xx = xx;
+            s->gg = gg;
+        }
+    }
+    if (threadIdx.x != 0) return;
     cudaGraphSetConditional (h_new, 0);
     if (s->done) {
         cudaGraphSetConditional (h_while, 0);

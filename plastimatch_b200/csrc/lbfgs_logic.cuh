@@ -136,6 +136,27 @@ lb_stop_rule (int max_its, int max_feval, int k, int fevals)
     return k > max_its || fevals > max_feval;
 }
 
+// Slots of the graph-resident run's partial sums (one block's partial per
+// slot entry; each slot holds one dot product's partials): the correction
+// pair's y.s and y.y, gp.d of a new line search, the evaluated point's g.d,
+// x.x and g.g, then the two-loop recursion's dot products (the first loop's
+// s_j.d at LP_REC + i, the second loop's y_j.d at LP_REC + m + i).
+enum { LP_YS, LP_YY, LP_DG0, LP_GD, LP_XX, LP_GG, LP_REC };
+
+#ifdef __CUDACC__
+// The sum of n partials by one whole warp: lane-strided sums, then a
+// butterfly, so every lane returns the same value.
+__device__ __forceinline__ double
+lb_warp_sum (const double* part, int n)
+{
+    double s = 0.0;
+    for (int k = threadIdx.x & 31; k < n; k += 32) s += part[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync (0xffffffffu, s, o);
+    return s;
+}
+#endif
+
 // The graph-resident optimiser's state (device memory).  The host writes
 // it before the launch (parameters, the prologue's evaluation and first
 // step) and reads the outcome after.

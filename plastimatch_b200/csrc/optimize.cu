@@ -213,7 +213,10 @@ struct Lbfgs {
         };
         a (&x, n); a (&g, n); a (&d, n); a (&xp, n); a (&gp, n);
         a (&s, (size_t) m * n); a (&y, (size_t) m * n);
-        a (&part, OPT_BLOCKS); a (&scalar, 2); a (&dsc, 2 * (size_t) m + 2);
+        // partial sums: one slot for the host-driven loop's dot products,
+        // LP_REC + 2 m slots for the graph-resident run's
+        a (&part, (size_t) OPT_BLOCKS * (LP_REC + 2 * m));
+        a (&scalar, 2); a (&dsc, 2 * (size_t) m + 2);
         if (!err && cudaMallocHost (&h_scalar, 2 * sizeof (double)) != cudaSuccess) {
             cudaGetLastError ();
             err = B200BSP_E_OOM;
@@ -590,119 +593,6 @@ lb_j2 (const LbDev* s, int i)
     return (s->end - s->bound + i + 2 * s->m) % s->m;
 }
 
-// s[newest] = x - xp, y[newest] = g - gp
-__global__ void
-lb_pair_kernel (const LbDev* __restrict__ st, double* __restrict__ S,
-    double* __restrict__ Y, const double* __restrict__ x,
-    const double* __restrict__ xp, const double* __restrict__ g,
-    const double* __restrict__ gp, long long n)
-{
-    if (st->first) return;
-    double* sj = S + (size_t) st->newest * n;
-    double* yj = Y + (size_t) st->newest * n;
-    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long) gridDim.x * blockDim.x) {
-        sj[i] = x[i] - xp[i];
-        yj[i] = g[i] - gp[i];
-    }
-}
-
-enum { LB_YS, LB_YY, LB_ALPHA, LB_BETA };
-
-// a block's partial dot product of the recursion: ys = y.s and yy = y.y of
-// the newest pair, s_j.d of the first loop, y_j.d of the second
-__global__ void __launch_bounds__ (OPT_THREADS)
-lb_dot_partial_kernel (const LbDev* __restrict__ st, int op, int i,
-    const double* __restrict__ S, const double* __restrict__ Y,
-    const double* __restrict__ d, long long n, double* __restrict__ part)
-{
-    const double *a, *b;
-    if (op == LB_YS || op == LB_YY) {
-        if (st->first) return;
-        a = Y + (size_t) st->newest * n;
-        b = op == LB_YS ? S + (size_t) st->newest * n : a;
-    } else {
-        if (lb_skip (st, i)) return;
-        a = op == LB_ALPHA ? S + (size_t) lb_j1 (st, i) * n
-                           : Y + (size_t) lb_j2 (st, i) * n;
-        b = d;
-    }
-    dot_partial_body (a, b, n, part);
-}
-
-// the partial sums in block order (dot_final_div_kernel's), into the
-// recursion's scalars: ys[newest], yy, alpha[j] = s_j.d / ys[j],
-// beta = y_j.d / ys[j]
-__global__ void
-lb_dot_final_kernel (const LbDev* __restrict__ st, int op, int i,
-    const double* __restrict__ part, int nparts, double* __restrict__ dsc)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int m = st->m;
-    if (op == LB_YS || op == LB_YY) {
-        if (st->first) return;
-    } else if (lb_skip (st, i)) {
-        return;
-    }
-    double s = 0.0;
-    for (int k = 0; k < nparts; k++) s += part[k];
-    if (op == LB_YS) {
-        dsc[st->newest] = s;
-    } else if (op == LB_YY) {
-        dsc[2 * m + 1] = s;
-    } else if (op == LB_ALPHA) {
-        const int j = lb_j1 (st, i);
-        dsc[m + j] = s / dsc[j];
-    } else {
-        dsc[2 * m] = s / dsc[lb_j2 (st, i)];
-    }
-}
-
-// d = -alpha[j] y_j + d (first loop)
-__global__ void
-lb_axpy1_kernel (const LbDev* __restrict__ st, int i,
-    const double* __restrict__ Y, const double* __restrict__ dsc,
-    double* __restrict__ d, long long n)
-{
-    if (lb_skip (st, i)) return;
-    const int j = lb_j1 (st, i);
-    const double av = -1.0 * dsc[st->m + j];
-    const double* yj = Y + (size_t) j * n;
-    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += (long long) gridDim.x * blockDim.x) {
-        d[k] = av * yj[k] + 1.0 * d[k];
-    }
-}
-
-// d = (ys / yy) d
-__global__ void
-lb_scale_kernel (const LbDev* __restrict__ st, const double* __restrict__ dsc,
-    double* __restrict__ d, long long n)
-{
-    if (st->first) return;
-    const double bv = dsc[st->newest] / dsc[2 * st->m + 1];
-    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += (long long) gridDim.x * blockDim.x) {
-        d[k] = 0.0 * d[k] + bv * d[k];
-    }
-}
-
-// d = (alpha[j] - beta) s_j + d (second loop)
-__global__ void
-lb_axpy2_kernel (const LbDev* __restrict__ st, int i,
-    const double* __restrict__ S, const double* __restrict__ dsc,
-    double* __restrict__ d, long long n)
-{
-    if (lb_skip (st, i)) return;
-    const int j = lb_j2 (st, i);
-    const double av = dsc[st->m + j] - dsc[2 * st->m];
-    const double* sj = S + (size_t) j * n;
-    for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += (long long) gridDim.x * blockDim.x) {
-        d[k] = av * sj[k] + 1.0 * d[k];
-    }
-}
-
 // The whole new-line-search branch in one block, for vectors of at most
 // LB_FUSED_MAX entries: correction pair, the two-loop recursion, xp = x,
 // gp = g and dginit = gp.d, each dot product a block reduction in a fixed
@@ -798,17 +688,243 @@ lb_branch_fused_kernel (const LbDev* __restrict__ st, double* __restrict__ S,
     if (t == 0) *dginit = dg0;
 }
 
-// x = xp + stp d (the trial point; x stays when the run is over)
+// x = xp + stp d (the trial point) and its float copy, the evaluation's
+// coefficients; both stay when the run is over (the float copy already
+// holds x then)
 __global__ void
 lb_trial_kernel (const LbDev* __restrict__ st, const double* __restrict__ xp,
-    const double* __restrict__ d, double* __restrict__ x, long long n)
+    const double* __restrict__ d, double* __restrict__ x,
+    float* __restrict__ xf, long long n)
 {
     if (st->done) return;
     const double a = st->stp;
     for (long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (long long) gridDim.x * blockDim.x) {
-        x[k] = xp[k] + a * d[k];
+        const double v = xp[k] + a * d[k];
+        x[k] = v;
+        xf[k] = (float) v;
     }
+}
+
+// ---- the recursion and the evaluation's dot products, fused ----------------
+//
+// Each kernel below runs on OPT_BLOCKS blocks of OPT_THREADS threads and
+// writes one block partial per dot product it forms (a thread sums its
+// indices in the order of dot_partial_body, then the block's tree); the
+// next kernel of the chain sums the partials it needs in every block (one
+// warp, lb_warp_sum) instead of waiting for a separate reduction launch.
+// Early returns depend on the run's state only, so whole blocks take them.
+
+// the block's partials of K dot products into slots out[k]
+template <int K>
+__device__ __forceinline__ void
+block_partials (const double (&v)[K], double* const (&out)[K])
+{
+    __shared__ double sh[K][OPT_THREADS];
+#pragma unroll
+    for (int k = 0; k < K; k++) sh[k][threadIdx.x] = v[k];
+    __syncthreads ();
+    for (int o = OPT_THREADS / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+#pragma unroll
+            for (int k = 0; k < K; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+        }
+        __syncthreads ();
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) out[k][blockIdx.x] = sh[k][0];
+    }
+}
+
+// the sum of slot `slot`'s partials, in every thread of the block
+__device__ __forceinline__ double
+block_final (const double* __restrict__ part, int slot)
+{
+    __shared__ double r;
+    if (threadIdx.x < 32) {
+        const double v = lb_warp_sum (part + (size_t) slot * OPT_BLOCKS,
+            OPT_BLOCKS);
+        if (threadIdx.x == 0) r = v;
+    }
+    __syncthreads ();
+    const double v = r;
+    __syncthreads ();
+    return v;
+}
+
+__device__ __forceinline__ double*
+slot_of (double* part, int slot)
+{
+    return part + (size_t) slot * OPT_BLOCKS;
+}
+
+// After an evaluation: g = (double) grad, and the partials of g.d, x.x and
+// g.g (slots LP_GD, LP_XX, LP_GG).
+__global__ void __launch_bounds__ (OPT_THREADS)
+lb_eval_dots_kernel (const float* __restrict__ grad, double* __restrict__ g,
+    const double* __restrict__ d, const double* __restrict__ x, long long n,
+    double* __restrict__ part)
+{
+    double gd = 0.0, xx = 0.0, gg = 0.0;
+    for (long long i = (long long) blockIdx.x * OPT_THREADS + threadIdx.x;
+         i < n; i += (long long) gridDim.x * OPT_THREADS) {
+        const double gi = (double) grad[i];
+        const double xi = x[i];
+        g[i] = gi;
+        gd += gi * d[i];
+        xx += xi * xi;
+        gg += gi * gi;
+    }
+    block_partials<3> ({gd, xx, gg}, {slot_of (part, LP_GD),
+        slot_of (part, LP_XX), slot_of (part, LP_GG)});
+}
+
+// Start of the new-line-search branch: d = -g and, with a correction pair
+// to form, s_new = x - xp, y_new = g - gp with the partials of y.s, y.y and
+// the first loop's first s_j.d; without one (the first line search), xp =
+// x, gp = g and the partials of gp.d.
+__global__ void __launch_bounds__ (OPT_THREADS)
+lb_rec_start_kernel (const LbDev* __restrict__ st, double* __restrict__ S,
+    double* __restrict__ Y, const double* __restrict__ x,
+    double* __restrict__ xp, const double* __restrict__ g,
+    double* __restrict__ gp, double* __restrict__ d, long long n,
+    double* __restrict__ part)
+{
+    const long long i0 = (long long) blockIdx.x * OPT_THREADS + threadIdx.x;
+    const long long step = (long long) gridDim.x * OPT_THREADS;
+    if (st->first) {
+        double dg = 0.0;
+        for (long long i = i0; i < n; i += step) {
+            const double gi = g[i];
+            const double di = -1.0 * gi + 0.0 * d[i];
+            d[i] = di;
+            xp[i] = x[i];
+            gp[i] = gi;
+            dg += gi * di;
+        }
+        block_partials<1> ({dg}, {slot_of (part, LP_DG0)});
+        return;
+    }
+    double* sn = S + (size_t) st->newest * n;
+    double* yn = Y + (size_t) st->newest * n;
+    // the first loop starts at the newest pair (the one formed here)
+    const bool a0 = !lb_skip (st, 0);
+    const bool s0_new = lb_j1 (st, 0) == st->newest;
+    const double* s0 = S + (size_t) lb_j1 (st, 0) * n;
+    double ys = 0.0, yy = 0.0, sd = 0.0;
+    for (long long i = i0; i < n; i += step) {
+        const double si = x[i] - xp[i];
+        const double yi = g[i] - gp[i];
+        sn[i] = si;
+        yn[i] = yi;
+        ys += yi * si;
+        yy += yi * yi;
+        const double di = -1.0 * g[i] + 0.0 * d[i];
+        d[i] = di;
+        if (a0) sd += (s0_new ? si : s0[i]) * di;
+    }
+    block_partials<3> ({ys, yy, sd}, {slot_of (part, LP_YS),
+        slot_of (part, LP_YY), slot_of (part, LP_REC)});
+}
+
+// Step i of the first loop: alpha_j = s_j.d / ys_j, d -= alpha_j y_j, and
+// the partials of the next step's s_j.d.
+__global__ void __launch_bounds__ (OPT_THREADS)
+lb_rec_alpha_kernel (const LbDev* __restrict__ st, int i,
+    const double* __restrict__ S, const double* __restrict__ Y,
+    double* __restrict__ d, double* __restrict__ dsc, long long n,
+    double* __restrict__ part)
+{
+    if (lb_skip (st, i)) return;
+    const int m = st->m;
+    const int j = lb_j1 (st, i);
+    // ys of the newest pair is formed here; the older ones are stored
+    const double ysj = i == 0 ? block_final (part, LP_YS) : dsc[j];
+    const double alpha = block_final (part, LP_REC + i) / ysj;
+    if (blockIdx.x == 0 && threadIdx.x == 0) dsc[m + j] = alpha;
+    const bool next = i + 1 < m && !lb_skip (st, i + 1);
+    const double* sn = S + (size_t) lb_j1 (st, next ? i + 1 : i) * n;
+    const double* yj = Y + (size_t) j * n;
+    const double av = -1.0 * alpha;
+    double sd = 0.0;
+    for (long long k = (long long) blockIdx.x * OPT_THREADS + threadIdx.x;
+         k < n; k += (long long) gridDim.x * OPT_THREADS) {
+        const double dk = av * yj[k] + 1.0 * d[k];
+        d[k] = dk;
+        if (next) sd += sn[k] * dk;
+    }
+    if (next) block_partials<1> ({sd}, {slot_of (part, LP_REC + i + 1)});
+}
+
+// Between the loops: d *= ys / yy of the newest pair (both stored for the
+// pairs to come), and the partials of the second loop's first y_j.d.
+__global__ void __launch_bounds__ (OPT_THREADS)
+lb_rec_scale_kernel (const LbDev* __restrict__ st, const double* __restrict__ Y,
+    double* __restrict__ d, double* __restrict__ dsc, long long n,
+    double* __restrict__ part)
+{
+    if (st->first) return;
+    const int m = st->m;
+    const double ys = block_final (part, LP_YS);
+    const double yy = block_final (part, LP_YY);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        dsc[st->newest] = ys;
+        dsc[2 * m + 1] = yy;
+    }
+    const double bv = ys / yy;
+    const bool next = !lb_skip (st, 0);
+    const double* yn = Y + (size_t) lb_j2 (st, 0) * n;
+    double yd = 0.0;
+    for (long long k = (long long) blockIdx.x * OPT_THREADS + threadIdx.x;
+         k < n; k += (long long) gridDim.x * OPT_THREADS) {
+        const double dk = 0.0 * d[k] + bv * d[k];
+        d[k] = dk;
+        if (next) yd += yn[k] * dk;
+    }
+    if (next) block_partials<1> ({yd}, {slot_of (part, LP_REC + m)});
+}
+
+// Step i of the second loop: beta = y_j.d / ys_j, d += (alpha_j - beta)
+// s_j, then the partials of the next step's y_j.d, or after the last step
+// xp = x, gp = g and the partials of gp.d.
+__global__ void __launch_bounds__ (OPT_THREADS)
+lb_rec_beta_kernel (const LbDev* __restrict__ st, int i,
+    const double* __restrict__ S, const double* __restrict__ Y,
+    const double* __restrict__ x, double* __restrict__ xp,
+    const double* __restrict__ g, double* __restrict__ gp,
+    double* __restrict__ d, const double* __restrict__ dsc, long long n,
+    double* __restrict__ part)
+{
+    if (lb_skip (st, i)) return;
+    const int m = st->m;
+    const int j = lb_j2 (st, i);
+    const double beta = block_final (part, LP_REC + m + i) / dsc[j];
+    const double av = dsc[m + j] - beta;
+    const bool last = i + 1 >= m || lb_skip (st, i + 1);
+    const double* yn = Y + (size_t) lb_j2 (st, last ? i : i + 1) * n;
+    const double* sj = S + (size_t) j * n;
+    double acc = 0.0;
+    const long long i0 = (long long) blockIdx.x * OPT_THREADS + threadIdx.x;
+    const long long step = (long long) gridDim.x * OPT_THREADS;
+    if (!last) {
+        for (long long k = i0; k < n; k += step) {
+            const double dk = av * sj[k] + 1.0 * d[k];
+            d[k] = dk;
+            acc += yn[k] * dk;
+        }
+        block_partials<1> ({acc}, {slot_of (part, LP_REC + m + i + 1)});
+        return;
+    }
+    for (long long k = i0; k < n; k += step) {
+        const double dk = av * sj[k] + 1.0 * d[k];
+        const double gk = g[k];
+        d[k] = dk;
+        xp[k] = x[k];
+        gp[k] = gk;
+        acc += gk * dk;
+    }
+    block_partials<1> ({acc}, {slot_of (part, LP_DG0)});
 }
 
 }  // namespace
@@ -857,44 +973,26 @@ build_lbfgs_graph (b200bsp_ctx* ctx, Lbfgs& w, LbDev* dst, float lambda,
             nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
         lb_branch_fused_kernel<<<1, LB_FUSED_THREADS, 0, st>>> (dst, w.s, w.y,
             w.x, w.xp, w.g, w.gp, w.d, ys_d, &dst->dginit, n);
-        lb_begin_search_kernel<<<1, 32, 0, st>>> (dst, h_while);
+        lb_begin_search_kernel<<<1, 32, 0, st>>> (dst, h_while, nullptr, 0);
         ok = cudaStreamEndCapture (st, &out) == cudaSuccess && out == branch;
     } else if (ok && cudaStreamBeginCaptureToGraph (st, branch, nullptr,
             nullptr, 0, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
-        lb_pair_kernel<<<grid, 256, 0, st>>> (dst, w.s, w.y, w.x, w.xp, w.g,
-            w.gp, n);
-        lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, LB_YS,
-            0, w.s, w.y, w.d, n, w.part);
-        lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_YS, 0, w.part,
-            OPT_BLOCKS, ys_d);
-        lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, LB_YY,
-            0, w.s, w.y, w.d, n, w.part);
-        lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_YY, 0, w.part,
-            OPT_BLOCKS, ys_d);
-        axpby_kernel<<<grid, 256, 0, st>>> (-1.0, w.g, 0.0, w.d, n);
+        // the correction pair, the two-loop recursion, xp, gp and gp.d:
+        // 2 m + 2 launches, each reducing the partials of the one before
+        lb_rec_start_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, w.s,
+            w.y, w.x, w.xp, w.g, w.gp, w.d, n, w.part);
         for (int i = 0; i < m; i++) {
-            lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst,
-                LB_ALPHA, i, w.s, w.y, w.d, n, w.part);
-            lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_ALPHA, i, w.part,
-                OPT_BLOCKS, ys_d);
-            lb_axpy1_kernel<<<grid, 256, 0, st>>> (dst, i, w.y, ys_d, w.d, n);
+            lb_rec_alpha_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, i,
+                w.s, w.y, w.d, ys_d, n, w.part);
         }
-        lb_scale_kernel<<<grid, 256, 0, st>>> (dst, ys_d, w.d, n);
+        lb_rec_scale_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, w.y, w.d,
+            ys_d, n, w.part);
         for (int i = 0; i < m; i++) {
-            lb_dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst,
-                LB_BETA, i, w.s, w.y, w.d, n, w.part);
-            lb_dot_final_kernel<<<1, 32, 0, st>>> (dst, LB_BETA, i, w.part,
-                OPT_BLOCKS, ys_d);
-            lb_axpy2_kernel<<<grid, 256, 0, st>>> (dst, i, w.s, ys_d, w.d, n);
+            lb_rec_beta_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (dst, i,
+                w.s, w.y, w.x, w.xp, w.g, w.gp, w.d, ys_d, n, w.part);
         }
-        cudaMemcpyAsync (w.xp, w.x, n * sizeof (double),
-            cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync (w.gp, w.g, n * sizeof (double),
-            cudaMemcpyDeviceToDevice, st);
-        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.gp, w.d, n,
-            w.part);
-        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->dginit);
-        lb_begin_search_kernel<<<1, 32, 0, st>>> (dst, h_while);
+        lb_begin_search_kernel<<<1, 32, 0, st>>> (dst, h_while, w.part,
+            OPT_BLOCKS);
         ok = cudaStreamEndCapture (st, &out) == cudaSuccess && out == branch;
     } else {
         ok = false;
@@ -902,22 +1000,15 @@ build_lbfgs_graph (b200bsp_ctx* ctx, Lbfgs& w, LbDev* dst, float lambda,
     // the trial: after the branch, every iteration of the loop
     if (ok && cudaStreamBeginCaptureToGraph (st, body, &inode, nullptr, 1,
             cudaStreamCaptureModeRelaxed) == cudaSuccess) {
-        lb_trial_kernel<<<grid, 256, 0, st>>> (dst, w.xp, w.d, w.x, n);
-        to_float_kernel<<<grid, 256, 0, st>>> (w.x, coeff_f, n);
+        lb_trial_kernel<<<grid, 256, 0, st>>> (dst, w.xp, w.d, w.x, coeff_f,
+            n);
         // bspline_score with device outputs: lambda * MSE (+ regulariser)
         const int rc = b200bsp_score (ctx, coeff_f, 0, lambda, reg,
             &dst->total, grad_f, nullptr, nullptr);
-        to_double_kernel<<<grid, 256, 0, st>>> (grad_f, w.g, n);
-        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.g, w.d, n,
-            w.part);
-        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->dg);
-        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.x, w.x, n,
-            w.part);
-        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->xx);
-        dot_partial_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (w.g, w.g, n,
-            w.part);
-        dot_final_kernel<<<1, 32, 0, st>>> (w.part, OPT_BLOCKS, &dst->gg);
-        lb_after_eval_kernel<<<1, 32, 0, st>>> (dst, h_while, h_new);
+        lb_eval_dots_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (grad_f, w.g,
+            w.d, w.x, n, w.part);
+        lb_after_eval_kernel<<<1, 32, 0, st>>> (dst, h_while, h_new, w.part,
+            OPT_BLOCKS);
         ok = cudaStreamEndCapture (st, &out) == cudaSuccess && out == body
             && rc == B200BSP_OK;
     } else {

@@ -92,10 +92,30 @@ def test_graph_run_matches_host_driven_run(form, vpr, with_reg):
     """The graph-resident iterations (one launch) against the host-driven
     loop on the same registration: MSE, optionally with the curvature
     regulariser.  The controller rounds as the host does; the two differ
-    only in the dot products' summation order of the new-line-search branch
-    for small grids (vpr 8: one block), so the bar is the same trials and
-    scores to 1e-5."""
-    fixed, moving = _blobs_case()
+    only in the summation order of their dot products (the graph sums each
+    one's block partials with one warp, and small grids' new-line-search
+    branch runs in one block), so the bar is the same trials and scores to
+    1e-5."""
+    _compare_graph_and_host(_blobs_case(), form, vpr, with_reg)
+
+
+@pytest.mark.parametrize("with_reg", [False, True])
+def test_graph_run_matches_host_driven_run_large_grid(with_reg):
+    """As above on a grid of more than 2^17 coefficients, whose
+    new-line-search branch is the multi-block chain (correction pair and
+    first loop step, each loop step fused with the next dot product's
+    partials, gp.d after the last step)."""
+    fixed = synth.gaussian_blobs((160, 160, 96), spacing=(1.0, 1.0, 1.5),
+                                 seed=20261209)
+    g0 = BsplineGrid.for_volume(fixed, 8)
+    moving = synth.warp_trilinear(fixed, fixed, g0,
+                                  synth.random_coeff(g0, 2.0, 20261210))
+    assert BsplineGrid.for_volume(fixed, 4).num_coeff > 1 << 17
+    _compare_graph_and_host((fixed, moving), "tc", 4, with_reg)
+
+
+def _compare_graph_and_host(case, form, vpr, with_reg):
+    fixed, moving = case
     grid = BsplineGrid.for_volume(fixed, vpr)
     reg = P.reg_parms(curvature=0.005) if with_reg else None
     x0 = np.zeros(grid.num_coeff, np.float32)
