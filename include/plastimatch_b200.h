@@ -83,12 +83,13 @@ typedef struct {
     int tc_kernel;      /* B200BSP_TC_KERNEL_* (0: chosen per context) */
 } b200bsp_opts;
 
-/* The tensor-core form's MSE kernel.  AUTO starts on the x-lane kernel
- * (voxel x on the TMEM lanes, 3 <= vox_per_rgn[1] <= 10) where the grid
- * allows it, else the tile kernel (125 voxels of one tile on the lanes),
- * and b200bsp_autotune may move between them; XLANE and TILE pin one (XLANE
- * on a grid it cannot take is B200BSP_E_UNSUPPORTED; TILE has no image
- * ROIs and runs MI on its FP32 kernels). */
+/* The tensor-core form's MSE kernel.  AUTO starts on the tile kernel (the
+ * voxels of one tile on the TMEM lanes); b200bsp_autotune may move it to
+ * the x-lane kernel (voxel x on the lanes, 3 <= vox_per_rgn[1] <= 10) and
+ * back, and image ROIs (b200bsp_set_roi) move it to the x-lane kernel,
+ * which is the one that tests them.  XLANE and TILE pin one (XLANE on a
+ * grid it cannot take is B200BSP_E_UNSUPPORTED; with TILE pinned, image
+ * ROIs are B200BSP_E_UNSUPPORTED in the tensor-core form). */
 #define B200BSP_TC_KERNEL_AUTO   0
 #define B200BSP_TC_KERNEL_XLANE  1
 #define B200BSP_TC_KERNEL_TILE   2
@@ -226,13 +227,14 @@ int b200bsp_set_landmarks (b200bsp_ctx* ctx, const float* fixed_xyz,
     int64_t n_fixed, const float* moving_xyz, int64_t n_moving,
     float stiffness);
 
-/* Bounded device-side waits of the tensor-core MSE kernel (no reference
+/* Bounded device-side waits of the tensor-core MSE kernels (no reference
  * counterpart; the reference exits on failures): `polls` mbarrier polls
  * before a wait gives up and the call returns B200BSP_E_TIMEOUT (0: the
  * default, 1 << 22, or opts.wait_limit).  withhold_mma != 0 is a testing
- * aid: the kernel's tensor-core warp then issues no MMA, so the compute
- * warps' first wait runs out after `polls` polls -- the failure path, on a
- * GPU, without a fault.  On expiry every warp leaves its loop, the issued
+ * aid of the x-lane kernel (B200BSP_E_UNSUPPORTED on a context that is not
+ * on it, e.g. opts.tc_kernel = B200BSP_TC_KERNEL_XLANE): its tensor-core
+ * warp then issues no MMA, so the compute warps' first wait runs out after
+ * `polls` polls -- the failure path, on a GPU, without a fault.  On expiry every warp leaves its loop, the issued
  * MMAs are drained and TMEM is released; the context stays usable. */
 int b200bsp_set_wait_limit (b200bsp_ctx* ctx, int polls, int withhold_mma);
 
@@ -484,12 +486,11 @@ const char* b200bsp_last_error (const b200bsp_ctx* ctx);
 /* ---- batched registrations (no reference counterpart) ----------------
  *
  * A batch groups contexts on one device (uneven volume sizes and grids) so
- * that one CUDA graph launch evaluates all of them: each context's tile
- * pass and finish kernel run on a branch of the graph, and a tensor-core
- * context's persistent kernel takes its share of the SM slots in
- * proportion to its work (kept until the batch is destroyed), so every
- * registration's kernel is resident at once.  The Plastimatch counterpart
- * is one registration per process, run one after another. */
+ * that one CUDA graph launch evaluates all of them (each context's tile
+ * pass and finish kernel run on a branch of the graph), and so that their
+ * registrations run at once.  The kernels of different contexts take the
+ * SMs as they free up.  The Plastimatch counterpart is one registration
+ * per process, run one after another. */
 typedef struct b200bsp_batch b200bsp_batch;
 
 /* The contexts must be distinct, on one device, with images set; the batch
@@ -508,11 +509,11 @@ int b200bsp_batch_score_mse (b200bsp_batch* batch, const float* const* coeffs,
     float* const* grads, float* scores, int64_t* num_vox);
 
 /* One L-BFGS registration per context (MSE, similarity weight lambda, no
- * regulariser), all advancing together: every round of function
- * evaluations is one batch graph launch over the registrations still
- * running.  Each registration follows b200bsp_optimize_lbfgs's trial
- * sequence; coeffs[i] (host or device) holds its start and receives its
- * result, results[i] its status. */
+ * regulariser), all advancing together: each runs b200bsp_optimize_lbfgs's
+ * graph-resident optimiser on its context's stream, all at once, so no
+ * registration waits for another.  Each follows b200bsp_optimize_lbfgs's
+ * trial sequence; coeffs[i] (host or device) holds its start and receives
+ * its result, results[i] its status. */
 int b200bsp_batch_optimize_lbfgs (b200bsp_batch* batch, float lambda,
     const b200bsp_lbfgs_parms* parms, float* const* coeffs,
     b200bsp_lbfgs_result* results);

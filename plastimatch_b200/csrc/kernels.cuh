@@ -54,7 +54,7 @@ cudaError_t launch_mse_tc (const BspGeom& g, const TcPlan& plan,
     int grad_mode, const float* fimg, const float* mimg, const float* mgrad,
     const float4* mgrad4, const float* coeff, const void* qlut_bf16,
     float* part, double* score_part, int* count_part, int* err_flag,
-    cudaStream_t st);
+    unsigned wait_limit, cudaStream_t st);
 
 // cudaFuncAttributeMaxDynamicSharedMemorySize for a kernel on the current
 // device, set once per (kernel, device) and size: the attribute call is a

@@ -129,6 +129,7 @@ struct TcArgs {
     const float* mi_nvf;
     unsigned long long* hist;
     float pz_mmin, pz_mdelta;    // Parzen: moving value -> window centre
+    unsigned wait_limit;         // polls before a wait gives up
 };
 
 __device__ __forceinline__ void
@@ -1161,7 +1162,7 @@ cwait (const TcArgs& a, const TcCtx& x, uint64_t* bar, uint32_t& ph,
 {
     if (x.lane == 0) {
         bool ok = false;
-        for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
+        for (uint32_t n = 0; n < a.wait_limit && !*s_abort; n++) {
             if (mbar_try_wait (bar, ph)) { ok = true; break; }
         }
         if (!ok) {
@@ -1199,7 +1200,7 @@ mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, bool adjoint,
     for (int i = 0; i < nb_local && !*s_abort; i++) {
         for (int mb = 0; mb < a.mblk; mb++) {
             bool ok = false;
-            for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
+            for (uint32_t n = 0; n < a.wait_limit && !*s_abort; n++) {
                 if (mbar_try_wait (&bars[0], ph_c)) { ok = true; break; }
             }
             if (!ok) { *s_abort = 1; atomicExch (a.err, 3); return; }
@@ -1207,7 +1208,7 @@ mma_loop (const TcArgs& a, const TcCtx& x, int nb_local, bool adjoint,
             issue_forward (a, x, &bars[2]);
             if (!adjoint) continue;
             ok = false;
-            for (uint32_t n = 0; n < TC_WAIT_LIMIT && !*s_abort; n++) {
+            for (uint32_t n = 0; n < a.wait_limit && !*s_abort; n++) {
                 if (mbar_try_wait (&bars[1], ph_dc)) { ok = true; break; }
             }
             if (!ok) { *s_abort = 1; atomicExch (a.err, 4); return; }
@@ -1509,6 +1510,7 @@ tc_args (const BspGeom& g, const TcPlan& p, TcArgs& a)
 {
     a = TcArgs ();
     a.g = g;
+    a.wait_limit = TC_WAIT_LIMIT;
     a.T = p.bx;
     a.N = p.n_mma;
     a.mblk = p.mblk;
@@ -1548,10 +1550,12 @@ cudaError_t
 launch_mse_tc (const BspGeom& g, const TcPlan& p, int grad_mode,
     const float* fimg, const float* mimg, const float* mgrad,
     const float4* mgrad4, const float* coeff, const void* qimg, float* part,
-    double* score_part, int* count_part, int* err, cudaStream_t st)
+    double* score_part, int* count_part, int* err, unsigned wait_limit,
+    cudaStream_t st)
 {
     TcArgs a;
     a.axis = tc_args (g, p, a) && (grad_mode == 1 || mgrad4 != nullptr);
+    if (wait_limit > 0) a.wait_limit = wait_limit;
     a.mgrad4 = mgrad4;
     a.fimg = fimg; a.mimg = mimg; a.mgrad = mgrad; a.coeff = coeff;
     a.qimg = (const uint4*) qimg;

@@ -68,26 +68,25 @@ dot_partial_kernel (const double* __restrict__ a, const double* __restrict__ b,
     dot_partial_body (a, b, n, part);
 }
 
+// *out = the sum of the block partials (one warp, lb_warp_sum's order: the
+// partials' loads all go out at once)
 __global__ void
 dot_final_kernel (const double* __restrict__ part, int n, double* out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n; i++) s += part[i];
-        *out = s;
-    }
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const double s = lb_warp_sum (part, n);
+    if (threadIdx.x == 0) *out = s;
 }
 
-// *out = sum of part (dot_final_kernel's order), divided by *den if given
+// *out = the sum of part (dot_final_kernel's order), divided by *den if
+// given
 __global__ void
 dot_final_div_kernel (const double* __restrict__ part, int n,
     const double* __restrict__ den, double* out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n; i++) s += part[i];
-        *out = den ? s / *den : s;
-    }
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const double s = lb_warp_sum (part, n);
+    if (threadIdx.x == 0) *out = den ? s / *den : s;
 }
 
 // y = (sign * *a) * x + b * y, the coefficient read on the device

@@ -64,9 +64,11 @@ struct b200bsp_ctx {
 
     PartLayout lay;
     TcPlan plan;
-    // the x-lane tensor-core MSE kernel (mse_xl.cu) where its plan exists
-    // and the autotuner has not preferred the tile kernel
+    // the x-lane tensor-core MSE kernel (mse_xl.cu): pinned, chosen by the
+    // autotuner, or needed for image ROIs; pref_xl is the choice without
+    // ROIs, restored when they are removed
     bool use_xl = false;
+    bool pref_xl = false;
     bool has_xl = false;
     XlPlan xplan;
     PartLayout xlay;
@@ -419,24 +421,6 @@ ctx_set_opt_ws (b200bsp_ctx* c, void* ws, void (*release) (void*))
     c->opt_ws_free = release;
 }
 
-// Work of one evaluation's tile pass (voxels of the ROI's tiles) and
-// whether that pass is the persistent tensor-core kernel.
-long long
-ctx_work (const b200bsp_ctx* c, bool* persistent)
-{
-    *persistent = c->opts.form == B200BSP_FORM_TC;
-    return (long long) c->geom.ntiles * c->geom.vpr[0] * c->geom.vpr[1]
-        * c->geom.vpr[2];
-}
-
-// CTAs the persistent tile kernel runs on (0: one pair per SM).
-void
-ctx_set_tc_grid (b200bsp_ctx* c, int ctas)
-{
-    if (c->tc_grid != ctas) c->gen++;
-    c->tc_grid = ctas;
-}
-
 // The device-side error flag of the tile kernel (nullptr for the FP32
 // form, which has no bounded waits).
 int*
@@ -587,7 +571,12 @@ b200bsp_create (const b200bsp_volume* fixed, const b200bsp_volume* moving,
         rc2 = fail (c, B200BSP_E_BADARG, "tc_kernel %d unknown", o.tc_kernel);
     } else if (o.form == B200BSP_FORM_TC
                && o.tc_kernel != B200BSP_TC_KERNEL_TILE) {
-        c->has_xl = c->use_xl = xl_plan (g, &c->xplan, sm_count);
+        // AUTO starts on the tile kernel (the faster one where both were
+        // measured: 256x256x128 at vpr 5 and 64^3 at vpr 8); image ROIs
+        // and the autotuner move it to the x-lane kernel
+        c->has_xl = xl_plan (g, &c->xplan, sm_count);
+        c->use_xl = c->pref_xl = c->has_xl
+            && o.tc_kernel == B200BSP_TC_KERNEL_XLANE;
         if (!c->has_xl && o.tc_kernel == B200BSP_TC_KERNEL_XLANE) {
             rc2 = fail (c, B200BSP_E_UNSUPPORTED,
                 "x-lane kernel: vox_per_rgn[1] = %d outside 3..10", g.vpr[1]);
@@ -743,6 +732,10 @@ b200bsp_set_wait_limit (b200bsp_ctx* c, int polls, int withhold_mma)
 {
     if (!c) return B200BSP_E_BADARG;
     if (polls < 0) return fail (c, B200BSP_E_BADARG, "polls must be >= 0");
+    if (withhold_mma && !(c->opts.form == B200BSP_FORM_TC && c->use_xl)) {
+        return fail (c, B200BSP_E_UNSUPPORTED,
+            "withholding MMAs is a testing aid of the x-lane kernel");
+    }
     c->wait_limit = polls > 0 ? (unsigned) polls : XL_DEFAULT_WAIT_LIMIT;
     c->withhold_mma = withhold_mma ? 1 : 0;
     c->gen++;
@@ -919,7 +912,7 @@ run_mse (b200bsp_ctx* c, const float* dcoeff, float* grad_out,
         CK (launch_mse_tc (g, plan, c->opts.mse_grad, c->d_fixed,
             c->d_moving, c->d_mgrad, c->d_mgrad4, dcoeff, c->d_qlut,
             c->d_part, c->d_score_part, c->d_count_part, c->d_err,
-            c->stream));
+            c->wait_limit, c->stream));
     }
     c->last_launches++;
     int rc = mark_main_done (c);
@@ -1099,6 +1092,7 @@ b200bsp_autotune (b200bsp_ctx* c, const float* coeff, int evals, int* tiles)
     use_tc_plan (c, rc ? start : best);
     if (c->has_xl) use_xl_plan (c, rc ? xstart : xbest);
     c->use_xl = rc ? start_xl : best_xl;
+    if (!roi) c->pref_xl = c->use_xl;
     if (rc) {
         cudaGetLastError ();
         return fail (c, rc, "autotuning failed");
@@ -1464,8 +1458,9 @@ b200bsp_set_roi (b200bsp_ctx* c, const b200bsp_volume* fixed_roi,
         for (int i = 0; i < 9; i++) g.mroi_proj[i] = mr.proj[i];
         g.mroi = c->d_mroi;
     }
-    // the tile kernel has no ROI tests: MSE stays on the x-lane kernel
-    if (any && c->opts.form == B200BSP_FORM_TC) c->use_xl = true;
+    // the tile kernel has no ROI tests: MSE moves to the x-lane kernel while
+    // ROIs are set, and back to the choice without them after
+    if (c->opts.form == B200BSP_FORM_TC) c->use_xl = any || c->pref_xl;
     return B200BSP_OK;
 }
 

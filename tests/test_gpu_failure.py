@@ -1,8 +1,8 @@
 """Failure detection without a GPU fault.
 
-* A bounded device-side wait that runs out: the tensor-core kernel's
-  tensor-core warp withholds its MMAs (b200bsp_set_wait_limit's testing
-  aid), so the compute warps' first wait -- on a barrier nothing completes
+* A bounded device-side wait that runs out: the x-lane tensor-core
+  kernel's tensor-core warp withholds its MMAs (b200bsp_set_wait_limit's
+  testing aid, refused on a context on the tile kernel), so the compute warps' first wait -- on a barrier nothing completes
   -- gives up after a short poll limit.  The call returns
   B200BSP_E_TIMEOUT, the kernel has released its TMEM (the next
   evaluation's allocation succeeds) and the same context then scores
@@ -29,7 +29,7 @@ from plastimatch_b200.geometry import BsplineGrid
 
 pytestmark = pytest.mark.gpu
 
-E_OOM, E_TIMEOUT = -2, -4
+E_OOM, E_TIMEOUT, E_UNSUPPORTED = -2, -4, -6
 
 
 def _case(seed=5):
@@ -51,9 +51,20 @@ def _score(ctx, coeff):
     return rc, s.value, g, n.value
 
 
+def test_withholding_mmas_needs_the_xlane_kernel():
+    fixed, moving, grid, coeff = _case()
+    with P.Context(fixed, moving, grid, form="tc", tc_kernel="tile") as ctx:
+        ctx.set_images()
+        lib = P.lib()
+        assert lib.b200bsp_set_wait_limit(ctx._h, 1000, 1) == E_UNSUPPORTED
+        rc, s0, g0, n0 = _score(ctx, coeff)        # nothing was withheld
+        assert rc == 0 and n0 > 0
+
+
 def test_wait_expiry_times_out_and_context_recovers():
     fixed, moving, grid, coeff = _case()
-    with P.Context(fixed, moving, grid, form="tc") as ctx:
+    # withholding the MMAs is the x-lane kernel's testing aid
+    with P.Context(fixed, moving, grid, form="tc", tc_kernel="xlane") as ctx:
         ctx.set_images()
         rc, s0, g0, n0 = _score(ctx, coeff)
         assert rc == 0

@@ -64,6 +64,14 @@ def test_headline_workload_parity(form, c2):
 
 @pytest.mark.parametrize("form", ["tc", "fp32"])
 def test_headline_workload_trilinear_gradient(form, c2):
+    """The trilinear-derivative gradient (the reference's flavour o): from
+    the double-precision evaluation no further than the float flavour o (its
+    restatement, oracle/bspline_oracle.c) is, plus 1e-4 -- flavour o is
+    1.17e-3 from double on this phantom, for the reason given above -- and
+    within 1.5e-3 of flavour o itself: the forms compute the sample
+    position in another float order than flavour o, so their float rounding
+    picks the other side of a cell face at other voxels, and two such float
+    evaluations differ by about the float floor (the FP32 form: 1.07e-3)."""
     fixed, moving, grid, coeff, _, _, _ = c2
     with P.Context(fixed, moving, grid, form=form,
                    mse_grad="trilinear") as ctx:
@@ -71,6 +79,11 @@ def test_headline_workload_trilinear_gradient(form, c2):
         s, g, n = ctx.score_mse(coeff)
     f64 = O.port_mse(grid, fixed, moving, coeff, grad_mode=1,
                      precision="f64")
+    f32 = O.port_mse(grid, fixed, moving, coeff, grad_mode=1)
     assert abs(s - f64.score) <= 1e-5 * abs(f64.score), (s, f64.score)
-    assert rel_err(g, f64.grad) < 1e-3, rel_err(g, f64.grad)
+    assert abs(s - f32.score) <= 1e-5 * abs(f32.score), (s, f32.score)
+    eref = rel_err(g, f32.grad)
+    assert eref < 1.5e-3, eref
+    e64, e64_ref = rel_err(g, f64.grad), rel_err(f32.grad, f64.grad)
+    assert e64 <= e64_ref + 1e-4, (e64, e64_ref)
     assert abs(n - f64.num_vox) <= 1e-4 * f64.num_vox + 2

@@ -83,8 +83,8 @@ def test_mse_roi_trilinear_gradient(form):
 
 def test_roi_set_replace_and_remove():
     """set_roi replaces the ROIs; no arguments remove them (the result is
-    then the ROI-free one, bit for bit); a geometry without its mask is an
-    argument error."""
+    then the ROI-free one, bit for bit: the context returns to the kernel it
+    used without ROIs); a geometry without its mask is an argument error."""
     fixed, moving, grid, coeff, rec = load_golden("roimask_mse_small")
     fr, mr = load_rois(rec)
     with P.Context(fixed, moving, grid) as ctx:
@@ -104,9 +104,11 @@ def test_roi_set_replace_and_remove():
         assert rc == -1                          # B200BSP_E_BADARG
     assert n1 < n2 < n0
     assert s3 == s0 and n3 == n0 and np.array_equal(g3, g0)
-    # a mask that holds everywhere changes nothing but the kernel variant
+    # a mask that holds everywhere changes nothing but the kernel: ROIs run
+    # on the x-lane kernel, the ROI-free context on the tile kernel, whose
+    # tensor-core sums group the same products differently
     assert n4 == n0 and abs(s4 - s0) <= 1e-6 * abs(s0)
-    assert rel_err(g4, g0) < 1e-6
+    assert rel_err(g4, g0) < 1e-5
 
 
 @pytest.mark.parametrize("form", FORMS)
