@@ -17,6 +17,11 @@ Bars (stated here):
             and across +-1000..3000 HU edges that moves its dc/dv a lot
   num_vox   within 0.01 % (+2) of the reference's count
 
+Mattes MI (PVI-8, 32 bins) on the same workload, as bench.py times it, has
+the same score and gradient bars against the reference's float MI flavour
+g (9.6e-4 from double on this phantom) and histograms within 1e-5 (L2) of
+flavour g's.
+
 The phantom's +-1000..2000 HU edges make this the hardest case for the
 tensor-core form's 3-term bf16 split: its products are f32-accurate to
 about 2^-16, and every MSE gradient entry is a sum of ~8000 such products
@@ -87,3 +92,35 @@ def test_headline_workload_trilinear_gradient(form, c2):
     e64, e64_ref = rel_err(g, f64.grad), rel_err(f32.grad, f64.grad)
     assert e64 <= e64_ref + 1e-4, (e64, e64_ref)
     assert abs(n - f64.num_vox) <= 1e-4 * f64.num_vox + 2
+
+
+@pytest.fixture(scope="module")
+def c2_mi(c2):
+    fixed, moving, grid, coeff = c2[:4]
+    f64 = O.port_mi(grid, fixed, moving, coeff, bins=32, precision="f64")
+    ref = (O.ref_metric(grid, fixed, moving, coeff, flavor="g", metric="mi",
+                        bins=32, threads=8)
+           if O.ref_available()
+           else O.port_mi(grid, fixed, moving, coeff, bins=32))
+    return f64, ref
+
+
+@pytest.mark.parametrize("form", ["tc", "tc-xlane", "fp32"])
+def test_headline_workload_mattes_mi(form, c2, c2_mi):
+    fixed, moving, grid, coeff = c2[:4]
+    f64, ref = c2_mi
+    kw = ({"form": "tc", "tc_kernel": "xlane"} if form == "tc-xlane"
+          else {"form": form})
+    with P.Context(fixed, moving, grid, mi_bins=32, **kw) as ctx:
+        ctx.set_images()
+        s, g, n, (fh, mh, jh) = ctx.score_mi(coeff, with_hist=True)
+    assert abs(n - ref.num_vox) <= 1e-4 * ref.num_vox + 2, (n, ref.num_vox)
+    assert abs(s - f64.score) <= 1e-5 * abs(f64.score), (s, f64.score)
+    assert abs(s - ref.score) <= 1e-5 * abs(ref.score), (s, ref.score)
+    eref = rel_err(g, ref.grad)
+    assert eref < 1e-3, eref
+    e64, e64_ref = rel_err(g, f64.grad), rel_err(ref.grad, f64.grad)
+    assert e64 <= e64_ref + 1e-4, (e64, e64_ref)
+    for a, b in ((fh, ref.f_hist), (mh, ref.m_hist), (jh, ref.j_hist)):
+        a, b = np.asarray(a, np.float64).ravel(), np.asarray(b).ravel()
+        assert rel_err(a, b) < 1e-5, rel_err(a, b)
