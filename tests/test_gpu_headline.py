@@ -17,6 +17,13 @@ Bars (stated here):
             and across +-1000..3000 HU edges that moves its dc/dv a lot
   num_vox   within 0.01 % (+2) of the reference's count
 
+The whole cost function with the curvature regulariser (0.005), as
+bench.py times it (b200bsp_score with device outputs: the regulariser's
+passes overlap the tensor-core kernel on a second stream): bit-identical to
+the host-output path; the regulariser within 1e-6 of the reference's
+analytic implementation c; the total score and gradient under the MSE bars
+against the reference's own bspline_score.
+
 Mattes MI (PVI-8, 32 bins) on the same workload, as bench.py times it, has
 the same score and gradient bars against the reference's float MI flavour
 g (9.6e-4 from double on this phantom) and histograms within 1e-5 (L2) of
@@ -124,3 +131,37 @@ def test_headline_workload_mattes_mi(form, c2, c2_mi):
     for a, b in ((fh, ref.f_hist), (mh, ref.m_hist), (jh, ref.j_hist)):
         a, b = np.asarray(a, np.float64).ravel(), np.asarray(b).ravel()
         assert rel_err(a, b) < 1e-5, rel_err(a, b)
+
+
+def test_headline_workload_with_regularizer(c2):
+    import ctypes as C
+    import torch
+    if not O.ref_available():
+        pytest.skip("the compiled reference (oracle/_ref) is not built")
+    fixed, moving, grid, coeff = c2[:4]
+    reg = P.reg_parms(curvature=0.005)
+    ref = O.ref_score(grid, fixed, moving, coeff, flavor="g", metric="mse",
+                      reg_impl="c", curvature=0.005, threads=8)
+    rreg = O.ref_regularize(grid, fixed, coeff, 0.005, impl="c", threads=8)
+    with P.Context(fixed, moving, grid) as ctx:
+        ctx.set_images()
+        ts, g, sm, n = ctx.score(coeff, lam=1.0, reg=reg)
+        rs, rg = ctx.regularize(coeff, reg)
+        d_c = torch.from_numpy(coeff).cuda()
+        d_g = torch.zeros(grid.num_coeff, device="cuda")
+        d_ts = torch.zeros(1, device="cuda")
+        d_sm = torch.zeros(1, device="cuda")
+        d_n = torch.zeros(1, dtype=torch.int64, device="cuda")
+        rc = P.lib().b200bsp_score(ctx._h, d_c.data_ptr(), 0, C.c_float(1.0),
+                                   C.byref(reg), d_ts.data_ptr(),
+                                   d_g.data_ptr(), d_sm.data_ptr(),
+                                   d_n.data_ptr())
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert float(d_ts.item()) == ts and float(d_sm.item()) == sm
+        assert int(d_n.item()) == n
+        assert np.array_equal(d_g.cpu().numpy(), g)
+    assert abs(rs - rreg.score) <= 1e-6 * abs(rreg.score), (rs, rreg.score)
+    assert rel_err(rg, rreg.grad) < 1e-6, rel_err(rg, rreg.grad)
+    assert abs(ts - ref.score) <= 1e-5 * abs(ref.score), (ts, ref.score)
+    assert rel_err(g, ref.grad) < 1e-3, rel_err(g, ref.grad)
