@@ -209,7 +209,11 @@ int b200bsp_regularize_f64 (b200bsp_ctx* ctx, const float* coeff,
 /* The whole cost function bspline_score() (src/register/bspline.cxx:
  * 558-632) for one similarity metric: metric_type 0 = MSE, 1 = MI;
  * total_score = lambda * smetric (+ rmetric when reg != NULL, + stiffness *
- * lmetric when landmarks are set), total_grad likewise, in that order. */
+ * lmetric when landmarks are set), total_grad likewise, in that order.
+ * With every output in device memory and no landmarks the call is
+ * stream-ordered on the context's stream and returns without waiting (for
+ * MSE the regulariser's passes overlap the metric kernel); otherwise it
+ * returns with the results in place. */
 int b200bsp_score (b200bsp_ctx* ctx, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
     float* total_grad, float* smetric, int64_t* num_vox);

@@ -562,11 +562,12 @@ struct ContextObjective : Objective {
 
 // ---- the graph-resident run --------------------------------------------------
 //
-// For MSE on a context (with or without the regulariser, no landmarks) the
-// iterations after the prologue run as one CUDA graph: a while node over
-// trial points whose body is [new line search?] -> x = xp + stp d ->
-// evaluation (the context's MSE kernel and finish kernel, the regulariser
-// beside them) -> g.d, x.x, g.g -> the controller (lbfgs_graph.cu).  The
+// For MSE or MI on a context (with or without the regulariser, no
+// landmarks) the iterations after the prologue run as one CUDA graph: a
+// while node over trial points whose body is [new line search?] -> x = xp +
+// stp d -> evaluation (MSE: the context's MSE kernel and finish kernel, the
+// regulariser beside them; MI: both passes, the regulariser, the combine
+// kernel) -> g.d, x.x, g.g -> the controller (lbfgs_graph.cu).  The
 // "new line search" branch (an if node) forms the correction pair, runs the
 // two-loop recursion with its indices read on the device, copies xp, gp and
 // takes dginit.  Only the outcome comes back to the host.
@@ -931,9 +932,9 @@ lb_rec_beta_kernel (const LbDev* __restrict__ st, int i,
 // Record the graph of the run's iterations on the context's stream (which
 // must be idle); false when a step of the construction is refused.
 static bool
-build_lbfgs_graph (b200bsp_ctx* ctx, Lbfgs& w, LbDev* dst, float lambda,
-    const b200bsp_reg_parms* reg, float* coeff_f, float* grad_f,
-    cudaGraphExec_t* exec)
+build_lbfgs_graph (b200bsp_ctx* ctx, Lbfgs& w, LbDev* dst, int metric,
+    float lambda, const b200bsp_reg_parms* reg, float* coeff_f,
+    float* grad_f, cudaGraphExec_t* exec)
 {
     cudaStream_t st = w.st;
     const long long n = w.n;
@@ -1001,8 +1002,9 @@ build_lbfgs_graph (b200bsp_ctx* ctx, Lbfgs& w, LbDev* dst, float lambda,
             cudaStreamCaptureModeRelaxed) == cudaSuccess) {
         lb_trial_kernel<<<grid, 256, 0, st>>> (dst, w.xp, w.d, w.x, coeff_f,
             n);
-        // bspline_score with device outputs: lambda * MSE (+ regulariser)
-        const int rc = b200bsp_score (ctx, coeff_f, 0, lambda, reg,
+        // bspline_score with device outputs: lambda * metric (+
+        // regulariser)
+        const int rc = b200bsp_score (ctx, coeff_f, metric, lambda, reg,
             &dst->total, grad_f, nullptr, nullptr);
         lb_eval_dots_kernel<<<OPT_BLOCKS, OPT_THREADS, 0, st>>> (grad_f, w.g,
             w.d, w.x, n, w.part);
@@ -1091,6 +1093,7 @@ struct OptWorkspace {
     // the recorded graph of the iterations, and what it was recorded for
     cudaGraphExec_t exec = nullptr;
     unsigned gen = 0;
+    int metric = 0;
     float lambda = 0.f;
     bool has_reg = false;
     b200bsp_reg_parms reg = {};
@@ -1125,8 +1128,8 @@ context_workspace (b200bsp_ctx* ctx, int64_t nc, int m)
     return ws;
 }
 
-// The iterations after the prologue as one graph launch (MSE on a context);
-// the host-driven loop when the graph cannot be built.
+// The iterations after the prologue as one graph launch (MSE or MI on a
+// context); the host-driven loop when the graph cannot be built.
 static int
 lbfgs_graph_run (b200bsp_ctx* ctx, Lbfgs& w, ContextObjective& obj,
     const b200bsp_lbfgs_parms& p, b200bsp_lbfgs_result* res, double f,
@@ -1161,17 +1164,18 @@ lbfgs_graph_run (b200bsp_ctx* ctx, Lbfgs& w, ContextObjective& obj,
     // record the graph once per (context state, lambda, regulariser); the
     // history length and the buffers are the workspace's own
     const bool fresh = ws->exec && ws->gen == ctx_generation (ctx)
-        && ws->lambda == obj.lambda && ws->has_reg == (obj.reg != nullptr)
+        && ws->metric == obj.metric && ws->lambda == obj.lambda && ws->has_reg == (obj.reg != nullptr)
         && (!obj.reg || memcmp (&ws->reg, obj.reg, sizeof ws->reg) == 0);
     if (!fresh) {
         if (ws->exec) cudaGraphExecDestroy (ws->exec);
         ws->exec = nullptr;
-        if (!build_lbfgs_graph (ctx, w, dst, obj.lambda, obj.reg, obj.coeff_f,
-                obj.grad_f, &ws->exec)) {
+        if (!build_lbfgs_graph (ctx, w, dst, obj.metric, obj.lambda, obj.reg,
+                obj.coeff_f, obj.grad_f, &ws->exec)) {
             ws->exec = nullptr;
             return lbfgs_loop (w, obj, p, res, f, step);
         }
         ws->gen = ctx_generation (ctx);
+        ws->metric = obj.metric;
         ws->lambda = obj.lambda;
         ws->has_reg = obj.reg != nullptr;
         if (obj.reg) ws->reg = *obj.reg;
@@ -1195,9 +1199,9 @@ lbfgs_graph_run (b200bsp_ctx* ctx, Lbfgs& w, ContextObjective& obj,
 static thread_local int g_host_lbfgs = 0;
 
 // L-BFGS over a context's coefficients (host or device floats, updated in
-// place with the last evaluated point), evaluations by `obj`: MSE without
-// landmarks runs its iterations as one graph launch (lbfgs_graph_run), the
-// rest from the host.
+// place with the last evaluated point), evaluations by `obj`: MSE or MI
+// without landmarks runs its iterations as one graph launch
+// (lbfgs_graph_run), the rest from the host.
 static int
 optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
     int64_t nc, float* coeff, b200bsp_lbfgs_result* res,
@@ -1225,8 +1229,8 @@ optimize_on_context (b200bsp_ctx* ctx, const b200bsp_lbfgs_parms& p,
     res->status = 0;
     res->fevals = 0;
     float stiffness = 0.f;
-    if (obj.metric == 0 && ctx_landmarks (ctx, &stiffness) == 0
-        && !g_host_lbfgs) {
+    if ((obj.metric == 0 || obj.metric == 1)
+        && ctx_landmarks (ctx, &stiffness) == 0 && !g_host_lbfgs) {
         double f = 0.0, step = 0.0;
         bool more = false;
         rc = lbfgs_prologue (w, obj, p, res, &f, &step, &more);

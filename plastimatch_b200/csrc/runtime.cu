@@ -1648,18 +1648,86 @@ score_mse_device (b200bsp_ctx* c, const float* coeff, float lambda,
     return end_eval (c, false);
 }
 
+// MI's combine on the device, as the finish kernel's for MSE: total_grad =
+// 0 + lambda * metric gradient in float, then the regulariser's double
+// gradient added with one rounding; total = lambda * score (+ the
+// regulariser's score in float), in Bspline_score's order.
+__global__ void
+mi_combine_kernel (const DevResult* __restrict__ res, float lambda,
+    const double* __restrict__ reg_grad, const double* __restrict__ reg_score,
+    float* __restrict__ grad, long long n, float* __restrict__ total,
+    float* __restrict__ smetric, long long* __restrict__ nvox)
+{
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+         i < n; i += (long long) gridDim.x * blockDim.x) {
+        const float t = 0.f + lambda * grad[i];
+        grad[i] = reg_grad ? (float) ((double) t + reg_grad[i]) : t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        float tot = 0.f;
+        tot += lambda * res->score_f;
+        if (reg_score) tot += (float) *reg_score;
+        *total = tot;
+        if (smetric) *smetric = res->score_f;
+        if (nvox) *nvox = res->num_vox;
+    }
+}
+
+// bspline_score with MI and device outputs, stream-ordered: both MI
+// passes, the regulariser, then mi_combine_kernel (no host round trip, so
+// the optimiser can record it in a graph).
+static int
+score_mi_device (b200bsp_ctx* c, const float* coeff, float lambda,
+    const b200bsp_reg_parms* reg, float* total_score, float* total_grad,
+    float* smetric, int64_t* num_vox)
+{
+    if (c->opts.mi_window == B200BSP_MI_PVI8 && mi_whole_image_pass1 (c) < 0) {
+        return fail (c, B200BSP_E_UNSUPPORTED,
+            "PVI-8 MI needs the grid to start at voxel 0 and its tiles to "
+            "cover the fixed image");
+    }
+    const float* dcoeff = nullptr;
+    int rc = begin_eval (c, coeff, &dcoeff);
+    if (rc) return rc;
+    rc = mi_passes (c, dcoeff, total_grad, nullptr,
+        MI_PASS_HIST | MI_PASS_GRAD);
+    if (rc) return fail (c, rc, "MI evaluation failed: %s",
+        cudaGetErrorString (cudaGetLastError ()));
+    mark_main_done (c);
+    if (reg) {
+        rc = reg_run (&c->reg, c->geom, reg, dcoeff, nullptr, c->stream,
+            c->d_reg_grad64);
+        if (rc) return fail (c, rc, "regulariser failed: %s",
+            cudaGetErrorString (cudaGetLastError ()));
+    }
+    const long long n = c->num_coeff;
+    const unsigned blocks = (unsigned) std::max<long long> (1,
+        std::min<long long> ((n + 255) / 256, 4LL * c->sm_count));
+    mi_combine_kernel<<<blocks, 256, 0, c->stream>>> (c->d_res, lambda,
+        reg ? c->d_reg_grad64 : nullptr, reg ? c->reg.d_score : nullptr,
+        total_grad, n, total_score ? total_score : c->d_total, smetric,
+        (long long*) num_vox);
+    CK (cudaGetLastError ());
+    c->last_launches++;
+    return end_eval (c, false);
+}
+
 extern "C" int
 b200bsp_score (b200bsp_ctx* c, const float* coeff, int metric_type,
     float lambda, const b200bsp_reg_parms* reg, float* total_score,
     float* total_grad, float* smetric, int64_t* num_vox)
 {
     if (!c || !total_grad) return fail (c, B200BSP_E_BADARG, "null argument");
-    if (metric_type == 0 && c->lm_n == 0 && is_device_ptr (total_grad)
+    if ((metric_type == 0 || metric_type == 1) && c->lm_n == 0
+        && is_device_ptr (total_grad)
         && (!total_score || is_device_ptr (total_score))
         && (!smetric || is_device_ptr (smetric))
         && (!num_vox || is_device_ptr (num_vox))) {
-        return score_mse_device (c, coeff, lambda, reg, total_score,
-            total_grad, smetric, num_vox);
+        return metric_type == 0
+            ? score_mse_device (c, coeff, lambda, reg, total_score,
+                total_grad, smetric, num_vox)
+            : score_mi_device (c, coeff, lambda, reg, total_score,
+                total_grad, smetric, num_vox);
     }
     std::vector<float> g ((size_t) c->num_coeff);
     float s = 0.f;

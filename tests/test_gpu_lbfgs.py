@@ -114,7 +114,16 @@ def test_graph_run_matches_host_driven_run_large_grid(with_reg):
     _compare_graph_and_host((fixed, moving), "tc", 4, with_reg)
 
 
-def _compare_graph_and_host(case, form, vpr, with_reg):
+@pytest.mark.parametrize("form", ["fp32", "tc"])
+@pytest.mark.parametrize("with_reg", [False, True])
+def test_graph_run_matches_host_driven_run_mattes_mi(form, with_reg):
+    """As above with Mattes MI (PVI-8, 32 bins) as the metric: its
+    evaluation in the graph is both passes, the regulariser and the combine
+    kernel, the same kernels the host-driven loop launches."""
+    _compare_graph_and_host(_blobs_case(), form, 8, with_reg, metric="mi")
+
+
+def _compare_graph_and_host(case, form, vpr, with_reg, metric="mse"):
     fixed, moving = case
     grid = BsplineGrid.for_volume(fixed, vpr)
     reg = P.reg_parms(curvature=0.005) if with_reg else None
@@ -125,8 +134,8 @@ def _compare_graph_and_host(case, form, vpr, with_reg):
         try:
             with P.Context(fixed, moving, grid, form=form) as ctx:
                 ctx.set_images()
-                out.append(ctx.optimize_lbfgs(x0, reg=reg, max_its=15,
-                                              max_feval=40))
+                out.append(ctx.optimize_lbfgs(x0, metric=metric, reg=reg,
+                                              max_its=15, max_feval=40))
         finally:
             P.lib().b200bsp_debug_host_lbfgs(0)
     (c_h, r_h), (c_g, r_g) = out

@@ -135,3 +135,33 @@ def test_mi_vopt_golden(form, name):
     _check(s, g, n, f64, rec["mi_grad"], int(rec["mi_num_vox"]))
     assert rel_err(fh, rec["f_hist"]) < 1e-5
     assert rel_err(jh, rec["j_hist"]) < 1e-5
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("with_reg", [False, True])
+def test_mi_score_device_path_matches_host_path(form, with_reg):
+    """b200bsp_score with MI and device outputs (stream-ordered: both
+    passes, the regulariser, the combine kernel) is bit-identical to the
+    host-output path."""
+    import ctypes as C
+    import torch
+    fixed, moving, grid, coeff = _case(vpr=(6, 5, 4))
+    reg = P.reg_parms(curvature=0.005) if with_reg else None
+    with _context(fixed, moving, grid, form=form) as ctx:
+        ctx.set_images()
+        ts, g, sm, n = ctx.score(coeff, metric="mi", lam=0.7, reg=reg)
+        d_c = torch.from_numpy(coeff).cuda()
+        d_g = torch.zeros(grid.num_coeff, device="cuda")
+        d_ts = torch.zeros(1, device="cuda")
+        d_sm = torch.zeros(1, device="cuda")
+        d_n = torch.zeros(1, dtype=torch.int64, device="cuda")
+        for _ in range(2):
+            rc = P.lib().b200bsp_score(
+                ctx._h, d_c.data_ptr(), 1, C.c_float(0.7),
+                C.byref(reg) if reg is not None else None, d_ts.data_ptr(),
+                d_g.data_ptr(), d_sm.data_ptr(), d_n.data_ptr())
+            assert rc == 0
+            torch.cuda.synchronize()
+            assert float(d_ts.item()) == ts and float(d_sm.item()) == sm
+            assert int(d_n.item()) == n
+            assert np.array_equal(d_g.cpu().numpy(), g)
