@@ -37,6 +37,8 @@ void* ctx_opt_ws (const b200bsp_ctx* c);
 int ctx_landmarks (const b200bsp_ctx* c, float* stiffness);
 void ctx_set_opt_ws (b200bsp_ctx* c, void* ws, void (*release) (void*));
 unsigned ctx_generation (const b200bsp_ctx* c);                // runtime.cu
+int* ctx_err_flag (b200bsp_ctx* c);
+int ctx_report_device_error (b200bsp_ctx* c, int e);
 
 constexpr int OPT_THREADS = 256;
 constexpr int OPT_BLOCKS = 296;
@@ -1187,6 +1189,18 @@ lbfgs_graph_run (b200bsp_ctx* ctx, Lbfgs& w, ContextObjective& obj,
     if (!ran) {
         cudaGetLastError ();
         return B200BSP_E_CUDA;
+    }
+    // a bounded device-side wait that gave up inside the run (the
+    // tensor-core kernels' error flag, read once per run): its evaluations
+    // are not to be trusted
+    if (int* flag = ctx_err_flag (ctx)) {
+        int e = 0;
+        if (cudaMemcpy (&e, flag, sizeof e, cudaMemcpyDeviceToHost)
+                != cudaSuccess) {
+            cudaGetLastError ();
+            return B200BSP_E_CUDA;
+        }
+        if (e) return ctx_report_device_error (ctx, e);
     }
     obj.fevals = h.fevals;
     obj.last = h.last;

@@ -61,6 +61,26 @@ def test_withholding_mmas_needs_the_xlane_kernel():
         assert rc == 0 and n0 > 0
 
 
+def test_optimiser_reports_wait_expiry_and_context_recovers():
+    """A registration whose evaluations give up (MMAs withheld) ends with
+    B200BSP_E_TIMEOUT, not with a result; with the default limit restored
+    the same context registers exactly as a fresh one does."""
+    fixed, moving, grid, coeff = _case()
+    x0 = np.zeros(grid.num_coeff, np.float32)
+    with P.Context(fixed, moving, grid, form="tc", tc_kernel="xlane") as ctx:
+        ctx.set_images()
+        c0, r0 = ctx.optimize_lbfgs(x0, max_its=5, max_feval=10)
+        lib = P.lib()
+        assert lib.b200bsp_set_wait_limit(ctx._h, 1000, 1) == 0
+        with pytest.raises(P.B200Error) as ei:
+            ctx.optimize_lbfgs(x0, max_its=5, max_feval=10)
+        assert ei.value.code == E_TIMEOUT
+        assert lib.b200bsp_set_wait_limit(ctx._h, 0, 0) == 0
+        c1, r1 = ctx.optimize_lbfgs(x0, max_its=5, max_feval=10)
+    assert r1["fevals"] == r0["fevals"] and r1["score"] == r0["score"]
+    assert np.array_equal(c1, c0)
+
+
 def test_wait_expiry_times_out_and_context_recovers():
     fixed, moving, grid, coeff = _case()
     # withholding the MMAs is the x-lane kernel's testing aid
